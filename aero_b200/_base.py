@@ -1,0 +1,406 @@
+"""Shared host logic of Solver (2D) and Solver3D: state mirroring, stepping,
+force histories, run loop and checkpoints.
+
+The public behaviour follows the reference solvers (aero/lbm/solver.py:74-727,
+aero/lbm/solver3d.py:70-838): same constructor options, same attributes
+(f, g, _f_outlet_prev, surface_links, q_vals, step_count, *_history), same
+_step() return values and run() result keys, same .npz checkpoint keys.  What
+changes is where the step runs: on the GPU, many steps per call, with the
+per-step forces kept in a device ring and read back in chunks.
+"""
+
+from __future__ import annotations
+
+import json
+import pathlib
+import time
+import warnings
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from .diagnostics import check_stability, coefficient_spectrum, detect_statistical_stationarity
+from .engine import Engine
+from .lattice import feq, macroscopic, scalar_weights, tables
+from .links import build_surface_links
+
+BACKENDS = ("b200", "auto")
+PRECISIONS = tuple(_lib.STORE)
+_PRISTINE_LIMIT = 1 << 28  # elements; above this a handed-out array is always re-uploaded
+
+
+class LatticeSolverBase:
+    dims = 2
+
+    # ------------------------------------------------------------------ set-up
+    def _setup(self, *, shape, solid, omega, u0, D, rho0, wall_bc, inlet_bc, outlet_bc,
+               streamwise_bc, backend, collision, inlet_perturbation, trt_lambda,
+               sponge_thickness, sponge_strength, les, les_cs, les_model, ibm_enabled, phi,
+               bouzidi, van_driest, van_driest_A, body_force, wall_velocity_top,
+               wall_velocity_bottom, synthetic_inflow, synthetic_inflow_intensity,
+               synthetic_inflow_seed, thermal, T_hot, T_cold, alpha_T, buoyancy, g_gravity, beta,
+               T_ref, precision, scalar_lattice, device, hist_capacity, rho_in=1.0, rho_out=1.0):
+        if backend not in BACKENDS:
+            raise ValueError(f"Unknown backend '{backend}'. Choose 'b200' or 'auto'.")
+        if collision not in ("bgk", "mrt", "trt"):
+            raise ValueError(f"Unknown collision '{collision}'. Choose 'bgk', 'mrt', or 'trt'.")
+        if les_model not in ("smagorinsky", "wale"):
+            raise ValueError("les_model must be 'smagorinsky' or 'wale'.")
+        if precision not in PRECISIONS:
+            raise ValueError(f"Unknown precision '{precision}'. Choose one of {PRECISIONS}.")
+        if scalar_lattice not in ("full", "reduced"):
+            raise ValueError("scalar_lattice must be 'full' or 'reduced'.")
+        if ibm_enabled:
+            raise NotImplementedError("ibm_enabled: immersed-boundary forcing is not part of the b200 engine")
+        if synthetic_inflow:
+            raise NotImplementedError("synthetic_inflow is not part of the b200 engine yet")
+        self.backend = "b200"
+        self.solid = np.ascontiguousarray(solid, dtype=np.bool_)
+        if self.solid.shape != tuple(shape):
+            raise ValueError(f"solid has shape {self.solid.shape}, expected {tuple(shape)}")
+        self.fluid = ~self.solid
+        self.omega = float(omega)
+        self.u0 = float(u0)
+        self.D = float(D)
+        self.rho0 = float(rho0)
+        self.wall_bc = wall_bc
+        self.inlet_bc = inlet_bc
+        self.outlet_bc = outlet_bc
+        self.rho_in = float(rho_in)
+        self.rho_out = float(rho_out)
+        self.collision = collision
+        self.inlet_perturbation = max(float(inlet_perturbation), 0.0)
+        self.trt_lambda = float(trt_lambda)
+        self.sponge_thickness = int(sponge_thickness)
+        self.sponge_strength = float(sponge_strength)
+        self.les = bool(les)
+        self.les_cs = float(les_cs)
+        self.les_model = str(les_model)
+        self.ibm_enabled = False
+        self.phi = phi
+        self.bouzidi = bool(bouzidi)
+        self.van_driest = bool(van_driest)
+        self.van_driest_A = float(van_driest_A)
+        self.wall_velocity_top = float(wall_velocity_top)
+        self.wall_velocity_bottom = float(wall_velocity_bottom)
+        self.synthetic_inflow = False
+        self.synthetic_inflow_intensity = float(synthetic_inflow_intensity)
+        self.thermal = bool(thermal)
+        self.T_hot = float(T_hot)
+        self.T_cold = float(T_cold)
+        self.alpha_T = float(alpha_T)
+        self.scalar_lattice = scalar_lattice
+        cs2inv = 4.0 if (scalar_lattice == "reduced" and self.dims == 3) else 3.0
+        self.omega_T = float(1.0 / (cs2inv * alpha_T + 0.5))
+        self.buoyancy = bool(buoyancy)
+        self.g_gravity = float(g_gravity)
+        self.beta = float(beta)
+        self.T_ref = float(T_ref)
+        self.tau = 1.0 / self.omega
+        self._base_nu = (self.tau - 0.5) / 3.0
+        self.precision = precision
+        self.streamwise_bc = streamwise_bc
+        self._body_force = tuple(float(v) for v in body_force)
+
+        phi_q = phi if (bouzidi and phi is not None) else None
+        self.surface_links, self.q_vals = build_surface_links(self.solid, phi_q)
+        idx = np.nonzero(self.solid)
+        ctr = [float(np.mean(a)) if a.size else 0.5 * (n - 1) for a, n in zip(idx, self.solid.shape)]
+        self._ref_center = ctr[::-1] + ([0.0] if self.dims == 2 else [])  # (x, y, z)
+
+        P = _lib.AeroParams()
+        P.abi_version = _lib.ABI_VERSION
+        P.dims = self.dims
+        if self.dims == 2:
+            P.ny, P.nx = shape
+            P.nz = 1
+        else:
+            P.nz, P.ny, P.nx = shape
+        P.storage = _lib.STORE[precision]
+        P.collision = _lib.COLLISION[collision]
+        P.inlet_bc = _lib.INLET.get(inlet_bc, 0)
+        if self.dims == 2:
+            P.outlet_bc = _lib.OUTLET.get(outlet_bc, 0)
+        else:  # solver3d.py:454-457: anything but "convective" is zero-gradient
+            P.outlet_bc = _lib.OUTLET["convective"] if outlet_bc == "convective" else _lib.OUTLET["zerogradient"]
+        P.wall_bc = _lib.WALL.get(wall_bc, 0)
+        P.streamwise_open = 1 if streamwise_bc == "open" else 0
+        P.les = int(self.les)
+        P.les_model = _lib.LES_MODEL[les_model]
+        P.van_driest = int(self.van_driest and phi is not None)
+        P.bouzidi = int(self.bouzidi)
+        P.thermal = int(self.thermal)
+        P.buoyancy = int(self.buoyancy)
+        P.scalar_reduced = int(scalar_lattice == "reduced")
+        P.sponge_thickness = self.sponge_thickness
+        P.hist_capacity = int(hist_capacity)
+        P.omega, P.u0, P.rho0 = self.omega, self.u0, self.rho0
+        P.rho_in, P.rho_out = self.rho_in, self.rho_out
+        P.inlet_perturbation = self.inlet_perturbation
+        P.trt_lambda = self.trt_lambda
+        P.sponge_strength = self.sponge_strength
+        P.les_cs, P.van_driest_A = self.les_cs, self.van_driest_A
+        P.wall_velocity_top, P.wall_velocity_bottom = self.wall_velocity_top, self.wall_velocity_bottom
+        P.body_force[:] = list(self._body_force)
+        P.alpha_T, P.T_hot, P.T_cold = self.alpha_T, self.T_hot, self.T_cold
+        P.g_gravity, P.beta, P.T_ref = self.g_gravity, self.beta, self.T_ref
+        P.center[:] = self._ref_center
+        self._params = P
+        self._engine = Engine(P, self.solid, self.surface_links, self.q_vals,
+                              phi if (self.van_driest and phi is not None) else None, device)
+
+        # initial state: equilibrium at (rho0, u0, 0) everywhere, solids included
+        # (solver.py:218-227, solver3d.py:239-247)
+        e, w, _ = tables(self.dims)
+        self.Q = len(w)
+        rho = np.full(shape, rho0)
+        ux = np.full(shape, u0)
+        zero = np.zeros(shape)
+        f0 = feq(self.dims, rho, ux, zero, zero if self.dims == 3 else None)
+        g0 = None
+        if self.thermal:
+            wg = scalar_weights(self.dims, scalar_lattice == "reduced")
+            g0 = wg.reshape((-1,) + (1,) * self.dims) * T_ref * np.ones((len(wg),) + tuple(shape))
+        self.step_count = 0
+        self._f_host = self._prev_host = self._g_host = None
+        self._pristine = {}
+        self._engine.set_state(f0, f0[..., -1], g0, 0)
+        self._init_histories()
+
+    # ------------------------------------------------------------------ state
+    def _cache(self):
+        if self._f_host is None:
+            f, p, g = self._engine.get_state()
+            self._f_host, self._prev_host, self._g_host = f, p, g
+            self._pristine = {}
+            for k, a in (("f", f), ("prev", p), ("g", g)):
+                if a is not None and a.size <= _PRISTINE_LIMIT:
+                    self._pristine[k] = a.copy()
+
+    def _mark_handed(self, key):
+        self._handed = getattr(self, "_handed", set())
+        self._handed.add(key)
+
+    @property
+    def f(self) -> np.ndarray:
+        self._cache()
+        self._mark_handed("f")
+        return self._f_host
+
+    @f.setter
+    def f(self, value):
+        self._cache()
+        self._f_host = np.ascontiguousarray(value, dtype=np.float64)
+        self._pristine.pop("f", None)
+        self._mark_handed("f")
+
+    @property
+    def _f_outlet_prev(self) -> np.ndarray:
+        self._cache()
+        self._mark_handed("prev")
+        return self._prev_host
+
+    @_f_outlet_prev.setter
+    def _f_outlet_prev(self, value):
+        self._cache()
+        self._prev_host = np.ascontiguousarray(value, dtype=np.float64)
+        self._pristine.pop("prev", None)
+        self._mark_handed("prev")
+
+    @property
+    def g(self) -> Optional[np.ndarray]:
+        if not self.thermal:
+            return None
+        self._cache()
+        self._mark_handed("g")
+        return self._g_host
+
+    @g.setter
+    def g(self, value):
+        if not self.thermal:
+            if value is not None:
+                raise ValueError("g can only be set when thermal=True")
+            return
+        self._cache()
+        self._g_host = np.ascontiguousarray(value, dtype=np.float64)
+        self._pristine.pop("g", None)
+        self._mark_handed("g")
+
+    def _flush_host_state(self):
+        """Uploads host-side edits of f / _f_outlet_prev / g before stepping."""
+        handed = getattr(self, "_handed", set())
+        if handed and self._f_host is not None:
+            changed = False
+            for k, a in (("f", self._f_host), ("prev", self._prev_host), ("g", self._g_host)):
+                if k not in handed or a is None:
+                    continue
+                ref = self._pristine.get(k)
+                if ref is None or ref.shape != a.shape or not np.array_equal(ref, a):
+                    changed = True
+            if changed:
+                self._engine.set_state(self._f_host, self._prev_host, self._g_host, self.step_count)
+        self._handed = set()
+        self._f_host = self._prev_host = self._g_host = None
+        self._pristine = {}
+
+    # ------------------------------------------------------------------ stepping
+    def _advance(self, n: int) -> np.ndarray:
+        """Runs n steps on the GPU and returns their raw force rows (n, 12)."""
+        self._flush_host_state()
+        rows = []
+        left = int(n)
+        cap = self._engine.hist_capacity
+        while left > 0:
+            k = min(left, cap)
+            self._engine.step(k)
+            rows.append(self._engine.read_forces(k))
+            left -= k
+        self.step_count += int(n)
+        raw = np.concatenate(rows) if rows else np.zeros((0, 12))
+        if len(raw):
+            self._set_last(raw[-1], self._engine.read_profile())
+        return raw
+
+    def _step(self):
+        raw = self._advance(1)
+        c = self._coefficients(raw)
+        return self._step_return(c, 0)
+
+    def status(self) -> int:
+        """Device divergence flags (bit 0: non-finite or non-positive density seen)."""
+        return self._engine.status()
+
+    # ------------------------------------------------------------------ checkpoints
+    def save_checkpoint(self, path: str) -> None:
+        params = self._checkpoint_params()
+        f = self.f
+        kwargs = dict(
+            f=f, f_outlet_prev=self._f_outlet_prev, solid=self.solid,
+            surface_links=self.surface_links, q_vals=self.q_vals,
+            step_count=np.array(self.step_count, dtype=np.int64),
+            params_json=np.array(json.dumps(params)),
+            **{k: np.array(getattr(self, k), dtype=np.float64) for k in self._history_keys()},
+        )
+        if self.phi is not None:
+            kwargs["phi"] = self.phi
+        if self.thermal:
+            kwargs["g"] = self.g
+        np.savez_compressed(path, **kwargs)
+
+    def load_checkpoint(self, path: str) -> None:
+        data = np.load(path, allow_pickle=False)
+        for k in self._history_keys():
+            if k in data:
+                setattr(self, k, list(data[k]))
+        self.step_count = int(data["step_count"])
+        if "surface_links" in data and not np.array_equal(data["surface_links"], self.surface_links):
+            warnings.warn("checkpoint link table differs from the one built from its solid mask; "
+                          "the engine keeps the rebuilt one", RuntimeWarning)
+        g = data["g"] if ("g" in data and self.thermal) else None
+        if self.thermal and g is None:
+            g = self.g
+        self._handed = set()
+        self._f_host = None
+        self._engine.set_state(data["f"], data["f_outlet_prev"], g, self.step_count)
+
+    @classmethod
+    def from_checkpoint(cls, path: str, backend: Optional[str] = None, **overrides):
+        data = np.load(path, allow_pickle=False)
+        params = json.loads(str(data["params_json"]))
+        params["backend"] = "b200"
+        params.update(overrides)
+        solid = data["solid"]
+        phi = data["phi"] if "phi" in data else None
+        s = cls(solid=solid, phi=phi, **params)
+        s.load_checkpoint(path)
+        return s
+
+    # ------------------------------------------------------------------ run loop
+    def run(self, steps: int, check_every: int = 500, verbose: bool = True, callback=None,
+            checkpoint_every: Optional[int] = None, checkpoint_dir: Optional[str] = None,
+            auto_stop: bool = False, convergence_window: int = 5000, convergence_tol: float = 0.01,
+            strouhal_window: int = 4096, strouhal_tol: float = 0.05, hdf5_path: Optional[str] = None,
+            hdf5_every: Optional[int] = None) -> dict:
+        """Runs ``steps`` steps with the semantics of Solver.run (solver.py:470-632)."""
+        if verbose:
+            self._print_banner()
+        if hdf5_path:
+            warnings.warn("hdf5_path is ignored by the b200 backend (h5py output is not part of the "
+                          "engine)", RuntimeWarning)
+        t0 = time.perf_counter()
+        avg_window = max(1, steps // 5)
+        stop_reason = "max_steps"
+        last_conv = last_st = None
+        step = 0
+        check_every = max(int(check_every), 1)
+        while step < steps:
+            nxt = steps
+            nxt = min(nxt, (step // check_every + 1) * check_every)
+            if checkpoint_every and checkpoint_dir:
+                nxt = min(nxt, (step // checkpoint_every + 1) * checkpoint_every)
+            raw = self._advance(nxt - step)
+            self._append_histories(self._coefficients(raw))
+            step = nxt
+            if checkpoint_every and checkpoint_dir and step % checkpoint_every == 0:
+                self.save_checkpoint(str(pathlib.Path(checkpoint_dir) / self._checkpoint_name()))
+            if step % check_every == 0:
+                macro = self._stability_check(step)
+                elapsed = time.perf_counter() - t0
+                if verbose:
+                    self._print_progress(step, steps, check_every, step / max(elapsed, 1e-12))
+                if callback is not None:
+                    self._callback(callback, step, macro)
+                if auto_stop:
+                    last_conv, last_st, stop = detect_statistical_stationarity(
+                        self.Cd_history, self._lift_history_for_stop(strouhal_window), self.D, self.u0,
+                        convergence_window=convergence_window, convergence_tol=convergence_tol,
+                        strouhal_window=strouhal_window, strouhal_tol=strouhal_tol)
+                    if stop:
+                        stop_reason = "auto_converged"
+                        break
+        return self._result(avg_window, stop_reason, last_conv, last_st)
+
+    # ------------------------------------------------------------------ helpers
+    def _scalar_stats(self):
+        if not self.thermal:
+            return None, None
+        T = self._scalar_field()
+        return T, {
+            "enabled": True, "mean": float(np.mean(T)), "std": float(np.std(T)),
+            "min": float(np.min(T)), "max": float(np.max(T)), "wall_hot": float(self.T_hot),
+            "wall_cold": float(self.T_cold), "diffusivity": float(self.alpha_T),
+            "buoyancy": bool(self.buoyancy), "gravity": float(self.g_gravity),
+            "beta": float(self.beta), "reference": float(self.T_ref),
+        }
+
+    def _scalar_field(self) -> np.ndarray:
+        _, _, g = self._engine.get_state_device(want_prev=False, want_g=True)
+        return g.sum(dim=0).cpu().numpy()
+
+    def _macroscopic_device(self):
+        """rho, u of the current state, computed slab by slab on the GPU."""
+        import torch
+        e, _, _ = tables(self.dims)
+        et = torch.tensor(e.astype(np.float64), device=self._engine.device)
+        if self.dims == 2:
+            f = self._engine.get_slab_device(0, 1)[:, 0]
+            return _moments_torch(f, et, 2)
+        nz = self.solid.shape[0]
+        plane = int(np.prod(self.solid.shape[1:]))
+        slab = max(1, min(nz, (1 << 27) // max(plane * self.Q, 1)))
+        outs = [[] for _ in range(4)]
+        for z0 in range(0, nz, slab):
+            nzs = min(slab, nz - z0)
+            f = self._engine.get_slab_device(z0, nzs)
+            for k, a in enumerate(_moments_torch(f, et, 3)):
+                outs[k].append(a)
+        return tuple(torch.cat(o) for o in outs)
+
+
+def _moments_torch(f, et, dims):
+    import torch
+    rho = f.sum(dim=0)
+    inv = torch.where(rho > 0, 1.0 / torch.where(rho > 0, rho, torch.ones_like(rho)), torch.zeros_like(rho))
+    u = [inv * torch.tensordot(et[:, a], f, dims=([0], [0])) for a in range(dims)]
+    return (rho, *u)

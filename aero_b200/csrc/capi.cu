@@ -1,0 +1,694 @@
+// capi.cu -- host runtime behind the C ABI (include/aero_b200.h).
+//
+// Owns no device memory: every device buffer is carved out of the workspace
+// the caller binds.  Keeps the A/B buffer parity, the host mirror of the
+// step counter and the force-history read cursor, and replays the step
+// sequence of two steps as a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/aero_b200.h"
+#include "lbm_dispatch.h"
+#include "lbm_kernels.cuh"
+
+using namespace aero;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                       \
+  do {                                                                                       \
+    cudaError_t e_ = (expr);                                                                 \
+    if (e_ != cudaSuccess) return fail(AERO_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr uint64_t kAlign = 256;
+uint64_t align_up(uint64_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+
+struct Layout {
+  uint64_t P[2], solid, lbits, loff, lc_mask, lc_q, lc_cell, lc_prof, prof_off, prev[2], g[2], U, cs_cell,
+      partials, hist, prof_out, counters, total;
+};
+
+struct WTab {
+  double w[19];
+};
+
+// small element-wise kernels for state I/O --------------------------------
+__global__ void k_set_i64(int64_t *p, int64_t v) { *p = v; }
+
+template <class Real>
+__global__ void k_prev_in(Real *dst, const double *src, int Q, int64_t plane, WTab w) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= (int64_t)Q * plane) return;
+  dst[k] = (Real)(src[k] - w.w[k / plane]);
+}
+template <class Real>
+__global__ void k_prev_out(double *dst, const Real *src, int Q, int64_t plane, WTab w) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= (int64_t)Q * plane) return;
+  dst[k] = w.w[k / plane] + (double)src[k];
+}
+template <class Real>
+__global__ void k_g_in(Real *dst, const double *src, int Qg, int64_t ncells, int64_t cs) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= (int64_t)Qg * ncells) return;
+  dst[(k / ncells) * cs + k % ncells] = (Real)src[k];
+}
+template <class Real>
+__global__ void k_g_out(double *dst, const Real *src, int Qg, int64_t ncells, int64_t cs) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= (int64_t)Qg * ncells) return;
+  dst[k] = (double)src[(k / ncells) * cs + k % ncells];
+}
+
+unsigned blocks_for(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+}  // namespace
+
+struct AeroLattice {
+  AeroParams prm;
+  int Q = 0, Qg = 0;
+  int64_t ncells = 0, cs = 0, nwords = 0, prev_plane = 0;
+  int nwx = 0, nprof = 0, hist_cap = 4096, n_force_blocks = 0;
+  uint32_t feat = 0;
+  // host geometry tables (kept until bind)
+  std::vector<uint8_t> solid;
+  std::vector<uint32_t> lbits, lc_mask;
+  std::vector<int32_t> loff, prof_off;
+  std::vector<float> lc_q;
+  std::vector<int64_t> lc_cell;
+  std::vector<double> cs_cell;
+  int64_t n_links = 0;
+  bool geometry = false;
+  // workspace
+  Layout lay{};
+  char *ws = nullptr;
+  bool bound = false, state_set = false;
+  int cur = 0;
+  bool old_is_state = false;
+  int64_t step_count = 0, read_upto = 0;
+  MrtCoeffs<double> mrt{};
+  WTab w{}, wg{};
+  // CUDA graphs of a two-step sequence, one per starting parity
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t pair_exec[2] = {nullptr, nullptr};
+  bool use_graphs = true;
+  int device = -1;  // device of the bound workspace
+};
+
+namespace {
+
+bool is_f64(const AeroLattice *L) { return L->prm.storage == AERO_STORE_F64; }
+
+template <class Real>
+const Ops<Real> *get_ops(const AeroLattice *L);
+template <>
+const Ops<double> *get_ops<double>(const AeroLattice *L) {
+  return ops_f64(L->prm.dims, L->prm.collision);
+}
+template <>
+const Ops<float> *get_ops<float>(const AeroLattice *L) {
+  switch (L->prm.storage) {
+    case AERO_STORE_F32: return ops_f32(L->prm.dims, L->prm.collision);
+    case AERO_STORE_F16: return ops_f16(L->prm.dims, L->prm.collision);
+    case AERO_STORE_BF16: return ops_bf16(L->prm.dims, L->prm.collision);
+  }
+  return nullptr;
+}
+
+template <class Real>
+StepParams<Real> make_params(const AeroLattice *L, int cur) {
+  const AeroParams &a = L->prm;
+  StepParams<Real> p;
+  std::memset(&p, 0, sizeof(p));
+  char *ws = L->ws;
+  const int nxt = 1 - cur;
+  p.nx = a.nx;
+  p.ny = a.ny;
+  p.nz = a.nz;
+  p.nwx = L->nwx;
+  p.cs = L->cs;
+  p.ncells = L->ncells;
+  p.feat = L->feat;
+  p.inlet = a.inlet_bc;
+  p.outlet = a.outlet_bc;
+  p.wall = a.wall_bc;
+  p.sponge_thickness = a.sponge_thickness;
+  p.sponge_start = std::max(a.nx - a.sponge_thickness, 0);
+  p.P = ws + L->lay.P[cur];
+  p.Pn = ws + L->lay.P[nxt];
+  p.solid = reinterpret_cast<const uint8_t *>(ws + L->lay.solid);
+  p.lbits = reinterpret_cast<const uint32_t *>(ws + L->lay.lbits);
+  p.loff = reinterpret_cast<const int32_t *>(ws + L->lay.loff);
+  p.lc_mask = reinterpret_cast<const uint32_t *>(ws + L->lay.lc_mask);
+  p.lc_q = reinterpret_cast<const float *>(ws + L->lay.lc_q);
+  p.lc_cell = reinterpret_cast<const int64_t *>(ws + L->lay.lc_cell);
+  p.n_lc = (int64_t)L->lc_cell.size();
+  p.prev = reinterpret_cast<const Real *>(ws + L->lay.prev[cur]);
+  p.prevn = reinterpret_cast<Real *>(ws + L->lay.prev[nxt]);
+  p.g = reinterpret_cast<const Real *>(ws + L->lay.g[cur]);
+  p.gn = reinterpret_cast<Real *>(ws + L->lay.g[nxt]);
+  p.U = reinterpret_cast<const Real *>(ws + L->lay.U);
+  p.Uw = reinterpret_cast<Real *>(ws + L->lay.U);
+  p.cs_cell = reinterpret_cast<const Real *>(ws + L->lay.cs_cell);
+  p.partials = reinterpret_cast<double *>(ws + L->lay.partials);
+  p.lc_prof = reinterpret_cast<double *>(ws + L->lay.lc_prof);
+  p.prof_off = reinterpret_cast<const int32_t *>(ws + L->lay.prof_off);
+  p.hist = reinterpret_cast<double *>(ws + L->lay.hist);
+  p.prof_out = reinterpret_cast<double *>(ws + L->lay.prof_out);
+  p.nprof = L->nprof;
+  p.hist_cap = L->hist_cap;
+  p.n_force_blocks = L->n_force_blocks;
+  p.want_profile = 1;
+  int64_t *ctr = reinterpret_cast<int64_t *>(ws + L->lay.counters);
+  p.step = ctr;
+  p.hist_base = ctr + 1;
+  p.status = reinterpret_cast<uint32_t *>(ctr + 2);
+  const double tau = 1.0 / a.omega;
+  const double tp = a.trt_lambda * tau + (1.0 - a.trt_lambda);
+  const double tm = (tp * tau - 0.5) / (tp - 0.5);
+  p.omega = (Real)a.omega;
+  p.u0 = (Real)a.u0;
+  p.rho_in = (Real)a.rho_in;
+  p.rho_out = (Real)a.rho_out;
+  p.pert_amp = (Real)std::max(a.inlet_perturbation, 0.0);
+  p.trt_lambda = (Real)a.trt_lambda;
+  p.trt_sminus = (Real)(1.0 / tm);
+  p.sponge_sigma_max = (Real)a.sponge_strength;
+  p.base_nu = (Real)((1.0 / a.omega - 0.5) / 3.0);
+  p.les_cs2 = (Real)(a.les_cs * a.les_cs);
+  p.wall_u_top = (Real)a.wall_velocity_top;
+  p.wall_u_bottom = (Real)a.wall_velocity_bottom;
+  p.bf_x = (Real)a.body_force[0];
+  p.bf_y = (Real)a.body_force[1];
+  p.bf_z = (Real)a.body_force[2];
+  p.bf_coeff = (Real)(1.0 - 0.5 / (1.0 / a.omega));
+  const double aT = (a.scalar_reduced && a.dims == 3) ? 4.0 : 3.0;
+  p.omega_T = (Real)(1.0 / (aT * a.alpha_T + 0.5));
+  p.T_hot = (Real)a.T_hot;
+  p.T_cold = (Real)a.T_cold;
+  p.gbeta = (Real)(a.g_gravity * a.beta);
+  p.T_ref = (Real)a.T_ref;
+  for (int k = 0; k < 3; k++) p.center[k] = a.center[k];
+  for (int k = 0; k < 100; k++) p.mrt.Ae[k] = (Real)L->mrt.Ae[k];
+  for (int k = 0; k < 70; k++) p.mrt.Ce[k] = (Real)L->mrt.Ce[k];
+  for (int k = 0; k < 81; k++) p.mrt.Ao[k] = (Real)L->mrt.Ao[k];
+  for (int k = 0; k < 27; k++) p.mrt.Co[k] = (Real)L->mrt.Co[k];
+  return p;
+}
+
+dim3 cell_grid(const AeroLattice *L) {
+  return dim3(blocks_for(L->prm.nx, kStepBlock), (unsigned)L->prm.ny, (unsigned)L->prm.nz);
+}
+
+bool les_active(const AeroLattice *L) { return (L->feat & FEAT_LES) != 0; }
+
+// Launches one step with buffer parity `cur` on stream st.
+template <class Real>
+int launch_step(AeroLattice *L, int cur, cudaStream_t st) {
+  const Ops<Real> *ops = get_ops<Real>(L);
+  const StepParams<Real> p = make_params<Real>(L, cur);
+  const dim3 grid = cell_grid(L);
+  if (L->n_force_blocks > 0) CUDA_TRY(ops->forces(p, L->n_force_blocks, st));
+  if (les_active(L)) CUDA_TRY(ops->moments(p, false, grid, st));
+  CUDA_TRY(ops->step(p, false, grid, st));
+  CUDA_TRY(ops->finalize(p, st));
+  return AERO_OK;
+}
+
+template <class Real>
+int build_pair_graph(AeroLattice *L, int cur) {
+  if (!L->cap_stream) CUDA_TRY(cudaStreamCreateWithFlags(&L->cap_stream, cudaStreamNonBlocking));
+  CUDA_TRY(cudaStreamBeginCapture(L->cap_stream, cudaStreamCaptureModeThreadLocal));
+  int rc = launch_step<Real>(L, cur, L->cap_stream);
+  if (rc == AERO_OK) rc = launch_step<Real>(L, 1 - cur, L->cap_stream);
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(L->cap_stream, &graph);
+  if (rc != AERO_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(AERO_ERR_CUDA, "stream capture: %s", cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&L->pair_exec[cur], graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return fail(AERO_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  return AERO_OK;
+}
+
+template <class Real>
+int do_steps(AeroLattice *L, int64_t n, cudaStream_t st) {
+  while (n > 0) {
+    if (n >= 2 && L->use_graphs) {
+      if (!L->pair_exec[L->cur]) {
+        const int rc = build_pair_graph<Real>(L, L->cur);
+        if (rc != AERO_OK) return rc;
+      }
+      CUDA_TRY(cudaGraphLaunch(L->pair_exec[L->cur], st));
+      n -= 2;
+      L->step_count += 2;
+    } else {
+      const int rc = launch_step<Real>(L, L->cur, st);
+      if (rc != AERO_OK) return rc;
+      L->cur ^= 1;
+      n -= 1;
+      L->step_count += 1;
+    }
+    L->old_is_state = false;
+  }
+  return AERO_OK;
+}
+
+template <class Real>
+int do_set_state(AeroLattice *L, const double *f, const double *prev, const double *g, int64_t steps,
+                 cudaStream_t st) {
+  const Ops<Real> *ops = get_ops<Real>(L);
+  const int old = 1 - L->cur;
+  const dim3 grid = cell_grid(L);
+  StepParams<Real> p = make_params<Real>(L, L->cur);
+  // raw state into the old buffer, then collide it into the current one
+  CUDA_TRY(ops->load_state(p, f, L->ws + L->lay.P[old], grid, st));
+  if (prev) {
+    const int64_t n = (int64_t)L->Q * L->prev_plane;
+    k_prev_in<Real><<<blocks_for(n, 256), 256, 0, st>>>(reinterpret_cast<Real *>(L->ws + L->lay.prev[L->cur]),
+                                                        prev, L->Q, L->prev_plane, L->w);
+    CUDA_TRY(cudaGetLastError());
+  }
+  if (g && L->prm.thermal) {
+    const int64_t n = (int64_t)L->Qg * L->ncells;
+    k_g_in<Real><<<blocks_for(n, 256), 256, 0, st>>>(reinterpret_cast<Real *>(L->ws + L->lay.g[L->cur]), g, L->Qg,
+                                                     L->ncells, L->cs);
+    CUDA_TRY(cudaGetLastError());
+  }
+  int64_t *ctr = reinterpret_cast<int64_t *>(L->ws + L->lay.counters);
+  k_set_i64<<<1, 1, 0, st>>>(ctr, steps);
+  CUDA_TRY(cudaGetLastError());
+  StepParams<Real> q = p;
+  q.P = L->ws + L->lay.P[old];
+  q.Pn = L->ws + L->lay.P[L->cur];
+  if (les_active(L)) CUDA_TRY(ops->moments(q, true, grid, st));
+  CUDA_TRY(ops->step(q, true, grid, st));
+  L->old_is_state = true;
+  L->step_count = steps;
+  L->read_upto = steps;
+  L->state_set = true;
+  return AERO_OK;
+}
+
+template <class Real>
+int do_get_state(AeroLattice *L, double *f, double *prev, double *g, int z0, int nzs, cudaStream_t st) {
+  const Ops<Real> *ops = get_ops<Real>(L);
+  const int old = 1 - L->cur;
+  if (f) {
+    // the state of the last step is evaluated from the previous buffers
+    StepParams<Real> p = make_params<Real>(L, old);
+    dim3 grid = cell_grid(L);
+    grid.z = (unsigned)nzs;
+    CUDA_TRY(ops->state_out(p, f, -1, L->old_is_state, z0, grid, st));
+  }
+  if (prev) {
+    const int64_t n = (int64_t)L->Q * L->prev_plane;
+    k_prev_out<Real><<<blocks_for(n, 256), 256, 0, st>>>(
+        prev, reinterpret_cast<const Real *>(L->ws + L->lay.prev[L->cur]), L->Q, L->prev_plane, L->w);
+    CUDA_TRY(cudaGetLastError());
+  }
+  if (g && L->prm.thermal) {
+    const int64_t n = (int64_t)L->Qg * L->ncells;
+    k_g_out<Real><<<blocks_for(n, 256), 256, 0, st>>>(g, reinterpret_cast<const Real *>(L->ws + L->lay.g[L->cur]),
+                                                      L->Qg, L->ncells, L->cs);
+    CUDA_TRY(cudaGetLastError());
+  }
+  return AERO_OK;
+}
+
+int check_params(const AeroParams *a) {
+  if (!a) return fail(AERO_ERR_INVALID, "params is NULL");
+  if (a->abi_version != AERO_ABI_VERSION)
+    return fail(AERO_ERR_INVALID, "abi_version %d != %d", a->abi_version, AERO_ABI_VERSION);
+  if (a->dims != 2 && a->dims != 3) return fail(AERO_ERR_INVALID, "dims must be 2 or 3");
+  if (a->dims == 2 && a->nz != 1) return fail(AERO_ERR_INVALID, "nz must be 1 in 2D");
+  if (a->nx < 3 || a->ny < 2 || a->nz < 1) return fail(AERO_ERR_INVALID, "grid too small (nx>=3, ny>=2)");
+  if (a->ny > 65535 || a->nz > 65535) return fail(AERO_ERR_INVALID, "ny and nz must be <= 65535");
+  if ((int64_t)a->nx * a->ny * a->nz > ((int64_t)1 << 40)) return fail(AERO_ERR_INVALID, "grid too large");
+  if (a->storage < 0 || a->storage > 3) return fail(AERO_ERR_INVALID, "unknown storage %d", a->storage);
+  if (a->collision < 0 || a->collision > 2) return fail(AERO_ERR_INVALID, "unknown collision %d", a->collision);
+  if (!(a->omega > 0.0) || !std::isfinite(a->omega)) return fail(AERO_ERR_INVALID, "omega must be > 0");
+  if (a->inlet_bc < 0 || a->inlet_bc > 2) return fail(AERO_ERR_INVALID, "unknown inlet_bc");
+  if (a->outlet_bc < 0 || a->outlet_bc > 3) return fail(AERO_ERR_INVALID, "unknown outlet_bc");
+  if (a->wall_bc < 0 || a->wall_bc > 3) return fail(AERO_ERR_INVALID, "unknown wall_bc");
+  if (a->dims == 3 && (a->inlet_bc == AERO_INLET_PRESSURE || a->outlet_bc == AERO_OUTLET_PRESSURE))
+    return fail(AERO_ERR_UNSUPPORTED, "pressure inlet/outlet exist only in 2D");
+  if (a->sponge_thickness < 0) return fail(AERO_ERR_INVALID, "sponge_thickness < 0");
+  if (a->hist_capacity < 0) return fail(AERO_ERR_INVALID, "hist_capacity < 0");
+  return AERO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int aero_abi_version(void) { return AERO_ABI_VERSION; }
+
+const char *aero_last_error(void) { return g_err.c_str(); }
+
+int aero_lattice_q(const AeroParams *a, int32_t *q, int32_t *qg) {
+  if (!a) return fail(AERO_ERR_INVALID, "params is NULL");
+  const int Q = a->dims == 2 ? 9 : 19;
+  if (q) *q = Q;
+  if (qg) *qg = a->thermal ? (a->scalar_reduced ? (a->dims == 2 ? 5 : 7) : Q) : 0;
+  return AERO_OK;
+}
+
+int aero_create(const AeroParams *params, AeroLattice **out) {
+  if (!out) return fail(AERO_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  const int rc = check_params(params);
+  if (rc != AERO_OK) return rc;
+  AeroLattice *L = new AeroLattice();
+  L->prm = *params;
+  const AeroParams &a = L->prm;
+  L->Q = a.dims == 2 ? 9 : 19;
+  L->Qg = a.thermal ? (a.scalar_reduced ? (a.dims == 2 ? 5 : 7) : L->Q) : 0;
+  L->ncells = (int64_t)a.nx * a.ny * a.nz;
+  L->cs = (L->ncells + 63) / 64 * 64;
+  L->nwx = (a.nx + 31) / 32;
+  L->nwords = (int64_t)a.nz * a.ny * L->nwx;
+  L->prev_plane = (int64_t)a.nz * a.ny;
+  L->nprof = a.dims == 3 ? a.nz : a.ny;
+  L->hist_cap = a.hist_capacity > 0 ? a.hist_capacity : 4096;
+  for (int i = 0; i < L->Q; i++) L->w.w[i] = a.dims == 2 ? D2Q9::w[i] : D3Q19::w[i];
+  uint32_t f = 0;
+  if (a.dims == 2 || a.streamwise_open) f |= FEAT_OPEN;
+  if (a.bouzidi) f |= FEAT_BOUZIDI;
+  if (a.dims == 3 && (std::fabs(a.body_force[0]) >= 1e-16 || std::fabs(a.body_force[1]) >= 1e-16 ||
+                      std::fabs(a.body_force[2]) >= 1e-16))
+    f |= FEAT_BODY_FORCE;
+  if (a.sponge_thickness > 0 && a.sponge_strength > 0.0) f |= FEAT_SPONGE;
+  if (a.les && a.collision != AERO_MRT) {
+    f |= FEAT_LES;
+    if (a.les_model == AERO_LES_WALE) f |= FEAT_LES_WALE;
+  }
+  if (a.thermal) {
+    f |= FEAT_THERMAL;
+    if (a.buoyancy) f |= FEAT_BUOYANCY;
+    if (a.scalar_reduced) f |= FEAT_SCALAR_REDUCED;
+  }
+  L->feat = f;
+  if (a.collision == AERO_MRT && !build_mrt(a.dims, a.omega, L->mrt, nullptr, nullptr)) {
+    delete L;
+    return fail(AERO_ERR_INVALID, "MRT operator is not block diagonal in the pair basis");
+  }
+  const char *ng = std::getenv("AERO_B200_NO_GRAPHS");
+  L->use_graphs = !(ng && ng[0] == '1');
+  *out = L;
+  return AERO_OK;
+}
+
+int aero_set_geometry(AeroLattice *L, const uint8_t *solid, const int32_t *links, const float *q, int64_t n_links,
+                      const double *phi) {
+  if (!L) return fail(AERO_ERR_INVALID, "lattice is NULL");
+  if (L->bound) return fail(AERO_ERR_STATE, "geometry must be set before the workspace is bound");
+  if (!solid) return fail(AERO_ERR_INVALID, "solid is NULL");
+  if (n_links < 0 || (n_links > 0 && (!links || !q))) return fail(AERO_ERR_INVALID, "bad link list");
+  const AeroParams &a = L->prm;
+  const int lw = a.dims == 3 ? 4 : 3;
+  L->solid.assign(solid, solid + L->ncells);
+  for (auto &v : L->solid) v = v ? 1 : 0;
+  // group links by cell, keep cells in increasing index order
+  std::vector<std::pair<int64_t, int64_t>> order;  // (cell, link index)
+  order.reserve((size_t)n_links);
+  for (int64_t k = 0; k < n_links; k++) {
+    const int32_t *lk = links + k * lw;
+    const int i = lk[0];
+    const int z = a.dims == 3 ? lk[1] : 0, y = lk[lw - 2], x = lk[lw - 1];
+    if (i < 1 || i >= L->Q || x < 0 || x >= a.nx || y < 0 || y >= a.ny || z < 0 || z >= a.nz)
+      return fail(AERO_ERR_INVALID, "link %lld out of range", (long long)k);
+    const int64_t c = ((int64_t)z * a.ny + y) * a.nx + x;
+    if (L->solid[c]) return fail(AERO_ERR_INVALID, "link %lld starts in a solid cell", (long long)k);
+    if (!(q[k] > 0.0f) || !(q[k] <= 1.0f)) return fail(AERO_ERR_INVALID, "link %lld has q outside (0, 1]", (long long)k);
+    order.emplace_back(c, k);
+  }
+  std::stable_sort(order.begin(), order.end(), [](const auto &u, const auto &v) { return u.first < v.first; });
+  L->lc_cell.clear();
+  L->lc_mask.clear();
+  L->lc_q.clear();
+  for (const auto &e : order) {
+    if (L->lc_cell.empty() || L->lc_cell.back() != e.first) {
+      L->lc_cell.push_back(e.first);
+      L->lc_mask.push_back(0u);
+      L->lc_q.insert(L->lc_q.end(), L->Q, 0.5f);
+    }
+    const int i = links[e.second * lw];
+    L->lc_mask.back() |= 1u << i;
+    L->lc_q[(L->lc_cell.size() - 1) * L->Q + i] = q[e.second];
+  }
+  L->n_links = n_links;
+  L->lbits.assign((size_t)L->nwords, 0u);
+  L->loff.assign((size_t)L->nwords, 0);
+  for (size_t k = 0; k < L->lc_cell.size(); k++) {
+    const int64_t c = L->lc_cell[k];
+    const int x = (int)(c % a.nx);
+    const int64_t row = c / a.nx;
+    const int64_t word = row * L->nwx + (x >> 5);
+    if (L->lbits[word] == 0u) L->loff[word] = (int32_t)k;
+    L->lbits[word] |= 1u << (x & 31);
+  }
+  // profile segments: link cells are sorted by cell index, hence by y (2D) / z (3D)
+  L->prof_off.assign(L->nprof + 1, 0);
+  {
+    size_t k = 0;
+    for (int b = 0; b <= L->nprof; b++) {
+      while (k < L->lc_cell.size()) {
+        const int64_t c = L->lc_cell[k];
+        const int bin = a.dims == 3 ? (int)(c / ((int64_t)a.nx * a.ny)) : (int)((c / a.nx) % a.ny);
+        if (bin >= b) break;
+        k++;
+      }
+      L->prof_off[b] = (int32_t)k;
+    }
+  }
+  if (n_links > 0) L->feat |= FEAT_OBSTACLE_BB; else L->feat &= ~FEAT_OBSTACLE_BB;
+  L->n_force_blocks = (int)((L->lc_cell.size() + kForceBlock - 1) / kForceBlock);
+  L->cs_cell.clear();
+  L->feat &= ~FEAT_LES_CS_FIELD;
+  if ((L->feat & FEAT_LES) && a.van_driest && phi) {
+    L->cs_cell.resize(L->ncells);
+    for (int64_t c = 0; c < L->ncells; c++) {
+      const double dmp = 1.0 - std::exp(-std::fabs(phi[c]) / a.van_driest_A);
+      L->cs_cell[c] = a.les_cs * dmp * dmp;
+    }
+    L->feat |= FEAT_LES_CS_FIELD;
+  }
+  // workspace layout
+  Layout &y = L->lay;
+  const uint64_t sb = is_f64(L) ? 8 : (L->prm.storage == AERO_STORE_F32 ? 4 : 2);
+  const uint64_t rb = is_f64(L) ? 8 : 4;
+  const uint64_t nlc = L->lc_cell.size();
+  uint64_t o = 0;
+  auto take = [&](uint64_t bytes) {
+    const uint64_t at = o;
+    o = align_up(o + std::max<uint64_t>(bytes, 1));
+    return at;
+  };
+  y.P[0] = take(sb * L->Q * L->cs);
+  y.P[1] = take(sb * L->Q * L->cs);
+  y.solid = take(L->cs);
+  y.lbits = take(4 * L->nwords);
+  y.loff = take(4 * L->nwords);
+  y.lc_mask = take(4 * nlc);
+  y.lc_q = take(4 * nlc * L->Q);
+  y.lc_cell = take(8 * nlc);
+  y.lc_prof = take(24 * nlc);
+  y.prof_off = take(4 * (L->nprof + 1));
+  y.prev[0] = take(rb * L->Q * L->prev_plane);
+  y.prev[1] = take(rb * L->Q * L->prev_plane);
+  y.g[0] = take(L->Qg ? rb * L->Qg * L->cs : 0);
+  y.g[1] = take(L->Qg ? rb * L->Qg * L->cs : 0);
+  y.U = take((L->feat & FEAT_LES) ? rb * 3 * L->cs : 0);
+  y.cs_cell = take(L->cs_cell.empty() ? 0 : rb * L->cs);
+  y.partials = take(8 * 12 * std::max(L->n_force_blocks, 1));
+  y.hist = take(8 * 12 * (uint64_t)L->hist_cap);
+  y.prof_out = take(24 * (uint64_t)L->nprof);
+  y.counters = take(64);
+  y.total = o;
+  L->geometry = true;
+  return AERO_OK;
+}
+
+int aero_workspace_size(const AeroLattice *L, uint64_t *bytes) {
+  if (!L || !bytes) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->geometry) return fail(AERO_ERR_STATE, "aero_set_geometry must come first");
+  *bytes = L->lay.total;
+  return AERO_OK;
+}
+
+int aero_bind_workspace(AeroLattice *L, void *dptr, uint64_t bytes, void *stream) {
+  if (!L || !dptr) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->geometry) return fail(AERO_ERR_STATE, "aero_set_geometry must come first");
+  if (L->bound) return fail(AERO_ERR_STATE, "workspace already bound");
+  if (bytes < L->lay.total) return fail(AERO_ERR_INVALID, "workspace too small: %llu < %llu",
+                                        (unsigned long long)bytes, (unsigned long long)L->lay.total);
+  if (reinterpret_cast<uintptr_t>(dptr) % kAlign) return fail(AERO_ERR_INVALID, "workspace must be 256-byte aligned");
+  cudaPointerAttributes attr;
+  CUDA_TRY(cudaPointerGetAttributes(&attr, dptr));
+  if (attr.type != cudaMemoryTypeDevice) return fail(AERO_ERR_INVALID, "workspace is not device memory");
+  L->device = attr.device;
+  CUDA_TRY(cudaSetDevice(L->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  L->ws = static_cast<char *>(dptr);
+  auto up = [&](uint64_t off, const void *src, uint64_t n) -> cudaError_t {
+    if (n == 0) return cudaSuccess;
+    return cudaMemcpyAsync(L->ws + off, src, n, cudaMemcpyHostToDevice, st);
+  };
+  CUDA_TRY(cudaMemsetAsync(L->ws, 0, L->lay.total, st));
+  CUDA_TRY(up(L->lay.solid, L->solid.data(), L->solid.size()));
+  CUDA_TRY(up(L->lay.lbits, L->lbits.data(), 4 * L->lbits.size()));
+  CUDA_TRY(up(L->lay.loff, L->loff.data(), 4 * L->loff.size()));
+  CUDA_TRY(up(L->lay.lc_mask, L->lc_mask.data(), 4 * L->lc_mask.size()));
+  CUDA_TRY(up(L->lay.lc_q, L->lc_q.data(), 4 * L->lc_q.size()));
+  CUDA_TRY(up(L->lay.lc_cell, L->lc_cell.data(), 8 * L->lc_cell.size()));
+  CUDA_TRY(up(L->lay.prof_off, L->prof_off.data(), 4 * L->prof_off.size()));
+  if (!L->cs_cell.empty()) {
+    if (is_f64(L)) {
+      CUDA_TRY(up(L->lay.cs_cell, L->cs_cell.data(), 8 * L->cs_cell.size()));
+    } else {
+      std::vector<float> tmp(L->cs_cell.begin(), L->cs_cell.end());
+      CUDA_TRY(up(L->lay.cs_cell, tmp.data(), 4 * tmp.size()));
+      CUDA_TRY(cudaStreamSynchronize(st));  // tmp goes out of scope
+    }
+  }
+  // host vectors must outlive the async copies
+  CUDA_TRY(cudaStreamSynchronize(st));
+  L->bound = true;
+  return AERO_OK;
+}
+
+int aero_set_state(AeroLattice *L, const double *f, const double *prev, const double *g, int64_t steps,
+                   void *stream) {
+  if (!L || !f) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
+  if (steps < 0) return fail(AERO_ERR_INVALID, "negative step count");
+  if (!L->state_set && !prev && (L->prm.outlet_bc == AERO_OUTLET_CONVECTIVE))
+    return fail(AERO_ERR_INVALID, "the first state must include f_outlet_prev");
+  if (!L->state_set && !g && L->prm.thermal) return fail(AERO_ERR_INVALID, "the first state must include g");
+  CUDA_TRY(cudaSetDevice(L->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return is_f64(L) ? do_set_state<double>(L, f, prev, g, steps, st) : do_set_state<float>(L, f, prev, g, steps, st);
+}
+
+int aero_get_state(AeroLattice *L, double *f, double *prev, double *g, void *stream) {
+  if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->state_set) return fail(AERO_ERR_STATE, "no state set");
+  CUDA_TRY(cudaSetDevice(L->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return is_f64(L) ? do_get_state<double>(L, f, prev, g, 0, L->prm.nz, st)
+                    : do_get_state<float>(L, f, prev, g, 0, L->prm.nz, st);
+}
+
+int aero_get_state_slab(AeroLattice *L, int32_t z0, int32_t nzs, double *f, void *stream) {
+  if (!L || !f) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->state_set) return fail(AERO_ERR_STATE, "no state set");
+  if (z0 < 0 || nzs < 1 || z0 + nzs > L->prm.nz) return fail(AERO_ERR_INVALID, "slab outside the grid");
+  CUDA_TRY(cudaSetDevice(L->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return is_f64(L) ? do_get_state<double>(L, f, nullptr, nullptr, z0, nzs, st)
+                    : do_get_state<float>(L, f, nullptr, nullptr, z0, nzs, st);
+}
+
+int aero_params_size(void) { return (int)sizeof(AeroParams); }
+
+int aero_step(AeroLattice *L, int64_t n, void *stream) {
+  if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->state_set) return fail(AERO_ERR_STATE, "aero_set_state must come first");
+  if (n < 0) return fail(AERO_ERR_INVALID, "negative step count");
+  if (L->step_count + n - L->read_upto > L->hist_cap)
+    return fail(AERO_ERR_CAPACITY, "force history holds %d steps; read it before stepping further", L->hist_cap);
+  CUDA_TRY(cudaSetDevice(L->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return is_f64(L) ? do_steps<double>(L, n, st) : do_steps<float>(L, n, st);
+}
+
+int aero_read_forces(AeroLattice *L, double *out, int64_t max_steps, int64_t *n_out, void *stream) {
+  if (!L || !out || !n_out) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
+  CUDA_TRY(cudaSetDevice(L->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t n = std::min(L->step_count - L->read_upto, max_steps);
+  const double *hist = reinterpret_cast<const double *>(L->ws + L->lay.hist);
+  int64_t done = 0;
+  while (done < n) {
+    const int64_t slot = (L->read_upto + done) % L->hist_cap;
+    const int64_t run = std::min(n - done, (int64_t)L->hist_cap - slot);
+    CUDA_TRY(cudaMemcpyAsync(out + done * 12, hist + slot * 12, sizeof(double) * 12 * run, cudaMemcpyDeviceToHost, st));
+    done += run;
+  }
+  CUDA_TRY(cudaStreamSynchronize(st));
+  L->read_upto += n;
+  *n_out = n;
+  return AERO_OK;
+}
+
+int aero_read_profile(AeroLattice *L, double *out, void *stream) {
+  if (!L || !out) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
+  CUDA_TRY(cudaSetDevice(L->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CUDA_TRY(cudaMemcpyAsync(out, L->ws + L->lay.prof_out, 24 * (size_t)L->nprof, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return AERO_OK;
+}
+
+int aero_status(AeroLattice *L, uint32_t *status, void *stream) {
+  if (!L || !status) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
+  CUDA_TRY(cudaSetDevice(L->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t *ctr = reinterpret_cast<const int64_t *>(L->ws + L->lay.counters);
+  CUDA_TRY(cudaMemcpyAsync(status, ctr + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return AERO_OK;
+}
+
+int aero_step_count(const AeroLattice *L, int64_t *steps) {
+  if (!L || !steps) return fail(AERO_ERR_INVALID, "NULL argument");
+  *steps = L->step_count;
+  return AERO_OK;
+}
+
+int aero_destroy(AeroLattice *L) {
+  if (!L) return AERO_OK;
+  for (auto &e : L->pair_exec)
+    if (e) cudaGraphExecDestroy(e);
+  if (L->cap_stream) cudaStreamDestroy(L->cap_stream);
+  delete L;
+  return AERO_OK;
+}
+
+int aero_mrt_operator(int32_t dims, double omega, double *A, double *B) {
+  if ((dims != 2 && dims != 3) || !A || !B) return fail(AERO_ERR_INVALID, "bad argument");
+  MrtCoeffs<double> tmp;
+  if (!build_mrt(dims, omega, tmp, A, B)) return fail(AERO_ERR_INVALID, "MRT operator not block diagonal");
+  return AERO_OK;
+}
+
+}  // extern "C"

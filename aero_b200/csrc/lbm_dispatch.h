@@ -1,0 +1,31 @@
+// lbm_dispatch.h -- per-(lattice, storage, collision) launch tables.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "lbm_params.h"
+
+namespace aero {
+
+template <class Real>
+struct Ops {
+  // grid covers (ceil(nx / kStepBlock), ny, nz)
+  cudaError_t (*step)(const StepParams<Real> &, bool from_state, dim3 grid, cudaStream_t);
+  cudaError_t (*moments)(const StepParams<Real> &, bool from_state, dim3 grid, cudaStream_t);
+  cudaError_t (*forces)(const StepParams<Real> &, int nblocks, cudaStream_t);
+  cudaError_t (*finalize)(const StepParams<Real> &, cudaStream_t);
+  // grid.z = planes written, starting at plane z0; out holds (Q, grid.z, ny, nx)
+  cudaError_t (*state_out)(const StepParams<Real> &, double *out, int step_delta, bool raw, int z0, dim3 grid,
+                           cudaStream_t);
+  cudaError_t (*load_state)(const StepParams<Real> &, const double *in, void *dst, dim3 grid, cudaStream_t);
+  int store_bytes;
+};
+
+const Ops<float> *ops_f32(int dims, int coll);
+const Ops<double> *ops_f64(int dims, int coll);
+const Ops<float> *ops_f16(int dims, int coll);
+const Ops<float> *ops_bf16(int dims, int coll);
+
+bool build_mrt(int dims, double omega, MrtCoeffs<double> &out, double *A_full, double *B_full);
+bool mrt_pinv_basis(int dims, double *M_out, double *Minv_out);
+
+}  // namespace aero

@@ -1,0 +1,72 @@
+// lbm_inst.cuh -- explicit instantiation of the kernels for one storage type.
+// Included by lbm_inst_<storage>.cu with AERO_STORE / AERO_OPS_FN defined.
+#pragma once
+#include "lbm_dispatch.h"
+#include "lbm_kernels.cuh"
+
+namespace aero {
+namespace inst {
+
+template <class L, class S, int COLL>
+struct Launch {
+  using Real = typename StoreOps<S>::Real;
+  static cudaError_t step(const StepParams<Real> &p, bool from_state, dim3 grid, cudaStream_t st) {
+    if (from_state)
+      k_step<L, S, COLL, true><<<grid, kStepBlock, 0, st>>>(p);
+    else
+      k_step<L, S, COLL, false><<<grid, kStepBlock, 0, st>>>(p);
+    return cudaGetLastError();
+  }
+  static cudaError_t moments(const StepParams<Real> &p, bool from_state, dim3 grid, cudaStream_t st) {
+    if (from_state)
+      k_moments<L, S, true><<<grid, kStepBlock, 0, st>>>(p);
+    else
+      k_moments<L, S, false><<<grid, kStepBlock, 0, st>>>(p);
+    return cudaGetLastError();
+  }
+  static cudaError_t forces(const StepParams<Real> &p, int nblocks, cudaStream_t st) {
+    k_forces<L, S><<<nblocks, kForceBlock, 0, st>>>(p);
+    return cudaGetLastError();
+  }
+  static cudaError_t finalize(const StepParams<Real> &p, cudaStream_t st) {
+    k_finalize<Real><<<1, kFinalizeBlock, 0, st>>>(p);
+    return cudaGetLastError();
+  }
+  static cudaError_t state_out(const StepParams<Real> &p, double *out, int delta, bool raw, int z0, dim3 grid,
+                               cudaStream_t st) {
+    const int64_t plane = (int64_t)grid.z * p.ny * p.nx;
+    if (raw)
+      k_state_out<L, S, true><<<grid, kStepBlock, 0, st>>>(p, out, delta, z0, plane);
+    else
+      k_state_out<L, S, false><<<grid, kStepBlock, 0, st>>>(p, out, delta, z0, plane);
+    return cudaGetLastError();
+  }
+  static cudaError_t load_state(const StepParams<Real> &p, const double *in, void *dst, dim3 grid,
+                                cudaStream_t st) {
+    k_load_state<L, S><<<grid, kStepBlock, 0, st>>>(p, in, static_cast<S *>(dst));
+    return cudaGetLastError();
+  }
+  static constexpr Ops<Real> table = {&step, &moments, &forces, &finalize, &state_out, &load_state,
+                                      (int)sizeof(S)};
+};
+
+template <class S>
+const Ops<typename StoreOps<S>::Real> *lookup(int dims, int coll) {
+  if (dims == 2) {
+    switch (coll) {
+      case COLL_BGK: return &Launch<D2Q9, S, COLL_BGK>::table;
+      case COLL_TRT: return &Launch<D2Q9, S, COLL_TRT>::table;
+      case COLL_MRT: return &Launch<D2Q9, S, COLL_MRT>::table;
+    }
+  } else if (dims == 3) {
+    switch (coll) {
+      case COLL_BGK: return &Launch<D3Q19, S, COLL_BGK>::table;
+      case COLL_TRT: return &Launch<D3Q19, S, COLL_TRT>::table;
+      case COLL_MRT: return &Launch<D3Q19, S, COLL_MRT>::table;
+    }
+  }
+  return nullptr;
+}
+
+}  // namespace inst
+}  // namespace aero

@@ -1,0 +1,836 @@
+// lbm_kernels.cuh -- sm_100a kernels of the aero_b200 lattice Boltzmann engine.
+//
+// Stored state.  The population buffers hold POST-COLLISION populations P of
+// the current step, as deviations from the rest weights (lbm_store.cuh), in
+// SoA planes (Q, Nz, Ny, Nx) with a padded plane stride.  One fused pull
+// kernel (k_step) then performs the rest of the reference step and the
+// collision of the next one:
+//
+//   gather P at x - e_i (periodic)                 solver.py:351-353 (push stream)
+//   uniform body force on fluid cells (3D)          solver3d.py:411-423
+//   mid-link / Bouzidi bounce-back at link cells    solver.py:379-383
+//   inlet (x = 0), outlet (x = Nx-1)                solver.py:385-407, solver3d.py:432-461
+//   sponge relaxation                               solver.py:409-413
+//   slip / no-slip / moving walls (y rows)          solver.py:415-424
+//   Boussinesq buoyancy + scalar collide/push       solver.py:427-443
+//   LES omega, then BGK / TRT / MRT collision       solver.py:287-345 (next step)
+//
+// Every step of that chain is cell-local once the gather is done, except the
+// outlet copy (which reads the column x = Nx-2 after bounce-back): an outlet
+// cell simply evaluates the chain for its x = Nx-2 neighbour.  The momentum-
+// exchange forces of the step (forces.py:15-162, forces3d.py:8-171) need the
+// pre-stream P and the post-BC state at link cells; k_forces recomputes the
+// state of each link cell from the same P buffer, so it reads only buffers
+// that k_step does not write and the pair can run in either order.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "lbm_lattice.cuh"
+#include "lbm_params.h"
+#include "lbm_store.cuh"
+
+namespace aero {
+
+constexpr int kStepBlock = 128;
+constexpr int kForceBlock = 128;
+constexpr int kFinalizeBlock = 256;
+
+__device__ __forceinline__ int wrap_n(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+__device__ __forceinline__ int clamp_n(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
+
+template <class Real>
+__device__ __forceinline__ int64_t cell_index(const StepParams<Real> &p, int x, int y, int z) {
+  return ((int64_t)z * p.ny + y) * p.nx + x;
+}
+
+// Link-cell slot of cell (x, y, z), or -1 when the cell has no link.
+template <class Real>
+__device__ __forceinline__ int64_t link_slot(const StepParams<Real> &p, int x, int y, int z) {
+  const int64_t word = ((int64_t)z * p.ny + y) * p.nwx + (x >> 5);
+  const uint32_t bits = __ldg(p.lbits + word);
+  const int lane = x & 31;
+  if (!((bits >> lane) & 1u)) return -1;
+  return (int64_t)__ldg(p.loff + word) + __popc(bits & ((1u << lane) - 1u));
+}
+
+template <class Real> __device__ __forceinline__ Real sqrt_(Real v);
+template <> __device__ __forceinline__ float sqrt_(float v) { return sqrtf(v); }
+template <> __device__ __forceinline__ double sqrt_(double v) { return sqrt(v); }
+
+// --------------------------------------------------------------------------
+// Inlet / outlet / wall formulas in deviation form.  With f_i = w_i + d_i
+// every reference formula keeps its shape because the weights cancel in
+// pairs (w_i = w_opp(i) = w_mirror(i)) and the weighted sums used for the
+// Zou-He densities total exactly 1.
+// --------------------------------------------------------------------------
+
+// Zou-He velocity inlet at x = 0.  2D: boundary.py:15-45; 3D: boundary3d.py:24-68
+// (the 3D solver passes the perturbation as uz_amp, solver3d.py:447-452).
+template <class L, class Real>
+__device__ __forceinline__ void inlet_velocity(const StepParams<Real> &p, Real (&d)[L::Q], int y, int z,
+                                               int64_t step_now) {
+  const Real u0 = p.u0;
+  if constexpr (L::DIMS == 2) {
+    const Real rho_in = (Real(1) + (d[0] + d[2] + d[4]) + Real(2) * (d[3] + d[6] + d[7])) / (Real(1) - u0);
+    d[1] = d[3] + Real(2.0 / 3.0) * rho_in * u0;
+    d[5] = d[7] - Real(0.5) * (d[2] - d[4]) + Real(1.0 / 6.0) * rho_in * u0;
+    d[8] = d[6] + Real(0.5) * (d[2] - d[4]) + Real(1.0 / 6.0) * rho_in * u0;
+    if (p.pert_amp > Real(0)) {
+      const double ph = 2.0 * 3.14159265358979323846 * (double)y / (double)(p.ny > 1 ? p.ny : 1) +
+                        0.17 * (double)(step_now + 1);
+      const Real uy = p.pert_amp * u0 * (Real)sin(ph);
+      d[2] += uy * Real(0.25);
+      d[4] -= uy * Real(0.25);
+      d[5] += uy * Real(0.15);
+      d[8] -= uy * Real(0.15);
+    }
+  } else {
+    const Real Fm = d[2] + d[8] + d[10] + d[12] + d[14];
+    const Real Fn = d[0] + d[3] + d[4] + d[5] + d[6] + d[15] + d[16] + d[17] + d[18];
+    const Real rho_in = (Real(1) + Real(2) * Fm + Fn) / (Real(1) - u0);
+    const Real cy = d[3] - d[4] + d[15] - d[16] + d[17] - d[18];
+    Real cz = d[5] - d[6] + d[15] + d[16] - d[17] - d[18];
+    if (p.pert_amp > Real(0)) {
+      const double ph = 2.0 * 3.14159265358979323846 * (double)z / (double)(p.nz > 1 ? p.nz : 1) +
+                        0.17 * (double)(step_now + 1);
+      cz = cz + rho_in * (p.pert_amp * u0 * (Real)sin(ph));
+    }
+    const Real r6 = Real(1.0 / 6.0) * rho_in * u0;
+    d[1] = d[2] + Real(1.0 / 3.0) * rho_in * u0;
+    d[7] = d[10] + r6 - Real(0.5) * cy;
+    d[9] = d[8] + r6 + Real(0.5) * cy;
+    d[11] = d[14] + r6 - Real(0.5) * cz;
+    d[13] = d[12] + r6 + Real(0.5) * cz;
+  }
+}
+
+// Zou-He pressure inlet (2D): boundary.py:116-136
+template <class Real>
+__device__ __forceinline__ void inlet_pressure_2d(const StepParams<Real> &p, Real (&d)[9]) {
+  const Real rin = p.rho_in;
+  const Real ux = Real(1) - (Real(1) + (d[0] + d[2] + d[4]) + Real(2) * (d[3] + d[6] + d[7])) / rin;
+  d[1] = d[3] + Real(2.0 / 3.0) * rin * ux;
+  d[5] = d[7] - Real(0.5) * (d[2] - d[4]) + Real(1.0 / 6.0) * rin * ux;
+  d[8] = d[6] + Real(0.5) * (d[2] - d[4]) + Real(1.0 / 6.0) * rin * ux;
+}
+
+// Zou-He pressure outlet (2D): boundary.py:139-159
+template <class Real>
+__device__ __forceinline__ void outlet_pressure_2d(const StepParams<Real> &p, Real (&d)[9]) {
+  const Real ro = p.rho_out;
+  const Real ux = Real(-1) + (Real(1) + (d[0] + d[2] + d[4]) + Real(2) * (d[1] + d[5] + d[8])) / ro;
+  d[3] = d[1] - Real(2.0 / 3.0) * ro * ux;
+  d[7] = d[5] + Real(0.5) * (d[2] - d[4]) - Real(1.0 / 6.0) * ro * ux;
+  d[6] = d[8] - Real(0.5) * (d[2] - d[4]) - Real(1.0 / 6.0) * ro * ux;
+}
+
+template <class L, class Real>
+__device__ __forceinline__ Real sum_dev(const Real (&d)[L::Q]) {
+  Real s = Real(0);
+  static_for<L::Q>([&](auto ic) { s += d[decltype(ic)::value]; });
+  return s;
+}
+
+// Walls on the y = 0 / y = Ny-1 rows.  2D: boundary.py:162-226;
+// 3D: boundary3d.py:205-271.
+template <class L, class Real>
+__device__ __forceinline__ void walls(const StepParams<Real> &p, Real (&d)[L::Q], bool bottom) {
+  const Real k6 = Real(6.0 * (1.0 / 36.0));
+  if constexpr (L::DIMS == 2) {
+    if (p.wall == WALL_SLIP) {
+      if (bottom) { d[2] = d[4]; d[5] = d[8]; d[6] = d[7]; }
+      else        { d[4] = d[2]; d[8] = d[5]; d[7] = d[6]; }
+    } else if (p.wall == WALL_NOSLIP) {
+      if (bottom) { d[2] = d[4]; d[5] = d[7]; d[6] = d[8]; }
+      else        { d[4] = d[2]; d[7] = d[5]; d[8] = d[6]; }
+    } else {
+      Real r = Real(1) + sum_dev<L>(d);
+      r = r > Real(1e-12) ? r : Real(1e-12);
+      if (bottom) {
+        const Real m = k6 * r * p.wall_u_bottom;
+        d[2] = d[4]; d[5] = d[7] + m; d[6] = d[8] - m;
+      } else {
+        const Real m = k6 * r * p.wall_u_top;
+        d[4] = d[2]; d[7] = d[5] - m; d[8] = d[6] + m;
+      }
+    }
+  } else {
+    if (p.wall == WALL_SLIP) {
+      if (bottom) { d[3] = d[4]; d[7] = d[9]; d[8] = d[10]; d[15] = d[16]; d[17] = d[18]; }
+      else        { d[4] = d[3]; d[9] = d[7]; d[10] = d[8]; d[16] = d[15]; d[18] = d[17]; }
+    } else if (p.wall == WALL_NOSLIP) {
+      if (bottom) { d[3] = d[4]; d[7] = d[10]; d[8] = d[9]; d[15] = d[18]; d[17] = d[16]; }
+      else        { d[4] = d[3]; d[10] = d[7]; d[9] = d[8]; d[18] = d[15]; d[16] = d[17]; }
+    } else {
+      Real r = Real(1) + sum_dev<L>(d);
+      r = r > Real(1e-12) ? r : Real(1e-12);
+      if (bottom) {
+        const Real m = k6 * r * p.wall_u_bottom;
+        d[3] = d[4]; d[7] = d[10] + m; d[8] = d[9] - m; d[15] = d[18]; d[17] = d[16];
+      } else {
+        const Real m = k6 * r * p.wall_u_top;
+        d[4] = d[3]; d[10] = d[7] - m; d[9] = d[8] + m; d[18] = d[15]; d[16] = d[17];
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// State of one cell after stream and every boundary condition of the
+// reference step, evaluated from the post-collision buffer P.
+// --------------------------------------------------------------------------
+
+// gather + body force + obstacle bounce-back + inlet (everything the
+// reference applies before the outlet copy reads column Nx-2).
+template <class L, class S, class Real>
+__device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, int y, int z, int64_t step_now,
+                                              Real (&d)[L::Q]) {
+  using SO = StoreOps<S>;
+  const S *P = static_cast<const S *>(p.P);
+  const int64_t cs = p.cs;
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    const int xs = wrap_n(x - Dir<L, i>::x, p.nx);
+    const int ys = wrap_n(y - Dir<L, i>::y, p.ny);
+    const int zs = L::DIMS == 3 ? wrap_n(z - Dir<L, i>::z, p.nz) : 0;
+    d[i] = SO::template load<i, L>(P, i * cs + cell_index(p, xs, ys, zs));
+  });
+  const int64_t c = cell_index(p, x, y, z);
+  if constexpr (L::DIMS == 3) {
+    // Guo-style uniform body force on fluid cells (ibm_guo.py:263-301)
+    if ((p.feat & FEAT_BODY_FORCE) && !p.solid[c]) {
+      Real drho = 0, jx = 0, jy = 0, jz = 0;
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        drho += d[i];
+        if (Dir<L, i>::x) jx += Dir<L, i>::x * d[i];
+        if (Dir<L, i>::y) jy += Dir<L, i>::y * d[i];
+        if (Dir<L, i>::z) jz += Dir<L, i>::z * d[i];
+      });
+      const Real rho = Real(1) + drho;
+      if (rho > Real(0)) {
+        const Real ux = jx / rho, uy = jy / rho, uz = jz / rho;
+        const Real uf = ux * p.bf_x + uy * p.bf_y + uz * p.bf_z;
+        static_for<L::Q>([&](auto ic) {
+          constexpr int i = decltype(ic)::value;
+          const Real eu = Dir<L, i>::x * ux + Dir<L, i>::y * uy + Dir<L, i>::z * uz;
+          const Real ef = Dir<L, i>::x * p.bf_x + Dir<L, i>::y * p.bf_y + Dir<L, i>::z * p.bf_z;
+          const Real term = (ef - uf) * Real(3) + (eu * ef) * Real(9);
+          d[i] += p.bf_coeff * Real(Dir<L, i>::w) * rho * term;
+        });
+      }
+    }
+  }
+  // obstacle bounce-back (boundary.py:283-352, boundary3d.py:333-393)
+  if (p.feat & FEAT_OBSTACLE_BB) {
+    const int64_t slot = link_slot(p, x, y, z);
+    if (slot >= 0) {
+      const uint32_t mask = __ldg(p.lc_mask + slot);
+      const bool bouzidi = p.feat & FEAT_BOUZIDI;
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        if constexpr (i > 0) {
+          if ((mask >> i) & 1u) {
+            constexpr int o = L::opp[i];
+            const Real fi = SO::template load<i, L>(P, i * cs + c);
+            if (!bouzidi) {
+              d[o] = fi;
+            } else {
+              const Real q = (Real)__ldg(p.lc_q + slot * L::Q + i);
+              if (q < Real(0.5)) {
+                const Real fo = SO::template load<o, L>(P, o * cs + c);
+                d[o] = Real(2) * q * fi + (Real(1) - Real(2) * q) * fo;
+              } else {
+                const int xn = clamp_n(x + Dir<L, o>::x, p.nx);
+                const int yn = clamp_n(y + Dir<L, o>::y, p.ny);
+                const int zn = L::DIMS == 3 ? clamp_n(z + Dir<L, o>::z, p.nz) : 0;
+                const Real fn = SO::template load<i, L>(P, i * cs + cell_index(p, xn, yn, zn));
+                const Real inv2q = Real(1) / (Real(2) * q);
+                d[o] = inv2q * fi + (Real(1) - inv2q) * fn;
+              }
+            }
+          }
+        }
+      });
+    }
+  }
+  if ((p.feat & FEAT_OPEN) && x == 0) {
+    if (p.inlet == INLET_VELOCITY) {
+      inlet_velocity<L>(p, d, y, z, step_now);
+    } else if constexpr (L::DIMS == 2) {
+      if (p.inlet == INLET_PRESSURE) inlet_pressure_2d(p, d);
+    }
+  }
+}
+
+// Thermal outputs of the state evaluation.
+template <class Real>
+struct ScalarCtx {
+  Real T;       // sum of the current scalar populations at the cell
+  Real u[3];    // flow velocity before buoyancy (drives the scalar collision)
+};
+
+// Full post-BC state.  When prev_out is non-null the convective outlet writes
+// its advanced state there (only k_step does).
+template <class L, class S, class Real>
+__device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int y, int z, int64_t step_now,
+                                           Real (&d)[L::Q], Real *prev_out, ScalarCtx<Real> *sc) {
+  const bool open = p.feat & FEAT_OPEN;
+  const bool copy_out =
+      open && x == p.nx - 1 && (p.outlet == OUTLET_CONVECTIVE || p.outlet == OUTLET_ZEROGRAD);
+  partial_state<L, S, Real>(p, copy_out ? p.nx - 2 : x, y, z, step_now, d);
+  if (copy_out) {
+    if (p.outlet == OUTLET_CONVECTIVE) {
+      // boundary.py:78-113, boundary3d.py:149-164
+      Real u = p.u0 < Real(0) ? Real(0) : (p.u0 > Real(1) ? Real(1) : p.u0);
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        const int64_t pi = ((int64_t)i * p.nz + z) * p.ny + y;
+        d[i] = (Real(1) - u) * p.prev[pi] + u * d[i];
+        if (prev_out) prev_out[pi] = d[i];
+      });
+    }
+  } else if constexpr (L::DIMS == 2) {
+    if (open && x == p.nx - 1 && p.outlet == OUTLET_PRESSURE) outlet_pressure_2d(p, d);
+  }
+  // sponge (sponge.py:8-70)
+  if ((p.feat & FEAT_SPONGE) && x >= p.sponge_start) {
+    const double frac = (double)(x - p.sponge_start + 1) / (double)(p.sponge_thickness > 1 ? p.sponge_thickness : 1);
+    const Real sg = (Real)((double)p.sponge_sigma_max * frac * frac);
+    if (sg > Real(0)) {
+      const Real drho = sum_dev<L>(d);
+      const Real rho = Real(1) + drho;
+      const Real u0 = p.u0, usq = u0 * u0;
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        const Real eu = Dir<L, i>::x * u0;
+        const Real deq = Real(Dir<L, i>::w) * (drho + rho * (Real(3) * eu + Real(4.5) * eu * eu - Real(1.5) * usq));
+        d[i] = (Real(1) - sg) * d[i] + sg * deq;
+      });
+    }
+  }
+  if (p.wall != WALL_NONE) {
+    if (y == 0) walls<L>(p, d, true);
+    if (y == p.ny - 1) walls<L>(p, d, false);
+  }
+  if (p.feat & FEAT_THERMAL) {
+    // thermal.py:103-124 / :206-222 with the order of solver.py:432-439
+    const int64_t c = cell_index(p, x, y, z);
+    Real T = 0;
+    if (p.feat & FEAT_SCALAR_REDUCED) {
+      using G = typename ScalarReduced<L>::Lat;
+      static_for<G::Q>([&](auto ic) { T += p.g[decltype(ic)::value * p.cs + c]; });
+    } else {
+      static_for<L::Q>([&](auto ic) { T += p.g[decltype(ic)::value * p.cs + c]; });
+    }
+    Real drho = 0, jx = 0, jy = 0, jz = 0;
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      drho += d[i];
+      if (Dir<L, i>::x) jx += Dir<L, i>::x * d[i];
+      if (Dir<L, i>::y) jy += Dir<L, i>::y * d[i];
+      if (Dir<L, i>::z) jz += Dir<L, i>::z * d[i];
+    });
+    const Real rho = Real(1) + drho;
+    if (sc) {
+      const Real inv = rho > Real(0) ? Real(1) / rho : Real(0);
+      sc->T = T;
+      sc->u[0] = jx * inv;
+      sc->u[1] = jy * inv;
+      sc->u[2] = jz * inv;
+    }
+    if (p.feat & FEAT_BUOYANCY) {
+      const Real buoy = p.gbeta * (T - p.T_ref);
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        if constexpr (Dir<L, i>::y != 0) d[i] += Real(Dir<L, i>::w) * Real(3) * rho * buoy * Real(Dir<L, i>::y);
+      });
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// LES relaxation rate from the velocity side buffer (les.py:24-78,
+// :177-266, :273-344).  Edge planes and solid cells keep the base rate.
+// --------------------------------------------------------------------------
+template <class L, class Real>
+__device__ __forceinline__ Real les_omega(const StepParams<Real> &p, int x, int y, int z, int64_t c, bool solid) {
+  Real nu_t = Real(0);
+  bool interior = x >= 1 && x <= p.nx - 2 && y >= 1 && y <= p.ny - 2;
+  if constexpr (L::DIMS == 3) interior = interior && z >= 1 && z <= p.nz - 2;
+  if (interior && !solid) {
+    const Real *UX = p.U, *UY = p.U + p.cs, *UZ = p.U + 2 * p.cs;
+    const int64_t sx = 1, sy = p.nx;
+    Real g[3][3];
+    g[0][0] = Real(0.5) * (UX[c + sx] - UX[c - sx]);
+    g[0][1] = Real(0.5) * (UX[c + sy] - UX[c - sy]);
+    g[1][0] = Real(0.5) * (UY[c + sx] - UY[c - sx]);
+    g[1][1] = Real(0.5) * (UY[c + sy] - UY[c - sy]);
+    g[0][2] = g[1][2] = g[2][0] = g[2][1] = g[2][2] = Real(0);
+    if constexpr (L::DIMS == 3) {
+      const int64_t sz = (int64_t)p.nx * p.ny;
+      g[0][2] = Real(0.5) * (UX[c + sz] - UX[c - sz]);
+      g[1][2] = Real(0.5) * (UY[c + sz] - UY[c - sz]);
+      g[2][0] = Real(0.5) * (UZ[c + sx] - UZ[c - sx]);
+      g[2][1] = Real(0.5) * (UZ[c + sy] - UZ[c - sy]);
+      g[2][2] = Real(0.5) * (UZ[c + sz] - UZ[c - sz]);
+    }
+    Real cs2 = p.les_cs2;
+    if (p.feat & FEAT_LES_CS_FIELD) {
+      const Real cc = p.cs_cell[c];
+      cs2 = cc * cc;
+    }
+    constexpr int D = L::DIMS;
+    if (p.feat & FEAT_LES_WALE) {
+      Real s_sq = 0, sd_sq = 0, gsq[3][3], tr = 0;
+#pragma unroll
+      for (int a = 0; a < D; a++)
+#pragma unroll
+        for (int b = 0; b < D; b++) {
+          const Real sab = Real(0.5) * (g[a][b] + g[b][a]);
+          s_sq += sab * sab;
+          Real acc = 0;
+#pragma unroll
+          for (int k = 0; k < D; k++) acc += g[a][k] * g[k][b];
+          gsq[a][b] = acc;
+        }
+#pragma unroll
+      for (int a = 0; a < D; a++) tr += gsq[a][a];
+      tr = tr / Real(D);
+#pragma unroll
+      for (int a = 0; a < D; a++)
+#pragma unroll
+        for (int b = 0; b < D; b++) {
+          const Real sd = Real(0.5) * (gsq[a][b] + gsq[b][a]) - (a == b ? tr : Real(0));
+          sd_sq += sd * sd;
+        }
+      // pow(sd, 1.5) / (pow(s, 2.5) + pow(sd, 1.25) + 1e-30) via square roots
+      const Real r_sd = sqrt_(sd_sq), r_s = sqrt_(s_sq);
+      const Real num = sd_sq * r_sd;
+      const Real den = s_sq * s_sq * r_s + sd_sq * sqrt_(r_sd) + Real(1e-30);
+      nu_t = cs2 * num / den;
+    } else {
+      const Real s11 = g[0][0], s22 = g[1][1], s33 = g[2][2];
+      const Real s12 = Real(0.5) * (g[0][1] + g[1][0]);
+      const Real s13 = Real(0.5) * (g[0][2] + g[2][0]);
+      const Real s23 = Real(0.5) * (g[1][2] + g[2][1]);
+      Real smag;
+      if constexpr (D == 2)
+        smag = sqrt_(Real(2) * (s11 * s11 + s22 * s22 + Real(2) * s12 * s12));
+      else
+        smag = sqrt_(Real(2) * (s11 * s11 + s22 * s22 + s33 * s33) +
+                      Real(4) * (s12 * s12 + s13 * s13 + s23 * s23));
+      nu_t = cs2 * smag;
+    }
+  }
+  return Real(1) / (Real(3) * (p.base_nu + nu_t) + Real(0.5));
+}
+
+// --------------------------------------------------------------------------
+// Collision (deviation form).  BGK: kernels.py:42-92; TRT: kernels_trt.py:
+// 125-174 with trt2d.py:8-18; MRT: kernels_mrt.py:190-241,
+// kernels3d_mrt.py:24-82.  Solid cells relax toward feq(rho, 0).
+// --------------------------------------------------------------------------
+template <class L, class Real, int COLL>
+__device__ __forceinline__ void collide(const StepParams<Real> &p, Real (&d)[L::Q], bool solid, Real om,
+                                        bool per_cell_omega) {
+  Real drho = 0, jx = 0, jy = 0, jz = 0;
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    drho += d[i];
+    if (Dir<L, i>::x) jx += Dir<L, i>::x * d[i];
+    if (Dir<L, i>::y) jy += Dir<L, i>::y * d[i];
+    if (Dir<L, i>::z) jz += Dir<L, i>::z * d[i];
+  });
+  const Real rho = Real(1) + drho;
+  const Real inv = rho > Real(0) ? Real(1) / rho : Real(0);
+  Real ux = jx * inv, uy = jy * inv, uz = jz * inv;
+  if (solid) ux = uy = uz = Real(0);
+  if constexpr (COLL == COLL_MRT) {
+    constexpr int NE = L::NP + 1, NO = L::NP, KE = L::DIMS == 2 ? 4 : 7, KO = L::DIMS;
+    Real s[NE], t[NO], me[KE], mo[KO];
+    s[0] = d[0];
+    static_for<NO>([&](auto pc) {
+      constexpr int k = decltype(pc)::value;
+      constexpr int i = L::pair[k], o = L::opp[L::pair[k]];
+      s[k + 1] = d[i] + d[o];
+      t[k] = d[i] - d[o];
+    });
+    const Real rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
+    me[0] = drho;
+    me[1] = rux * ux;
+    me[2] = ruy * uy;
+    if constexpr (L::DIMS == 2) {
+      me[3] = rux * uy;
+      mo[0] = rux;
+      mo[1] = ruy;
+    } else {
+      me[3] = ruz * uz;
+      me[4] = rux * uy;
+      me[5] = rux * uz;
+      me[6] = ruy * uz;
+      mo[0] = rux;
+      mo[1] = ruy;
+      mo[2] = ruz;
+    }
+    Real sp[NE], tp[NO];
+#pragma unroll
+    for (int r = 0; r < NE; r++) {
+      Real acc = 0;
+#pragma unroll
+      for (int k = 0; k < KE; k++) acc += p.mrt.Ce[r * 7 + k] * me[k];
+#pragma unroll
+      for (int k = 0; k < NE; k++) acc += p.mrt.Ae[r * 10 + k] * s[k];
+      sp[r] = acc;
+    }
+#pragma unroll
+    for (int r = 0; r < NO; r++) {
+      Real acc = 0;
+#pragma unroll
+      for (int k = 0; k < KO; k++) acc += p.mrt.Co[r * 3 + k] * mo[k];
+#pragma unroll
+      for (int k = 0; k < NO; k++) acc += p.mrt.Ao[r * 9 + k] * t[k];
+      tp[r] = acc;
+    }
+    d[0] = sp[0];
+    static_for<NO>([&](auto pc) {
+      constexpr int k = decltype(pc)::value;
+      constexpr int i = L::pair[k], o = L::opp[L::pair[k]];
+      d[i] = Real(0.5) * (sp[k + 1] + tp[k]);
+      d[o] = Real(0.5) * (sp[k + 1] - tp[k]);
+    });
+    (void)om;
+    (void)per_cell_omega;
+  } else {
+    const Real usq = ux * ux + uy * uy + uz * uz;
+    Real deq[L::Q];
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      const Real eu = Dir<L, i>::x * ux + Dir<L, i>::y * uy + Dir<L, i>::z * uz;
+      deq[i] = Real(Dir<L, i>::w) * (drho + rho * (Real(3) * eu + Real(4.5) * eu * eu - Real(1.5) * usq));
+    });
+    if constexpr (COLL == COLL_TRT) {
+      Real sm = p.trt_sminus;
+      if (per_cell_omega) {
+        const Real tau = Real(1) / om, lam = p.trt_lambda;
+        const Real tp = lam * tau + (Real(1) - lam);
+        const Real tm = (tp * tau - Real(0.5)) / (tp - Real(0.5));
+        sm = Real(1) / tm;
+      }
+      Real out[L::Q];
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        constexpr int j = L::opp[i];
+        const Real fpl = Real(0.5) * (d[i] + d[j]), fmi = Real(0.5) * (d[i] - d[j]);
+        const Real epl = Real(0.5) * (deq[i] + deq[j]), emi = Real(0.5) * (deq[i] - deq[j]);
+        out[i] = deq[i] + (Real(1) - om) * (fpl - epl) + (Real(1) - sm) * (fmi - emi);
+      });
+      static_for<L::Q>([&](auto ic) { d[decltype(ic)::value] = out[decltype(ic)::value]; });
+    } else {
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        d[i] = (Real(1) - om) * d[i] + om * deq[i];
+      });
+    }
+  }
+}
+
+// Scalar lattice collision + push (thermal.py:47-100, :149-203).  Rows y = 0
+// and y = Ny-1 are Dirichlet rows: every population there is overwritten by
+// w_i T_wall, so pushes into them are skipped and the row's own thread writes
+// them.
+template <class L, class G, class Real>
+__device__ __forceinline__ void scalar_step(const StepParams<Real> &p, int x, int y, int z, int64_t c, bool solid,
+                                            const ScalarCtx<Real> &sc, Real cs2inv) {
+  const Real oT = p.omega_T, T = sc.T;
+  static_for<G::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    const Real gi = p.g[i * p.cs + c];
+    Real gp;
+    if (solid) {
+      gp = Real(Dir<G, i>::w) * T;
+    } else {
+      const Real eu = Dir<G, i>::x * sc.u[0] + Dir<G, i>::y * sc.u[1] + Dir<G, i>::z * sc.u[2];
+      const Real geq = Real(Dir<G, i>::w) * T * (Real(1) + cs2inv * eu);
+      gp = gi - oT * (gi - geq);
+    }
+    const int xd = wrap_n(x + Dir<G, i>::x, p.nx);
+    const int yd = wrap_n(y + Dir<G, i>::y, p.ny);
+    const int zd = L::DIMS == 3 ? wrap_n(z + Dir<G, i>::z, p.nz) : 0;
+    if (yd != 0 && yd != p.ny - 1) p.gn[i * p.cs + cell_index(p, xd, yd, zd)] = gp;
+  });
+  if (y == 0 || y == p.ny - 1) {
+    const Real Tw = y == 0 ? p.T_hot : p.T_cold;
+    static_for<G::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      p.gn[i * p.cs + c] = Real(Dir<G, i>::w) * Tw;
+    });
+  }
+}
+
+// --------------------------------------------------------------------------
+// Kernels
+// --------------------------------------------------------------------------
+
+// One full step: state of step n from P_n, scalar step, collision -> P_{n+1}.
+// FROM_STATE: P holds a state (deviations) to be collided as is (used after
+// the host sets f, and to start from an initial state).
+template <class L, class S, int COLL, bool FROM_STATE>
+__global__ void __launch_bounds__(kStepBlock) k_step(const StepParams<typename StoreOps<S>::Real> p) {
+  using Real = typename StoreOps<S>::Real;
+  using SO = StoreOps<S>;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y, z = blockIdx.z;
+  if (x >= p.nx) return;
+  const int64_t c = cell_index(p, x, y, z);
+  const bool solid = p.solid[c];
+  Real d[L::Q];
+  ScalarCtx<Real> sc;
+  if constexpr (FROM_STATE) {
+    const S *P = static_cast<const S *>(p.P);
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      d[i] = SO::template load<i, L>(P, i * p.cs + c);
+    });
+  } else {
+    const int64_t step_now = *p.step;
+    full_state<L, S, Real>(p, x, y, z, step_now, d, p.prevn, &sc);
+    // divergence guard (diagnostics.py:32-71): non-finite or non-positive rho
+    const Real rho = Real(1) + sum_dev<L>(d);
+    const bool bad = !(rho > Real(0)) || !isfinite(rho);
+    const unsigned badm = __ballot_sync(__activemask(), bad);
+    if (bad && (threadIdx.x & 31) == __ffs(badm) - 1) atomicOr(p.status, STATUS_NONFINITE_OR_NONPOSITIVE_RHO);
+    if (p.feat & FEAT_THERMAL) {
+      if (p.feat & FEAT_SCALAR_REDUCED) {
+        using G = typename ScalarReduced<L>::Lat;
+        scalar_step<L, G>(p, x, y, z, c, solid, sc, Real(G::cs2inv));
+      } else {
+        scalar_step<L, L>(p, x, y, z, c, solid, sc, Real(3));
+      }
+    }
+  }
+  Real om = p.omega;
+  const bool les = (COLL != COLL_MRT) && (p.feat & FEAT_LES);
+  if (les) om = les_omega<L>(p, x, y, z, c, solid);
+  collide<L, Real, COLL>(p, d, solid, om, les);
+  S *Pn = static_cast<S *>(p.Pn);
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    SO::template store<i, L>(Pn, i * p.cs + c, d[i]);
+  });
+}
+
+// LES side pass: velocity of the current state (les.py:288 / :325 use
+// compute_macroscopic of the pre-collision state, solids not zeroed).
+template <class L, class S, bool FROM_STATE>
+__global__ void __launch_bounds__(kStepBlock) k_moments(const StepParams<typename StoreOps<S>::Real> p) {
+  using Real = typename StoreOps<S>::Real;
+  using SO = StoreOps<S>;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y, z = blockIdx.z;
+  if (x >= p.nx) return;
+  const int64_t c = cell_index(p, x, y, z);
+  Real d[L::Q];
+  if constexpr (FROM_STATE) {
+    const S *P = static_cast<const S *>(p.P);
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      d[i] = SO::template load<i, L>(P, i * p.cs + c);
+    });
+  } else {
+    full_state<L, S, Real>(p, x, y, z, *p.step, d, nullptr, nullptr);
+  }
+  Real drho = 0, jx = 0, jy = 0, jz = 0;
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    drho += d[i];
+    if (Dir<L, i>::x) jx += Dir<L, i>::x * d[i];
+    if (Dir<L, i>::y) jy += Dir<L, i>::y * d[i];
+    if (Dir<L, i>::z) jz += Dir<L, i>::z * d[i];
+  });
+  const Real rho = Real(1) + drho;
+  const Real inv = rho > Real(0) ? Real(1) / rho : Real(0);
+  p.Uw[c] = jx * inv;
+  p.Uw[p.cs + c] = jy * inv;
+  p.Uw[2 * p.cs + c] = jz * inv;
+}
+
+// Deterministic block reduction of N doubles (fixed shuffle/smem order).
+template <int N, int BLOCK>
+__device__ __forceinline__ void block_reduce_store(double (&v)[N], double *out) {
+  __shared__ double sm[BLOCK / 32][N];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    double a = v[j];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
+    if (lane == 0) sm[wid][j] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x < N) {
+    double a = 0.0;
+#pragma unroll
+    for (int w = 0; w < BLOCK / 32; w++) a += sm[w][threadIdx.x];
+    out[threadIdx.x] = a;
+  }
+}
+
+// Momentum-exchange forces, pressure/viscous split, moments and the
+// per-y (2D) / per-z (3D) profile, one thread per link cell, FP64 sums.
+template <class L, class S>
+__global__ void __launch_bounds__(kForceBlock) k_forces(const StepParams<typename StoreOps<S>::Real> p) {
+  using Real = typename StoreOps<S>::Real;
+  using SO = StoreOps<S>;
+  const int64_t k = (int64_t)blockIdx.x * kForceBlock + threadIdx.x;
+  double acc[12];
+#pragma unroll
+  for (int j = 0; j < 12; j++) acc[j] = 0.0;
+  if (k < p.n_lc) {
+    const int64_t c = p.lc_cell[k];
+    const int x = (int)(c % p.nx);
+    const int y = (int)((c / p.nx) % p.ny);
+    const int z = (int)(c / ((int64_t)p.nx * p.ny));
+    Real d[L::Q];
+    full_state<L, S, Real>(p, x, y, z, *p.step, d, nullptr, nullptr);
+    const S *P = static_cast<const S *>(p.P);
+    double fp[L::Q];
+    double drho = 0, jx = 0, jy = 0, jz = 0;
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      fp[i] = (double)SO::template load<i, L>(P, i * p.cs + c);
+      drho += fp[i];
+      jx += Dir<L, i>::x * fp[i];
+      jy += Dir<L, i>::y * fp[i];
+      jz += Dir<L, i>::z * fp[i];
+    });
+    const double rho = 1.0 + drho;
+    const double inv = rho > 0.0 ? 1.0 / rho : 0.0;
+    const double ux = jx * inv, uy = jy * inv, uz = jz * inv, usq = ux * ux + uy * uy + uz * uz;
+    const uint32_t mask = p.lc_mask[k];
+    const double rx = x - p.center[0], ry = y - p.center[1], rz = z - p.center[2];
+    double prof[3] = {0.0, 0.0, 0.0};
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      if constexpr (i > 0) {
+        if ((mask >> i) & 1u) {
+          constexpr int o = L::opp[i];
+          const double eui = Dir<L, i>::x * ux + Dir<L, i>::y * uy + Dir<L, i>::z * uz;
+          const double deq_i = Dir<L, i>::w * (drho + rho * (3.0 * eui + 4.5 * eui * eui - 1.5 * usq));
+          const double deq_o = Dir<L, o>::w * (drho + rho * (-3.0 * eui + 4.5 * eui * eui - 1.5 * usq));
+          const double din = (double)d[o];
+          const double mom = (Dir<L, i>::w + Dir<L, o>::w) + (fp[i] + din);
+          const double mp = (Dir<L, i>::w + Dir<L, o>::w) + (deq_i + deq_o);
+          const double mv = (fp[i] - deq_i) + (din - deq_o);
+          const double df[3] = {Dir<L, i>::x * mom, Dir<L, i>::y * mom, Dir<L, i>::z * mom};
+          acc[0] += df[0];
+          acc[1] += df[1];
+          acc[2] += df[2];
+          acc[3] += Dir<L, i>::x * mp;
+          acc[4] += Dir<L, i>::y * mp;
+          acc[5] += Dir<L, i>::z * mp;
+          acc[6] += Dir<L, i>::x * mv;
+          acc[7] += Dir<L, i>::y * mv;
+          acc[8] += Dir<L, i>::z * mv;
+          acc[9] += ry * df[2] - rz * df[1];
+          acc[10] += rz * df[0] - rx * df[2];
+          acc[11] += rx * df[1] - ry * df[0];
+          prof[0] += df[0];
+          prof[1] += df[1];
+          prof[2] += df[2];
+        }
+      }
+    });
+    p.lc_prof[k * 3 + 0] = prof[0];
+    p.lc_prof[k * 3 + 1] = prof[1];
+    p.lc_prof[k * 3 + 2] = prof[2];
+  }
+  block_reduce_store<12, kForceBlock>(acc, p.partials + (int64_t)blockIdx.x * 12);
+}
+
+// Sums the per-block partials in a fixed order into the device history ring,
+// optionally sums the profile segments, then advances the step counter.
+template <class Real>
+__global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const StepParams<Real> p) {
+  __shared__ double sm[kFinalizeBlock];
+  const int t = threadIdx.x;
+  const int64_t step = *p.step;
+  const int64_t slot = (step - *p.hist_base) % p.hist_cap;
+  for (int j = 0; j < 12; j++) {
+    double a = 0.0;
+    for (int b = t; b < p.n_force_blocks; b += kFinalizeBlock) a += p.partials[(int64_t)b * 12 + j];
+    sm[t] = a;
+    __syncthreads();
+    for (int s = kFinalizeBlock / 2; s > 0; s >>= 1) {
+      if (t < s) sm[t] += sm[t + s];
+      __syncthreads();
+    }
+    if (t == 0) p.hist[slot * 12 + j] = sm[0];
+    __syncthreads();
+  }
+  if (p.want_profile) {
+    for (int b = t; b < p.nprof; b += kFinalizeBlock) {
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+      for (int k = p.prof_off[b]; k < p.prof_off[b + 1]; k++) {
+        a0 += p.lc_prof[(int64_t)k * 3 + 0];
+        a1 += p.lc_prof[(int64_t)k * 3 + 1];
+        a2 += p.lc_prof[(int64_t)k * 3 + 2];
+      }
+      p.prof_out[b * 3 + 0] = a0;
+      p.prof_out[b * 3 + 1] = a1;
+      p.prof_out[b * 3 + 2] = a2;
+    }
+  }
+  __syncthreads();
+  if (t == 0) *p.step = step + 1;
+}
+
+// State of the step that produced P (f as the reference stores it), written
+// as absolute FP64 populations (Q, planes, ny, nx) for the planes z0 ..
+// z0 + gridDim.z - 1.  step_delta selects the step index the inlet
+// perturbation phase uses.  RAW: P already holds a state.
+template <class L, class S, bool RAW>
+__global__ void __launch_bounds__(kStepBlock) k_state_out(const StepParams<typename StoreOps<S>::Real> p,
+                                                          double *out, int step_delta, int z0, int64_t plane) {
+  using Real = typename StoreOps<S>::Real;
+  using SO = StoreOps<S>;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y, z = blockIdx.z + z0;
+  if (x >= p.nx) return;
+  const int64_t c = cell_index(p, x, y, z);
+  Real d[L::Q];
+  if constexpr (RAW) {
+    const S *P = static_cast<const S *>(p.P);
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      d[i] = SO::template load<i, L>(P, i * p.cs + c);
+    });
+  } else {
+    full_state<L, S, Real>(p, x, y, z, *p.step + step_delta, d, nullptr, nullptr);
+  }
+  const int64_t oc = c - (int64_t)z0 * p.ny * p.nx;
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    out[(int64_t)i * plane + oc] = Dir<L, i>::w + (double)d[i];
+  });
+}
+
+// Converts absolute FP64 populations (Q, ncells) into the storage format.
+template <class L, class S>
+__global__ void __launch_bounds__(kStepBlock) k_load_state(const StepParams<typename StoreOps<S>::Real> p,
+                                                           const double *in, S *dst) {
+  using Real = typename StoreOps<S>::Real;
+  using SO = StoreOps<S>;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y, z = blockIdx.z;
+  if (x >= p.nx) return;
+  const int64_t c = cell_index(p, x, y, z);
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    SO::template store<i, L>(dst, i * p.cs + c, (Real)(in[(int64_t)i * p.ncells + c] - Dir<L, i>::w));
+  });
+}
+
+}  // namespace aero

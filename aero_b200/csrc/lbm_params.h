@@ -1,0 +1,101 @@
+// lbm_params.h -- launch parameters shared by the host runtime and the
+// sm_100a kernels of the aero_b200 lattice Boltzmann engine.
+#pragma once
+#include <stdint.h>
+
+namespace aero {
+
+enum Collision : int32_t { COLL_BGK = 0, COLL_TRT = 1, COLL_MRT = 2 };
+enum StoreKind : int32_t { STORE_F32 = 0, STORE_F64 = 1, STORE_F16 = 2, STORE_BF16 = 3 };
+enum Inlet : int32_t { INLET_NONE = 0, INLET_VELOCITY = 1, INLET_PRESSURE = 2 };
+enum Outlet : int32_t { OUTLET_NONE = 0, OUTLET_CONVECTIVE = 1, OUTLET_ZEROGRAD = 2, OUTLET_PRESSURE = 3 };
+enum Wall : int32_t { WALL_NONE = 0, WALL_SLIP = 1, WALL_NOSLIP = 2, WALL_MOVING = 3 };
+
+enum Feature : uint32_t {
+  FEAT_BOUZIDI = 1u << 0,
+  FEAT_BODY_FORCE = 1u << 1,
+  FEAT_SPONGE = 1u << 2,
+  FEAT_LES = 1u << 3,
+  FEAT_LES_WALE = 1u << 4,
+  FEAT_LES_CS_FIELD = 1u << 5,  // per-cell Smagorinsky constant (van Driest damping)
+  FEAT_THERMAL = 1u << 6,
+  FEAT_BUOYANCY = 1u << 7,
+  FEAT_SCALAR_REDUCED = 1u << 8,  // D2Q5 / D3Q7 scalar lattice
+  FEAT_OPEN = 1u << 9,            // streamwise open: inlet/outlet active
+  FEAT_OBSTACLE_BB = 1u << 10,    // obstacle bounce-back active (links present)
+};
+
+// Status bits raised by the kernels (atomicOr into a device word).
+enum Status : uint32_t {
+  STATUS_NONFINITE_OR_NONPOSITIVE_RHO = 1u << 0,
+};
+
+// MRT operator in the even/odd pair basis (see lbm_mrt.cpp).  For D3Q19:
+// even block 10x10, 7 equilibrium moments; odd block 9x9, 3 momenta.
+template <class Real>
+struct MrtCoeffs {
+  Real Ae[10 * 10];
+  Real Ce[10 * 7];
+  Real Ao[9 * 9];
+  Real Co[9 * 3];
+};
+
+// Everything a kernel needs for one step of one lattice.  Passed by value
+// (kernel parameter space), so per-step variation lives in device memory
+// (step counter) and the struct can be captured once in a CUDA graph.
+template <class Real>
+struct StepParams {
+  int32_t nx, ny, nz;
+  int32_t nwx;          // 32-cell words per x row = ceil(nx / 32)
+  int64_t cs;           // population plane stride (cells, padded)
+  int64_t ncells;       // nx * ny * nz
+  uint32_t feat;
+  int32_t inlet, outlet, wall;
+  int32_t sponge_start; // first sponge x plane (>= nx when off)
+  int32_t sponge_thickness;
+
+  // populations (deviation from the rest weights, see Store<>)
+  const void *P;        // current post-collision populations (read)
+  void *Pn;             // next post-collision populations (written)
+  const uint8_t *solid; // (cells) 1 = solid
+  const uint32_t *lbits;  // per 32-cell word: bit k set when cell k of the word has links
+  const int32_t *loff;    // per 32-cell word: index of its first link cell
+  const uint32_t *lc_mask;  // per link cell: bit i set when direction i is a link
+  const float *lc_q;        // per link cell: q for each direction (Q floats)
+  const int64_t *lc_cell;   // per link cell: cell index
+  int64_t n_lc;
+
+  const Real *prev;     // convective outlet state (Q, nz, ny), deviations
+  Real *prevn;
+  const Real *g;        // scalar state (Qg, cells) -- populations, not deviations
+  Real *gn;
+  const Real *U;        // LES velocities (3, cells) of the current state
+  Real *Uw;             // LES velocity side output (written by the moments pass)
+  const Real *cs_cell;  // per-cell LES constant (van Driest), optional
+
+  // force reduction
+  double *partials;     // per force-block: 12 doubles
+  double *lc_prof;      // per link cell: 3 doubles (profile contributions)
+  const int32_t *prof_off;  // nprof + 1 segment offsets into the link-cell list
+  double *hist;         // force history ring: hist_cap * 12 doubles
+  double *prof_out;     // last profile: nprof * 3 doubles
+  int32_t nprof;
+  int32_t hist_cap;
+  int32_t n_force_blocks;
+  int32_t want_profile;
+  int64_t *step;        // device step counter (steps completed)
+  int64_t *hist_base;   // step index stored in hist slot 0
+  uint32_t *status;
+
+  // physics (Real)
+  Real omega, u0, rho_in, rho_out, pert_amp, trt_lambda, trt_sminus;
+  Real sponge_sigma_max;
+  Real base_nu, les_cs2;
+  Real wall_u_top, wall_u_bottom;
+  Real bf_x, bf_y, bf_z, bf_coeff;
+  Real omega_T, T_hot, T_cold, gbeta, T_ref;
+  double center[3];
+  MrtCoeffs<Real> mrt;
+};
+
+}  // namespace aero

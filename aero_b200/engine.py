@@ -1,0 +1,152 @@
+"""One lattice on one GPU: the C-ABI handle plus its torch-owned workspace.
+
+PyTorch provides the device memory (a single uint8 workspace tensor and the
+FP64 staging tensors for state I/O) and the CUDA stream; all arithmetic on
+the lattice runs in the sm_100a kernels of libaero_b200.so.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import AeroParams, check
+
+FORCE_VALUES = _lib.FORCE_VALUES
+
+
+def _require_cuda(device):
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("aero_b200 needs a CUDA GPU (sm_100a); none is visible")
+    dev = torch.device(device if device is not None else "cuda")
+    if dev.type != "cuda":
+        raise ValueError(f"aero_b200 runs on CUDA devices only, got {dev}")
+    if dev.index is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+    return dev
+
+
+class Engine:
+    """Owns an AeroLattice handle and the device workspace bound to it."""
+
+    def __init__(self, params: AeroParams, solid: np.ndarray, links: np.ndarray, q: np.ndarray,
+                 phi: Optional[np.ndarray] = None, device=None):
+        import torch
+        self.torch = torch
+        self.lib = _lib.load()
+        self.device = _require_cuda(device)
+        self.params = params
+        self.dims = params.dims
+        self.shape = (params.nz, params.ny, params.nx) if params.dims == 3 else (params.ny, params.nx)
+        self.ncells = params.nx * params.ny * params.nz
+        q_ = ctypes.c_int32()
+        qg = ctypes.c_int32()
+        check("aero_lattice_q", self.lib.aero_lattice_q(ctypes.byref(params), ctypes.byref(q_), ctypes.byref(qg)))
+        self.Q, self.Qg = q_.value, qg.value
+        h = ctypes.c_void_p()
+        check("aero_create", self.lib.aero_create(ctypes.byref(params), ctypes.byref(h)))
+        self.h = h
+        solid_u8 = np.ascontiguousarray(solid, dtype=np.uint8)
+        links = np.ascontiguousarray(links, dtype=np.int32)
+        q = np.ascontiguousarray(q, dtype=np.float32)
+        phi_c = None if phi is None else np.ascontiguousarray(phi, dtype=np.float64)
+        check("aero_set_geometry", self.lib.aero_set_geometry(
+            h, solid_u8.ctypes.data, links.ctypes.data if len(links) else None,
+            q.ctypes.data if len(q) else None, len(links), None if phi_c is None else phi_c.ctypes.data))
+        nbytes = ctypes.c_uint64()
+        check("aero_workspace_size", self.lib.aero_workspace_size(h, ctypes.byref(nbytes)))
+        self.workspace_bytes = int(nbytes.value)
+        with torch.cuda.device(self.device):
+            self.workspace = torch.empty(self.workspace_bytes, dtype=torch.uint8, device=self.device)
+            check("aero_bind_workspace", self.lib.aero_bind_workspace(
+                h, self.workspace.data_ptr(), self.workspace_bytes, self.stream()))
+        self.hist_capacity = params.hist_capacity or 4096
+        self.nprof = params.nz if params.dims == 3 else params.ny
+
+    # ------------------------------------------------------------------
+    def stream(self):
+        return self.torch.cuda.current_stream(self.device).cuda_stream
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            try:
+                self.lib.aero_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+    # ------------------------------------------------------------------
+    def _dev(self, a, shape):
+        t = self.torch
+        if isinstance(a, t.Tensor):
+            x = a.to(device=self.device, dtype=t.float64)
+        else:
+            x = t.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(self.device)
+        return x.reshape(shape).contiguous()
+
+    def set_state(self, f, f_outlet_prev=None, g=None, step_count: int = 0) -> None:
+        """f: (Q, ...) absolute populations (numpy or torch); optional outlet state and scalar."""
+        fd = self._dev(f, (self.Q,) + self.shape)
+        pd = None if f_outlet_prev is None else self._dev(
+            f_outlet_prev, (self.Q,) + self.shape[:-1])
+        gd = None if g is None else self._dev(g, (self.Qg,) + self.shape)
+        with self.torch.cuda.device(self.device):
+            check("aero_set_state", self.lib.aero_set_state(
+                self.h, fd.data_ptr(), None if pd is None else pd.data_ptr(),
+                None if gd is None else gd.data_ptr(), int(step_count), self.stream()))
+            # keep the staging tensors alive until the copies ran
+            self.torch.cuda.current_stream(self.device).synchronize()
+
+    def get_state_device(self, want_prev=True, want_g=True):
+        t = self.torch
+        f = t.empty((self.Q,) + self.shape, dtype=t.float64, device=self.device)
+        p = t.empty((self.Q,) + self.shape[:-1], dtype=t.float64, device=self.device) if want_prev else None
+        g = (t.empty((self.Qg,) + self.shape, dtype=t.float64, device=self.device)
+             if (want_g and self.Qg) else None)
+        with t.cuda.device(self.device):
+            check("aero_get_state", self.lib.aero_get_state(
+                self.h, f.data_ptr(), None if p is None else p.data_ptr(),
+                None if g is None else g.data_ptr(), self.stream()))
+        return f, p, g
+
+    def get_state(self):
+        f, p, g = self.get_state_device()
+        return (f.cpu().numpy(), p.cpu().numpy(), None if g is None else g.cpu().numpy())
+
+    def get_slab_device(self, z0: int, nzs: int):
+        t = self.torch
+        out = t.empty((self.Q, nzs) + self.shape[-2:], dtype=t.float64, device=self.device)
+        with t.cuda.device(self.device):
+            check("aero_get_state_slab", self.lib.aero_get_state_slab(
+                self.h, int(z0), int(nzs), out.data_ptr(), self.stream()))
+        return out
+
+    def step(self, n: int) -> None:
+        with self.torch.cuda.device(self.device):
+            check("aero_step", self.lib.aero_step(self.h, int(n), self.stream()))
+
+    def read_forces(self, max_steps: Optional[int] = None) -> np.ndarray:
+        cap = self.hist_capacity if max_steps is None else int(max_steps)
+        out = np.empty((cap, FORCE_VALUES), dtype=np.float64)
+        n = ctypes.c_int64()
+        with self.torch.cuda.device(self.device):
+            check("aero_read_forces", self.lib.aero_read_forces(
+                self.h, out.ctypes.data, cap, ctypes.byref(n), self.stream()))
+        return out[: n.value]
+
+    def read_profile(self) -> np.ndarray:
+        out = np.empty((self.nprof, 3), dtype=np.float64)
+        with self.torch.cuda.device(self.device):
+            check("aero_read_profile", self.lib.aero_read_profile(self.h, out.ctypes.data, self.stream()))
+        return out
+
+    def status(self) -> int:
+        v = ctypes.c_uint32()
+        with self.torch.cuda.device(self.device):
+            check("aero_status", self.lib.aero_status(self.h, ctypes.byref(v), self.stream()))
+        return int(v.value)

@@ -1,0 +1,173 @@
+/*
+ * aero_b200.h -- C ABI of the aero_b200 lattice Boltzmann engine (sm_100a).
+ *
+ * The engine replaces the per-step hot path of the Aero wind-tunnel solver:
+ * the body of Solver._step / Solver3D._step (aero/lbm/solver.py:276-464,
+ * aero/lbm/solver3d.py:325-541) and the kernels it calls.  Plain C types
+ * only; every function returns AERO_OK (0) or a negative AERO_ERR_* code and
+ * leaves a message for aero_last_error().
+ *
+ * Memory ownership: the caller allocates ONE device workspace of
+ * aero_workspace_size() bytes (e.g. a torch uint8 tensor) and binds it; the
+ * library never allocates or frees device memory for a lattice.  Bulk state
+ * I/O (populations, outlet state, scalar) goes through caller-owned DEVICE
+ * buffers in the reference layout.  Calls are ordered on the caller's CUDA
+ * stream (a cudaStream_t passed as void*; NULL = legacy default stream).
+ * A handle is not thread-safe: one host thread per handle.
+ */
+#ifndef AERO_B200_H
+#define AERO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AERO_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define AERO_API __attribute__((visibility("default")))
+#else
+#define AERO_API
+#endif
+
+enum {
+  AERO_OK = 0,
+  AERO_ERR_INVALID = -1,     /* bad argument or parameter combination */
+  AERO_ERR_CUDA = -2,        /* a CUDA call failed */
+  AERO_ERR_STATE = -3,       /* call out of order (e.g. step before bind) */
+  AERO_ERR_UNSUPPORTED = -4, /* option outside the engine (IBM, SEM inlet, ...) */
+  AERO_ERR_CAPACITY = -5     /* force history full: read it first */
+};
+
+enum { AERO_STORE_F32 = 0, AERO_STORE_F64 = 1, AERO_STORE_F16 = 2, AERO_STORE_BF16 = 3 };
+enum { AERO_BGK = 0, AERO_TRT = 1, AERO_MRT = 2 };
+enum { AERO_INLET_NONE = 0, AERO_INLET_VELOCITY = 1, AERO_INLET_PRESSURE = 2 };
+enum { AERO_OUTLET_NONE = 0, AERO_OUTLET_CONVECTIVE = 1, AERO_OUTLET_ZEROGRADIENT = 2, AERO_OUTLET_PRESSURE = 3 };
+enum { AERO_WALL_NONE = 0, AERO_WALL_SLIP = 1, AERO_WALL_NOSLIP = 2, AERO_WALL_MOVING = 3 };
+enum { AERO_LES_SMAGORINSKY = 0, AERO_LES_WALE = 1 };
+
+/* Solver options.  Field meanings follow the keyword arguments of the
+ * reference constructors (aero/lbm/solver.py:75-116,
+ * aero/lbm/solver3d.py:71-119). */
+typedef struct AeroParams {
+  int32_t abi_version;      /* AERO_ABI_VERSION */
+  int32_t dims;             /* 2 = D2Q9, 3 = D3Q19 */
+  int32_t nx, ny, nz;       /* nz = 1 in 2D */
+  int32_t storage;          /* AERO_STORE_* */
+  int32_t collision;        /* AERO_BGK / AERO_TRT / AERO_MRT */
+  int32_t inlet_bc;         /* AERO_INLET_* */
+  int32_t outlet_bc;        /* AERO_OUTLET_* */
+  int32_t wall_bc;          /* AERO_WALL_* */
+  int32_t streamwise_open;  /* 1: inlet/outlet active; 0: streamwise periodic (3D) */
+  int32_t les;              /* Smagorinsky/WALE eddy viscosity (ignored by MRT, as in the reference) */
+  int32_t les_model;        /* AERO_LES_* */
+  int32_t van_driest;       /* damp the LES constant with |phi| (needs phi) */
+  int32_t bouzidi;          /* interpolated bounce-back with per-link q */
+  int32_t thermal;          /* passive scalar lattice */
+  int32_t buoyancy;         /* Boussinesq forcing of the flow by the scalar */
+  int32_t scalar_reduced;   /* 0: D2Q9/D3Q19 scalar (reference); 1: D2Q5/D3Q7 */
+  int32_t sponge_thickness; /* outlet sponge planes (0 = off) */
+  int32_t hist_capacity;    /* steps of force history kept on the device (0 = 4096) */
+  double omega, u0, rho0, rho_in, rho_out;
+  double inlet_perturbation, trt_lambda, sponge_strength;
+  double les_cs, van_driest_A;
+  double wall_velocity_top, wall_velocity_bottom;
+  double body_force[3];     /* (fx, fy, fz); 3D only */
+  double alpha_T, T_hot, T_cold, g_gravity, beta, T_ref;
+  double center[3];         /* moment reference point (x, y, z): mean solid cell */
+} AeroParams;
+
+typedef struct AeroLattice AeroLattice;
+
+/* Number of per-step force values returned by aero_read_forces. Layout of one
+ * step: Fx Fy Fz | pressure Fx Fy Fz | viscous Fx Fy Fz | Mx My Mz, raw
+ * lattice units (forces.py:15-127, forces3d.py:8-131). */
+#define AERO_FORCE_VALUES 12
+
+/* Creates a handle and validates the options.  Replaces the option handling
+ * and backend selection of Solver.__init__ (solver.py:143-203,
+ * solver3d.py:136-221). */
+AERO_API int aero_create(const AeroParams *params, AeroLattice **out);
+
+/* Geometry on the host: solid (nz*ny*nx bytes, 1 = solid), the surface link
+ * list (n_links rows of [i, (z,) y, x] int32, as built by
+ * build_surface_links(_3d), boundary.py:232-280, boundary3d.py:279-329) with
+ * its q values (float32), and phi (float64 per cell, only read when
+ * van_driest is set; may be NULL).  Must precede aero_workspace_size. */
+AERO_API int aero_set_geometry(AeroLattice *lat, const uint8_t *solid, const int32_t *links, const float *q,
+                      int64_t n_links, const double *phi);
+
+/* Device bytes the lattice needs; the caller allocates them. */
+AERO_API int aero_workspace_size(const AeroLattice *lat, uint64_t *bytes);
+
+/* Binds the caller's device workspace (256-byte aligned) and uploads the
+ * geometry tables.  Replaces the array set-up of solver.py:205-257. */
+AERO_API int aero_bind_workspace(AeroLattice *lat, void *device_ptr, uint64_t bytes, void *stream);
+
+/* Sets the solver state from caller DEVICE buffers in the reference layout:
+ * f (Q, nz, ny, nx) float64, f_outlet_prev (Q, [nz,] ny) float64 (NULL keeps
+ * the current one), g (Qg, nz, ny, nx) float64 (thermal only, NULL keeps),
+ * and the number of steps already taken.  Replaces the initial-state code of
+ * solver.py:218-227 / solver3d.py:239-247 and load_checkpoint
+ * (solver.py:688-709). */
+AERO_API int aero_set_state(AeroLattice *lat, const double *f, const double *f_outlet_prev, const double *g,
+                   int64_t step_count, void *stream);
+
+/* Writes the current state into caller DEVICE buffers (same layouts; any
+ * pointer may be NULL).  The state is the reference's self.f after the last
+ * step. */
+AERO_API int aero_get_state(AeroLattice *lat, double *f, double *f_outlet_prev, double *g, void *stream);
+
+/* Advances n_steps steps (Solver._step, solver.py:276-464; Solver3D._step,
+ * solver3d.py:325-541), forces included.  Asynchronous on the stream. */
+AERO_API int aero_step(AeroLattice *lat, int64_t n_steps, void *stream);
+
+/* Copies the force values of the steps taken since the previous read into
+ * host memory (max_steps * AERO_FORCE_VALUES doubles) and synchronises the
+ * stream.  *n_out receives the number of steps copied. */
+AERO_API int aero_read_forces(AeroLattice *lat, double *out, int64_t max_steps, int64_t *n_out, void *stream);
+
+/* Force profile of the last step: 3 doubles (fx, fy, fz) per y row (2D,
+ * force_profile_2d, forces.py:142-162) or per z plane (3D,
+ * spanwise_force_profile_3d, forces3d.py:148-171); host memory, synchronous. */
+AERO_API int aero_read_profile(AeroLattice *lat, double *out, void *stream);
+
+/* Divergence flags raised on the device since creation (bit 0: a cell had a
+ * non-finite or non-positive density; the test of check_stability,
+ * diagnostics.py:32-71).  Synchronous. */
+AERO_API int aero_status(AeroLattice *lat, uint32_t *status, void *stream);
+
+/* Steps taken (host mirror of the reference's step_count). */
+AERO_API int aero_step_count(const AeroLattice *lat, int64_t *steps);
+
+/* Releases the handle (never the caller's workspace). */
+AERO_API int aero_destroy(AeroLattice *lat);
+
+/* Message of the last failed call on this thread. */
+AERO_API const char *aero_last_error(void);
+
+/* FP64 MRT operator f_post = A f + B feq of the reference basis
+ * (mrt2d.py:36-77, mrt3d.py:46-135): A, B are Q x Q row-major.  Exposed so a
+ * caller can check the engine's operator. */
+AERO_API int aero_mrt_operator(int32_t dims, double omega, double *A, double *B);
+
+/* Number of lattice directions and scalar directions for the options. */
+AERO_API int aero_lattice_q(const AeroParams *params, int32_t *q, int32_t *q_scalar);
+
+AERO_API int aero_abi_version(void);
+
+/* sizeof(AeroParams), so bindings can check their struct layout. */
+AERO_API int aero_params_size(void);
+
+/* Like aero_get_state for f only, restricted to the planes z0 .. z0+nzs-1:
+ * f receives (Q, nzs, ny, nx) float64 in caller DEVICE memory.  Lets a
+ * caller inspect one plane of a large lattice (the 3D stability check reads
+ * the mid plane, solver3d.py:608-615). */
+AERO_API int aero_get_state_slab(AeroLattice *lat, int32_t z0, int32_t nzs, double *f, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,177 @@
+"""GPU parity of the B200 engine against the reference and the FP64 oracle.
+
+Tolerances (stated per test):
+  * fp64 storage: the engine performs the reference's arithmetic in a
+    different association order (deviation form, pair-basis MRT), so states
+    and coefficients agree to FP64 round-off amplified by at most 40 steps:
+    |df| <= 1e-10 * max|f|, coefficients <= 1e-8 * max|C|.
+  * fp32 storage: relative L2 of rho and u <= 1e-5 against the FP64 oracle
+    (the acceptance bound for the plain FP32 form), coefficients <= 1e-4.
+"""
+
+import numpy as np
+import pytest
+
+from tests.golden_cases import CASES, load_case, make_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _solver(c, **extra):
+    from aero_b200 import Solver, Solver3D
+    kw = dict(c["kwargs"])
+    kw.update(extra)
+    if c["dims"] == 2:
+        s = Solver(Ny=c["ny"], Nx=c["nx"], solid=c["solid"], omega=c["omega"], u0=c["u0"], D=c["D"],
+                   phi=c["phi"], **kw)
+    else:
+        s = Solver3D(Nz=c["nz"], Ny=c["ny"], Nx=c["nx"], solid=c["solid"], omega=c["omega"],
+                     u0=c["u0"], D=c["D"], phi=c["phi"], **kw)
+    s.f = c["f0"].copy()
+    if "g0" in c:
+        s.g = c["g0"].copy()
+    return s
+
+
+def _hist_names(dims):
+    return ("Cd", "Cl", "Cm", "Cd_p", "Cd_v") if dims == 2 else (
+        "Cd", "Cly", "Clz", "Cmx", "Cmy", "Cmz", "Cd_p", "Cd_v")
+
+
+def _macro(f, dims):
+    from aero_b200.lattice import macroscopic
+    return macroscopic(f, dims)
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_engine_matches_reference_golden(name):
+    c = load_case(name)
+    s = _solver(c, precision="fp64")
+    hist = {k: [] for k in _hist_names(c["dims"])}
+    for _ in range(c["steps"]):
+        out = s._step()
+        hist["Cd"].append(out[0])
+        if c["dims"] == 2:
+            hist["Cl"].append(out[1])
+            hist["Cm"].append(s._last_cm)
+        else:
+            hist["Cly"].append(out[1])
+            hist["Clz"].append(out[2])
+            hist["Cmx"].append(s._last_cmx)
+            hist["Cmy"].append(s._last_cmy)
+            hist["Cmz"].append(s._last_cmz)
+        hist["Cd_p"].append(s._last_cd_p)
+        hist["Cd_v"].append(s._last_cd_v)
+    scale = np.abs(c["f"]).max()
+    np.testing.assert_allclose(s.f, c["f"], rtol=0, atol=1e-10 * scale)
+    np.testing.assert_allclose(s._f_outlet_prev, c["f_outlet_prev"], rtol=0, atol=1e-10 * scale)
+    if "g" in c:
+        np.testing.assert_allclose(s.g, c["g"], rtol=0, atol=1e-10 * np.abs(c["g"]).max())
+    for k, ref in c["hist"].items():
+        np.testing.assert_allclose(np.array(hist[k]), ref, rtol=0,
+                                   atol=1e-8 * max(np.abs(ref).max(), 1e-3), err_msg=k)
+    prof = s._last_force_profile if c["dims"] == 2 else s._last_spanwise_profile
+    got = np.array([prof["fx"], prof["fy"]] + ([prof["fz"]] if c["dims"] == 3 else []))
+    np.testing.assert_allclose(got, c["profile"], rtol=0, atol=1e-10 * max(np.abs(c["profile"]).max(), 1))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp32_engine_close_to_reference(name):
+    c = load_case(name)
+    s = _solver(c, precision="fp32")
+    cd = [s._step()[0] for _ in range(c["steps"])]
+    got = _macro(s.f, c["dims"])
+    ref = _macro(c["f"], c["dims"])
+    assert rel_l2(got[0], ref[0]) <= 1e-5
+    assert rel_l2(np.stack(got[1:]), np.stack(ref[1:])) <= 1e-5
+    np.testing.assert_allclose(cd, c["hist"]["Cd"], rtol=0, atol=1e-4 * np.abs(c["hist"]["Cd"]).max())
+
+
+def test_run_chunks_equal_single_steps():
+    """run() (multi-step graphs, chunked force reads) == repeated _step()."""
+    c = load_case("c2d_bgk_slip_convective_pert")
+    a = _solver(c, precision="fp32")
+    b = _solver(c, precision="fp32")
+    cd_a = [a._step()[0] for _ in range(37)]
+    r = b.run(37, check_every=10, verbose=False)
+    assert np.array_equal(a.f, b.f)
+    assert np.array_equal(a._f_outlet_prev, b._f_outlet_prev)
+    assert r["Cd_history"] == cd_a
+    assert r["steps_completed"] == 37
+
+
+def test_run_matches_oracle_1000_steps_fp32():
+    """Acceptance bound of the plain form: rel-L2(rho, u) <= 1e-5 after 1000 steps."""
+    from aero_b200 import Solver, Cylinder
+    from oracle.oracle import OracleSolver
+    ny, nx = 64, 160
+    geo = Cylinder(radius=6, cx_frac=0.25, cy_frac=0.5)
+    solid = geo.mark_solid(ny, nx)
+    u0, D = 0.05, geo.reference_length()
+    omega = 1.0 / (3.0 * u0 * D / 100.0 + 0.5)
+    kw = dict(wall_bc="noslip", outlet_bc="zerogradient", inlet_bc="velocity", collision="bgk")
+    rng = np.random.default_rng(11)
+    from aero_b200.lattice import feq
+    f0 = feq(2, np.ones((ny, nx)), np.full((ny, nx), u0), rng.uniform(-1e-4, 1e-4, (ny, nx)))
+    s = Solver(Ny=ny, Nx=nx, solid=solid, omega=omega, u0=u0, D=D, precision="fp32", **kw)
+    s.f = f0
+    r = s.run(1000, check_every=250, verbose=False)
+    o = OracleSolver(solid=solid, omega=omega, u0=u0, D=D, **kw)
+    o.f = f0.copy()
+    cd = []
+    for _ in range(1000):
+        cd.append(o.step()[0]["Cd"])
+    got = _macro(s.f, 2)
+    ref = _macro(o.f, 2)
+    for a, b in zip(got, ref):
+        assert rel_l2(a, b) <= 1e-5
+    assert abs(np.mean(r["Cd_history"][-200:]) - np.mean(cd[-200:])) <= 1e-3 * abs(np.mean(cd[-200:]))
+
+
+def test_state_roundtrip_and_checkpoint(tmp_path):
+    c = load_case("c3d_trt_wale_periodic_bodyforce_thermal")
+    s = _solver(c, precision="fp64")
+    for _ in range(3):
+        s._step()
+    p = tmp_path / "ck.npz"
+    s.save_checkpoint(str(p))
+    from aero_b200 import Solver3D
+    t = Solver3D.from_checkpoint(str(p), precision="fp64")
+    for _ in range(4):
+        s._step()
+        t._step()
+    np.testing.assert_allclose(t.f, s.f, rtol=0, atol=1e-14)
+    np.testing.assert_allclose(t.g, s.g, rtol=0, atol=1e-14)
+    assert t.step_count == s.step_count == 7
+
+
+def test_divergence_flag_and_run_raises():
+    """Host-injected NaN: the device status word records it and run() raises."""
+    c = load_case("c2d_bgk_noslip_zerograd")
+    s = _solver(c, precision="fp32")
+    s._step()
+    assert s.status() == 0
+    f = s.f
+    f[:, 5, 7] = np.nan
+    s.f = f
+    s._step()
+    assert s.status() & 1
+    with pytest.raises(RuntimeError, match="NaN detected"):
+        s.run(10, check_every=5, verbose=False)
+
+
+@pytest.mark.parametrize("precision", ["fp16s", "bf16s"])
+def test_reduced_precision_storage_tracks_fp64(precision):
+    c = load_case("c3d_mrt_smag_bouzidi_sponge")
+    a = _solver(c, precision="fp64")
+    b = _solver(c, precision=precision)
+    cda = [a._step()[0] for _ in range(c["steps"])]
+    cdb = [b._step()[0] for _ in range(c["steps"])]
+    ra, rb = _macro(a.f, 3), _macro(b.f, 3)
+    tol = 5e-3 if precision == "fp16s" else 3e-2
+    assert rel_l2(rb[1], ra[1]) < tol  # ux
+    assert abs(cdb[-1] - cda[-1]) <= tol * abs(cda[-1]) * 10
