@@ -151,22 +151,40 @@ class LatticeSolverBase:
                               phi if (self.van_driest and phi is not None) else None, device)
 
         # initial state: equilibrium at (rho0, u0, 0) everywhere, solids included
-        # (solver.py:218-227, solver3d.py:239-247)
+        # (solver.py:218-227, solver3d.py:239-247); built on the GPU
         e, w, _ = tables(self.dims)
         self.Q = len(w)
-        rho = np.full(shape, rho0)
-        ux = np.full(shape, u0)
-        zero = np.zeros(shape)
-        f0 = feq(self.dims, rho, ux, zero, zero if self.dims == 3 else None)
-        g0 = None
-        if self.thermal:
-            wg = scalar_weights(self.dims, scalar_lattice == "reduced")
-            g0 = wg.reshape((-1,) + (1,) * self.dims) * T_ref * np.ones((len(wg),) + tuple(shape))
         self.step_count = 0
         self._f_host = self._prev_host = self._g_host = None
         self._pristine = {}
-        self._engine.set_state(f0, f0[..., -1], g0, 0)
+        f0, prev0, g0 = self._uniform_state_device()
+        self._engine.set_state(f0, prev0, g0, 0)
+        del f0, prev0, g0
         self._init_histories()
+
+    def _uniform_state_device(self, ux=None):
+        """Equilibrium populations for rho0 and velocity (ux, 0, 0) as device
+        tensors; ux defaults to u0 everywhere.  Also returns the matching
+        outlet column and the scalar at T_ref."""
+        import torch
+        dev = self._engine.device
+        shape = self.solid.shape
+        if ux is None:
+            vec = feq(self.dims, np.array(self.rho0), np.array(self.u0), np.array(0.0),
+                      np.array(0.0) if self.dims == 3 else None)
+            f0 = torch.tensor(vec, dtype=torch.float64, device=dev).reshape(
+                (self.Q,) + (1,) * self.dims).expand((self.Q,) + tuple(shape)).contiguous()
+        else:
+            rho = torch.full(tuple(shape), self.rho0, dtype=torch.float64, device=dev)
+            zero = torch.zeros_like(rho)
+            f0 = feq(self.dims, rho, ux, zero, zero if self.dims == 3 else None, xp=torch)
+        prev0 = f0[..., -1].contiguous()
+        g0 = None
+        if self.thermal:
+            wg = scalar_weights(self.dims, self.scalar_lattice == "reduced")
+            g0 = (torch.tensor(wg * self.T_ref, dtype=torch.float64, device=dev).reshape(
+                (-1,) + (1,) * self.dims).expand((len(wg),) + tuple(shape)).contiguous())
+        return f0, prev0, g0
 
     # ------------------------------------------------------------------ state
     def _cache(self):

@@ -62,6 +62,9 @@ SIGNATURES = {
     "aero_step_count": ([_VP, ctypes.POINTER(_I64)], ctypes.c_int),
     "aero_destroy": ([_VP], ctypes.c_int),
     "aero_mrt_operator": ([_I32, _D, _VP, _VP], ctypes.c_int),
+    "aero_enable_timing": ([_VP, _I32], ctypes.c_int),
+    "aero_kernel_times": ([_VP, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_I64), _VP],
+                          ctypes.c_int),
 }
 
 
@@ -82,7 +85,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     if _lib is not None:
         return _lib
     path = _build.LIB
-    if not path.exists() or (build_if_missing and not _build.up_to_date()):
+    if not path.exists():
         if not build_if_missing:
             raise ImportError(f"aero_b200: {path.name} not found; build it with python -m aero_b200._build")
         try:

@@ -115,6 +115,10 @@ struct AeroLattice {
   cudaGraphExec_t pair_exec[2] = {nullptr, nullptr};
   bool use_graphs = true;
   int device = -1;  // device of the bound workspace
+  // optional per-kernel event timing (eager launches only)
+  bool timing = false;
+  std::vector<cudaEvent_t> ev;  // 4 events per timed step
+  int64_t timed_steps = 0;
 };
 
 namespace {
@@ -224,16 +228,35 @@ dim3 cell_grid(const AeroLattice *L) {
 
 bool les_active(const AeroLattice *L) { return (L->feat & FEAT_LES) != 0; }
 
-// Launches one step with buffer parity `cur` on stream st.
+// Launches one step with buffer parity `cur` on stream st.  With timing on,
+// events bracket the force kernels (forces + finalize) and the fused step
+// (moments pass + step kernel).
 template <class Real>
-int launch_step(AeroLattice *L, int cur, cudaStream_t st) {
+int launch_step(AeroLattice *L, int cur, cudaStream_t st, bool timed = false) {
   const Ops<Real> *ops = get_ops<Real>(L);
   const StepParams<Real> p = make_params<Real>(L, cur);
   const dim3 grid = cell_grid(L);
+  cudaEvent_t *e = nullptr;
+  if (timed) {
+    const size_t need = 4 * (size_t)(L->timed_steps + 1);
+    while (L->ev.size() < need) {
+      cudaEvent_t x;
+      CUDA_TRY(cudaEventCreate(&x));
+      L->ev.push_back(x);
+    }
+    e = &L->ev[4 * (size_t)L->timed_steps];
+    CUDA_TRY(cudaEventRecord(e[0], st));
+  }
   if (L->n_force_blocks > 0) CUDA_TRY(ops->forces(p, L->n_force_blocks, st));
+  if (timed) CUDA_TRY(cudaEventRecord(e[1], st));
   if (les_active(L)) CUDA_TRY(ops->moments(p, false, grid, st));
   CUDA_TRY(ops->step(p, false, grid, st));
+  if (timed) CUDA_TRY(cudaEventRecord(e[2], st));
   CUDA_TRY(ops->finalize(p, st));
+  if (timed) {
+    CUDA_TRY(cudaEventRecord(e[3], st));
+    L->timed_steps++;
+  }
   return AERO_OK;
 }
 
@@ -259,7 +282,7 @@ int build_pair_graph(AeroLattice *L, int cur) {
 template <class Real>
 int do_steps(AeroLattice *L, int64_t n, cudaStream_t st) {
   while (n > 0) {
-    if (n >= 2 && L->use_graphs) {
+    if (n >= 2 && L->use_graphs && !L->timing) {
       if (!L->pair_exec[L->cur]) {
         const int rc = build_pair_graph<Real>(L, L->cur);
         if (rc != AERO_OK) return rc;
@@ -268,7 +291,7 @@ int do_steps(AeroLattice *L, int64_t n, cudaStream_t st) {
       n -= 2;
       L->step_count += 2;
     } else {
-      const int rc = launch_step<Real>(L, L->cur, st);
+      const int rc = launch_step<Real>(L, L->cur, st, L->timing);
       if (rc != AERO_OK) return rc;
       L->cur ^= 1;
       n -= 1;
@@ -617,6 +640,34 @@ int aero_get_state_slab(AeroLattice *L, int32_t z0, int32_t nzs, double *f, void
 
 int aero_params_size(void) { return (int)sizeof(AeroParams); }
 
+int aero_enable_timing(AeroLattice *L, int32_t on) {
+  if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
+  L->timing = on != 0;
+  return AERO_OK;
+}
+
+int aero_kernel_times(AeroLattice *L, double *step_ms, double *forces_ms, int64_t *steps, void *stream) {
+  if (!L || !step_ms || !forces_ms || !steps) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
+  CUDA_TRY(cudaSetDevice(L->device));
+  CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  double a = 0.0, b = 0.0;
+  for (int64_t k = 0; k < L->timed_steps; k++) {
+    float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+    cudaEvent_t *e = &L->ev[4 * (size_t)k];
+    CUDA_TRY(cudaEventElapsedTime(&t0, e[0], e[1]));
+    CUDA_TRY(cudaEventElapsedTime(&t1, e[1], e[2]));
+    CUDA_TRY(cudaEventElapsedTime(&t2, e[2], e[3]));
+    a += t1;
+    b += t0 + t2;
+  }
+  *step_ms = a;
+  *forces_ms = b;
+  *steps = L->timed_steps;
+  L->timed_steps = 0;
+  return AERO_OK;
+}
+
 int aero_step(AeroLattice *L, int64_t n, void *stream) {
   if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
   if (!L->state_set) return fail(AERO_ERR_STATE, "aero_set_state must come first");
@@ -680,6 +731,7 @@ int aero_destroy(AeroLattice *L) {
   for (auto &e : L->pair_exec)
     if (e) cudaGraphExecDestroy(e);
   if (L->cap_stream) cudaStreamDestroy(L->cap_stream);
+  for (auto e : L->ev) cudaEventDestroy(e);
   delete L;
   return AERO_OK;
 }

@@ -150,3 +150,15 @@ class Engine:
         with self.torch.cuda.device(self.device):
             check("aero_status", self.lib.aero_status(self.h, ctypes.byref(v), self.stream()))
         return int(v.value)
+
+    # ------------------------------------------------------------------ timing
+    def enable_timing(self, on: bool = True) -> None:
+        check("aero_enable_timing", self.lib.aero_enable_timing(self.h, 1 if on else 0))
+
+    def kernel_times(self):
+        """(summed ms of the fused step kernel, of the force kernels, steps timed)."""
+        a, b, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
+        with self.torch.cuda.device(self.device):
+            check("aero_kernel_times", self.lib.aero_kernel_times(
+                self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(n), self.stream()))
+        return a.value, b.value, n.value

@@ -1,0 +1,390 @@
+#!/usr/bin/env python
+"""Headline benchmark: D3Q19 lattice updates per second (MLUPS) on B200.
+
+Workload (default, ``--workload sphere512``): the 3D sphere wind tunnel of
+the Aero reference, D3Q19 MRT collision + Smagorinsky LES (Cs 0.1) + Bouzidi
+bounce-back on a 512x256x256 lattice (33.5 M cells), sphere radius 16 at
+(96, 128, 128), u0 = 0.05, nu = 0.0016 (tau 0.5048), free-slip y walls,
+periodic z, Zou-He inlet, convective outlet, sponge over the last 32 planes,
+initial velocity with a seeded +-1 % uniform perturbation.  Populations are
+stored in FP32 (``--precision``).  A "step" is one full solver step: the fused
+stream/BC/collide kernel plus the momentum-exchange force reduction.
+
+One JSON line on stdout (rank 0):
+  value   : whole-job MLUPS from CUDA events around K steps with the state
+            resident in HBM (two 2.5 GB population buffers, larger than L2,
+            so no flush is needed), max over ranks;
+  e2e     : MLUPS through the public API, Solver3D.run(K), timed on the host,
+            including the upload of the initial state from pinned host memory
+            and the read-back of forces, stability plane and final fields;
+  roofline: the fused step kernel's algorithmic bytes per launch
+            (2 Q bytes-per-population + 1 flag byte per cell) over its
+            average CUDA-event duration, against the measured HBM copy rate;
+  cpu_baseline: the FP64 oracle (C/OpenMP restatement of the reference step)
+            on a bounded slab of the same workload, on this host's cores.
+
+``--impl reference`` times that CPU path alone (rank 0; other ranks exit).
+Multi-GPU (torchrun): every rank advances its own replica (no exchange);
+``scaling`` is "weak".
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    "sphere512": dict(
+        dims=3, nx=512, ny=256, nz=256, shape=("sphere", 16.0, 96 / 512, 0.5, 0.5),
+        kwargs=dict(collision="mrt", les=True, les_cs=0.1, bouzidi=True, wall_bc="slip",
+                    inlet_bc="velocity", outlet_bc="convective", streamwise_bc="open",
+                    sponge_thickness=32, sponge_strength=0.1),
+        u0=0.05, nu=0.0016, perturb=0.01,
+        desc="D3Q19 MRT+Smagorinsky(0.1)+Bouzidi sphere r16, 512x256x256, slip walls, sponge 32"),
+    "sphere256": dict(
+        dims=3, nx=256, ny=128, nz=128, shape=("sphere", 8.0, 48 / 256, 0.5, 0.5),
+        kwargs=dict(collision="mrt", les=True, les_cs=0.1, bouzidi=True, wall_bc="slip",
+                    inlet_bc="velocity", outlet_bc="convective", streamwise_bc="open",
+                    sponge_thickness=16, sponge_strength=0.1),
+        u0=0.05, nu=0.0016, perturb=0.01,
+        desc="half-size sphere512 (256x128x128, r8), for profiling captures"),
+    "box256": dict(
+        dims=3, nx=256, ny=128, nz=128, shape=("box", 24.0, 24.0, 128.0, 76 / 256, 12 / 128, 0.5),
+        kwargs=dict(collision="trt", trt_lambda=3 / 16, les=True, les_model="wale", les_cs=0.5,
+                    wall_bc="noslip", streamwise_bc="periodic", body_force_x=1e-6, thermal=True,
+                    T_hot=1.0, T_cold=0.0, alpha_T=0.01, buoyancy=True, g_gravity=1e-5, beta=1.0,
+                    T_ref=0.5, scalar_lattice="reduced"),
+        u0=0.05, nu=0.01, perturb=0.0,
+        desc="D3Q19 TRT+WALE thermal channel 256x128x128, D3Q7 scalar, box obstacle, body force"),
+}
+
+PEAK_FALLBACK_GBS = 6650.0
+
+
+def _rank_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def _peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return PEAK_FALLBACK_GBS, "fallback"
+
+
+def _geometry(w):
+    from aero_b200 import Box, Sphere
+    s = w["shape"]
+    if s[0] == "sphere":
+        g = Sphere(radius=s[1], cx_frac=s[2], cy_frac=s[3], cz_frac=s[4])
+    else:
+        g = Box(width=s[1], height=s[2], depth=s[3], cx_frac=s[4], cy_frac=s[5], cz_frac=s[6])
+    return g
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                mhz.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def cpu_oracle_sample(w, target_s=15.0, max_steps=50, nz_sample=32, threads=None):
+    """Times the FP64 oracle on a slab (nz_sample planes) of the workload."""
+    import numpy as np
+    from oracle.oracle import OracleSolver
+    threads = threads or len(os.sched_getaffinity(0))
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    g = _geometry(w)
+    nz = min(nz_sample, w["nz"])
+    solid = g.mark_solid(nz, w["ny"], w["nx"])
+    phi = g.sdf_field(nz, w["ny"], w["nx"])
+    D = g.reference_length()
+    omega = 1.0 / (3.0 * w["nu"] + 0.5)
+    kw = dict(w["kwargs"])
+    kw.pop("scalar_lattice", None)
+    o = OracleSolver(solid=solid, omega=omega, u0=w["u0"], D=D, phi=phi, threads=threads, **kw)
+    o.step()  # warm-up (page-in, OpenMP start)
+    cells = solid.size
+    t0 = time.perf_counter()
+    n = 0
+    while n < max_steps:
+        o.step()
+        n += 1
+        if time.perf_counter() - t0 >= target_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": cells * n / dt / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
+            "sample": f"{n} FP64 oracle steps of a {w['nx']}x{w['ny']}x{nz} slab of the workload "
+                      f"({cells} cells, same physics options), {dt:.1f} s"}
+
+
+def run_reference(args, w):
+    rank, world, _ = _rank_env()
+    if rank != 0:
+        return 0
+    import numpy as np
+    from oracle.oracle import OracleSolver
+    threads = len(os.sched_getaffinity(0))
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    g = _geometry(w)
+    # each step is a bounded sample: a slab sized so that W + K steps stay near a minute
+    nz = 16 if args.steps <= 20 else 4
+    solid = g.mark_solid(nz, w["ny"], w["nx"])
+    phi = g.sdf_field(nz, w["ny"], w["nx"])
+    kw = dict(w["kwargs"])
+    kw.pop("scalar_lattice", None)
+    o = OracleSolver(solid=solid, omega=1.0 / (3.0 * w["nu"] + 0.5), u0=w["u0"],
+                     D=g.reference_length(), phi=phi, threads=threads, **kw)
+    for _ in range(args.warmup):
+        o.step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.step()
+    dt = time.perf_counter() - t0
+    v = solid.size * args.steps / dt / 1e6
+    sample = (f"each step: FP64 oracle step of a {w['nx']}x{w['ny']}x{nz} slab of the workload "
+              f"({solid.size} cells), {args.steps} steps in {dt:.1f} s")
+    line = {
+        "impl": "reference", "metric": "D3Q19 MLUPS", "value": v, "unit": "MLUPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": w["desc"], "sample_cells": solid.size},
+        "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default="sphere512", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16s", "bf16s", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, w)
+    args.warmup = max(args.warmup, 3)
+
+    import numpy as np
+    import torch
+    rank, world, local = _rank_env()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(dev)
+
+    from aero_b200 import Solver3D
+    g = _geometry(w)
+    nz, ny, nx = w["nz"], w["ny"], w["nx"]
+    solid = g.mark_solid(nz, ny, nx)
+    phi = g.sdf_field(nz, ny, nx) if w["kwargs"].get("bouzidi") else None
+    D = g.reference_length()
+    omega = 1.0 / (3.0 * w["nu"] + 0.5)
+    cap = max(4096, args.steps + args.warmup + 8)
+    s = Solver3D(Nz=nz, Ny=ny, Nx=nx, solid=solid, omega=omega, u0=w["u0"], D=D, phi=phi,
+                 precision=args.precision, device=dev, hist_capacity=cap, **w["kwargs"])
+    del phi
+    eng = s._engine
+    ncells = nx * ny * nz
+    # seeded +-1% uniform perturbation of the initial streamwise velocity
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234 + rank)
+    ux0 = w["u0"] * (1.0 + w["perturb"] * (2.0 * torch.rand((nz, ny, nx), generator=gen, device=dev,
+                                                            dtype=torch.float64) - 1.0))
+    f0, prev0, g0 = s._uniform_state_device(ux=ux0)
+    del ux0
+    eng.set_state(f0, prev0, g0, 0)
+    stream = torch.cuda.current_stream(dev)
+
+    # ---------------- device-timed region --------------------------------
+    eng.enable_timing(True)
+    eng.step(args.warmup)
+    eng.read_forces()
+    eng.kernel_times()  # reset
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index if world == 1 else local) as clk:
+        e0.record(stream)
+        eng.step(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    step_ms, force_ms, nt = eng.kernel_times()
+    raw = eng.read_forces()
+    s.step_count += args.warmup + args.steps
+    eng.enable_timing(False)
+    status = eng.status()
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = ncells * world * args.steps / (ms / 1e3) / 1e6
+    launches_per_step = 3 + (1 if (s.les and s.collision != "mrt") else 0)
+
+    # roofline of the fused step kernel
+    peak, peak_kind = _peak_hbm()
+    sb = {"fp32": 4, "fp64": 8, "fp16s": 2, "bf16s": 2}[args.precision]
+    Q = 19
+    bytes_per_cell = 2 * Q * sb + 1
+    if s.thermal:
+        qg = 7 if s.scalar_lattice == "reduced" else 19
+        bytes_per_cell += 2 * qg * (8 if args.precision == "fp64" else 4)
+    alg_bytes = bytes_per_cell * ncells
+    k_ms = step_ms / max(nt, 1)
+    achieved = alg_bytes / (k_ms / 1e3) / 1e9
+    traffic = None
+    prof_json = ROOT / "profiles" / f"k_step_{args.workload}_{args.precision}.json"
+    if prof_json.exists():
+        try:
+            traffic = json.loads(prof_json.read_text()).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    # ---------------- end to end through the public API ------------------
+    e2e = None
+    if not args.no_e2e:
+        f0_host = f0.cpu().pin_memory()
+        prev_host = prev0.cpu().pin_memory()
+        g_host = None if g0 is None else g0.cpu().pin_memory()
+        del f0, prev0, g0
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        eng.set_state(f0_host, prev_host, g_host, 0)
+        s.step_count = 0
+        s._init_histories()
+        r = s.run(args.steps, check_every=args.steps, verbose=False)
+        torch.cuda.synchronize(dev)
+        dt = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([dt], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        h2d = f0_host.numel() * 8 + prev_host.numel() * 8 + (0 if g_host is None else g_host.numel() * 8)
+        d2h = (args.steps * 12 * 8 + nz * 3 * 8 + Q * ny * nx * 8 + 4 * ncells * 8
+               + (ncells * 8 if s.thermal else 0))
+        e2e = {"value": ncells * world * args.steps / dt / 1e6, "unit": "MLUPS",
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "call": "Solver3D.run(K) after uploading the initial state from pinned host memory",
+               "Cd_mean": r["Cd_mean"]}
+    else:
+        del f0, prev0, g0
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_oracle_sample(w)
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    cd = raw[:, 0] / (0.5 * s.rho0 * s.u0 ** 2 * D * D) if len(raw) else np.zeros(1)
+    line = {
+        "metric": "D3Q19 MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": {"fp32": "f32", "fp64": "f64", "fp16s": "f16 storage / f32 compute",
+                  "bf16s": "bf16 storage / f32 compute"}[args.precision],
+        "data": "synthetic",
+        "config": {"workload": args.workload, "desc": w["desc"], "cells": ncells,
+                   "precision": args.precision, "parallelism": f"replicas x{world}",
+                   "l2": "state (2 x Q x cells) far larger than L2; no flush needed",
+                   "links": int(len(s.surface_links))},
+        "gpu_launches": launches_per_step * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic, "kernel": "k_step (fused stream/BC/collide)",
+                     "alg_bytes_per_launch": alg_bytes, "bytes_per_cell": bytes_per_cell,
+                     "kernel_ms": k_ms, "force_kernels_ms": force_ms / max(nt, 1)},
+        "clocks": clk.summary(),
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "status": status,
+        "Cd_last": float(cd[-1]),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -158,6 +158,16 @@ AERO_API int aero_lattice_q(const AeroParams *params, int32_t *q, int32_t *q_sca
 
 AERO_API int aero_abi_version(void);
 
+/* Per-kernel timing of aero_step (no counterpart in the reference, which
+ * has no GPU path): while enabled, aero_step launches each step without
+ * CUDA graphs and brackets the fused step kernel and the force kernels with
+ * CUDA events on the caller's stream.  aero_kernel_times synchronises the
+ * stream, returns the summed event times in milliseconds and the number of
+ * steps timed, and resets the sums. */
+AERO_API int aero_enable_timing(AeroLattice *lat, int32_t on);
+AERO_API int aero_kernel_times(AeroLattice *lat, double *step_ms, double *forces_ms, int64_t *steps,
+                               void *stream);
+
 /* sizeof(AeroParams), so bindings can check their struct layout. */
 AERO_API int aero_params_size(void);
 
