@@ -189,6 +189,7 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   p.step = ctr;
   p.hist_base = ctr + 1;
   p.status = reinterpret_cast<uint32_t *>(ctr + 2);
+  p.first_bad_step = reinterpret_cast<unsigned long long *>(ctr + 3);
   const double tau = 1.0 / a.omega;
   const double tp = a.trt_lambda * tau + (1.0 - a.trt_lambda);
   const double tm = (tp * tau - 0.5) / (tp - 0.5);
@@ -584,6 +585,8 @@ int aero_bind_workspace(AeroLattice *L, void *dptr, uint64_t bytes, void *stream
     return cudaMemcpyAsync(L->ws + off, src, n, cudaMemcpyHostToDevice, st);
   };
   CUDA_TRY(cudaMemsetAsync(L->ws, 0, L->lay.total, st));
+  // first divergent step starts at "never"
+  CUDA_TRY(cudaMemsetAsync(L->ws + L->lay.counters + 3 * sizeof(int64_t), 0xff, sizeof(int64_t), st));
   CUDA_TRY(up(L->lay.solid, L->solid.data(), L->solid.size()));
   CUDA_TRY(up(L->lay.lbits, L->lbits.data(), 4 * L->lbits.size()));
   CUDA_TRY(up(L->lay.loff, L->loff.data(), 4 * L->loff.size()));
@@ -717,6 +720,18 @@ int aero_status(AeroLattice *L, uint32_t *status, void *stream) {
   const int64_t *ctr = reinterpret_cast<const int64_t *>(L->ws + L->lay.counters);
   CUDA_TRY(cudaMemcpyAsync(status, ctr + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
+  return AERO_OK;
+}
+
+int aero_first_bad_step(AeroLattice *L, int64_t *step, void *stream) {
+  if (!L || !step) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
+  CUDA_TRY(cudaSetDevice(L->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  unsigned long long v = 0;
+  CUDA_TRY(cudaMemcpyAsync(&v, L->ws + L->lay.counters + 3 * sizeof(int64_t), sizeof(v), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  *step = v == ~0ull ? -1 : (int64_t)v;
   return AERO_OK;
 }
 

@@ -601,7 +601,10 @@ __global__ void __launch_bounds__(kStepBlock) k_step(const StepParams<typename S
     const Real rho = Real(1) + sum_dev<L>(d);
     const bool bad = !(rho > Real(0)) || !isfinite(rho);
     const unsigned badm = __ballot_sync(__activemask(), bad);
-    if (bad && (threadIdx.x & 31) == __ffs(badm) - 1) atomicOr(p.status, STATUS_NONFINITE_OR_NONPOSITIVE_RHO);
+    if (bad && (threadIdx.x & 31) == __ffs(badm) - 1) {
+      atomicOr(p.status, STATUS_NONFINITE_OR_NONPOSITIVE_RHO);
+      atomicMin(p.first_bad_step, (unsigned long long)(step_now + 1));
+    }
     if (p.feat & FEAT_THERMAL) {
       if (p.feat & FEAT_SCALAR_REDUCED) {
         using G = typename ScalarReduced<L>::Lat;

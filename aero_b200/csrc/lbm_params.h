@@ -86,6 +86,7 @@ struct StepParams {
   int64_t *step;        // device step counter (steps completed)
   int64_t *hist_base;   // step index stored in hist slot 0
   uint32_t *status;
+  unsigned long long *first_bad_step;  // smallest step whose state had a bad density
 
   // physics (Real)
   Real omega, u0, rho_in, rho_out, pert_amp, trt_lambda, trt_sminus;

@@ -151,6 +151,12 @@ class Engine:
             check("aero_status", self.lib.aero_status(self.h, ctypes.byref(v), self.stream()))
         return int(v.value)
 
+    def first_bad_step(self) -> int:
+        v = ctypes.c_int64()
+        with self.torch.cuda.device(self.device):
+            check("aero_first_bad_step", self.lib.aero_first_bad_step(self.h, ctypes.byref(v), self.stream()))
+        return int(v.value)
+
     # ------------------------------------------------------------------ timing
     def enable_timing(self, on: bool = True) -> None:
         check("aero_enable_timing", self.lib.aero_enable_timing(self.h, 1 if on else 0))

@@ -139,6 +139,10 @@ AERO_API int aero_read_profile(AeroLattice *lat, double *out, void *stream);
  * diagnostics.py:32-71).  Synchronous. */
 AERO_API int aero_status(AeroLattice *lat, uint32_t *status, void *stream);
 
+/* The first step (1-based, as counted by step_count) whose state had a
+ * non-finite or non-positive density, or -1 if none has.  Synchronous. */
+AERO_API int aero_first_bad_step(AeroLattice *lat, int64_t *step, void *stream);
+
 /* Steps taken (host mirror of the reference's step_count). */
 AERO_API int aero_step_count(const AeroLattice *lat, int64_t *steps);
 
