@@ -58,7 +58,8 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
         obj = OUT_DIR / (src.name + ".o")
         if not force and obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime, hdr_t):
             return obj
-        cmd = [nvcc, *NVCC_FLAGS, *ARCH, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+        extra = os.environ.get("AERO_NVCC_DEFINES", "").split()
+        cmd = [nvcc, *NVCC_FLAGS, *extra, *ARCH, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
         if src.suffix == ".cpp":
             cmd = [nvcc, "-x", "cu", *cmd[1:]]
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -216,10 +216,12 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   p.gbeta = (Real)(a.g_gravity * a.beta);
   p.T_ref = (Real)a.T_ref;
   for (int k = 0; k < 3; k++) p.center[k] = a.center[k];
-  for (int k = 0; k < 100; k++) p.mrt.Ae[k] = (Real)L->mrt.Ae[k];
-  for (int k = 0; k < 70; k++) p.mrt.Ce[k] = (Real)L->mrt.Ce[k];
-  for (int k = 0; k < 81; k++) p.mrt.Ao[k] = (Real)L->mrt.Ao[k];
-  for (int k = 0; k < 27; k++) p.mrt.Co[k] = (Real)L->mrt.Co[k];
+  // rows r >= 1 of the even block and all odd rows carry the 1/2 of the
+  // pair-basis inverse (f_i = (s + t) / 2), folded in here
+  for (int k = 0; k < 100; k++) p.mrt.Ae[k] = (Real)(L->mrt.Ae[k] * (k < 10 ? 1.0 : 0.5));
+  for (int k = 0; k < 70; k++) p.mrt.Ce[k] = (Real)(L->mrt.Ce[k] * (k < 7 ? 1.0 : 0.5));
+  for (int k = 0; k < 81; k++) p.mrt.Ao[k] = (Real)(L->mrt.Ao[k] * 0.5);
+  for (int k = 0; k < 27; k++) p.mrt.Co[k] = (Real)(L->mrt.Co[k] * 0.5);
   return p;
 }
 
@@ -373,7 +375,8 @@ int check_params(const AeroParams *a) {
   if (a->dims == 2 && a->nz != 1) return fail(AERO_ERR_INVALID, "nz must be 1 in 2D");
   if (a->nx < 3 || a->ny < 2 || a->nz < 1) return fail(AERO_ERR_INVALID, "grid too small (nx>=3, ny>=2)");
   if (a->ny > 65535 || a->nz > 65535) return fail(AERO_ERR_INVALID, "ny and nz must be <= 65535");
-  if ((int64_t)a->nx * a->ny * a->nz > ((int64_t)1 << 40)) return fail(AERO_ERR_INVALID, "grid too large");
+  if ((int64_t)a->nx * a->ny * a->nz >= ((int64_t)1 << 31) - 64)
+    return fail(AERO_ERR_UNSUPPORTED, "lattices are limited to 2^31 - 64 cells (32-bit cell indices)");
   if (a->storage < 0 || a->storage > 3) return fail(AERO_ERR_INVALID, "unknown storage %d", a->storage);
   if (a->collision < 0 || a->collision > 2) return fail(AERO_ERR_INVALID, "unknown collision %d", a->collision);
   if (!(a->omega > 0.0) || !std::isfinite(a->omega)) return fail(AERO_ERR_INVALID, "omega must be > 0");

@@ -33,16 +33,30 @@
 
 namespace aero {
 
-constexpr int kStepBlock = 128;
+#ifndef AERO_STEP_BLOCK
+#define AERO_STEP_BLOCK 128
+#endif
+#ifndef AERO_STEP_MINB
+#define AERO_STEP_MINB 1
+#endif
+constexpr int kStepBlock = AERO_STEP_BLOCK;  // threads along x per block
+constexpr int kStepMinBlocks = AERO_STEP_MINB;  // resident blocks per SM the step kernel is built for
 constexpr int kForceBlock = 128;
 constexpr int kFinalizeBlock = 256;
 
 __device__ __forceinline__ int wrap_n(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 __device__ __forceinline__ int clamp_n(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
 
+// Cell indices are 32-bit (the host limits a lattice to fewer than 2^31
+// cells); direction planes are addressed through warp-uniform base pointers.
 template <class Real>
-__device__ __forceinline__ int64_t cell_index(const StepParams<Real> &p, int x, int y, int z) {
-  return ((int64_t)z * p.ny + y) * p.nx + x;
+__device__ __forceinline__ uint32_t cell_index(const StepParams<Real> &p, int x, int y, int z) {
+  return ((uint32_t)z * (uint32_t)p.ny + (uint32_t)y) * (uint32_t)p.nx + (uint32_t)x;
+}
+
+template <class T>
+__device__ __forceinline__ T *plane(T *base, int i, int64_t cs) {
+  return base + (int64_t)i * cs;
 }
 
 // Link-cell slot of cell (x, y, z), or -1 when the cell has no link.
@@ -190,14 +204,29 @@ __device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, 
   using SO = StoreOps<S>;
   const S *P = static_cast<const S *>(p.P);
   const int64_t cs = p.cs;
+  // Source of direction i is (x - ex, y - ey, z - ez) with periodic wrap: per
+  // axis only three values occur, so each source index is one 3-way add.
+  const uint32_t nx = p.nx, nxy = (uint32_t)p.nx * (uint32_t)p.ny;
+  const uint32_t xs_p = x == 0 ? nx - 1 : x - 1;            // ex = +1
+  const uint32_t xs_m = x == p.nx - 1 ? 0 : x + 1;          // ex = -1
+  const uint32_t ry_0 = (uint32_t)y * nx;
+  const uint32_t ry_p = (y == 0 ? p.ny - 1 : y - 1) * nx;   // ey = +1
+  const uint32_t ry_m = (y == p.ny - 1 ? 0 : y + 1) * nx;   // ey = -1
+  uint32_t pz_0 = 0, pz_p = 0, pz_m = 0;
+  if constexpr (L::DIMS == 3) {
+    pz_0 = (uint32_t)z * nxy;
+    pz_p = (z == 0 ? p.nz - 1 : z - 1) * nxy;
+    pz_m = (z == p.nz - 1 ? 0 : z + 1) * nxy;
+  }
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    const int xs = wrap_n(x - Dir<L, i>::x, p.nx);
-    const int ys = wrap_n(y - Dir<L, i>::y, p.ny);
-    const int zs = L::DIMS == 3 ? wrap_n(z - Dir<L, i>::z, p.nz) : 0;
-    d[i] = SO::template load<i, L>(P, i * cs + cell_index(p, xs, ys, zs));
+    constexpr int ex = Dir<L, i>::x, ey = Dir<L, i>::y, ez = Dir<L, i>::z;
+    const uint32_t src = (ex > 0 ? xs_p : (ex < 0 ? xs_m : (uint32_t)x)) +
+                         (ey > 0 ? ry_p : (ey < 0 ? ry_m : ry_0)) +
+                         (ez > 0 ? pz_p : (ez < 0 ? pz_m : pz_0));
+    d[i] = SO::template load<i, L>(plane(P, i, cs), src);
   });
-  const int64_t c = cell_index(p, x, y, z);
+  const uint32_t c = cell_index(p, x, y, z);
   if constexpr (L::DIMS == 3) {
     // Guo-style uniform body force on fluid cells (ibm_guo.py:263-301)
     if ((p.feat & FEAT_BODY_FORCE) && !p.solid[c]) {
@@ -234,19 +263,19 @@ __device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, 
         if constexpr (i > 0) {
           if ((mask >> i) & 1u) {
             constexpr int o = L::opp[i];
-            const Real fi = SO::template load<i, L>(P, i * cs + c);
+            const Real fi = SO::template load<i, L>(plane(P, i, cs), c);
             if (!bouzidi) {
               d[o] = fi;
             } else {
               const Real q = (Real)__ldg(p.lc_q + slot * L::Q + i);
               if (q < Real(0.5)) {
-                const Real fo = SO::template load<o, L>(P, o * cs + c);
+                const Real fo = SO::template load<o, L>(plane(P, o, cs), c);
                 d[o] = Real(2) * q * fi + (Real(1) - Real(2) * q) * fo;
               } else {
                 const int xn = clamp_n(x + Dir<L, o>::x, p.nx);
                 const int yn = clamp_n(y + Dir<L, o>::y, p.ny);
                 const int zn = L::DIMS == 3 ? clamp_n(z + Dir<L, o>::z, p.nz) : 0;
-                const Real fn = SO::template load<i, L>(P, i * cs + cell_index(p, xn, yn, zn));
+                const Real fn = SO::template load<i, L>(plane(P, i, cs), cell_index(p, xn, yn, zn));
                 const Real inv2q = Real(1) / (Real(2) * q);
                 d[o] = inv2q * fi + (Real(1) - inv2q) * fn;
               }
@@ -317,13 +346,13 @@ __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int
   }
   if (p.feat & FEAT_THERMAL) {
     // thermal.py:103-124 / :206-222 with the order of solver.py:432-439
-    const int64_t c = cell_index(p, x, y, z);
+    const uint32_t c = cell_index(p, x, y, z);
     Real T = 0;
     if (p.feat & FEAT_SCALAR_REDUCED) {
       using G = typename ScalarReduced<L>::Lat;
-      static_for<G::Q>([&](auto ic) { T += p.g[decltype(ic)::value * p.cs + c]; });
+      static_for<G::Q>([&](auto ic) { T += plane(p.g, decltype(ic)::value, p.cs)[c]; });
     } else {
-      static_for<L::Q>([&](auto ic) { T += p.g[decltype(ic)::value * p.cs + c]; });
+      static_for<L::Q>([&](auto ic) { T += plane(p.g, decltype(ic)::value, p.cs)[c]; });
     }
     Real drho = 0, jx = 0, jy = 0, jz = 0;
     static_for<L::Q>([&](auto ic) {
@@ -356,13 +385,13 @@ __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int
 // :177-266, :273-344).  Edge planes and solid cells keep the base rate.
 // --------------------------------------------------------------------------
 template <class L, class Real>
-__device__ __forceinline__ Real les_omega(const StepParams<Real> &p, int x, int y, int z, int64_t c, bool solid) {
+__device__ __forceinline__ Real les_omega(const StepParams<Real> &p, int x, int y, int z, uint32_t c, bool solid) {
   Real nu_t = Real(0);
   bool interior = x >= 1 && x <= p.nx - 2 && y >= 1 && y <= p.ny - 2;
   if constexpr (L::DIMS == 3) interior = interior && z >= 1 && z <= p.nz - 2;
   if (interior && !solid) {
     const Real *UX = p.U, *UY = p.U + p.cs, *UZ = p.U + 2 * p.cs;
-    const int64_t sx = 1, sy = p.nx;
+    const uint32_t sx = 1, sy = p.nx;
     Real g[3][3];
     g[0][0] = Real(0.5) * (UX[c + sx] - UX[c - sx]);
     g[0][1] = Real(0.5) * (UX[c + sy] - UX[c - sy]);
@@ -370,7 +399,7 @@ __device__ __forceinline__ Real les_omega(const StepParams<Real> &p, int x, int 
     g[1][1] = Real(0.5) * (UY[c + sy] - UY[c - sy]);
     g[0][2] = g[1][2] = g[2][0] = g[2][1] = g[2][2] = Real(0);
     if constexpr (L::DIMS == 3) {
-      const int64_t sz = (int64_t)p.nx * p.ny;
+      const uint32_t sz = (uint32_t)p.nx * (uint32_t)p.ny;
       g[0][2] = Real(0.5) * (UX[c + sz] - UX[c - sz]);
       g[1][2] = Real(0.5) * (UY[c + sz] - UY[c - sz]);
       g[2][0] = Real(0.5) * (UZ[c + sx] - UZ[c - sx]);
@@ -434,7 +463,7 @@ __device__ __forceinline__ Real les_omega(const StepParams<Real> &p, int x, int 
 // kernels3d_mrt.py:24-82.  Solid cells relax toward feq(rho, 0).
 // --------------------------------------------------------------------------
 template <class L, class Real, int COLL>
-__device__ __forceinline__ void collide(const StepParams<Real> &p, Real (&d)[L::Q], bool solid, Real om,
+__device__ __forceinline__ Real collide(const StepParams<Real> &p, Real (&d)[L::Q], bool solid, Real om,
                                         bool per_cell_omega) {
   Real drho = 0, jx = 0, jy = 0, jz = 0;
   static_for<L::Q>([&](auto ic) {
@@ -494,12 +523,14 @@ __device__ __forceinline__ void collide(const StepParams<Real> &p, Real (&d)[L::
       for (int k = 0; k < NO; k++) acc += p.mrt.Ao[r * 9 + k] * t[k];
       tp[r] = acc;
     }
+    // rows 1.. of the even block and the odd block carry the factor 1/2 of
+    // f_i = (s + t) / 2, f_opp = (s - t) / 2 (folded in on the host)
     d[0] = sp[0];
     static_for<NO>([&](auto pc) {
       constexpr int k = decltype(pc)::value;
       constexpr int i = L::pair[k], o = L::opp[L::pair[k]];
-      d[i] = Real(0.5) * (sp[k + 1] + tp[k]);
-      d[o] = Real(0.5) * (sp[k + 1] - tp[k]);
+      d[i] = sp[k + 1] + tp[k];
+      d[o] = sp[k + 1] - tp[k];
     });
     (void)om;
     (void)per_cell_omega;
@@ -535,6 +566,7 @@ __device__ __forceinline__ void collide(const StepParams<Real> &p, Real (&d)[L::
       });
     }
   }
+  return rho;
 }
 
 // Scalar lattice collision + push (thermal.py:47-100, :149-203).  Rows y = 0
@@ -542,12 +574,12 @@ __device__ __forceinline__ void collide(const StepParams<Real> &p, Real (&d)[L::
 // w_i T_wall, so pushes into them are skipped and the row's own thread writes
 // them.
 template <class L, class G, class Real>
-__device__ __forceinline__ void scalar_step(const StepParams<Real> &p, int x, int y, int z, int64_t c, bool solid,
+__device__ __forceinline__ void scalar_step(const StepParams<Real> &p, int x, int y, int z, uint32_t c, bool solid,
                                             const ScalarCtx<Real> &sc, Real cs2inv) {
   const Real oT = p.omega_T, T = sc.T;
   static_for<G::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    const Real gi = p.g[i * p.cs + c];
+    const Real gi = plane(p.g, i, p.cs)[c];
     Real gp;
     if (solid) {
       gp = Real(Dir<G, i>::w) * T;
@@ -559,13 +591,13 @@ __device__ __forceinline__ void scalar_step(const StepParams<Real> &p, int x, in
     const int xd = wrap_n(x + Dir<G, i>::x, p.nx);
     const int yd = wrap_n(y + Dir<G, i>::y, p.ny);
     const int zd = L::DIMS == 3 ? wrap_n(z + Dir<G, i>::z, p.nz) : 0;
-    if (yd != 0 && yd != p.ny - 1) p.gn[i * p.cs + cell_index(p, xd, yd, zd)] = gp;
+    if (yd != 0 && yd != p.ny - 1) plane(p.gn, i, p.cs)[cell_index(p, xd, yd, zd)] = gp;
   });
   if (y == 0 || y == p.ny - 1) {
     const Real Tw = y == 0 ? p.T_hot : p.T_cold;
     static_for<G::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      p.gn[i * p.cs + c] = Real(Dir<G, i>::w) * Tw;
+      plane(p.gn, i, p.cs)[c] = Real(Dir<G, i>::w) * Tw;
     });
   }
 }
@@ -578,33 +610,26 @@ __device__ __forceinline__ void scalar_step(const StepParams<Real> &p, int x, in
 // FROM_STATE: P holds a state (deviations) to be collided as is (used after
 // the host sets f, and to start from an initial state).
 template <class L, class S, int COLL, bool FROM_STATE>
-__global__ void __launch_bounds__(kStepBlock) k_step(const StepParams<typename StoreOps<S>::Real> p) {
+__global__ void __launch_bounds__(kStepBlock, kStepMinBlocks) k_step(const StepParams<typename StoreOps<S>::Real> p) {
   using Real = typename StoreOps<S>::Real;
   using SO = StoreOps<S>;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z;
   if (x >= p.nx) return;
-  const int64_t c = cell_index(p, x, y, z);
+  const uint32_t c = cell_index(p, x, y, z);
   const bool solid = p.solid[c];
   Real d[L::Q];
   ScalarCtx<Real> sc;
+  int64_t step_now = 0;
   if constexpr (FROM_STATE) {
     const S *P = static_cast<const S *>(p.P);
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      d[i] = SO::template load<i, L>(P, i * p.cs + c);
+      d[i] = SO::template load<i, L>(plane(P, i, p.cs), c);
     });
   } else {
-    const int64_t step_now = *p.step;
+    step_now = *p.step;
     full_state<L, S, Real>(p, x, y, z, step_now, d, p.prevn, &sc);
-    // divergence guard (diagnostics.py:32-71): non-finite or non-positive rho
-    const Real rho = Real(1) + sum_dev<L>(d);
-    const bool bad = !(rho > Real(0)) || !isfinite(rho);
-    const unsigned badm = __ballot_sync(__activemask(), bad);
-    if (bad && (threadIdx.x & 31) == __ffs(badm) - 1) {
-      atomicOr(p.status, STATUS_NONFINITE_OR_NONPOSITIVE_RHO);
-      atomicMin(p.first_bad_step, (unsigned long long)(step_now + 1));
-    }
     if (p.feat & FEAT_THERMAL) {
       if (p.feat & FEAT_SCALAR_REDUCED) {
         using G = typename ScalarReduced<L>::Lat;
@@ -617,11 +642,23 @@ __global__ void __launch_bounds__(kStepBlock) k_step(const StepParams<typename S
   Real om = p.omega;
   const bool les = (COLL != COLL_MRT) && (p.feat & FEAT_LES);
   if (les) om = les_omega<L>(p, x, y, z, c, solid);
-  collide<L, Real, COLL>(p, d, solid, om, les);
+  const Real rho = collide<L, Real, COLL>(p, d, solid, om, les);
+  if constexpr (!FROM_STATE) {
+    // divergence guard (diagnostics.py:32-71): non-finite or non-positive rho
+    // of the state; one lane per warp reports, and only until it is recorded
+    const bool bad = !(rho > Real(0)) || !isfinite(rho);
+    const unsigned badm = __ballot_sync(__activemask(), bad);
+    if (bad && (threadIdx.x & 31) == __ffs(badm) - 1) {
+      if (!(*(volatile uint32_t *)p.status & STATUS_NONFINITE_OR_NONPOSITIVE_RHO))
+        atomicOr(p.status, STATUS_NONFINITE_OR_NONPOSITIVE_RHO);
+      if (*(volatile unsigned long long *)p.first_bad_step > (unsigned long long)(step_now + 1))
+        atomicMin(p.first_bad_step, (unsigned long long)(step_now + 1));
+    }
+  }
   S *Pn = static_cast<S *>(p.Pn);
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    SO::template store<i, L>(Pn, i * p.cs + c, d[i]);
+    SO::template store<i, L>(plane(Pn, i, p.cs), c, d[i]);
   });
 }
 
@@ -634,13 +671,13 @@ __global__ void __launch_bounds__(kStepBlock) k_moments(const StepParams<typenam
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z;
   if (x >= p.nx) return;
-  const int64_t c = cell_index(p, x, y, z);
+  const uint32_t c = cell_index(p, x, y, z);
   Real d[L::Q];
   if constexpr (FROM_STATE) {
     const S *P = static_cast<const S *>(p.P);
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      d[i] = SO::template load<i, L>(P, i * p.cs + c);
+      d[i] = SO::template load<i, L>(plane(P, i, p.cs), c);
     });
   } else {
     full_state<L, S, Real>(p, x, y, z, *p.step, d, nullptr, nullptr);
@@ -692,10 +729,10 @@ __global__ void __launch_bounds__(kForceBlock) k_forces(const StepParams<typenam
 #pragma unroll
   for (int j = 0; j < 12; j++) acc[j] = 0.0;
   if (k < p.n_lc) {
-    const int64_t c = p.lc_cell[k];
-    const int x = (int)(c % p.nx);
-    const int y = (int)((c / p.nx) % p.ny);
-    const int z = (int)(c / ((int64_t)p.nx * p.ny));
+    const uint32_t c = (uint32_t)p.lc_cell[k];
+    const int x = (int)(c % (uint32_t)p.nx);
+    const int y = (int)((c / (uint32_t)p.nx) % (uint32_t)p.ny);
+    const int z = (int)(c / ((uint32_t)p.nx * (uint32_t)p.ny));
     Real d[L::Q];
     full_state<L, S, Real>(p, x, y, z, *p.step, d, nullptr, nullptr);
     const S *P = static_cast<const S *>(p.P);
@@ -703,7 +740,7 @@ __global__ void __launch_bounds__(kForceBlock) k_forces(const StepParams<typenam
     double drho = 0, jx = 0, jy = 0, jz = 0;
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      fp[i] = (double)SO::template load<i, L>(P, i * p.cs + c);
+      fp[i] = (double)SO::template load<i, L>(plane(P, i, p.cs), c);
       drho += fp[i];
       jx += Dir<L, i>::x * fp[i];
       jy += Dir<L, i>::y * fp[i];
@@ -796,27 +833,27 @@ __global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const StepParams<Re
 // perturbation phase uses.  RAW: P already holds a state.
 template <class L, class S, bool RAW>
 __global__ void __launch_bounds__(kStepBlock) k_state_out(const StepParams<typename StoreOps<S>::Real> p,
-                                                          double *out, int step_delta, int z0, int64_t plane) {
+                                                          double *out, int step_delta, int z0, int64_t out_plane) {
   using Real = typename StoreOps<S>::Real;
   using SO = StoreOps<S>;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z + z0;
   if (x >= p.nx) return;
-  const int64_t c = cell_index(p, x, y, z);
+  const uint32_t c = cell_index(p, x, y, z);
   Real d[L::Q];
   if constexpr (RAW) {
     const S *P = static_cast<const S *>(p.P);
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      d[i] = SO::template load<i, L>(P, i * p.cs + c);
+      d[i] = SO::template load<i, L>(plane(P, i, p.cs), c);
     });
   } else {
     full_state<L, S, Real>(p, x, y, z, *p.step + step_delta, d, nullptr, nullptr);
   }
-  const int64_t oc = c - (int64_t)z0 * p.ny * p.nx;
+  const int64_t oc = (int64_t)c - (int64_t)z0 * p.ny * p.nx;
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    out[(int64_t)i * plane + oc] = Dir<L, i>::w + (double)d[i];
+    out[(int64_t)i * out_plane + oc] = Dir<L, i>::w + (double)d[i];
   });
 }
 
@@ -829,10 +866,10 @@ __global__ void __launch_bounds__(kStepBlock) k_load_state(const StepParams<type
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z;
   if (x >= p.nx) return;
-  const int64_t c = cell_index(p, x, y, z);
+  const uint32_t c = cell_index(p, x, y, z);
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    SO::template store<i, L>(dst, i * p.cs + c, (Real)(in[(int64_t)i * p.ncells + c] - Dir<L, i>::w));
+    SO::template store<i, L>(plane(dst, i, p.cs), c, (Real)(in[(int64_t)i * p.ncells + c] - Dir<L, i>::w));
   });
 }
 

@@ -7,6 +7,8 @@
 //                    FP16 subnormal range; |d_i / w_i| < 1000 before overflow)
 //   __nv_bfloat16  : d_i as is (8-bit exponent, no scaling needed)
 // Arithmetic is always done in Real (float, or double for double storage).
+// load/store take the base of one direction plane (a warp-uniform pointer)
+// and a 32-bit cell index, so each access is one wide multiply-add.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -20,28 +22,28 @@ template <class S> struct StoreOps;
 template <> struct StoreOps<float> {
   using Real = float;
   template <int I, class L>
-  static __device__ __forceinline__ float load(const float *p, int64_t o) { return __ldg(p + o); }
+  static __device__ __forceinline__ float load(const float *p, uint32_t o) { return __ldg(p + o); }
   template <int I, class L>
-  static __device__ __forceinline__ void store(float *p, int64_t o, float v) { p[o] = v; }
+  static __device__ __forceinline__ void store(float *p, uint32_t o, float v) { p[o] = v; }
 };
 
 template <> struct StoreOps<double> {
   using Real = double;
   template <int I, class L>
-  static __device__ __forceinline__ double load(const double *p, int64_t o) { return __ldg(p + o); }
+  static __device__ __forceinline__ double load(const double *p, uint32_t o) { return __ldg(p + o); }
   template <int I, class L>
-  static __device__ __forceinline__ void store(double *p, int64_t o, double v) { p[o] = v; }
+  static __device__ __forceinline__ void store(double *p, uint32_t o, double v) { p[o] = v; }
 };
 
 template <> struct StoreOps<__half> {
   using Real = float;
   template <int I, class L>
-  static __device__ __forceinline__ float load(const __half *p, int64_t o) {
+  static __device__ __forceinline__ float load(const __half *p, uint32_t o) {
     constexpr float s = float(L::w[I] / 64.0);
     return __half2float(__ldg(p + o)) * s;
   }
   template <int I, class L>
-  static __device__ __forceinline__ void store(__half *p, int64_t o, float v) {
+  static __device__ __forceinline__ void store(__half *p, uint32_t o, float v) {
     constexpr float s = float(64.0 / L::w[I]);
     p[o] = __float2half_rn(v * s);
   }
@@ -50,11 +52,11 @@ template <> struct StoreOps<__half> {
 template <> struct StoreOps<__nv_bfloat16> {
   using Real = float;
   template <int I, class L>
-  static __device__ __forceinline__ float load(const __nv_bfloat16 *p, int64_t o) {
+  static __device__ __forceinline__ float load(const __nv_bfloat16 *p, uint32_t o) {
     return __bfloat162float(__ldg(p + o));
   }
   template <int I, class L>
-  static __device__ __forceinline__ void store(__nv_bfloat16 *p, int64_t o, float v) {
+  static __device__ __forceinline__ void store(__nv_bfloat16 *p, uint32_t o, float v) {
     p[o] = __float2bfloat16_rn(v);
   }
 };
