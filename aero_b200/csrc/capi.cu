@@ -46,8 +46,8 @@ constexpr uint64_t kAlign = 256;
 uint64_t align_up(uint64_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
 struct Layout {
-  uint64_t P[2], solid, lbits, loff, lc_mask, lc_q, lc_cell, lc_prof, prof_off, prev[2], g[2], U, cs_cell,
-      partials, hist, prof_out, counters, total;
+  uint64_t P[2], solid, lbits, loff, lc_mask, lc_q, lc_cell, lc_contrib, prof_off, force_const, prof_const,
+      prev[2], g[2], U, cs_cell, hist, prof_out, counters, total;
 };
 
 struct WTab {
@@ -90,7 +90,8 @@ struct AeroLattice {
   AeroParams prm;
   int Q = 0, Qg = 0;
   int64_t ncells = 0, cs = 0, nwords = 0, prev_plane = 0;
-  int nwx = 0, nprof = 0, hist_cap = 4096, n_force_blocks = 0;
+  int nwx = 0, nprof = 0, hist_cap = 4096;
+  std::vector<double> force_const, prof_const;  // rest-weight parts of forces / profile
   uint32_t feat = 0;
   // host geometry tables (kept until bind)
   std::vector<uint8_t> solid;
@@ -176,14 +177,14 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   p.U = reinterpret_cast<const Real *>(ws + L->lay.U);
   p.Uw = reinterpret_cast<Real *>(ws + L->lay.U);
   p.cs_cell = reinterpret_cast<const Real *>(ws + L->lay.cs_cell);
-  p.partials = reinterpret_cast<double *>(ws + L->lay.partials);
-  p.lc_prof = reinterpret_cast<double *>(ws + L->lay.lc_prof);
+  p.lc_contrib = reinterpret_cast<double *>(ws + L->lay.lc_contrib);
+  p.force_const = reinterpret_cast<const double *>(ws + L->lay.force_const);
+  p.prof_const = reinterpret_cast<const double *>(ws + L->lay.prof_const);
   p.prof_off = reinterpret_cast<const int32_t *>(ws + L->lay.prof_off);
   p.hist = reinterpret_cast<double *>(ws + L->lay.hist);
   p.prof_out = reinterpret_cast<double *>(ws + L->lay.prof_out);
   p.nprof = L->nprof;
   p.hist_cap = L->hist_cap;
-  p.n_force_blocks = L->n_force_blocks;
   p.want_profile = 1;
   int64_t *ctr = reinterpret_cast<int64_t *>(ws + L->lay.counters);
   p.step = ctr;
@@ -232,8 +233,8 @@ dim3 cell_grid(const AeroLattice *L) {
 bool les_active(const AeroLattice *L) { return (L->feat & FEAT_LES) != 0; }
 
 // Launches one step with buffer parity `cur` on stream st.  With timing on,
-// events bracket the force kernels (forces + finalize) and the fused step
-// (moments pass + step kernel).
+// events bracket the fused step (moments pass + step kernel, which also
+// computes the link-cell force contributions) and the force finalisation.
 template <class Real>
 int launch_step(AeroLattice *L, int cur, cudaStream_t st, bool timed = false) {
   const Ops<Real> *ops = get_ops<Real>(L);
@@ -241,23 +242,21 @@ int launch_step(AeroLattice *L, int cur, cudaStream_t st, bool timed = false) {
   const dim3 grid = cell_grid(L);
   cudaEvent_t *e = nullptr;
   if (timed) {
-    const size_t need = 4 * (size_t)(L->timed_steps + 1);
+    const size_t need = 3 * (size_t)(L->timed_steps + 1);
     while (L->ev.size() < need) {
       cudaEvent_t x;
       CUDA_TRY(cudaEventCreate(&x));
       L->ev.push_back(x);
     }
-    e = &L->ev[4 * (size_t)L->timed_steps];
+    e = &L->ev[3 * (size_t)L->timed_steps];
     CUDA_TRY(cudaEventRecord(e[0], st));
   }
-  if (L->n_force_blocks > 0) CUDA_TRY(ops->forces(p, L->n_force_blocks, st));
-  if (timed) CUDA_TRY(cudaEventRecord(e[1], st));
   if (les_active(L)) CUDA_TRY(ops->moments(p, false, grid, st));
   CUDA_TRY(ops->step(p, false, grid, st));
-  if (timed) CUDA_TRY(cudaEventRecord(e[2], st));
+  if (timed) CUDA_TRY(cudaEventRecord(e[1], st));
   CUDA_TRY(ops->finalize(p, st));
   if (timed) {
-    CUDA_TRY(cudaEventRecord(e[3], st));
+    CUDA_TRY(cudaEventRecord(e[2], st));
     L->timed_steps++;
   }
   return AERO_OK;
@@ -515,7 +514,33 @@ int aero_set_geometry(AeroLattice *L, const uint8_t *solid, const int32_t *links
     }
   }
   if (n_links > 0) L->feat |= FEAT_OBSTACLE_BB; else L->feat &= ~FEAT_OBSTACLE_BB;
-  L->n_force_blocks = (int)((L->lc_cell.size() + kForceBlock - 1) / kForceBlock);
+  // rest-weight part of the momentum exchange: each link contributes
+  // e_i (w_i + w_opp) to F and to its pressure part, and r x that to M
+  L->force_const.assign(12, 0.0);
+  L->prof_const.assign(3 * (size_t)L->nprof, 0.0);
+  for (size_t k = 0; k < L->lc_cell.size(); k++) {
+    const int64_t c = L->lc_cell[k];
+    const double x = (double)(c % a.nx), y = (double)((c / a.nx) % a.ny), z = (double)(c / ((int64_t)a.nx * a.ny));
+    const double r[3] = {x - a.center[0], y - a.center[1], z - a.center[2]};
+    const int bin = a.dims == 3 ? (int)z : (int)y;
+    for (int i = 1; i < L->Q; i++) {
+      if (!((L->lc_mask[k] >> i) & 1u)) continue;
+      double e[3], w2;
+      if (a.dims == 2) {
+        e[0] = D2Q9::ex[i]; e[1] = D2Q9::ey[i]; e[2] = 0.0; w2 = 2.0 * D2Q9::w[i];
+      } else {
+        e[0] = D3Q19::ex[i]; e[1] = D3Q19::ey[i]; e[2] = D3Q19::ez[i]; w2 = 2.0 * D3Q19::w[i];
+      }
+      for (int dd = 0; dd < 3; dd++) {
+        L->force_const[dd] += e[dd] * w2;
+        L->force_const[3 + dd] += e[dd] * w2;
+        L->prof_const[3 * bin + dd] += e[dd] * w2;
+      }
+      L->force_const[9] += (r[1] * e[2] - r[2] * e[1]) * w2;
+      L->force_const[10] += (r[2] * e[0] - r[0] * e[2]) * w2;
+      L->force_const[11] += (r[0] * e[1] - r[1] * e[0]) * w2;
+    }
+  }
   L->cs_cell.clear();
   L->feat &= ~FEAT_LES_CS_FIELD;
   if ((L->feat & FEAT_LES) && a.van_driest && phi) {
@@ -545,15 +570,16 @@ int aero_set_geometry(AeroLattice *L, const uint8_t *solid, const int32_t *links
   y.lc_mask = take(4 * nlc);
   y.lc_q = take(4 * nlc * L->Q);
   y.lc_cell = take(8 * nlc);
-  y.lc_prof = take(24 * nlc);
+  y.lc_contrib = take(96 * nlc);
   y.prof_off = take(4 * (L->nprof + 1));
+  y.force_const = take(8 * 12);
+  y.prof_const = take(24 * (uint64_t)L->nprof);
   y.prev[0] = take(rb * L->Q * L->prev_plane);
   y.prev[1] = take(rb * L->Q * L->prev_plane);
   y.g[0] = take(L->Qg ? rb * L->Qg * L->cs : 0);
   y.g[1] = take(L->Qg ? rb * L->Qg * L->cs : 0);
   y.U = take((L->feat & FEAT_LES) ? rb * 3 * L->cs : 0);
   y.cs_cell = take(L->cs_cell.empty() ? 0 : rb * L->cs);
-  y.partials = take(8 * 12 * std::max(L->n_force_blocks, 1));
   y.hist = take(8 * 12 * (uint64_t)L->hist_cap);
   y.prof_out = take(24 * (uint64_t)L->nprof);
   y.counters = take(64);
@@ -597,6 +623,8 @@ int aero_bind_workspace(AeroLattice *L, void *dptr, uint64_t bytes, void *stream
   CUDA_TRY(up(L->lay.lc_q, L->lc_q.data(), 4 * L->lc_q.size()));
   CUDA_TRY(up(L->lay.lc_cell, L->lc_cell.data(), 8 * L->lc_cell.size()));
   CUDA_TRY(up(L->lay.prof_off, L->prof_off.data(), 4 * L->prof_off.size()));
+  CUDA_TRY(up(L->lay.force_const, L->force_const.data(), 8 * L->force_const.size()));
+  CUDA_TRY(up(L->lay.prof_const, L->prof_const.data(), 8 * L->prof_const.size()));
   if (!L->cs_cell.empty()) {
     if (is_f64(L)) {
       CUDA_TRY(up(L->lay.cs_cell, L->cs_cell.data(), 8 * L->cs_cell.size()));
@@ -659,13 +687,12 @@ int aero_kernel_times(AeroLattice *L, double *step_ms, double *forces_ms, int64_
   CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
   double a = 0.0, b = 0.0;
   for (int64_t k = 0; k < L->timed_steps; k++) {
-    float t0 = 0.f, t1 = 0.f, t2 = 0.f;
-    cudaEvent_t *e = &L->ev[4 * (size_t)k];
+    float t0 = 0.f, t1 = 0.f;
+    cudaEvent_t *e = &L->ev[3 * (size_t)k];
     CUDA_TRY(cudaEventElapsedTime(&t0, e[0], e[1]));
     CUDA_TRY(cudaEventElapsedTime(&t1, e[1], e[2]));
-    CUDA_TRY(cudaEventElapsedTime(&t2, e[2], e[3]));
-    a += t1;
-    b += t0 + t2;
+    a += t0;
+    b += t1;
   }
   *step_ms = a;
   *forces_ms = b;

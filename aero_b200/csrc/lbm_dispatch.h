@@ -11,7 +11,6 @@ struct Ops {
   // grid covers (ceil(nx / kStepBlock), ny, nz)
   cudaError_t (*step)(const StepParams<Real> &, bool from_state, dim3 grid, cudaStream_t);
   cudaError_t (*moments)(const StepParams<Real> &, bool from_state, dim3 grid, cudaStream_t);
-  cudaError_t (*forces)(const StepParams<Real> &, int nblocks, cudaStream_t);
   cudaError_t (*finalize)(const StepParams<Real> &, cudaStream_t);
   // grid.z = planes written, starting at plane z0; out holds (Q, grid.z, ny, nx)
   cudaError_t (*state_out)(const StepParams<Real> &, double *out, int step_delta, bool raw, int z0, dim3 grid,

@@ -24,10 +24,6 @@ struct Launch {
       k_moments<L, S, false><<<grid, kStepBlock, 0, st>>>(p);
     return cudaGetLastError();
   }
-  static cudaError_t forces(const StepParams<Real> &p, int nblocks, cudaStream_t st) {
-    k_forces<L, S><<<nblocks, kForceBlock, 0, st>>>(p);
-    return cudaGetLastError();
-  }
   static cudaError_t finalize(const StepParams<Real> &p, cudaStream_t st) {
     k_finalize<Real><<<1, kFinalizeBlock, 0, st>>>(p);
     return cudaGetLastError();
@@ -46,7 +42,7 @@ struct Launch {
     k_load_state<L, S><<<grid, kStepBlock, 0, st>>>(p, in, static_cast<S *>(dst));
     return cudaGetLastError();
   }
-  static constexpr Ops<Real> table = {&step, &moments, &forces, &finalize, &state_out, &load_state,
+  static constexpr Ops<Real> table = {&step, &moments, &finalize, &state_out, &load_state,
                                       (int)sizeof(S)};
 };
 

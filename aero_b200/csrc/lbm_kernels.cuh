@@ -37,11 +37,10 @@ namespace aero {
 #define AERO_STEP_BLOCK 128
 #endif
 #ifndef AERO_STEP_MINB
-#define AERO_STEP_MINB 1
+#define AERO_STEP_MINB 8
 #endif
 constexpr int kStepBlock = AERO_STEP_BLOCK;  // threads along x per block
 constexpr int kStepMinBlocks = AERO_STEP_MINB;  // resident blocks per SM the step kernel is built for
-constexpr int kForceBlock = 128;
 constexpr int kFinalizeBlock = 256;
 
 __device__ __forceinline__ int wrap_n(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
@@ -606,11 +605,75 @@ __device__ __forceinline__ void scalar_step(const StepParams<Real> &p, int x, in
 // Kernels
 // --------------------------------------------------------------------------
 
+// Momentum-exchange force, pressure/viscous split and moment contributions
+// of the links of one cell (forces.py:15-127, forces3d.py:8-131): for each
+// link i, f_pre[i] + f_post[opp i] with f_pre = P at the cell and f_post = its
+// post-BC state d; the split uses feq of the f_pre moments at the cell.  The
+// rest-weight part of every term (2 w_i e_i, and r x 2 w_i e_i) is constant
+// and added once per step by k_finalize, so only deviations are summed here.
+template <class L, class S, class Real>
+__device__ __forceinline__ void link_cell_forces(const StepParams<Real> &p, int x, int y, int z, uint32_t c,
+                                                 int64_t slot, const Real (&d)[L::Q]) {
+  using SO = StoreOps<S>;
+  const S *P = static_cast<const S *>(p.P);
+  Real drho = 0, jx = 0, jy = 0, jz = 0;
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    const Real v = SO::template load<i, L>(plane(P, i, p.cs), c);
+    drho += v;
+    if (Dir<L, i>::x) jx += Dir<L, i>::x * v;
+    if (Dir<L, i>::y) jy += Dir<L, i>::y * v;
+    if (Dir<L, i>::z) jz += Dir<L, i>::z * v;
+  });
+  const Real rho = Real(1) + drho;
+  const Real inv = rho > Real(0) ? Real(1) / rho : Real(0);
+  const Real ux = jx * inv, uy = jy * inv, uz = jz * inv, usq = ux * ux + uy * uy + uz * uz;
+  const uint32_t mask = __ldg(p.lc_mask + slot);
+  const Real rx = Real(x - p.center[0]), ry = Real(y - p.center[1]), rz = Real(z - p.center[2]);
+  Real acc[12];
+#pragma unroll
+  for (int j = 0; j < 12; j++) acc[j] = Real(0);
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    if constexpr (i > 0) {
+      if ((mask >> i) & 1u) {
+        constexpr int o = L::opp[i];
+        constexpr Real ex = Dir<L, i>::x, ey = Dir<L, i>::y, ez = Dir<L, i>::z;
+        const Real fi = SO::template load<i, L>(plane(P, i, p.cs), c);
+        const Real eui = ex * ux + ey * uy + ez * uz;
+        const Real quad = Real(4.5) * eui * eui - Real(1.5) * usq;
+        const Real deq_i = Real(Dir<L, i>::w) * (drho + rho * (Real(3) * eui + quad));
+        const Real deq_o = Real(Dir<L, o>::w) * (drho + rho * (Real(-3) * eui + quad));
+        const Real din = d[o];
+        const Real mom = fi + din;
+        const Real mp = deq_i + deq_o;
+        const Real mv = (fi - deq_i) + (din - deq_o);
+        acc[0] += ex * mom;
+        acc[1] += ey * mom;
+        acc[2] += ez * mom;
+        acc[3] += ex * mp;
+        acc[4] += ey * mp;
+        acc[5] += ez * mp;
+        acc[6] += ex * mv;
+        acc[7] += ey * mv;
+        acc[8] += ez * mv;
+        acc[9] += (ry * ez - rz * ey) * mom;
+        acc[10] += (rz * ex - rx * ez) * mom;
+        acc[11] += (rx * ey - ry * ex) * mom;
+      }
+    }
+  });
+  double *out = p.lc_contrib + slot * 12;
+#pragma unroll
+  for (int j = 0; j < 12; j++) out[j] = (double)acc[j];
+}
+
 // One full step: state of step n from P_n, scalar step, collision -> P_{n+1}.
 // FROM_STATE: P holds a state (deviations) to be collided as is (used after
 // the host sets f, and to start from an initial state).
 template <class L, class S, int COLL, bool FROM_STATE>
-__global__ void __launch_bounds__(kStepBlock, kStepMinBlocks) k_step(const StepParams<typename StoreOps<S>::Real> p) {
+__global__ void __launch_bounds__(kStepBlock, sizeof(typename StoreOps<S>::Real) == 4 ? kStepMinBlocks : 4)
+    k_step(const StepParams<typename StoreOps<S>::Real> p) {
   using Real = typename StoreOps<S>::Real;
   using SO = StoreOps<S>;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -630,6 +693,10 @@ __global__ void __launch_bounds__(kStepBlock, kStepMinBlocks) k_step(const StepP
   } else {
     step_now = *p.step;
     full_state<L, S, Real>(p, x, y, z, step_now, d, p.prevn, &sc);
+    if (p.feat & FEAT_OBSTACLE_BB) {
+      const int64_t slot = link_slot(p, x, y, z);
+      if (slot >= 0) link_cell_forces<L, S, Real>(p, x, y, z, c, slot, d);
+    }
     if (p.feat & FEAT_THERMAL) {
       if (p.feat & FEAT_SCALAR_REDUCED) {
         using G = typename ScalarReduced<L>::Lat;
@@ -718,105 +785,43 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[N], double *out) 
   }
 }
 
-// Momentum-exchange forces, pressure/viscous split, moments and the
-// per-y (2D) / per-z (3D) profile, one thread per link cell, FP64 sums.
-template <class L, class S>
-__global__ void __launch_bounds__(kForceBlock) k_forces(const StepParams<typename StoreOps<S>::Real> p) {
-  using Real = typename StoreOps<S>::Real;
-  using SO = StoreOps<S>;
-  const int64_t k = (int64_t)blockIdx.x * kForceBlock + threadIdx.x;
-  double acc[12];
-#pragma unroll
-  for (int j = 0; j < 12; j++) acc[j] = 0.0;
-  if (k < p.n_lc) {
-    const uint32_t c = (uint32_t)p.lc_cell[k];
-    const int x = (int)(c % (uint32_t)p.nx);
-    const int y = (int)((c / (uint32_t)p.nx) % (uint32_t)p.ny);
-    const int z = (int)(c / ((uint32_t)p.nx * (uint32_t)p.ny));
-    Real d[L::Q];
-    full_state<L, S, Real>(p, x, y, z, *p.step, d, nullptr, nullptr);
-    const S *P = static_cast<const S *>(p.P);
-    double fp[L::Q];
-    double drho = 0, jx = 0, jy = 0, jz = 0;
-    static_for<L::Q>([&](auto ic) {
-      constexpr int i = decltype(ic)::value;
-      fp[i] = (double)SO::template load<i, L>(plane(P, i, p.cs), c);
-      drho += fp[i];
-      jx += Dir<L, i>::x * fp[i];
-      jy += Dir<L, i>::y * fp[i];
-      jz += Dir<L, i>::z * fp[i];
-    });
-    const double rho = 1.0 + drho;
-    const double inv = rho > 0.0 ? 1.0 / rho : 0.0;
-    const double ux = jx * inv, uy = jy * inv, uz = jz * inv, usq = ux * ux + uy * uy + uz * uz;
-    const uint32_t mask = p.lc_mask[k];
-    const double rx = x - p.center[0], ry = y - p.center[1], rz = z - p.center[2];
-    double prof[3] = {0.0, 0.0, 0.0};
-    static_for<L::Q>([&](auto ic) {
-      constexpr int i = decltype(ic)::value;
-      if constexpr (i > 0) {
-        if ((mask >> i) & 1u) {
-          constexpr int o = L::opp[i];
-          const double eui = Dir<L, i>::x * ux + Dir<L, i>::y * uy + Dir<L, i>::z * uz;
-          const double deq_i = Dir<L, i>::w * (drho + rho * (3.0 * eui + 4.5 * eui * eui - 1.5 * usq));
-          const double deq_o = Dir<L, o>::w * (drho + rho * (-3.0 * eui + 4.5 * eui * eui - 1.5 * usq));
-          const double din = (double)d[o];
-          const double mom = (Dir<L, i>::w + Dir<L, o>::w) + (fp[i] + din);
-          const double mp = (Dir<L, i>::w + Dir<L, o>::w) + (deq_i + deq_o);
-          const double mv = (fp[i] - deq_i) + (din - deq_o);
-          const double df[3] = {Dir<L, i>::x * mom, Dir<L, i>::y * mom, Dir<L, i>::z * mom};
-          acc[0] += df[0];
-          acc[1] += df[1];
-          acc[2] += df[2];
-          acc[3] += Dir<L, i>::x * mp;
-          acc[4] += Dir<L, i>::y * mp;
-          acc[5] += Dir<L, i>::z * mp;
-          acc[6] += Dir<L, i>::x * mv;
-          acc[7] += Dir<L, i>::y * mv;
-          acc[8] += Dir<L, i>::z * mv;
-          acc[9] += ry * df[2] - rz * df[1];
-          acc[10] += rz * df[0] - rx * df[2];
-          acc[11] += rx * df[1] - ry * df[0];
-          prof[0] += df[0];
-          prof[1] += df[1];
-          prof[2] += df[2];
-        }
-      }
-    });
-    p.lc_prof[k * 3 + 0] = prof[0];
-    p.lc_prof[k * 3 + 1] = prof[1];
-    p.lc_prof[k * 3 + 2] = prof[2];
-  }
-  block_reduce_store<12, kForceBlock>(acc, p.partials + (int64_t)blockIdx.x * 12);
-}
-
-// Sums the per-block partials in a fixed order into the device history ring,
-// optionally sums the profile segments, then advances the step counter.
+// Sums the per-link-cell contributions (in a fixed order, FP64) plus the
+// constant rest-weight part into the device history ring, sums the profile
+// segments, then advances the step counter.
 template <class Real>
 __global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const StepParams<Real> p) {
-  __shared__ double sm[kFinalizeBlock];
-  const int t = threadIdx.x;
+  __shared__ double sm[12][kFinalizeBlock / 32];
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   const int64_t step = *p.step;
   const int64_t slot = (step - *p.hist_base) % p.hist_cap;
+  double a[12];
+#pragma unroll
+  for (int j = 0; j < 12; j++) a[j] = 0.0;
+  for (int64_t k = t; k < p.n_lc; k += kFinalizeBlock) {
+#pragma unroll
+    for (int j = 0; j < 12; j++) a[j] += p.lc_contrib[k * 12 + j];
+  }
+#pragma unroll
   for (int j = 0; j < 12; j++) {
-    double a = 0.0;
-    for (int b = t; b < p.n_force_blocks; b += kFinalizeBlock) a += p.partials[(int64_t)b * 12 + j];
-    sm[t] = a;
-    __syncthreads();
-    for (int s = kFinalizeBlock / 2; s > 0; s >>= 1) {
-      if (t < s) sm[t] += sm[t + s];
-      __syncthreads();
-    }
-    if (t == 0) p.hist[slot * 12 + j] = sm[0];
-    __syncthreads();
+    double v = a[j];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (lane == 0) sm[j][wid] = v;
+  }
+  __syncthreads();
+  if (t < 12) {
+    double v = p.force_const[t];
+#pragma unroll
+    for (int w = 0; w < kFinalizeBlock / 32; w++) v += sm[t][w];
+    p.hist[slot * 12 + t] = v;
   }
   if (p.want_profile) {
     for (int b = t; b < p.nprof; b += kFinalizeBlock) {
-      double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+      double a0 = p.prof_const[b * 3 + 0], a1 = p.prof_const[b * 3 + 1], a2 = p.prof_const[b * 3 + 2];
       for (int k = p.prof_off[b]; k < p.prof_off[b + 1]; k++) {
-        a0 += p.lc_prof[(int64_t)k * 3 + 0];
-        a1 += p.lc_prof[(int64_t)k * 3 + 1];
-        a2 += p.lc_prof[(int64_t)k * 3 + 2];
+        a0 += p.lc_contrib[(int64_t)k * 12 + 0];
+        a1 += p.lc_contrib[(int64_t)k * 12 + 1];
+        a2 += p.lc_contrib[(int64_t)k * 12 + 2];
       }
       p.prof_out[b * 3 + 0] = a0;
       p.prof_out[b * 3 + 1] = a1;

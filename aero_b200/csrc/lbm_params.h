@@ -74,14 +74,14 @@ struct StepParams {
   const Real *cs_cell;  // per-cell LES constant (van Driest), optional
 
   // force reduction
-  double *partials;     // per force-block: 12 doubles
-  double *lc_prof;      // per link cell: 3 doubles (profile contributions)
+  double *lc_contrib;   // per link cell: 12 doubles (deviation part of its forces)
+  const double *force_const;  // 12 doubles: rest-weight part of the forces
+  const double *prof_const;   // nprof * 3 doubles: rest-weight part of the profile
   const int32_t *prof_off;  // nprof + 1 segment offsets into the link-cell list
   double *hist;         // force history ring: hist_cap * 12 doubles
   double *prof_out;     // last profile: nprof * 3 doubles
   int32_t nprof;
   int32_t hist_cap;
-  int32_t n_force_blocks;
   int32_t want_profile;
   int64_t *step;        // device step counter (steps completed)
   int64_t *hist_base;   // step index stored in hist slot 0
