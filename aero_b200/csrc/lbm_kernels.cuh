@@ -197,15 +197,14 @@ __device__ __forceinline__ void walls(const StepParams<Real> &p, Real (&d)[L::Q]
 
 // gather + body force + obstacle bounce-back + inlet (everything the
 // reference applies before the outlet copy reads column Nx-2).
-// Pull gather with periodic wrap (the reference's push stream,
-// kernels.py:94-114, kernels3d.py:63-80): the source of direction i is
-// (x - ex, y - ey, z - ez); per axis only three values occur, so each source
-// index is one 3-way add.
 template <class L, class S, class Real>
-__device__ __forceinline__ void gather(const StepParams<Real> &p, int x, int y, int z, Real (&d)[L::Q]) {
+__device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, int y, int z, int64_t step_now,
+                                              Real (&d)[L::Q]) {
   using SO = StoreOps<S>;
   const S *P = static_cast<const S *>(p.P);
   const int64_t cs = p.cs;
+  // Source of direction i is (x - ex, y - ey, z - ez) with periodic wrap: per
+  // axis only three values occur, so each source index is one 3-way add.
   const uint32_t nx = p.nx, nxy = (uint32_t)p.nx * (uint32_t)p.ny;
   const uint32_t xs_p = x == 0 ? nx - 1 : x - 1;            // ex = +1
   const uint32_t xs_m = x == p.nx - 1 ? 0 : x + 1;          // ex = -1
@@ -226,13 +225,9 @@ __device__ __forceinline__ void gather(const StepParams<Real> &p, int x, int y, 
                          (ez > 0 ? pz_p : (ez < 0 ? pz_m : pz_0));
     d[i] = SO::template load<i, L>(plane(P, i, cs), src);
   });
-}
-
-// Guo-style uniform body force on fluid cells, after streaming
-// (ibm_guo.py:263-301, solver3d.py:411-423).
-template <class L, class Real>
-__device__ __forceinline__ void body_force(const StepParams<Real> &p, uint32_t c, Real (&d)[L::Q]) {
+  const uint32_t c = cell_index(p, x, y, z);
   if constexpr (L::DIMS == 3) {
+    // Guo-style uniform body force on fluid cells (ibm_guo.py:263-301)
     if ((p.feat & FEAT_BODY_FORCE) && !p.solid[c]) {
       Real drho = 0, jx = 0, jy = 0, jz = 0;
       static_for<L::Q>([&](auto ic) {
@@ -256,56 +251,38 @@ __device__ __forceinline__ void body_force(const StepParams<Real> &p, uint32_t c
       }
     }
   }
-}
-
-// Mid-link or Bouzidi bounce-back of the links of one cell
-// (boundary.py:283-352, boundary3d.py:333-393), reading the pre-stream P.
-template <class L, class S, class Real>
-__device__ __forceinline__ void bounce_back(const StepParams<Real> &p, int x, int y, int z, uint32_t c, int64_t slot,
-                                            Real (&d)[L::Q]) {
-  using SO = StoreOps<S>;
-  const S *P = static_cast<const S *>(p.P);
-  const int64_t cs = p.cs;
-  const uint32_t mask = __ldg(p.lc_mask + slot);
-  const bool bouzidi = p.feat & FEAT_BOUZIDI;
-  static_for<L::Q>([&](auto ic) {
-    constexpr int i = decltype(ic)::value;
-    if constexpr (i > 0) {
-      if ((mask >> i) & 1u) {
-        constexpr int o = L::opp[i];
-        const Real fi = SO::template load<i, L>(plane(P, i, cs), c);
-        if (!bouzidi) {
-          d[o] = fi;
-        } else {
-          const Real q = (Real)__ldg(p.lc_q + slot * L::Q + i);
-          if (q < Real(0.5)) {
-            const Real fo = SO::template load<o, L>(plane(P, o, cs), c);
-            d[o] = Real(2) * q * fi + (Real(1) - Real(2) * q) * fo;
-          } else {
-            const int xn = clamp_n(x + Dir<L, o>::x, p.nx);
-            const int yn = clamp_n(y + Dir<L, o>::y, p.ny);
-            const int zn = L::DIMS == 3 ? clamp_n(z + Dir<L, o>::z, p.nz) : 0;
-            const Real fn = SO::template load<i, L>(plane(P, i, cs), cell_index(p, xn, yn, zn));
-            const Real inv2q = Real(1) / (Real(2) * q);
-            d[o] = inv2q * fi + (Real(1) - inv2q) * fn;
-          }
-        }
-      }
-    }
-  });
-}
-
-// gather + body force + obstacle bounce-back + inlet: everything the
-// reference applies before the outlet copy reads column Nx-2.
-template <class L, class S, class Real>
-__device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, int y, int z, int64_t step_now,
-                                              Real (&d)[L::Q]) {
-  gather<L, S, Real>(p, x, y, z, d);
-  const uint32_t c = cell_index(p, x, y, z);
-  body_force<L, Real>(p, c, d);
+  // obstacle bounce-back (boundary.py:283-352, boundary3d.py:333-393)
   if (p.feat & FEAT_OBSTACLE_BB) {
     const int64_t slot = link_slot(p, x, y, z);
-    if (slot >= 0) bounce_back<L, S, Real>(p, x, y, z, c, slot, d);
+    if (slot >= 0) {
+      const uint32_t mask = __ldg(p.lc_mask + slot);
+      const bool bouzidi = p.feat & FEAT_BOUZIDI;
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        if constexpr (i > 0) {
+          if ((mask >> i) & 1u) {
+            constexpr int o = L::opp[i];
+            const Real fi = SO::template load<i, L>(plane(P, i, cs), c);
+            if (!bouzidi) {
+              d[o] = fi;
+            } else {
+              const Real q = (Real)__ldg(p.lc_q + slot * L::Q + i);
+              if (q < Real(0.5)) {
+                const Real fo = SO::template load<o, L>(plane(P, o, cs), c);
+                d[o] = Real(2) * q * fi + (Real(1) - Real(2) * q) * fo;
+              } else {
+                const int xn = clamp_n(x + Dir<L, o>::x, p.nx);
+                const int yn = clamp_n(y + Dir<L, o>::y, p.ny);
+                const int zn = L::DIMS == 3 ? clamp_n(z + Dir<L, o>::z, p.nz) : 0;
+                const Real fn = SO::template load<i, L>(plane(P, i, cs), cell_index(p, xn, yn, zn));
+                const Real inv2q = Real(1) / (Real(2) * q);
+                d[o] = inv2q * fi + (Real(1) - inv2q) * fn;
+              }
+            }
+          }
+        }
+      });
+    }
   }
   if ((p.feat & FEAT_OPEN) && x == 0) {
     if (p.inlet == INLET_VELOCITY) {
@@ -322,65 +299,6 @@ struct ScalarCtx {
   Real T;       // sum of the current scalar populations at the cell
   Real u[3];    // flow velocity before buoyancy (drives the scalar collision)
 };
-
-// Sponge relaxation toward feq(rho, u0, 0) over the last planes (sponge.py:8-70).
-template <class L, class Real>
-__device__ __forceinline__ void sponge(const StepParams<Real> &p, int x, Real (&d)[L::Q]) {
-  if ((p.feat & FEAT_SPONGE) && x >= p.sponge_start) {
-    const double frac = (double)(x - p.sponge_start + 1) / (double)(p.sponge_thickness > 1 ? p.sponge_thickness : 1);
-    const Real sg = (Real)((double)p.sponge_sigma_max * frac * frac);
-    if (sg > Real(0)) {
-      const Real drho = sum_dev<L>(d);
-      const Real rho = Real(1) + drho;
-      const Real u0 = p.u0, usq = u0 * u0;
-      static_for<L::Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        const Real eu = Dir<L, i>::x * u0;
-        const Real deq = Real(Dir<L, i>::w) * (drho + rho * (Real(3) * eu + Real(4.5) * eu * eu - Real(1.5) * usq));
-        d[i] = (Real(1) - sg) * d[i] + sg * deq;
-      });
-    }
-  }
-}
-
-// Scalar coupling of the flow state (thermal.py:103-124 / :206-222, in the
-// order of solver.py:432-439): T of the current scalar populations, the
-// velocity before buoyancy (returned for the scalar collision), buoyancy.
-template <class L, class Real>
-__device__ __forceinline__ void scalar_coupling(const StepParams<Real> &p, uint32_t c, Real (&d)[L::Q],
-                                                ScalarCtx<Real> *sc) {
-  if (!(p.feat & FEAT_THERMAL)) return;
-  Real T = 0;
-  if (p.feat & FEAT_SCALAR_REDUCED) {
-    using G = typename ScalarReduced<L>::Lat;
-    static_for<G::Q>([&](auto ic) { T += plane(p.g, decltype(ic)::value, p.cs)[c]; });
-  } else {
-    static_for<L::Q>([&](auto ic) { T += plane(p.g, decltype(ic)::value, p.cs)[c]; });
-  }
-  Real drho = 0, jx = 0, jy = 0, jz = 0;
-  static_for<L::Q>([&](auto ic) {
-    constexpr int i = decltype(ic)::value;
-    drho += d[i];
-    if (Dir<L, i>::x) jx += Dir<L, i>::x * d[i];
-    if (Dir<L, i>::y) jy += Dir<L, i>::y * d[i];
-    if (Dir<L, i>::z) jz += Dir<L, i>::z * d[i];
-  });
-  const Real rho = Real(1) + drho;
-  if (sc) {
-    const Real inv = rho > Real(0) ? Real(1) / rho : Real(0);
-    sc->T = T;
-    sc->u[0] = jx * inv;
-    sc->u[1] = jy * inv;
-    sc->u[2] = jz * inv;
-  }
-  if (p.feat & FEAT_BUOYANCY) {
-    const Real buoy = p.gbeta * (T - p.T_ref);
-    static_for<L::Q>([&](auto ic) {
-      constexpr int i = decltype(ic)::value;
-      if constexpr (Dir<L, i>::y != 0) d[i] += Real(Dir<L, i>::w) * Real(3) * rho * buoy * Real(Dir<L, i>::y);
-    });
-  }
-}
 
 // Full post-BC state.  When prev_out is non-null the convective outlet writes
 // its advanced state there (only k_step does).
@@ -405,12 +323,60 @@ __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int
   } else if constexpr (L::DIMS == 2) {
     if (open && x == p.nx - 1 && p.outlet == OUTLET_PRESSURE) outlet_pressure_2d(p, d);
   }
-  sponge<L>(p, x, d);
+  // sponge (sponge.py:8-70)
+  if ((p.feat & FEAT_SPONGE) && x >= p.sponge_start) {
+    const double frac = (double)(x - p.sponge_start + 1) / (double)(p.sponge_thickness > 1 ? p.sponge_thickness : 1);
+    const Real sg = (Real)((double)p.sponge_sigma_max * frac * frac);
+    if (sg > Real(0)) {
+      const Real drho = sum_dev<L>(d);
+      const Real rho = Real(1) + drho;
+      const Real u0 = p.u0, usq = u0 * u0;
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        const Real eu = Dir<L, i>::x * u0;
+        const Real deq = Real(Dir<L, i>::w) * (drho + rho * (Real(3) * eu + Real(4.5) * eu * eu - Real(1.5) * usq));
+        d[i] = (Real(1) - sg) * d[i] + sg * deq;
+      });
+    }
+  }
   if (p.wall != WALL_NONE) {
     if (y == 0) walls<L>(p, d, true);
     if (y == p.ny - 1) walls<L>(p, d, false);
   }
-  scalar_coupling<L>(p, cell_index(p, x, y, z), d, sc);
+  if (p.feat & FEAT_THERMAL) {
+    // thermal.py:103-124 / :206-222 with the order of solver.py:432-439
+    const uint32_t c = cell_index(p, x, y, z);
+    Real T = 0;
+    if (p.feat & FEAT_SCALAR_REDUCED) {
+      using G = typename ScalarReduced<L>::Lat;
+      static_for<G::Q>([&](auto ic) { T += plane(p.g, decltype(ic)::value, p.cs)[c]; });
+    } else {
+      static_for<L::Q>([&](auto ic) { T += plane(p.g, decltype(ic)::value, p.cs)[c]; });
+    }
+    Real drho = 0, jx = 0, jy = 0, jz = 0;
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      drho += d[i];
+      if (Dir<L, i>::x) jx += Dir<L, i>::x * d[i];
+      if (Dir<L, i>::y) jy += Dir<L, i>::y * d[i];
+      if (Dir<L, i>::z) jz += Dir<L, i>::z * d[i];
+    });
+    const Real rho = Real(1) + drho;
+    if (sc) {
+      const Real inv = rho > Real(0) ? Real(1) / rho : Real(0);
+      sc->T = T;
+      sc->u[0] = jx * inv;
+      sc->u[1] = jy * inv;
+      sc->u[2] = jz * inv;
+    }
+    if (p.feat & FEAT_BUOYANCY) {
+      const Real buoy = p.gbeta * (T - p.T_ref);
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        if constexpr (Dir<L, i>::y != 0) d[i] += Real(Dir<L, i>::w) * Real(3) * rho * buoy * Real(Dir<L, i>::y);
+      });
+    }
+  }
 }
 
 // --------------------------------------------------------------------------
@@ -726,21 +692,10 @@ __global__ void __launch_bounds__(kStepBlock, sizeof(typename StoreOps<S>::Real)
     });
   } else {
     step_now = *p.step;
-    // Cells on a link, the inlet/outlet columns or a wall row take the full
-    // boundary chain; all others need only gather, body force, sponge and
-    // the scalar coupling (the same result as full_state for them).
-    int64_t slot = -1;
-    if (p.feat & FEAT_OBSTACLE_BB) slot = link_slot(p, x, y, z);
-    const bool special = slot >= 0 || ((p.feat & FEAT_OPEN) && (x == 0 || x == p.nx - 1)) ||
-                         (p.wall != WALL_NONE && (y == 0 || y == p.ny - 1));
-    if (special) {
-      full_state<L, S, Real>(p, x, y, z, step_now, d, p.prevn, &sc);
+    full_state<L, S, Real>(p, x, y, z, step_now, d, p.prevn, &sc);
+    if (p.feat & FEAT_OBSTACLE_BB) {
+      const int64_t slot = link_slot(p, x, y, z);
       if (slot >= 0) link_cell_forces<L, S, Real>(p, x, y, z, c, slot, d);
-    } else {
-      gather<L, S, Real>(p, x, y, z, d);
-      body_force<L, Real>(p, c, d);
-      sponge<L>(p, x, d);
-      scalar_coupling<L>(p, c, d, &sc);
     }
     if (p.feat & FEAT_THERMAL) {
       if (p.feat & FEAT_SCALAR_REDUCED) {
