@@ -229,8 +229,12 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16s", "bf16s", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--collision", default=None, choices=["bgk", "trt", "mrt"],
+                    help="override the workload's collision operator (profiling)")
     args = ap.parse_args()
-    w = WORKLOADS[args.workload]
+    w = dict(WORKLOADS[args.workload])
+    if args.collision:
+        w["kwargs"] = dict(w["kwargs"], collision=args.collision)
     if args.impl == "reference":
         return run_reference(args, w)
     args.warmup = max(args.warmup, 3)
