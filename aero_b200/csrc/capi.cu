@@ -110,6 +110,7 @@ struct AeroLattice {
   bool old_is_state = false;
   int64_t step_count = 0, read_upto = 0;
   MrtCoeffs<double> mrt{};
+  Mrt3Adapted<double> mrt3{};
   WTab w{}, wg{};
   // CUDA graphs of a two-step sequence, one per starting parity
   cudaStream_t cap_stream = nullptr;
@@ -223,6 +224,21 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   for (int k = 0; k < 70; k++) p.mrt.Ce[k] = (Real)(L->mrt.Ce[k] * (k < 7 ? 1.0 : 0.5));
   for (int k = 0; k < 81; k++) p.mrt.Ao[k] = (Real)(L->mrt.Ao[k] * 0.5);
   for (int k = 0; k < 27; k++) p.mrt.Co[k] = (Real)(L->mrt.Co[k] * 0.5);
+  {
+    const Mrt3Adapted<double> &m = L->mrt3;
+    for (int k = 0; k < 9; k++) p.mrt3.a1[k] = (Real)m.a1[k];
+    for (int k = 0; k < 6; k++) p.mrt3.ca1[k] = (Real)m.ca1[k];
+    for (int k = 0; k < 4; k++) {
+      p.mrt3.e[k] = (Real)m.e[k];
+      p.mrt3.v[k] = (Real)m.v[k];
+    }
+    for (int k = 0; k < 2; k++) {
+      p.mrt3.ce[k] = (Real)m.ce[k];
+      p.mrt3.cv[k] = (Real)m.cv[k];
+    }
+    p.mrt3.t2 = (Real)m.t2;
+    p.mrt3.ct2 = (Real)m.ct2;
+  }
   return p;
 }
 
@@ -444,6 +460,10 @@ int aero_create(const AeroParams *params, AeroLattice **out) {
     delete L;
     return fail(AERO_ERR_INVALID, "MRT operator is not block diagonal in the pair basis");
   }
+  if (a.collision == AERO_MRT && a.dims == 3 && !build_mrt3_adapted(a.omega, L->mrt3)) {
+    delete L;
+    return fail(AERO_ERR_INVALID, "MRT operator does not have the cubic block structure");
+  }
   const char *ng = std::getenv("AERO_B200_NO_GRAPHS");
   L->use_graphs = !(ng && ng[0] == '1');
   *out = L;
@@ -514,6 +534,8 @@ int aero_set_geometry(AeroLattice *L, const uint8_t *solid, const int32_t *links
     }
   }
   if (n_links > 0) L->feat |= FEAT_OBSTACLE_BB; else L->feat &= ~FEAT_OBSTACLE_BB;
+  if ((uint64_t)std::max(L->Q, 3) * (uint64_t)L->cs >= (1ull << 32))
+    return fail(AERO_ERR_UNSUPPORTED, "lattice too large: Q x cells must stay below 2^32 (32-bit element offsets)");
   // rest-weight part of the momentum exchange: each link contributes
   // e_i (w_i + w_opp) to F and to its pressure part, and r x that to M
   L->force_const.assign(12, 0.0);
@@ -778,6 +800,39 @@ int aero_destroy(AeroLattice *L) {
   if (L->cap_stream) cudaStreamDestroy(L->cap_stream);
   for (auto e : L->ev) cudaEventDestroy(e);
   delete L;
+  return AERO_OK;
+}
+
+int aero_collide_host(const AeroParams *a, const double *f_in, double *f_out, const uint8_t *solid, int64_t n) {
+  const int rc = check_params(a);
+  if (rc != AERO_OK) return rc;
+  if (!f_in || !f_out || n < 0) return fail(AERO_ERR_INVALID, "bad argument");
+  AeroLattice *L = nullptr;
+  const int rc2 = aero_create(a, &L);
+  if (rc2 != AERO_OK) return rc2;
+  StepParams<double> p = make_params<double>(L, 0);
+  const int Q = L->Q;
+  for (int64_t c = 0; c < n; c++) {
+    double d[19];
+    for (int i = 0; i < Q; i++) d[i] = f_in[i * n + c] - L->w.w[i];
+    const bool sol = solid && solid[c];
+    if (a->dims == 2) {
+      double (&dd)[9] = *reinterpret_cast<double (*)[9]>(d);
+      switch (a->collision) {
+        case AERO_BGK: collide<D2Q9, double, COLL_BGK>(p, dd, sol, p.omega, false); break;
+        case AERO_TRT: collide<D2Q9, double, COLL_TRT>(p, dd, sol, p.omega, false); break;
+        default: collide<D2Q9, double, COLL_MRT>(p, dd, sol, p.omega, false); break;
+      }
+    } else {
+      switch (a->collision) {
+        case AERO_BGK: collide<D3Q19, double, COLL_BGK>(p, d, sol, p.omega, false); break;
+        case AERO_TRT: collide<D3Q19, double, COLL_TRT>(p, d, sol, p.omega, false); break;
+        default: collide<D3Q19, double, COLL_MRT>(p, d, sol, p.omega, false); break;
+      }
+    }
+    for (int i = 0; i < Q; i++) f_out[i * n + c] = L->w.w[i] + d[i];
+  }
+  aero_destroy(L);
   return AERO_OK;
 }
 

@@ -25,6 +25,7 @@ const Ops<float> *ops_f16(int dims, int coll);
 const Ops<float> *ops_bf16(int dims, int coll);
 
 bool build_mrt(int dims, double omega, MrtCoeffs<double> &out, double *A_full, double *B_full);
+bool build_mrt3_adapted(double omega, Mrt3Adapted<double> &out);
 bool mrt_pinv_basis(int dims, double *M_out, double *Minv_out);
 
 }  // namespace aero

@@ -53,9 +53,12 @@ __device__ __forceinline__ uint32_t cell_index(const StepParams<Real> &p, int x,
   return ((uint32_t)z * (uint32_t)p.ny + (uint32_t)y) * (uint32_t)p.nx + (uint32_t)x;
 }
 
-template <class T>
-__device__ __forceinline__ T *plane(T *base, int i, int64_t cs) {
-  return base + (int64_t)i * cs;
+// Element offset of direction i at cell c: every population access is the
+// buffer base plus one 32-bit offset (the host keeps Q * cs below 2^32), so
+// the address costs one add and one wide multiply-add.
+template <class Real>
+__device__ __forceinline__ uint32_t elem(const StepParams<Real> &p, int i, uint32_t c) {
+  return (uint32_t)i * (uint32_t)p.cs + c;
 }
 
 // Link-cell slot of cell (x, y, z), or -1 when the cell has no link.
@@ -223,7 +226,7 @@ __device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, 
     const uint32_t src = (ex > 0 ? xs_p : (ex < 0 ? xs_m : (uint32_t)x)) +
                          (ey > 0 ? ry_p : (ey < 0 ? ry_m : ry_0)) +
                          (ez > 0 ? pz_p : (ez < 0 ? pz_m : pz_0));
-    d[i] = SO::template load<i, L>(plane(P, i, cs), src);
+    d[i] = SO::template load<i, L>(P, elem(p, i, src));
   });
   const uint32_t c = cell_index(p, x, y, z);
   if constexpr (L::DIMS == 3) {
@@ -262,19 +265,19 @@ __device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, 
         if constexpr (i > 0) {
           if ((mask >> i) & 1u) {
             constexpr int o = L::opp[i];
-            const Real fi = SO::template load<i, L>(plane(P, i, cs), c);
+            const Real fi = SO::template load<i, L>(P, elem(p, i, c));
             if (!bouzidi) {
               d[o] = fi;
             } else {
               const Real q = (Real)__ldg(p.lc_q + slot * L::Q + i);
               if (q < Real(0.5)) {
-                const Real fo = SO::template load<o, L>(plane(P, o, cs), c);
+                const Real fo = SO::template load<o, L>(P, elem(p, o, c));
                 d[o] = Real(2) * q * fi + (Real(1) - Real(2) * q) * fo;
               } else {
                 const int xn = clamp_n(x + Dir<L, o>::x, p.nx);
                 const int yn = clamp_n(y + Dir<L, o>::y, p.ny);
                 const int zn = L::DIMS == 3 ? clamp_n(z + Dir<L, o>::z, p.nz) : 0;
-                const Real fn = SO::template load<i, L>(plane(P, i, cs), cell_index(p, xn, yn, zn));
+                const Real fn = SO::template load<i, L>(P, elem(p, i, cell_index(p, xn, yn, zn)));
                 const Real inv2q = Real(1) / (Real(2) * q);
                 d[o] = inv2q * fi + (Real(1) - inv2q) * fn;
               }
@@ -349,9 +352,9 @@ __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int
     Real T = 0;
     if (p.feat & FEAT_SCALAR_REDUCED) {
       using G = typename ScalarReduced<L>::Lat;
-      static_for<G::Q>([&](auto ic) { T += plane(p.g, decltype(ic)::value, p.cs)[c]; });
+      static_for<G::Q>([&](auto ic) { T += p.g[elem(p, decltype(ic)::value, c)]; });
     } else {
-      static_for<L::Q>([&](auto ic) { T += plane(p.g, decltype(ic)::value, p.cs)[c]; });
+      static_for<L::Q>([&](auto ic) { T += p.g[elem(p, decltype(ic)::value, c)]; });
     }
     Real drho = 0, jx = 0, jy = 0, jz = 0;
     static_for<L::Q>([&](auto ic) {
@@ -461,9 +464,105 @@ __device__ __forceinline__ Real les_omega(const StepParams<Real> &p, int x, int 
 // 125-174 with trt2d.py:8-18; MRT: kernels_mrt.py:190-241,
 // kernels3d_mrt.py:24-82.  Solid cells relax toward feq(rho, 0).
 // --------------------------------------------------------------------------
+// D3Q19 MRT in the cubic-symmetry-adapted basis.  The reference operator
+// (dense M19 / pseudo-inverse, see lbm_mrt.cpp) commutes with the lattice's
+// cubic symmetry, so in coordinates built from sums and differences of
+// populations it splits into: a 3x3 block on the scalars (rest, face sum,
+// edge sum), one 2x2 block shared by both components of the face/edge
+// doublets, the scalar 1 - omega on the three shear-type edge differences, a
+// 2x2 block shared by the x, y, z momentum-like pairs, and zero on the three
+// remaining odd edge combinations (the directions the rank-16 basis projects
+// out).  The host derives the block entries from the dense operator and
+// checks that nothing outside them is non-zero.
+template <class Real>
+AERO_HD Real mrt3_adapted(const StepParams<Real> &p, Real (&d)[19], bool solid, Real drho_in) {
+  const Mrt3Adapted<Real> &m = p.mrt3;
+  // pair sums (even) and differences (odd)
+  const Real X = d[1] + d[2], Y = d[3] + d[4], Z = d[5] + d[6];
+  const Real p710 = d[7] + d[10], p89 = d[8] + d[9], p1114 = d[11] + d[14], p1213 = d[12] + d[13];
+  const Real p1518 = d[15] + d[18], p1617 = d[16] + d[17];
+  const Real t1 = d[1] - d[2], t2 = d[3] - d[4], t3 = d[5] - d[6];
+  const Real q710 = d[7] - d[10], q89 = d[8] - d[9], q1114 = d[11] - d[14], q1213 = d[12] - d[13];
+  const Real q1518 = d[15] - d[18], q1617 = d[16] - d[17];
+  // even adapted coordinates
+  const Real Pxy = p710 + p89, Pxz = p1114 + p1213, Pyz = p1518 + p1617;
+  const Real g0 = d[0], g1 = X + Y + Z, g2 = Pxy + Pxz + Pyz;
+  const Real g3 = Real(2) * X - Y - Z, g4 = Y - Z;
+  const Real g5 = Real(2) * Pyz - Pxz - Pxy, g6 = Pxz - Pxy;
+  const Real g7 = p710 - p89, g8 = p1114 - p1213, g9 = p1518 - p1617;
+  // odd adapted coordinates (momentum-like edge sums)
+  const Real Wx = (q710 - q89) + (q1114 - q1213);
+  const Real Wy = (q710 + q89) + (q1518 - q1617);
+  const Real Wz = (q1114 + q1213) + (q1518 + q1617);
+  // moments
+  const Real drho = g0 + g1 + g2;
+  (void)drho_in;
+  const Real jx = t1 + Wx, jy = t2 + Wy, jz = t3 + Wz;
+  const Real rho = Real(1) + drho;
+  const Real inv = rho > Real(0) ? Real(1) / rho : Real(0);
+  Real ux = jx * inv, uy = jy * inv, uz = jz * inv;
+  if (solid) ux = uy = uz = Real(0);
+  const Real rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
+  const Real kxx = rux * ux, kyy = ruy * uy, kzz = ruz * uz;
+  const Real ru2 = kxx + kyy + kzz;
+  const Real mE1 = Real(2) * kxx - kyy - kzz, mE2 = kyy - kzz;
+  // blocks
+  const Real h0 = m.a1[0] * g0 + m.a1[1] * g1 + m.a1[2] * g2 + m.ca1[0] * drho + m.ca1[1] * ru2;
+  const Real h1 = m.a1[3] * g0 + m.a1[4] * g1 + m.a1[5] * g2 + m.ca1[2] * drho + m.ca1[3] * ru2;
+  const Real h2 = m.a1[6] * g0 + m.a1[7] * g1 + m.a1[8] * g2 + m.ca1[4] * drho + m.ca1[5] * ru2;
+  const Real h3 = m.e[0] * g3 + m.e[1] * g5 + m.ce[0] * mE1;
+  const Real h5 = m.e[2] * g3 + m.e[3] * g5 + m.ce[1] * mE1;
+  const Real h4 = m.e[0] * g4 + m.e[1] * g6 + m.ce[0] * mE2;
+  const Real h6 = m.e[2] * g4 + m.e[3] * g6 + m.ce[1] * mE2;
+  const Real h7 = m.t2 * g7 + m.ct2 * (rux * uy);
+  const Real h8 = m.t2 * g8 + m.ct2 * (rux * uz);
+  const Real h9 = m.t2 * g9 + m.ct2 * (ruy * uz);
+  const Real vx = m.v[0] * t1 + m.v[1] * Wx + m.cv[0] * rux;
+  const Real Vx = m.v[2] * t1 + m.v[3] * Wx + m.cv[1] * rux;
+  const Real vy = m.v[0] * t2 + m.v[1] * Wy + m.cv[0] * ruy;
+  const Real Vy = m.v[2] * t2 + m.v[3] * Wy + m.cv[1] * ruy;
+  const Real vz = m.v[0] * t3 + m.v[1] * Wz + m.cv[0] * ruz;
+  const Real Vz = m.v[2] * t3 + m.v[3] * Wz + m.cv[1] * ruz;
+  // back to populations
+  const Real Xn = (h1 + h3) * Real(1.0 / 3.0);
+  const Real Yn = Real(0.5) * (h1 - Xn + h4), Zn = Real(0.5) * (h1 - Xn - h4);
+  const Real Pyzn = (h2 + h5) * Real(1.0 / 3.0);
+  const Real Pxzn = Real(0.5) * (h2 - Pyzn + h6), Pxyn = Real(0.5) * (h2 - Pyzn - h6);
+  const Real p710n = Real(0.5) * (Pxyn + h7), p89n = Real(0.5) * (Pxyn - h7);
+  const Real p1114n = Real(0.5) * (Pxzn + h8), p1213n = Real(0.5) * (Pxzn - h8);
+  const Real p1518n = Real(0.5) * (Pyzn + h9), p1617n = Real(0.5) * (Pyzn - h9);
+  const Real q710n = Real(0.25) * (Vx + Vy), q89n = Real(0.25) * (Vy - Vx);
+  const Real q1114n = Real(0.25) * (Vx + Vz), q1213n = Real(0.25) * (Vz - Vx);
+  const Real q1518n = Real(0.25) * (Vy + Vz), q1617n = Real(0.25) * (Vz - Vy);
+  d[0] = h0;
+  d[1] = Real(0.5) * (Xn + vx);
+  d[2] = Real(0.5) * (Xn - vx);
+  d[3] = Real(0.5) * (Yn + vy);
+  d[4] = Real(0.5) * (Yn - vy);
+  d[5] = Real(0.5) * (Zn + vz);
+  d[6] = Real(0.5) * (Zn - vz);
+  d[7] = Real(0.5) * (p710n + q710n);
+  d[10] = Real(0.5) * (p710n - q710n);
+  d[8] = Real(0.5) * (p89n + q89n);
+  d[9] = Real(0.5) * (p89n - q89n);
+  d[11] = Real(0.5) * (p1114n + q1114n);
+  d[14] = Real(0.5) * (p1114n - q1114n);
+  d[12] = Real(0.5) * (p1213n + q1213n);
+  d[13] = Real(0.5) * (p1213n - q1213n);
+  d[15] = Real(0.5) * (p1518n + q1518n);
+  d[18] = Real(0.5) * (p1518n - q1518n);
+  d[16] = Real(0.5) * (p1617n + q1617n);
+  d[17] = Real(0.5) * (p1617n - q1617n);
+  return rho;
+}
+
 template <class L, class Real, int COLL>
-__device__ __forceinline__ Real collide(const StepParams<Real> &p, Real (&d)[L::Q], bool solid, Real om,
-                                        bool per_cell_omega) {
+AERO_HD Real collide(const StepParams<Real> &p, Real (&d)[L::Q], bool solid, Real om, bool per_cell_omega) {
+  if constexpr (COLL == COLL_MRT && L::DIMS == 3) {
+    (void)om;
+    (void)per_cell_omega;
+    return mrt3_adapted<Real>(p, d, solid, Real(0));
+  }
   Real drho = 0, jx = 0, jy = 0, jz = 0;
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
@@ -477,7 +576,8 @@ __device__ __forceinline__ Real collide(const StepParams<Real> &p, Real (&d)[L::
   Real ux = jx * inv, uy = jy * inv, uz = jz * inv;
   if (solid) ux = uy = uz = Real(0);
   if constexpr (COLL == COLL_MRT) {
-    constexpr int NE = L::NP + 1, NO = L::NP, KE = L::DIMS == 2 ? 4 : 7, KO = L::DIMS;
+    // D2Q9: dense blocks in the pair basis (see lbm_mrt.cpp)
+    constexpr int NE = L::NP + 1, NO = L::NP, KE = 4, KO = 2;
     Real s[NE], t[NO], me[KE], mo[KO];
     s[0] = d[0];
     static_for<NO>([&](auto pc) {
@@ -486,23 +586,13 @@ __device__ __forceinline__ Real collide(const StepParams<Real> &p, Real (&d)[L::
       s[k + 1] = d[i] + d[o];
       t[k] = d[i] - d[o];
     });
-    const Real rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
+    const Real rux = rho * ux, ruy = rho * uy;
     me[0] = drho;
     me[1] = rux * ux;
     me[2] = ruy * uy;
-    if constexpr (L::DIMS == 2) {
-      me[3] = rux * uy;
-      mo[0] = rux;
-      mo[1] = ruy;
-    } else {
-      me[3] = ruz * uz;
-      me[4] = rux * uy;
-      me[5] = rux * uz;
-      me[6] = ruy * uz;
-      mo[0] = rux;
-      mo[1] = ruy;
-      mo[2] = ruz;
-    }
+    me[3] = rux * uy;
+    mo[0] = rux;
+    mo[1] = ruy;
     Real sp[NE], tp[NO];
 #pragma unroll
     for (int r = 0; r < NE; r++) {
@@ -534,36 +624,40 @@ __device__ __forceinline__ Real collide(const StepParams<Real> &p, Real (&d)[L::
     (void)om;
     (void)per_cell_omega;
   } else {
-    const Real usq = ux * ux + uy * uy + uz * uz;
-    Real deq[L::Q];
-    static_for<L::Q>([&](auto ic) {
-      constexpr int i = decltype(ic)::value;
-      const Real eu = Dir<L, i>::x * ux + Dir<L, i>::y * uy + Dir<L, i>::z * uz;
-      deq[i] = Real(Dir<L, i>::w) * (drho + rho * (Real(3) * eu + Real(4.5) * eu * eu - Real(1.5) * usq));
-    });
+    // BGK / TRT per +/- pair: feq_i - w_i = A + B, feq_opp - w_opp = A - B with
+    // A = w (drho + rho (4.5 (e.u)^2 - 1.5 u.u)) and B = 3 w rho (e.u).
+    const Real usq15 = Real(1.5) * (ux * ux + uy * uy + uz * uz);
+    Real sm = p.trt_sminus;
     if constexpr (COLL == COLL_TRT) {
-      Real sm = p.trt_sminus;
       if (per_cell_omega) {
         const Real tau = Real(1) / om, lam = p.trt_lambda;
         const Real tp = lam * tau + (Real(1) - lam);
         const Real tm = (tp * tau - Real(0.5)) / (tp - Real(0.5));
         sm = Real(1) / tm;
       }
-      Real out[L::Q];
-      static_for<L::Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        constexpr int j = L::opp[i];
-        const Real fpl = Real(0.5) * (d[i] + d[j]), fmi = Real(0.5) * (d[i] - d[j]);
-        const Real epl = Real(0.5) * (deq[i] + deq[j]), emi = Real(0.5) * (deq[i] - deq[j]);
-        out[i] = deq[i] + (Real(1) - om) * (fpl - epl) + (Real(1) - sm) * (fmi - emi);
-      });
-      static_for<L::Q>([&](auto ic) { d[decltype(ic)::value] = out[decltype(ic)::value]; });
-    } else {
-      static_for<L::Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        d[i] = (Real(1) - om) * d[i] + om * deq[i];
-      });
     }
+    const Real omc = Real(1) - om, smc = Real(1) - sm;
+    {
+      const Real A0 = Real(Dir<L, 0>::w) * (drho - rho * usq15);
+      d[0] = omc * d[0] + om * A0;  // the rest population is even: both rates give omega
+    }
+    static_for<L::NP>([&](auto pc) {
+      constexpr int k = decltype(pc)::value;
+      constexpr int i = L::pair[k], o = L::opp[L::pair[k]];
+      constexpr Real wi = Real(Dir<L, i>::w);
+      const Real eu = Real(Dir<L, i>::x) * ux + Real(Dir<L, i>::y) * uy + Real(Dir<L, i>::z) * uz;
+      const Real A = wi * (drho + rho * (Real(4.5) * eu * eu - usq15));
+      const Real B = (Real(3) * wi) * rho * eu;
+      if constexpr (COLL == COLL_TRT) {
+        const Real fp = Real(0.5) * (d[i] + d[o]), fm = Real(0.5) * (d[i] - d[o]);
+        const Real a = omc * (fp - A), b = smc * (fm - B);
+        d[i] = (A + B) + (a + b);
+        d[o] = (A - B) + (a - b);
+      } else {
+        d[i] = omc * d[i] + om * (A + B);
+        d[o] = omc * d[o] + om * (A - B);
+      }
+    });
   }
   return rho;
 }
@@ -578,7 +672,7 @@ __device__ __forceinline__ void scalar_step(const StepParams<Real> &p, int x, in
   const Real oT = p.omega_T, T = sc.T;
   static_for<G::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    const Real gi = plane(p.g, i, p.cs)[c];
+    const Real gi = p.g[elem(p, i, c)];
     Real gp;
     if (solid) {
       gp = Real(Dir<G, i>::w) * T;
@@ -590,13 +684,13 @@ __device__ __forceinline__ void scalar_step(const StepParams<Real> &p, int x, in
     const int xd = wrap_n(x + Dir<G, i>::x, p.nx);
     const int yd = wrap_n(y + Dir<G, i>::y, p.ny);
     const int zd = L::DIMS == 3 ? wrap_n(z + Dir<G, i>::z, p.nz) : 0;
-    if (yd != 0 && yd != p.ny - 1) plane(p.gn, i, p.cs)[cell_index(p, xd, yd, zd)] = gp;
+    if (yd != 0 && yd != p.ny - 1) p.gn[elem(p, i, cell_index(p, xd, yd, zd))] = gp;
   });
   if (y == 0 || y == p.ny - 1) {
     const Real Tw = y == 0 ? p.T_hot : p.T_cold;
     static_for<G::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      plane(p.gn, i, p.cs)[c] = Real(Dir<G, i>::w) * Tw;
+      p.gn[elem(p, i, c)] = Real(Dir<G, i>::w) * Tw;
     });
   }
 }
@@ -619,7 +713,7 @@ __device__ __forceinline__ void link_cell_forces(const StepParams<Real> &p, int 
   Real drho = 0, jx = 0, jy = 0, jz = 0;
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    const Real v = SO::template load<i, L>(plane(P, i, p.cs), c);
+    const Real v = SO::template load<i, L>(P, elem(p, i, c));
     drho += v;
     if (Dir<L, i>::x) jx += Dir<L, i>::x * v;
     if (Dir<L, i>::y) jy += Dir<L, i>::y * v;
@@ -639,7 +733,7 @@ __device__ __forceinline__ void link_cell_forces(const StepParams<Real> &p, int 
       if ((mask >> i) & 1u) {
         constexpr int o = L::opp[i];
         constexpr Real ex = Dir<L, i>::x, ey = Dir<L, i>::y, ez = Dir<L, i>::z;
-        const Real fi = SO::template load<i, L>(plane(P, i, p.cs), c);
+        const Real fi = SO::template load<i, L>(P, elem(p, i, c));
         const Real eui = ex * ux + ey * uy + ez * uz;
         const Real quad = Real(4.5) * eui * eui - Real(1.5) * usq;
         const Real deq_i = Real(Dir<L, i>::w) * (drho + rho * (Real(3) * eui + quad));
@@ -688,7 +782,7 @@ __global__ void __launch_bounds__(kStepBlock, sizeof(typename StoreOps<S>::Real)
     const S *P = static_cast<const S *>(p.P);
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      d[i] = SO::template load<i, L>(plane(P, i, p.cs), c);
+      d[i] = SO::template load<i, L>(P, elem(p, i, c));
     });
   } else {
     step_now = *p.step;
@@ -725,7 +819,7 @@ __global__ void __launch_bounds__(kStepBlock, sizeof(typename StoreOps<S>::Real)
   S *Pn = static_cast<S *>(p.Pn);
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    SO::template store<i, L>(plane(Pn, i, p.cs), c, d[i]);
+    SO::template store<i, L>(Pn, elem(p, i, c), d[i]);
   });
 }
 
@@ -744,7 +838,7 @@ __global__ void __launch_bounds__(kStepBlock) k_moments(const StepParams<typenam
     const S *P = static_cast<const S *>(p.P);
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      d[i] = SO::template load<i, L>(plane(P, i, p.cs), c);
+      d[i] = SO::template load<i, L>(P, elem(p, i, c));
     });
   } else {
     full_state<L, S, Real>(p, x, y, z, *p.step, d, nullptr, nullptr);
@@ -850,7 +944,7 @@ __global__ void __launch_bounds__(kStepBlock) k_state_out(const StepParams<typen
     const S *P = static_cast<const S *>(p.P);
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      d[i] = SO::template load<i, L>(plane(P, i, p.cs), c);
+      d[i] = SO::template load<i, L>(P, elem(p, i, c));
     });
   } else {
     full_state<L, S, Real>(p, x, y, z, *p.step + step_delta, d, nullptr, nullptr);
@@ -874,7 +968,7 @@ __global__ void __launch_bounds__(kStepBlock) k_load_state(const StepParams<type
   const uint32_t c = cell_index(p, x, y, z);
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    SO::template store<i, L>(plane(dst, i, p.cs), c, (Real)(in[(int64_t)i * p.ncells + c] - Dir<L, i>::w));
+    SO::template store<i, L>(dst, elem(p, i, c), (Real)(in[(int64_t)i * p.ncells + c] - Dir<L, i>::w));
   });
 }
 

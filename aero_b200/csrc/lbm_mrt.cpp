@@ -239,7 +239,212 @@ bool build(double omega, MrtCoeffs<double> &out, double *A_full, double *B_full)
   return true;
 }
 
+// D3Q19 blocks in the cubic-symmetry-adapted basis.  From the pair-basis
+// blocks (even Ae/Be 10x10 on s, odd Ao/Bo 9x9 on t) the change of basis
+//   g = V s: rest, face sum, edge sum, face doublet (2X-Y-Z, Y-Z), edge
+//            doublet (2Pyz-Pxz-Pxy, Pxz-Pxy), shear differences (3)
+//   h = W t: face differences (3), momentum-like edge sums (3), remaining
+//            odd edge combinations (3)
+// makes the operator block diagonal.  Every entry outside the expected
+// blocks, every mismatch between blocks that symmetry makes equal, and any
+// non-zero on the last three odd coordinates is rejected.
+bool build_adapted(const Mat &Ap, const Mat &Bp, Mrt3Adapted<double> &m) {
+  const int Q = 19;
+  double V[10][10] = {{0}}, W[9][9] = {{0}};
+  V[0][0] = 1;
+  V[1][1] = V[1][2] = V[1][3] = 1;
+  for (int k = 4; k < 10; k++) V[2][k] = 1;
+  V[3][1] = 2; V[3][2] = -1; V[3][3] = -1;
+  V[4][2] = 1; V[4][3] = -1;
+  V[5][4] = V[5][5] = -1; V[5][6] = V[5][7] = -1; V[5][8] = V[5][9] = 2;
+  V[6][4] = V[6][5] = -1; V[6][6] = V[6][7] = 1;
+  V[7][4] = 1; V[7][5] = -1;
+  V[8][6] = 1; V[8][7] = -1;
+  V[9][8] = 1; V[9][9] = -1;
+  // odd: t index k -> pair k (t4..t9 at columns 3..8)
+  W[0][0] = 1; W[1][1] = 1; W[2][2] = 1;
+  const double xy_x[9] = {0, 0, 0, 1, -1, 0, 0, 0, 0}, xz_x[9] = {0, 0, 0, 0, 0, 1, -1, 0, 0};
+  const double xy_y[9] = {0, 0, 0, 1, 1, 0, 0, 0, 0}, yz_y[9] = {0, 0, 0, 0, 0, 0, 0, 1, -1};
+  const double xz_z[9] = {0, 0, 0, 0, 0, 1, 1, 0, 0}, yz_z[9] = {0, 0, 0, 0, 0, 0, 0, 1, 1};
+  for (int k = 0; k < 9; k++) {
+    W[3][k] = xy_x[k] + xz_x[k];
+    W[4][k] = xy_y[k] + yz_y[k];
+    W[5][k] = xz_z[k] + yz_z[k];
+    W[6][k] = xy_x[k] - xz_x[k];
+    W[7][k] = xy_y[k] - yz_y[k];
+    W[8][k] = xz_z[k] - yz_z[k];
+  }
+  Mat Vm(100), Wm(81), Vi, Wi;
+  for (int r = 0; r < 10; r++)
+    for (int c = 0; c < 10; c++) Vm[r * 10 + c] = V[r][c];
+  for (int r = 0; r < 9; r++)
+    for (int c = 0; c < 9; c++) Wm[r * 9 + c] = W[r][c];
+  pinv(Vm, 10, Vi);
+  pinv(Wm, 9, Wi);
+  Mat Ae(100), Be(100), Ao(81), Bo(81);
+  for (int r = 0; r < 10; r++)
+    for (int c = 0; c < 10; c++) {
+      Ae[r * 10 + c] = Ap[r * Q + c];
+      Be[r * 10 + c] = Bp[r * Q + c];
+    }
+  for (int r = 0; r < 9; r++)
+    for (int c = 0; c < 9; c++) {
+      Ao[r * 9 + c] = Ap[(10 + r) * Q + 10 + c];
+      Bo[r * 9 + c] = Bp[(10 + r) * Q + 10 + c];
+    }
+  Mat T1, Aa, Ba, Oa, Ob;
+  matmul(Vm, Ae, 10, T1); matmul(T1, Vi, 10, Aa);
+  matmul(Vm, Be, 10, T1); matmul(T1, Vi, 10, Ba);
+  matmul(Wm, Ao, 9, T1); matmul(T1, Wi, 9, Oa);
+  matmul(Wm, Bo, 9, T1); matmul(T1, Wi, 9, Ob);
+  // equilibrium: even pair-basis seq = G me_std, me_std = (drho, kxx, kyy, kzz, kxy, kxz, kyz)
+  // with k_ab = rho u_a u_b; adapted inputs m_ad = (drho, ru2, mE1, mE2, kxy, kxz, kyz)
+  double G[10][7] = {{0}};
+  for (int k = 0; k < 10; k++) {
+    const int i = k == 0 ? 0 : D3Q19::pair[k - 1];
+    const double ww = k == 0 ? D3Q19::w[0] : 2.0 * D3Q19::w[i];
+    const double ex = D3Q19::ex[i], ey = D3Q19::ey[i], ez = D3Q19::ez[i];
+    G[k][0] = ww;
+    G[k][1] = ww * (4.5 * ex * ex - 1.5);
+    G[k][2] = ww * (4.5 * ey * ey - 1.5);
+    G[k][3] = ww * (4.5 * ez * ez - 1.5);
+    G[k][4] = ww * 9.0 * ex * ey;
+    G[k][5] = ww * 9.0 * ex * ez;
+    G[k][6] = ww * 9.0 * ey * ez;
+  }
+  const double Tm[7][7] = {{1, 0, 0, 0, 0, 0, 0},
+                           {0, 1.0 / 3, 1.0 / 3, 0, 0, 0, 0},
+                           {0, 1.0 / 3, -1.0 / 6, 0.5, 0, 0, 0},
+                           {0, 1.0 / 3, -1.0 / 6, -0.5, 0, 0, 0},
+                           {0, 0, 0, 0, 1, 0, 0},
+                           {0, 0, 0, 0, 0, 1, 0},
+                           {0, 0, 0, 0, 0, 0, 1}};
+  double K[10][7] = {{0}};  // adapted outputs x adapted inputs
+  for (int r = 0; r < 10; r++)
+    for (int q = 0; q < 7; q++) {
+      double acc = 0;
+      for (int a = 0; a < 10; a++) {
+        double vb = 0;  // (Ba V)[r][a]
+        for (int b = 0; b < 10; b++) vb += Ba[r * 10 + b] * Vm[b * 10 + a];
+        double gt = 0;  // (G Tm)[a][q]
+        for (int c = 0; c < 7; c++) gt += G[a][c] * Tm[c][q];
+        acc += vb * gt;
+      }
+      K[r][q] = acc;
+    }
+  // odd equilibrium: teq = H (rho u), H[k][a] = 6 w e_a of pair k
+  double Ko[9][3] = {{0}};
+  for (int r = 0; r < 9; r++)
+    for (int q = 0; q < 3; q++) {
+      double acc = 0;
+      for (int a = 0; a < 9; a++) {
+        double wb = 0;
+        for (int b = 0; b < 9; b++) wb += Ob[r * 9 + b] * Wm[b * 9 + a];
+        const int i = D3Q19::pair[a];
+        const double e = q == 0 ? D3Q19::ex[i] : (q == 1 ? D3Q19::ey[i] : D3Q19::ez[i]);
+        acc += wb * 6.0 * D3Q19::w[i] * e;
+      }
+      Ko[r][q] = acc;
+    }
+  // --- expected structure -------------------------------------------------
+  auto eb = [](int r) { return r < 3 ? 0 : (r == 3 || r == 5) ? 1 : (r == 4 || r == 6) ? 2 : r; };
+  auto ob = [](int r) { return r == 0 || r == 3 ? 0 : (r == 1 || r == 4) ? 1 : (r == 2 || r == 5) ? 2 : r; };
+  double scale = 0, err = 0;
+  for (int r = 0; r < 10; r++)
+    for (int c = 0; c < 10; c++) {
+      scale = std::fmax(scale, std::fabs(Aa[r * 10 + c]));
+      if (eb(r) != eb(c)) err = std::fmax(err, std::fabs(Aa[r * 10 + c]));
+    }
+  for (int r = 0; r < 9; r++)
+    for (int c = 0; c < 9; c++)
+      if (ob(r) != ob(c) || r >= 6) err = std::fmax(err, std::fabs(Oa[r * 9 + c]));
+  auto A = [&](int r, int c) { return Aa[r * 10 + c]; };
+  auto O = [&](int r, int c) { return Oa[r * 9 + c]; };
+  // doublet components share one block; triplets share one block
+  err = std::fmax(err, std::fabs(A(3, 3) - A(4, 4)));
+  err = std::fmax(err, std::fabs(A(3, 5) - A(4, 6)));
+  err = std::fmax(err, std::fabs(A(5, 3) - A(6, 4)));
+  err = std::fmax(err, std::fabs(A(5, 5) - A(6, 6)));
+  err = std::fmax(err, std::fmax(std::fabs(A(7, 7) - A(8, 8)), std::fabs(A(7, 7) - A(9, 9))));
+  for (int q = 1; q < 3; q++) {
+    err = std::fmax(err, std::fabs(O(0, 0) - O(q, q)));
+    err = std::fmax(err, std::fabs(O(0, 3) - O(q, 3 + q)));
+    err = std::fmax(err, std::fabs(O(3, 0) - O(3 + q, q)));
+    err = std::fmax(err, std::fabs(O(3, 3) - O(3 + q, 3 + q)));
+  }
+  // equilibrium couplings: A1 rows take (drho, ru2); doublets take mE1 / mE2
+  // with equal weights; shear rows take their own k; nothing else
+  for (int r = 0; r < 10; r++)
+    for (int q = 0; q < 7; q++) {
+      const bool allowed = (r < 3 && q < 2) || ((r == 3 || r == 5) && q == 2) || ((r == 4 || r == 6) && q == 3) ||
+                           (r >= 7 && q == r - 3);
+      if (!allowed) err = std::fmax(err, std::fabs(K[r][q]));
+    }
+  err = std::fmax(err, std::fabs(K[3][2] - K[4][3]));
+  err = std::fmax(err, std::fabs(K[5][2] - K[6][3]));
+  err = std::fmax(err, std::fmax(std::fabs(K[7][4] - K[8][5]), std::fabs(K[7][4] - K[9][6])));
+  for (int r = 0; r < 9; r++)
+    for (int q = 0; q < 3; q++) {
+      const bool allowed = (r < 3 && q == r) || (r >= 3 && r < 6 && q == r - 3);
+      if (!allowed) err = std::fmax(err, std::fabs(Ko[r][q]));
+    }
+  for (int q = 1; q < 3; q++) {
+    err = std::fmax(err, std::fabs(Ko[0][0] - Ko[q][q]));
+    err = std::fmax(err, std::fabs(Ko[3][0] - Ko[3 + q][q]));
+  }
+  if (!(err <= 1e-12 * std::fmax(scale, 1.0))) return false;
+  for (int r = 0; r < 3; r++) {
+    for (int c = 0; c < 3; c++) m.a1[r * 3 + c] = A(r, c);
+    m.ca1[r * 2 + 0] = K[r][0];
+    m.ca1[r * 2 + 1] = K[r][1];
+  }
+  m.e[0] = A(3, 3); m.e[1] = A(3, 5); m.e[2] = A(5, 3); m.e[3] = A(5, 5);
+  m.ce[0] = K[3][2]; m.ce[1] = K[5][2];
+  m.t2 = A(7, 7); m.ct2 = K[7][4];
+  m.v[0] = O(0, 0); m.v[1] = O(0, 3); m.v[2] = O(3, 0); m.v[3] = O(3, 3);
+  m.cv[0] = Ko[0][0]; m.cv[1] = Ko[3][0];
+  return true;
+}
+
 }  // namespace
+
+bool build_mrt3_adapted(double omega, Mrt3Adapted<double> &m) {
+  // pair-basis operator of the reference D3Q19 basis
+  const int Q = 19;
+  Mat M, Minv;
+  moment_basis<D3Q19>(M);
+  std::vector<double> s;
+  relax_vector<D3Q19>(omega, s);
+  pinv(M, Q, Minv);
+  Mat ImS(Q * Q), SM(Q * Q);
+  for (int r = 0; r < Q; r++)
+    for (int c = 0; c < Q; c++) {
+      ImS[r * Q + c] = (1.0 - s[r]) * M[r * Q + c];
+      SM[r * Q + c] = s[r] * M[r * Q + c];
+    }
+  Mat A, B, U(Q * Q, 0.0), Uinv(Q * Q, 0.0), T, Ap, Bp;
+  matmul(Minv, ImS, Q, A);
+  matmul(Minv, SM, Q, B);
+  const int NE = 10;
+  U[0] = 1.0;
+  Uinv[0] = 1.0;
+  for (int k = 0; k < 9; k++) {
+    const int i = D3Q19::pair[k], o = D3Q19::opp[i];
+    U[(k + 1) * Q + i] = 1.0;
+    U[(k + 1) * Q + o] = 1.0;
+    U[(NE + k) * Q + i] = 1.0;
+    U[(NE + k) * Q + o] = -1.0;
+    Uinv[i * Q + (k + 1)] = 0.5;
+    Uinv[i * Q + (NE + k)] = 0.5;
+    Uinv[o * Q + (k + 1)] = 0.5;
+    Uinv[o * Q + (NE + k)] = -0.5;
+  }
+  matmul(U, A, Q, T);
+  matmul(T, Uinv, Q, Ap);
+  matmul(U, B, Q, T);
+  matmul(T, Uinv, Q, Bp);
+  return build_adapted(Ap, Bp, m);
+}
 
 bool build_mrt(int dims, double omega, MrtCoeffs<double> &out, double *A_full, double *B_full) {
   return dims == 2 ? build<D2Q9>(omega, out, A_full, B_full) : build<D3Q19>(omega, out, A_full, B_full);

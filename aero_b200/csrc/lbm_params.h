@@ -40,6 +40,15 @@ struct MrtCoeffs {
   Real Co[9 * 3];
 };
 
+// D3Q19 MRT blocks in the cubic-symmetry-adapted basis (see lbm_mrt.cpp):
+// a1 3x3 (scalars), ca1 3x2 (their equilibrium inputs drho, rho u.u),
+// e 2x2 and ce 2x1 (doublets), t2 / ct2 (shear-type edge differences),
+// v 2x2 and cv 2x1 (momentum-like pairs).
+template <class Real>
+struct Mrt3Adapted {
+  Real a1[9], ca1[6], e[4], ce[2], t2, ct2, v[4], cv[2];
+};
+
 // Everything a kernel needs for one step of one lattice.  Passed by value
 // (kernel parameter space), so per-step variation lives in device memory
 // (step counter) and the struct can be captured once in a CUDA graph.
@@ -96,7 +105,8 @@ struct StepParams {
   Real bf_x, bf_y, bf_z, bf_coeff;
   Real omega_T, T_hot, T_cold, gbeta, T_ref;
   double center[3];
-  MrtCoeffs<Real> mrt;
+  MrtCoeffs<Real> mrt;      // D2Q9
+  Mrt3Adapted<Real> mrt3;   // D3Q19
 };
 
 }  // namespace aero

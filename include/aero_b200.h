@@ -157,6 +157,13 @@ AERO_API const char *aero_last_error(void);
  * caller can check the engine's operator. */
 AERO_API int aero_mrt_operator(int32_t dims, double omega, double *A, double *B);
 
+/* Runs the engine's collision arithmetic (the device code compiled for the
+ * host, FP64) on n cells: f_in / f_out are (Q, n) absolute populations,
+ * solid may be NULL.  Lets a caller check the collision operators on a CPU
+ * (kernels.py:42-92, kernels_trt.py:125-174, kernels3d_mrt.py:24-82). */
+AERO_API int aero_collide_host(const AeroParams *params, const double *f_in, double *f_out,
+                               const uint8_t *solid, int64_t n);
+
 /* Number of lattice directions and scalar directions for the options. */
 AERO_API int aero_lattice_q(const AeroParams *params, int32_t *q, int32_t *q_scalar);
 
