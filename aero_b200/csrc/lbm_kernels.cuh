@@ -637,9 +637,12 @@ AERO_HD Real collide(const StepParams<Real> &p, Real (&d)[L::Q], bool solid, Rea
       }
     }
     const Real omc = Real(1) - om, smc = Real(1) - sm;
+    (void)omc;
     {
+      // the rest population is even: both rates give omega.  BGK is written
+      // as d + omega (feq - d) so that FP32 rounds only the small correction.
       const Real A0 = Real(Dir<L, 0>::w) * (drho - rho * usq15);
-      d[0] = omc * d[0] + om * A0;  // the rest population is even: both rates give omega
+      d[0] = d[0] + om * (A0 - d[0]);
     }
     static_for<L::NP>([&](auto pc) {
       constexpr int k = decltype(pc)::value;
@@ -649,13 +652,14 @@ AERO_HD Real collide(const StepParams<Real> &p, Real (&d)[L::Q], bool solid, Rea
       const Real A = wi * (drho + rho * (Real(4.5) * eu * eu - usq15));
       const Real B = (Real(3) * wi) * rho * eu;
       if constexpr (COLL == COLL_TRT) {
+        // d_i + (f+ relaxation) + (f- relaxation), small corrections only
         const Real fp = Real(0.5) * (d[i] + d[o]), fm = Real(0.5) * (d[i] - d[o]);
-        const Real a = omc * (fp - A), b = smc * (fm - B);
-        d[i] = (A + B) + (a + b);
-        d[o] = (A - B) + (a - b);
+        const Real a = om * (A - fp), b = sm * (B - fm);
+        d[i] = d[i] + (a + b);
+        d[o] = d[o] + (a - b);
       } else {
-        d[i] = omc * d[i] + om * (A + B);
-        d[o] = omc * d[o] + om * (A - B);
+        d[i] = d[i] + om * ((A + B) - d[i]);
+        d[o] = d[o] + om * ((A - B) - d[o]);
       }
     });
   }

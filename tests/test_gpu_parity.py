@@ -129,8 +129,9 @@ def test_run_matches_oracle_1000_steps_fp32():
         cd.append(o.step()[0]["Cd"])
     got = _macro(s.f, 2)
     ref = _macro(o.f, 2)
-    assert rel_l2(got[0], ref[0]) <= 1e-5                                   # rho
-    assert rel_l2(np.stack(got[1:]), np.stack(ref[1:])) <= 1e-5             # u = (ux, uy)
+    e_rho, e_u = rel_l2(got[0], ref[0]), rel_l2(np.stack(got[1:]), np.stack(ref[1:]))
+    assert e_rho <= 1e-5, e_rho                                             # rho
+    assert e_u <= 1e-5, e_u                                                 # u = (ux, uy)
     assert abs(np.mean(r["Cd_history"][-200:]) - np.mean(cd[-200:])) <= 1e-3 * abs(np.mean(cd[-200:]))
 
 
