@@ -624,44 +624,42 @@ AERO_HD Real collide(const StepParams<Real> &p, Real (&d)[L::Q], bool solid, Rea
     (void)om;
     (void)per_cell_omega;
   } else {
-    // BGK / TRT per +/- pair: feq_i - w_i = A + B, feq_opp - w_opp = A - B with
-    // A = w (drho + rho (4.5 (e.u)^2 - 1.5 u.u)) and B = 3 w rho (e.u).
-    const Real usq15 = Real(1.5) * (ux * ux + uy * uy + uz * uz);
-    Real sm = p.trt_sminus;
+    // BGK / TRT.  The equilibrium is evaluated per direction exactly as the
+    // reference writes it, and the update is applied as a correction to d
+    // (d + omega (feq - d)); both choices keep the FP32 rounding smallest
+    // (measured against the FP64 oracle on the 400x200 channel).
+    const Real usq = ux * ux + uy * uy + uz * uz;
+    Real deq[L::Q];
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      const Real eu = Dir<L, i>::x * ux + Dir<L, i>::y * uy + Dir<L, i>::z * uz;
+      deq[i] = Real(Dir<L, i>::w) * (drho + rho * (Real(3) * eu + Real(4.5) * eu * eu - Real(1.5) * usq));
+    });
     if constexpr (COLL == COLL_TRT) {
+      Real sm = p.trt_sminus;
       if (per_cell_omega) {
         const Real tau = Real(1) / om, lam = p.trt_lambda;
         const Real tp = lam * tau + (Real(1) - lam);
         const Real tm = (tp * tau - Real(0.5)) / (tp - Real(0.5));
         sm = Real(1) / tm;
       }
-    }
-    const Real omc = Real(1) - om, smc = Real(1) - sm;
-    (void)omc;
-    {
-      // the rest population is even: both rates give omega.  BGK is written
-      // as d + omega (feq - d) so that FP32 rounds only the small correction.
-      const Real A0 = Real(Dir<L, 0>::w) * (drho - rho * usq15);
-      d[0] = d[0] + om * (A0 - d[0]);
-    }
-    static_for<L::NP>([&](auto pc) {
-      constexpr int k = decltype(pc)::value;
-      constexpr int i = L::pair[k], o = L::opp[L::pair[k]];
-      constexpr Real wi = Real(Dir<L, i>::w);
-      const Real eu = Real(Dir<L, i>::x) * ux + Real(Dir<L, i>::y) * uy + Real(Dir<L, i>::z) * uz;
-      const Real A = wi * (drho + rho * (Real(4.5) * eu * eu - usq15));
-      const Real B = (Real(3) * wi) * rho * eu;
-      if constexpr (COLL == COLL_TRT) {
-        // d_i + (f+ relaxation) + (f- relaxation), small corrections only
+      d[0] = d[0] + om * (deq[0] - d[0]);  // the rest population is even
+      static_for<L::NP>([&](auto pc) {
+        constexpr int k = decltype(pc)::value;
+        constexpr int i = L::pair[k], o = L::opp[L::pair[k]];
         const Real fp = Real(0.5) * (d[i] + d[o]), fm = Real(0.5) * (d[i] - d[o]);
-        const Real a = om * (A - fp), b = sm * (B - fm);
+        const Real ep = Real(0.5) * (deq[i] + deq[o]), em = Real(0.5) * (deq[i] - deq[o]);
+        const Real a = om * (ep - fp), b = sm * (em - fm);
         d[i] = d[i] + (a + b);
         d[o] = d[o] + (a - b);
-      } else {
-        d[i] = d[i] + om * ((A + B) - d[i]);
-        d[o] = d[o] + om * ((A - B) - d[o]);
-      }
-    });
+      });
+    } else {
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        d[i] = d[i] + om * (deq[i] - d[i]);
+      });
+    }
+    (void)per_cell_omega;
   }
   return rho;
 }

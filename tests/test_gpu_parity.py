@@ -135,6 +135,30 @@ def test_run_matches_oracle_1000_steps_fp32():
     assert abs(np.mean(r["Cd_history"][-200:]) - np.mean(cd[-200:])) <= 1e-3 * abs(np.mean(cd[-200:]))
 
 
+@pytest.mark.parametrize("collision", ["mrt", "trt"])
+def test_sphere_fp32_matches_oracle_300_steps(collision):
+    """D3Q19 sphere channel with Bouzidi links, slip walls, sponge and
+    convective outlet at a stable tau (0.6): rel-L2(rho, u) <= 1e-5 after 300
+    steps against the FP64 oracle (guards the FP32 accuracy of the
+    symmetry-adapted MRT and of TRT)."""
+    from aero_b200 import Solver3D, Sphere
+    from oracle.oracle import OracleSolver
+    nz, ny, nx = 40, 40, 96
+    sph = Sphere(radius=6, cx_frac=0.25, cy_frac=0.5, cz_frac=0.5)
+    solid, phi = sph.mark_solid(nz, ny, nx), sph.sdf_field(nz, ny, nx)
+    kw = dict(omega=1 / 0.6, u0=0.05, D=sph.reference_length(), collision=collision, bouzidi=True,
+              phi=phi, wall_bc="slip", outlet_bc="convective", sponge_thickness=8, trt_lambda=0.25)
+    s = Solver3D(Nz=nz, Ny=ny, Nx=nx, solid=solid, precision="fp32", **kw)
+    o = OracleSolver(solid=solid, **kw)
+    s.run(300, check_every=301, verbose=False)
+    for _ in range(300):
+        o.step_raw()
+    got, ref = _macro(s.f, 3), _macro(o.f, 3)
+    e_rho, e_u = rel_l2(got[0], ref[0]), rel_l2(np.stack(got[1:]), np.stack(ref[1:]))
+    assert e_rho <= 1e-5, e_rho
+    assert e_u <= 1e-5, e_u
+
+
 def test_state_roundtrip_and_checkpoint(tmp_path):
     c = load_case("c3d_trt_wale_periodic_bodyforce_thermal")
     s = _solver(c, precision="fp64")
