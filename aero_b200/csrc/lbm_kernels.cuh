@@ -19,9 +19,10 @@
 // outlet copy (which reads the column x = Nx-2 after bounce-back): an outlet
 // cell simply evaluates the chain for its x = Nx-2 neighbour.  The momentum-
 // exchange forces of the step (forces.py:15-162, forces3d.py:8-171) need the
-// pre-stream P and the post-BC state at link cells; k_forces recomputes the
-// state of each link cell from the same P buffer, so it reads only buffers
-// that k_step does not write and the pair can run in either order.
+// pre-stream P and the post-BC state at link cells; k_step has both in
+// registers at every link cell and writes that cell's twelve sums to a slot
+// of lc_contrib, and k_finalize (one block, launched after k_step) adds the
+// slots in a fixed order in FP64.
 #pragma once
 #include <cuda_runtime.h>
 

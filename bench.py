@@ -34,6 +34,7 @@ import argparse
 import json
 import os
 import pathlib
+import re
 import statistics
 import subprocess
 import sys
@@ -74,6 +75,21 @@ PEAK_FALLBACK_GBS = 6650.0
 def _rank_env():
     return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
             int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def max_over_ranks(x: float, dist=None, device=None) -> float:
+    """The largest x over all ranks (x itself without a process group)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_mlups(cells_per_rank: int, world: int, steps: int, seconds: float) -> float:
+    """Cell updates of all replicas per second, in millions."""
+    return cells_per_rank * world * steps / seconds / 1e6
 
 
 def _peak_hbm():
@@ -297,11 +313,8 @@ def main():
     eng.enable_timing(False)
     status = eng.status()
     first_bad = eng.first_bad_step()
-    if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = ncells * world * args.steps / (ms / 1e3) / 1e6
+    ms = max_over_ranks(ms, dist, dev)
+    value = whole_job_mlups(ncells, world, args.steps, ms / 1e3)
     launches_per_step = 2 + (1 if (s.les and s.collision != "mrt") else 0)
 
     # roofline of the fused step kernel
@@ -315,13 +328,16 @@ def main():
     alg_bytes = bytes_per_cell * ncells
     k_ms = step_ms / max(nt, 1)
     achieved = alg_bytes / (k_ms / 1e3) / 1e9
+    # DRAM bytes per launch from the committed ncu capture summary of this
+    # kernel and precision (a smaller case scaled by cells where the summary
+    # says so); None when no capture covers the workload
     traffic = None
-    prof_json = ROOT / "profiles" / f"k_step_{args.workload}_{args.precision}.json"
-    if prof_json.exists():
-        try:
-            traffic = json.loads(prof_json.read_text()).get("dram_bytes_per_launch")
-        except Exception:
-            traffic = None
+    pat = re.compile(rf"^- {re.escape(args.workload)}: dram bytes per launch = (\d+)\s*$", re.M)
+    for md in sorted((ROOT / "profiles").glob(f"k_step_*_{args.precision}.md")):
+        m = pat.search(md.read_text())
+        if m:
+            traffic = int(m.group(1))
+            break
 
     # ---------------- end to end through the public API ------------------
     e2e = None
@@ -342,14 +358,11 @@ def main():
         r = s.run(args.steps, check_every=args.steps + 1, verbose=False)
         torch.cuda.synchronize(dev)
         dt = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([dt], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
+        dt = max_over_ranks(dt, dist, dev)
         h2d = f0_host.numel() * 8 + prev_host.numel() * 8 + (0 if g_host is None else g_host.numel() * 8)
         d2h = (args.steps * 12 * 8 + nz * 3 * 8 + Q * ny * nx * 8 + 4 * ncells * 8
                + (ncells * 8 if s.thermal else 0))
-        e2e = {"value": ncells * world * args.steps / dt / 1e6, "unit": "MLUPS",
+        e2e = {"value": whole_job_mlups(ncells, world, args.steps, dt), "unit": "MLUPS",
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "call": "Solver3D.run(K) after uploading the initial state from pinned host memory",
                "Cd_mean": r["Cd_mean"]}
