@@ -65,6 +65,8 @@ SIGNATURES = {
     "aero_mrt_operator": ([_I32, _D, _VP, _VP], ctypes.c_int),
     "aero_enable_timing": ([_VP, _I32], ctypes.c_int),
     "aero_collide_host": ([ctypes.POINTER(AeroParams), _VP, _VP, _VP, _I64], ctypes.c_int),
+    "aero_link_forces_static": ([_I32, _I32, _I32, _I32, _VP, _VP, _VP, _I64, _VP, _VP, _VP, _VP],
+                                ctypes.c_int),
     "aero_kernel_times": ([_VP, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_I64), _VP],
                           ctypes.c_int),
 }

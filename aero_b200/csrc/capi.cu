@@ -86,6 +86,11 @@ unsigned blocks_for(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
 }  // namespace
 
+int aero::set_error(int code, const char *msg) {
+  g_err = msg ? msg : "";
+  return code;
+}
+
 struct AeroLattice {
   AeroParams prm;
   int Q = 0, Qg = 0;

@@ -28,4 +28,7 @@ bool build_mrt(int dims, double omega, MrtCoeffs<double> &out, double *A_full, d
 bool build_mrt3_adapted(double omega, Mrt3Adapted<double> &out);
 bool mrt_pinv_basis(int dims, double *M_out, double *Minv_out);
 
+// Records the message returned by aero_last_error() and returns code.
+int set_error(int code, const char *msg);
+
 }  // namespace aero

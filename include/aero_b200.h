@@ -38,7 +38,8 @@ enum {
   AERO_ERR_CUDA = -2,        /* a CUDA call failed */
   AERO_ERR_STATE = -3,       /* call out of order (e.g. step before bind) */
   AERO_ERR_UNSUPPORTED = -4, /* option outside the engine (IBM, SEM inlet, ...) */
-  AERO_ERR_CAPACITY = -5     /* force history full: read it first */
+  AERO_ERR_CAPACITY = -5     /* a fixed capacity is exceeded: force history full (read it
+                                first), or a link list too long for a fixed scratch */
 };
 
 enum { AERO_STORE_F32 = 0, AERO_STORE_F64 = 1, AERO_STORE_F16 = 2, AERO_STORE_BF16 = 3 };
@@ -178,6 +179,26 @@ AERO_API int aero_abi_version(void);
 AERO_API int aero_enable_timing(AeroLattice *lat, int32_t on);
 AERO_API int aero_kernel_times(AeroLattice *lat, double *step_ms, double *forces_ms, int64_t *steps,
                                void *stream);
+
+/* Momentum-exchange forces for callers that cannot allocate GPU memory.
+ * No counterpart in the reference (its force sums run on host arrays).
+ * Real-time loops whose device memory is fixed in advance, and host
+ * frameworks that only lend out buffers they own and forbid a library to
+ * allocate behind their back, cannot call cudaMalloc (or a caching
+ * allocator); this entry point allocates nothing.  Given device arrays
+ * f_pre and f_post (Q, nz, ny, nx) float64 and the link list (n_links rows
+ * of [i, (z,) y, x] int32), it writes the AERO_FORCE_VALUES sums of
+ * forces.py / forces3d.py to out (device, 12 doubles) and, if profile is not
+ * NULL, the per-row (2D) / per-plane (3D) force profile (device, 3 doubles per
+ * row/plane).  center is a HOST pointer to (x, y, z).  Its per-link scratch is
+ * a fixed 4 MiB array in the library's device image, so n_links is limited to
+ * 32768 (larger lists return AERO_ERR_CAPACITY).  Every call shares that
+ * array: calls that overlap on the GPU race.  The first call on a device
+ * looks the array's address up (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture. */
+AERO_API int aero_link_forces_static(int32_t dims, int32_t nx, int32_t ny, int32_t nz, const double *f_pre,
+                                     const double *f_post, const int32_t *links, int64_t n_links,
+                                     const double *center, double *out, double *profile, void *stream);
 
 /* sizeof(AeroParams), so bindings can check their struct layout. */
 AERO_API int aero_params_size(void);
