@@ -46,7 +46,7 @@ constexpr uint64_t kAlign = 256;
 uint64_t align_up(uint64_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
 struct Layout {
-  uint64_t P[2], solid, lbits, loff, lc_mask, lc_q, lc_cell, lc_contrib, prof_off, force_const, prof_const,
+  uint64_t P[2], solid, lbits, loff, lc_mask, lc_q, lc_cell, lc_contrib, fin_partial, prof_off, force_const, prof_const,
       prev[2], g[2], U, cs_cell, hist, prof_out, counters, total;
 };
 
@@ -184,6 +184,14 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   p.Uw = reinterpret_cast<Real *>(ws + L->lay.U);
   p.cs_cell = reinterpret_cast<const Real *>(ws + L->lay.cs_cell);
   p.lc_contrib = reinterpret_cast<double *>(ws + L->lay.lc_contrib);
+  p.fin_partial = reinterpret_cast<double *>(ws + L->lay.fin_partial);
+  {
+    // about 1024 link cells per finalisation block (4 per thread)
+    const int64_t nlc = (int64_t)L->lc_cell.size();
+    const int64_t nb = std::min<int64_t>(std::max<int64_t>((nlc + 1023) / 1024, 1), kFinalizeMaxBlocks);
+    p.fin_blocks = (int32_t)nb;
+    p.fin_chunk = (nlc + nb - 1) / nb;
+  }
   p.force_const = reinterpret_cast<const double *>(ws + L->lay.force_const);
   p.prof_const = reinterpret_cast<const double *>(ws + L->lay.prof_const);
   p.prof_off = reinterpret_cast<const int32_t *>(ws + L->lay.prof_off);
@@ -195,6 +203,8 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   int64_t *ctr = reinterpret_cast<int64_t *>(ws + L->lay.counters);
   p.step = ctr;
   p.hist_base = ctr + 1;
+  p.profile_step = ctr + 4;
+  p.fin_ticket = reinterpret_cast<uint32_t *>(ctr + 5);
   p.status = reinterpret_cast<uint32_t *>(ctr + 2);
   p.first_bad_step = reinterpret_cast<unsigned long long *>(ctr + 3);
   const double tau = 1.0 / a.omega;
@@ -598,6 +608,7 @@ int aero_set_geometry(AeroLattice *L, const uint8_t *solid, const int32_t *links
   y.lc_q = take(4 * nlc * L->Q);
   y.lc_cell = take(8 * nlc);
   y.lc_contrib = take(96 * nlc);
+  y.fin_partial = take(8 * 12 * (uint64_t)kFinalizeMaxBlocks);
   y.prof_off = take(4 * (L->nprof + 1));
   y.force_const = take(8 * 12);
   y.prof_const = take(24 * (uint64_t)L->nprof);
@@ -736,6 +747,12 @@ int aero_step(AeroLattice *L, int64_t n, void *stream) {
     return fail(AERO_ERR_CAPACITY, "force history holds %d steps; read it before stepping further", L->hist_cap);
   CUDA_TRY(cudaSetDevice(L->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (n == 0) return AERO_OK;
+  // only the last step's force profile can be read (aero_read_profile), so
+  // only that step sums it
+  int64_t *ctr = reinterpret_cast<int64_t *>(L->ws + L->lay.counters);
+  k_set_i64<<<1, 1, 0, st>>>(ctr + 4, L->step_count + n);
+  CUDA_TRY(cudaGetLastError());
   return is_f64(L) ? do_steps<double>(L, n, st) : do_steps<float>(L, n, st);
 }
 

@@ -25,7 +25,7 @@ struct Launch {
     return cudaGetLastError();
   }
   static cudaError_t finalize(const StepParams<Real> &p, cudaStream_t st) {
-    k_finalize<Real><<<1, kFinalizeBlock, 0, st>>>(p);
+    k_finalize<Real><<<p.fin_blocks, kFinalizeBlock, 0, st>>>(p);
     return cudaGetLastError();
   }
   static cudaError_t state_out(const StepParams<Real> &p, double *out, int delta, bool raw, int z0, dim3 grid,

@@ -21,8 +21,8 @@
 // exchange forces of the step (forces.py:15-162, forces3d.py:8-171) need the
 // pre-stream P and the post-BC state at link cells; k_step has both in
 // registers at every link cell and writes that cell's twelve sums to a slot
-// of lc_contrib, and k_finalize (one block, launched after k_step) adds the
-// slots in a fixed order in FP64.
+// of lc_contrib, and k_finalize (launched after k_step) adds the slots in a
+// fixed order in FP64.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -43,6 +43,7 @@ namespace aero {
 constexpr int kStepBlock = AERO_STEP_BLOCK;  // threads along x per block
 constexpr int kStepMinBlocks = AERO_STEP_MINB;  // resident blocks per SM the step kernel is built for
 constexpr int kFinalizeBlock = 256;
+constexpr int kFinalizeMaxBlocks = 64;
 
 __device__ __forceinline__ int wrap_n(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 __device__ __forceinline__ int clamp_n(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
@@ -760,9 +761,8 @@ __device__ __forceinline__ void link_cell_forces(const StepParams<Real> &p, int 
       }
     }
   });
-  double *out = p.lc_contrib + slot * 12;
 #pragma unroll
-  for (int j = 0; j < 12; j++) out[j] = (double)acc[j];
+  for (int j = 0; j < 12; j++) p.lc_contrib[j * p.n_lc + slot] = (double)acc[j];
 }
 
 // One full step: state of step n from P_n, scalar step, collision -> P_{n+1}.
@@ -861,42 +861,26 @@ __global__ void __launch_bounds__(kStepBlock) k_moments(const StepParams<typenam
   p.Uw[2 * p.cs + c] = jz * inv;
 }
 
-// Deterministic block reduction of N doubles (fixed shuffle/smem order).
-template <int N, int BLOCK>
-__device__ __forceinline__ void block_reduce_store(double (&v)[N], double *out) {
-  __shared__ double sm[BLOCK / 32][N];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int j = 0; j < N; j++) {
-    double a = v[j];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
-    if (lane == 0) sm[wid][j] = a;
-  }
-  __syncthreads();
-  if (threadIdx.x < N) {
-    double a = 0.0;
-#pragma unroll
-    for (int w = 0; w < BLOCK / 32; w++) a += sm[w][threadIdx.x];
-    out[threadIdx.x] = a;
-  }
-}
-
-// Sums the per-link-cell contributions (in a fixed order, FP64) plus the
-// constant rest-weight part into the device history ring, sums the profile
-// segments, then advances the step counter.
+// Sums the per-link-cell contributions plus the constant rest-weight part
+// into the device history ring, sums the profile segments when this step's
+// profile is the one that can be read, then advances the step counter.
+// Block b adds link cells [b * fin_chunk, (b + 1) * fin_chunk) in a fixed
+// order and stores 12 partial sums; the block that finishes last adds the
+// partials in block order, so the result does not depend on block timing.
 template <class Real>
 __global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const StepParams<Real> p) {
   __shared__ double sm[12][kFinalizeBlock / 32];
+  __shared__ bool last;
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-  const int64_t step = *p.step;
-  const int64_t slot = (step - *p.hist_base) % p.hist_cap;
+  const int64_t n = p.n_lc;
+  const int64_t k0 = (int64_t)blockIdx.x * p.fin_chunk;
+  const int64_t k1 = k0 + p.fin_chunk < n ? k0 + p.fin_chunk : n;
   double a[12];
 #pragma unroll
   for (int j = 0; j < 12; j++) a[j] = 0.0;
-  for (int64_t k = t; k < p.n_lc; k += kFinalizeBlock) {
+  for (int64_t k = k0 + t; k < k1; k += kFinalizeBlock) {
 #pragma unroll
-    for (int j = 0; j < 12; j++) a[j] += p.lc_contrib[k * 12 + j];
+    for (int j = 0; j < 12; j++) a[j] += __ldcg(p.lc_contrib + j * n + k);
   }
 #pragma unroll
   for (int j = 0; j < 12; j++) {
@@ -907,18 +891,31 @@ __global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const StepParams<Re
   }
   __syncthreads();
   if (t < 12) {
-    double v = p.force_const[t];
+    double v = 0.0;
 #pragma unroll
     for (int w = 0; w < kFinalizeBlock / 32; w++) v += sm[t][w];
+    p.fin_partial[blockIdx.x * 12 + t] = v;
+    __threadfence();
+  }
+  __syncthreads();
+  if (t == 0) last = atomicAdd(p.fin_ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int64_t step = *p.step;
+  const int64_t slot = (step - *p.hist_base) % p.hist_cap;
+  if (t < 12) {
+    double v = p.force_const[t];
+    for (int b = 0; b < (int)gridDim.x; b++) v += __ldcg(p.fin_partial + b * 12 + t);
     p.hist[slot * 12 + t] = v;
   }
-  if (p.want_profile) {
+  if (p.want_profile && step + 1 == *p.profile_step) {
     for (int b = t; b < p.nprof; b += kFinalizeBlock) {
       double a0 = p.prof_const[b * 3 + 0], a1 = p.prof_const[b * 3 + 1], a2 = p.prof_const[b * 3 + 2];
       for (int k = p.prof_off[b]; k < p.prof_off[b + 1]; k++) {
-        a0 += p.lc_contrib[(int64_t)k * 12 + 0];
-        a1 += p.lc_contrib[(int64_t)k * 12 + 1];
-        a2 += p.lc_contrib[(int64_t)k * 12 + 2];
+        a0 += __ldcg(p.lc_contrib + k);
+        a1 += __ldcg(p.lc_contrib + n + k);
+        a2 += __ldcg(p.lc_contrib + 2 * n + k);
       }
       p.prof_out[b * 3 + 0] = a0;
       p.prof_out[b * 3 + 1] = a1;
@@ -926,7 +923,10 @@ __global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const StepParams<Re
     }
   }
   __syncthreads();
-  if (t == 0) *p.step = step + 1;
+  if (t == 0) {
+    *p.fin_ticket = 0u;
+    *p.step = step + 1;
+  }
 }
 
 // State of the step that produced P (f as the reference stores it), written

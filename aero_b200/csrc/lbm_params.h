@@ -83,7 +83,11 @@ struct StepParams {
   const Real *cs_cell;  // per-cell LES constant (van Driest), optional
 
   // force reduction
-  double *lc_contrib;   // per link cell: 12 doubles (deviation part of its forces)
+  double *lc_contrib;   // 12 x n_lc doubles, component-major: deviation part of each link cell's forces
+  double *fin_partial;  // per k_finalize block: 12 partial sums
+  uint32_t *fin_ticket; // blocks of k_finalize done (reset by the last one)
+  int64_t fin_chunk;    // link cells per k_finalize block
+  int32_t fin_blocks;   // k_finalize grid size (<= kFinalizeMaxBlocks)
   const double *force_const;  // 12 doubles: rest-weight part of the forces
   const double *prof_const;   // nprof * 3 doubles: rest-weight part of the profile
   const int32_t *prof_off;  // nprof + 1 segment offsets into the link-cell list
@@ -93,6 +97,7 @@ struct StepParams {
   int32_t hist_cap;
   int32_t want_profile;
   int64_t *step;        // device step counter (steps completed)
+  const int64_t *profile_step;  // the profile is summed only by the step that completes this count
   int64_t *hist_base;   // step index stored in hist slot 0
   uint32_t *status;
   unsigned long long *first_bad_step;  // smallest step whose state had a bad density

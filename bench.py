@@ -390,7 +390,9 @@ def main():
                    "precision": args.precision, "parallelism": f"replicas x{world}",
                    "l2": "state (2 x Q x cells) far larger than L2; no flush needed",
                    "links": int(len(s.surface_links))},
-        "gpu_launches": launches_per_step * args.steps,
+        # per step: k_step, k_finalize (+ the LES moments pass for BGK/TRT);
+        # per aero_step call: one launch recording the step whose profile is summed
+        "gpu_launches": launches_per_step * args.steps + 1,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic, "kernel": "k_step (fused stream/BC/collide)",
