@@ -60,6 +60,7 @@ SIGNATURES = {
     "aero_read_profile": ([_VP, _VP, _VP], ctypes.c_int),
     "aero_status": ([_VP, ctypes.POINTER(ctypes.c_uint32), _VP], ctypes.c_int),
     "aero_step_count": ([_VP, ctypes.POINTER(_I64)], ctypes.c_int),
+    "aero_step_plan": ([_VP, ctypes.POINTER(_I32), ctypes.POINTER(_I32), ctypes.POINTER(_I32)], ctypes.c_int),
     "aero_first_bad_step": ([_VP, ctypes.POINTER(_I64), _VP], ctypes.c_int),
     "aero_destroy": ([_VP], ctypes.c_int),
     "aero_mrt_operator": ([_I32, _D, _VP, _VP], ctypes.c_int),

@@ -46,7 +46,7 @@ constexpr uint64_t kAlign = 256;
 uint64_t align_up(uint64_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
 struct Layout {
-  uint64_t P[2], solid, lbits, loff, lc_mask, lc_q, lc_cell, lc_contrib, fin_partial, prof_off, force_const, prof_const,
+  uint64_t P[2], flags, lbits, loff, lc_mask, lc_q, lc_cell, lc_contrib, fin_partial, prof_off, force_const, prof_const,
       prev[2], g[2], U, cs_cell, hist, prof_out, counters, total;
 };
 
@@ -57,17 +57,22 @@ struct WTab {
 // small element-wise kernels for state I/O --------------------------------
 __global__ void k_set_i64(int64_t *p, int64_t v) { *p = v; }
 
+// The outlet state is (Q, nz, ny) absolute populations at the boundary and
+// (nz, ny, QP) deviations on the device (one 16-byte-aligned row per cell
+// row, so a tile's rows are one contiguous copy).
 template <class Real>
-__global__ void k_prev_in(Real *dst, const double *src, int Q, int64_t plane, WTab w) {
+__global__ void k_prev_in(Real *dst, const double *src, int Q, int QP, int64_t plane, WTab w) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= (int64_t)Q * plane) return;
-  dst[k] = (Real)(src[k] - w.w[k / plane]);
+  const int64_t i = k / plane, r = k - i * plane;
+  dst[r * QP + i] = (Real)(src[k] - w.w[i]);
 }
 template <class Real>
-__global__ void k_prev_out(double *dst, const Real *src, int Q, int64_t plane, WTab w) {
+__global__ void k_prev_out(double *dst, const Real *src, int Q, int QP, int64_t plane, WTab w) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= (int64_t)Q * plane) return;
-  dst[k] = w.w[k / plane] + (double)src[k];
+  const int64_t i = k / plane, r = k - i * plane;
+  dst[k] = w.w[i] + (double)src[r * QP + i];
 }
 template <class Real>
 __global__ void k_g_in(Real *dst, const double *src, int Qg, int64_t ncells, int64_t cs) {
@@ -93,7 +98,7 @@ int aero::set_error(int code, const char *msg) {
 
 struct AeroLattice {
   AeroParams prm;
-  int Q = 0, Qg = 0;
+  int Q = 0, QP = 0, Qg = 0;
   int64_t ncells = 0, cs = 0, nwords = 0, prev_plane = 0;
   int nwx = 0, nprof = 0, hist_cap = 4096;
   std::vector<double> force_const, prof_const;  // rest-weight parts of forces / profile
@@ -122,6 +127,9 @@ struct AeroLattice {
   cudaGraphExec_t pair_exec[2] = {nullptr, nullptr};
   bool use_graphs = true;
   int device = -1;  // device of the bound workspace
+  // row-tiled step plan (k_step_tiled), fixed at bind time
+  bool tiled = false;
+  int tile_blocks = 0, tile_rows = 0, tiles_per_plane = 0, ntiles = 0;
   // optional per-kernel event timing (eager launches only)
   bool timing = false;
   std::vector<cudaEvent_t> ev;  // 4 events per timed step
@@ -167,9 +175,12 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   p.wall = a.wall_bc;
   p.sponge_thickness = a.sponge_thickness;
   p.sponge_start = std::max(a.nx - a.sponge_thickness, 0);
+  p.tile_rows = L->tile_rows;
+  p.tiles_per_plane = L->tiles_per_plane;
+  p.ntiles = L->ntiles;
   p.P = ws + L->lay.P[cur];
   p.Pn = ws + L->lay.P[nxt];
-  p.solid = reinterpret_cast<const uint8_t *>(ws + L->lay.solid);
+  p.flags = reinterpret_cast<const uint8_t *>(ws + L->lay.flags);
   p.lbits = reinterpret_cast<const uint32_t *>(ws + L->lay.lbits);
   p.loff = reinterpret_cast<const int32_t *>(ws + L->lay.loff);
   p.lc_mask = reinterpret_cast<const uint32_t *>(ws + L->lay.lc_mask);
@@ -283,7 +294,10 @@ int launch_step(AeroLattice *L, int cur, cudaStream_t st, bool timed = false) {
     CUDA_TRY(cudaEventRecord(e[0], st));
   }
   if (les_active(L)) CUDA_TRY(ops->moments(p, false, grid, st));
-  CUDA_TRY(ops->step(p, false, grid, st));
+  if (L->tiled)
+    CUDA_TRY(ops->step_tiled(p, L->tile_blocks, st));
+  else
+    CUDA_TRY(ops->step(p, false, grid, st));
   if (timed) CUDA_TRY(cudaEventRecord(e[1], st));
   CUDA_TRY(ops->finalize(p, st));
   if (timed) {
@@ -347,7 +361,7 @@ int do_set_state(AeroLattice *L, const double *f, const double *prev, const doub
   if (prev) {
     const int64_t n = (int64_t)L->Q * L->prev_plane;
     k_prev_in<Real><<<blocks_for(n, 256), 256, 0, st>>>(reinterpret_cast<Real *>(L->ws + L->lay.prev[L->cur]),
-                                                        prev, L->Q, L->prev_plane, L->w);
+                                                        prev, L->Q, L->QP, L->prev_plane, L->w);
     CUDA_TRY(cudaGetLastError());
   }
   if (g && L->prm.thermal) {
@@ -385,7 +399,7 @@ int do_get_state(AeroLattice *L, double *f, double *prev, double *g, int z0, int
   if (prev) {
     const int64_t n = (int64_t)L->Q * L->prev_plane;
     k_prev_out<Real><<<blocks_for(n, 256), 256, 0, st>>>(
-        prev, reinterpret_cast<const Real *>(L->ws + L->lay.prev[L->cur]), L->Q, L->prev_plane, L->w);
+        prev, reinterpret_cast<const Real *>(L->ws + L->lay.prev[L->cur]), L->Q, L->QP, L->prev_plane, L->w);
     CUDA_TRY(cudaGetLastError());
   }
   if (g && L->prm.thermal) {
@@ -394,6 +408,38 @@ int do_get_state(AeroLattice *L, double *f, double *prev, double *g, int z0, int
                                                       L->Qg, L->ncells, L->cs);
     CUDA_TRY(cudaGetLastError());
   }
+  return AERO_OK;
+}
+
+// The per-cell-gather kernel (k_step) is the default: on the 512x256x256
+// sphere it is faster than the row-tiled kernel in every storage format.
+// AERO_B200_TILES=1 at bind time selects the row-tiled kernel instead,
+// where a whole x row fits one shared-memory slab and every row starts on a
+// 16-byte boundary (the bulk-copy alignment): tiles of tile_rows rows, a
+// persistent grid of resident blocks.
+template <class Real>
+int plan_tiles(AeroLattice *L) {
+  L->tiled = false;
+  L->tile_blocks = L->tile_rows = L->tiles_per_plane = L->ntiles = 0;
+  const char *want = std::getenv("AERO_B200_TILES");
+  if (!(want && want[0] == '1')) return AERO_OK;
+  const Ops<Real> *ops = get_ops<Real>(L);
+  const AeroParams &a = L->prm;
+  const int sb = ops->store_bytes;
+  const uintptr_t P0 = reinterpret_cast<uintptr_t>(L->ws + L->lay.P[0]);
+  const uintptr_t P1 = reinterpret_cast<uintptr_t>(L->ws + L->lay.P[1]);
+  if (((int64_t)a.nx * sb) % 16 != 0 || (L->cs * sb) % 16 != 0 || P0 % 16 != 0 || P1 % 16 != 0) return AERO_OK;
+  int per_sm = 0, cap = 0, sms = 0;
+  CUDA_TRY(ops->tiled_setup(&per_sm, &cap));
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, L->device));
+  if (per_sm < 1 || a.nx > cap) return AERO_OK;
+  L->tile_rows = std::max(1, std::min(std::min(a.ny, cap / a.nx), kMaxTileRows));
+  L->tiles_per_plane = (a.ny + L->tile_rows - 1) / L->tile_rows;
+  const int64_t ntiles = (int64_t)L->tiles_per_plane * a.nz;
+  if (ntiles >= ((int64_t)1 << 31)) return AERO_OK;
+  L->ntiles = (int)ntiles;
+  L->tile_blocks = (int)std::min<int64_t>(ntiles, (int64_t)per_sm * sms);
+  L->tiled = true;
   return AERO_OK;
 }
 
@@ -445,6 +491,7 @@ int aero_create(const AeroParams *params, AeroLattice **out) {
   L->prm = *params;
   const AeroParams &a = L->prm;
   L->Q = a.dims == 2 ? 9 : 19;
+  L->QP = (L->Q + 3) / 4 * 4;
   L->Qg = a.thermal ? (a.scalar_reduced ? (a.dims == 2 ? 5 : 7) : L->Q) : 0;
   L->ncells = (int64_t)a.nx * a.ny * a.nz;
   L->cs = (L->ncells + 63) / 64 * 64;
@@ -601,7 +648,7 @@ int aero_set_geometry(AeroLattice *L, const uint8_t *solid, const int32_t *links
   };
   y.P[0] = take(sb * L->Q * L->cs);
   y.P[1] = take(sb * L->Q * L->cs);
-  y.solid = take(L->cs);
+  y.flags = take(L->cs + 32);  // slack for 16-byte-widened tile copies
   y.lbits = take(4 * L->nwords);
   y.loff = take(4 * L->nwords);
   y.lc_mask = take(4 * nlc);
@@ -612,8 +659,8 @@ int aero_set_geometry(AeroLattice *L, const uint8_t *solid, const int32_t *links
   y.prof_off = take(4 * (L->nprof + 1));
   y.force_const = take(8 * 12);
   y.prof_const = take(24 * (uint64_t)L->nprof);
-  y.prev[0] = take(rb * L->Q * L->prev_plane);
-  y.prev[1] = take(rb * L->Q * L->prev_plane);
+  y.prev[0] = take(rb * L->QP * L->prev_plane);
+  y.prev[1] = take(rb * L->QP * L->prev_plane);
   y.g[0] = take(L->Qg ? rb * L->Qg * L->cs : 0);
   y.g[1] = take(L->Qg ? rb * L->Qg * L->cs : 0);
   y.U = take((L->feat & FEAT_LES) ? rb * 3 * L->cs : 0);
@@ -654,7 +701,10 @@ int aero_bind_workspace(AeroLattice *L, void *dptr, uint64_t bytes, void *stream
   CUDA_TRY(cudaMemsetAsync(L->ws, 0, L->lay.total, st));
   // first divergent step starts at "never"
   CUDA_TRY(cudaMemsetAsync(L->ws + L->lay.counters + 3 * sizeof(int64_t), 0xff, sizeof(int64_t), st));
-  CUDA_TRY(up(L->lay.solid, L->solid.data(), L->solid.size()));
+  // per-cell flags: solid, and whether the cell has obstacle links
+  std::vector<uint8_t> flags(L->solid);
+  for (const int64_t c : L->lc_cell) flags[(size_t)c] |= FLAG_LINK;
+  CUDA_TRY(up(L->lay.flags, flags.data(), flags.size()));
   CUDA_TRY(up(L->lay.lbits, L->lbits.data(), 4 * L->lbits.size()));
   CUDA_TRY(up(L->lay.loff, L->loff.data(), 4 * L->loff.size()));
   CUDA_TRY(up(L->lay.lc_mask, L->lc_mask.data(), 4 * L->lc_mask.size()));
@@ -674,6 +724,8 @@ int aero_bind_workspace(AeroLattice *L, void *dptr, uint64_t bytes, void *stream
   }
   // host vectors must outlive the async copies
   CUDA_TRY(cudaStreamSynchronize(st));
+  const int rc = is_f64(L) ? plan_tiles<double>(L) : plan_tiles<float>(L);
+  if (rc != AERO_OK) return rc;
   L->bound = true;
   return AERO_OK;
 }
@@ -812,6 +864,15 @@ int aero_first_bad_step(AeroLattice *L, int64_t *step, void *stream) {
 int aero_step_count(const AeroLattice *L, int64_t *steps) {
   if (!L || !steps) return fail(AERO_ERR_INVALID, "NULL argument");
   *steps = L->step_count;
+  return AERO_OK;
+}
+
+int aero_step_plan(const AeroLattice *L, int32_t *tiled, int32_t *tile_rows, int32_t *blocks) {
+  if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
+  if (tiled) *tiled = L->tiled ? 1 : 0;
+  if (tile_rows) *tile_rows = L->tile_rows;
+  if (blocks) *blocks = L->tile_blocks;
   return AERO_OK;
 }
 

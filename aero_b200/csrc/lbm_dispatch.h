@@ -16,6 +16,11 @@ struct Ops {
   cudaError_t (*state_out)(const StepParams<Real> &, double *out, int step_delta, bool raw, int z0, dim3 grid,
                            cudaStream_t);
   cudaError_t (*load_state)(const StepParams<Real> &, const double *in, void *dst, dim3 grid, cudaStream_t);
+  // row-tiled step (k_step_tiled): persistent grid of `blocks` blocks
+  cudaError_t (*step_tiled)(const StepParams<Real> &, int blocks, cudaStream_t);
+  // on the current device: raises the kernel's dynamic shared-memory limit and
+  // reports resident blocks per SM and the cells one row slab holds
+  cudaError_t (*tiled_setup)(int *blocks_per_sm, int *cap_cells);
   int store_bytes;
 };
 

@@ -42,8 +42,26 @@ struct Launch {
     k_load_state<L, S><<<grid, kStepBlock, 0, st>>>(p, in, static_cast<S *>(dst));
     return cudaGetLastError();
   }
-  static constexpr Ops<Real> table = {&step, &moments, &finalize, &state_out, &load_state,
-                                      (int)sizeof(S)};
+  static cudaError_t step_tiled(const StepParams<Real> &p, int blocks, cudaStream_t st) {
+    k_step_tiled<L, S, COLL><<<blocks, TileCfg<L, S>::threads, TileCfg<L, S>::smem_bytes, st>>>(p);
+    return cudaGetLastError();
+  }
+  static cudaError_t tiled_setup(int *blocks_per_sm, int *cap_cells) {
+    cudaError_t e = cudaFuncSetAttribute(k_step_tiled<L, S, COLL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         TileCfg<L, S>::smem_bytes);
+    if (e != cudaSuccess) return e;
+    // without the largest carveout the driver may size shared memory for
+    // fewer resident blocks than the occupancy calculation assumes
+    e = cudaFuncSetAttribute(k_step_tiled<L, S, COLL>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_step_tiled<L, S, COLL>,
+                                                      TileCfg<L, S>::threads, TileCfg<L, S>::smem_bytes);
+    *cap_cells = TileCfg<L, S>::cap;
+    return e;
+  }
+  static constexpr Ops<Real> table = {&step,       &moments,     &finalize,     &state_out, &load_state,
+                                      &step_tiled, &tiled_setup, (int)sizeof(S)};
 };
 
 template <class S>

@@ -200,40 +200,86 @@ __device__ __forceinline__ void walls(const StepParams<Real> &p, Real (&d)[L::Q]
 // reference step, evaluated from the post-collision buffer P.
 // --------------------------------------------------------------------------
 
+// Pull gather of row (y, z) straight from the population buffer: direction
+// i of cell x reads P_i at (x - ex, y - ey, z - ez) with periodic wrap.
+template <class L, class S, class Real>
+struct GlobalGather {
+  const StepParams<Real> &p;
+  int y, z;
+  __device__ __forceinline__ void operator()(int x, Real (&d)[L::Q]) const {
+    using SO = StoreOps<S>;
+    const S *P = static_cast<const S *>(p.P);
+    // per axis only three source coordinates occur, so each source index is
+    // one 3-way add
+    const uint32_t nx = p.nx, nxy = (uint32_t)p.nx * (uint32_t)p.ny;
+    const uint32_t xs_p = x == 0 ? nx - 1 : x - 1;            // ex = +1
+    const uint32_t xs_m = x == p.nx - 1 ? 0 : x + 1;          // ex = -1
+    const uint32_t ry_0 = (uint32_t)y * nx;
+    const uint32_t ry_p = (y == 0 ? p.ny - 1 : y - 1) * nx;   // ey = +1
+    const uint32_t ry_m = (y == p.ny - 1 ? 0 : y + 1) * nx;   // ey = -1
+    uint32_t pz_0 = 0, pz_p = 0, pz_m = 0;
+    if constexpr (L::DIMS == 3) {
+      pz_0 = (uint32_t)z * nxy;
+      pz_p = (z == 0 ? p.nz - 1 : z - 1) * nxy;
+      pz_m = (z == p.nz - 1 ? 0 : z + 1) * nxy;
+    }
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      constexpr int ex = Dir<L, i>::x, ey = Dir<L, i>::y, ez = Dir<L, i>::z;
+      const uint32_t src = (ex > 0 ? xs_p : (ex < 0 ? xs_m : (uint32_t)x)) +
+                           (ey > 0 ? ry_p : (ey < 0 ? ry_m : ry_0)) +
+                           (ez > 0 ? pz_p : (ez < 0 ? pz_m : pz_0));
+      d[i] = SO::template load<i, L>(P, elem(p, i, src));
+    });
+  }
+  // flag byte of cell x of the row
+  __device__ __forceinline__ uint32_t flags(int x) const { return p.flags[cell_index(p, x, y, z)]; }
+  // convective outlet state of the row, direction i
+  __device__ __forceinline__ Real prev(int i) const { return p.prev[((int64_t)z * p.ny + y) * L::QP + i]; }
+};
+
+// Pull gather from a shared-memory tile: slab i (CAP elements) holds, for
+// every row of the tile, the whole source row of direction i, i.e. row
+// (y - ey, z - ez) with the y/z wrap already resolved when the tile was
+// loaded, so only the x shift (periodic within the row) is left.  `row` is
+// the tile-local offset of the cell's row (local row * nx).
+// The stage also holds the tile's flag bytes (`fl` points at the row's first
+// cell) and, for a convective outlet, the row's outlet state (`pv`).
+template <class L, class S, class Real, int CAP>
+struct SmemGather {
+  const S *tile;
+  uint32_t row;
+  int nx;
+  const uint8_t *fl;
+  const Real *pv;
+  __device__ __forceinline__ uint32_t flags(int x) const { return fl[x]; }
+  __device__ __forceinline__ Real prev(int i) const { return pv[i]; }
+  __device__ __forceinline__ void operator()(int x, Real (&d)[L::Q]) const {
+    using SO = StoreOps<S>;
+    const uint32_t o_0 = row + (uint32_t)x;
+    const uint32_t o_p = row + (uint32_t)(x == 0 ? nx - 1 : x - 1);   // ex = +1
+    const uint32_t o_m = row + (uint32_t)(x == nx - 1 ? 0 : x + 1);   // ex = -1
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      constexpr int ex = Dir<L, i>::x;
+      const uint32_t o = ex > 0 ? o_p : (ex < 0 ? o_m : o_0);
+      d[i] = SO::template lds<i, L>(tile + i * CAP, o);
+    });
+  }
+};
+
 // gather + body force + obstacle bounce-back + inlet (everything the
 // reference applies before the outlet copy reads column Nx-2).
-template <class L, class S, class Real>
+template <class L, class S, class Real, class Gather>
 __device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, int y, int z, int64_t step_now,
-                                              Real (&d)[L::Q]) {
+                                              Real (&d)[L::Q], const Gather &gather) {
   using SO = StoreOps<S>;
   const S *P = static_cast<const S *>(p.P);
-  const int64_t cs = p.cs;
-  // Source of direction i is (x - ex, y - ey, z - ez) with periodic wrap: per
-  // axis only three values occur, so each source index is one 3-way add.
-  const uint32_t nx = p.nx, nxy = (uint32_t)p.nx * (uint32_t)p.ny;
-  const uint32_t xs_p = x == 0 ? nx - 1 : x - 1;            // ex = +1
-  const uint32_t xs_m = x == p.nx - 1 ? 0 : x + 1;          // ex = -1
-  const uint32_t ry_0 = (uint32_t)y * nx;
-  const uint32_t ry_p = (y == 0 ? p.ny - 1 : y - 1) * nx;   // ey = +1
-  const uint32_t ry_m = (y == p.ny - 1 ? 0 : y + 1) * nx;   // ey = -1
-  uint32_t pz_0 = 0, pz_p = 0, pz_m = 0;
-  if constexpr (L::DIMS == 3) {
-    pz_0 = (uint32_t)z * nxy;
-    pz_p = (z == 0 ? p.nz - 1 : z - 1) * nxy;
-    pz_m = (z == p.nz - 1 ? 0 : z + 1) * nxy;
-  }
-  static_for<L::Q>([&](auto ic) {
-    constexpr int i = decltype(ic)::value;
-    constexpr int ex = Dir<L, i>::x, ey = Dir<L, i>::y, ez = Dir<L, i>::z;
-    const uint32_t src = (ex > 0 ? xs_p : (ex < 0 ? xs_m : (uint32_t)x)) +
-                         (ey > 0 ? ry_p : (ey < 0 ? ry_m : ry_0)) +
-                         (ez > 0 ? pz_p : (ez < 0 ? pz_m : pz_0));
-    d[i] = SO::template load<i, L>(P, elem(p, i, src));
-  });
+  gather(x, d);
   const uint32_t c = cell_index(p, x, y, z);
   if constexpr (L::DIMS == 3) {
     // Guo-style uniform body force on fluid cells (ibm_guo.py:263-301)
-    if ((p.feat & FEAT_BODY_FORCE) && !p.solid[c]) {
+    if ((p.feat & FEAT_BODY_FORCE) && !(gather.flags(x) & FLAG_SOLID)) {
       Real drho = 0, jx = 0, jy = 0, jz = 0;
       static_for<L::Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
@@ -257,7 +303,7 @@ __device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, 
     }
   }
   // obstacle bounce-back (boundary.py:283-352, boundary3d.py:333-393)
-  if (p.feat & FEAT_OBSTACLE_BB) {
+  if ((p.feat & FEAT_OBSTACLE_BB) && (gather.flags(x) & FLAG_LINK)) {
     const int64_t slot = link_slot(p, x, y, z);
     if (slot >= 0) {
       const uint32_t mask = __ldg(p.lc_mask + slot);
@@ -306,23 +352,23 @@ struct ScalarCtx {
 };
 
 // Full post-BC state.  When prev_out is non-null the convective outlet writes
-// its advanced state there (only k_step does).
-template <class L, class S, class Real>
+// its advanced state there (only the step kernels do).
+template <class L, class S, class Real, class Gather>
 __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int y, int z, int64_t step_now,
-                                           Real (&d)[L::Q], Real *prev_out, ScalarCtx<Real> *sc) {
+                                           Real (&d)[L::Q], Real *prev_out, ScalarCtx<Real> *sc,
+                                           const Gather &gather) {
   const bool open = p.feat & FEAT_OPEN;
   const bool copy_out =
       open && x == p.nx - 1 && (p.outlet == OUTLET_CONVECTIVE || p.outlet == OUTLET_ZEROGRAD);
-  partial_state<L, S, Real>(p, copy_out ? p.nx - 2 : x, y, z, step_now, d);
+  partial_state<L, S, Real>(p, copy_out ? p.nx - 2 : x, y, z, step_now, d, gather);
   if (copy_out) {
     if (p.outlet == OUTLET_CONVECTIVE) {
       // boundary.py:78-113, boundary3d.py:149-164
       Real u = p.u0 < Real(0) ? Real(0) : (p.u0 > Real(1) ? Real(1) : p.u0);
       static_for<L::Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        const int64_t pi = ((int64_t)i * p.nz + z) * p.ny + y;
-        d[i] = (Real(1) - u) * p.prev[pi] + u * d[i];
-        if (prev_out) prev_out[pi] = d[i];
+        d[i] = (Real(1) - u) * gather.prev(i) + u * d[i];
+        if (prev_out) prev_out[((int64_t)z * p.ny + y) * L::QP + i] = d[i];
       });
     }
   } else if constexpr (L::DIMS == 2) {
@@ -382,6 +428,12 @@ __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int
       });
     }
   }
+}
+
+template <class L, class S, class Real>
+__device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int y, int z, int64_t step_now,
+                                           Real (&d)[L::Q], Real *prev_out, ScalarCtx<Real> *sc) {
+  full_state<L, S, Real>(p, x, y, z, step_now, d, prev_out, sc, GlobalGather<L, S, Real>{p, y, z});
 }
 
 // --------------------------------------------------------------------------
@@ -765,6 +817,57 @@ __device__ __forceinline__ void link_cell_forces(const StepParams<Real> &p, int 
   for (int j = 0; j < 12; j++) p.lc_contrib[j * p.n_lc + slot] = (double)acc[j];
 }
 
+// Divergence guard (diagnostics.py:32-71): non-finite or non-positive rho of
+// the state; one lane per warp reports, and only until it is recorded.
+template <class Real>
+__device__ __forceinline__ void guard_rho(const StepParams<Real> &p, Real rho, int64_t step_now) {
+  const bool bad = !(rho > Real(0)) || !isfinite(rho);
+  const unsigned badm = __ballot_sync(__activemask(), bad);
+  if (bad && (threadIdx.x & 31) == __ffs(badm) - 1) {
+    if (!(*(volatile uint32_t *)p.status & STATUS_NONFINITE_OR_NONPOSITIVE_RHO))
+      atomicOr(p.status, STATUS_NONFINITE_OR_NONPOSITIVE_RHO);
+    if (*(volatile unsigned long long *)p.first_bad_step > (unsigned long long)(step_now + 1))
+      atomicMin(p.first_bad_step, (unsigned long long)(step_now + 1));
+  }
+}
+
+// One regular step of cell (x, y, z): state of step n from P_n (gathered by
+// `gather`), link-cell forces, scalar step, collision, P_{n+1} stored.
+template <class L, class S, int COLL, class Gather>
+__device__ __forceinline__ void step_cell(const StepParams<typename StoreOps<S>::Real> &p, int x, int y, int z,
+                                          int64_t step_now, const Gather &gather) {
+  using Real = typename StoreOps<S>::Real;
+  using SO = StoreOps<S>;
+  const uint32_t c = cell_index(p, x, y, z);
+  const uint32_t fl = gather.flags(x);
+  const bool solid = fl & FLAG_SOLID;
+  Real d[L::Q];
+  ScalarCtx<Real> sc;
+  full_state<L, S, Real>(p, x, y, z, step_now, d, p.prevn, &sc, gather);
+  if ((p.feat & FEAT_OBSTACLE_BB) && (fl & FLAG_LINK)) {
+    const int64_t slot = link_slot(p, x, y, z);
+    if (slot >= 0) link_cell_forces<L, S, Real>(p, x, y, z, c, slot, d);
+  }
+  if (p.feat & FEAT_THERMAL) {
+    if (p.feat & FEAT_SCALAR_REDUCED) {
+      using G = typename ScalarReduced<L>::Lat;
+      scalar_step<L, G>(p, x, y, z, c, solid, sc, Real(G::cs2inv));
+    } else {
+      scalar_step<L, L>(p, x, y, z, c, solid, sc, Real(3));
+    }
+  }
+  Real om = p.omega;
+  const bool les = (COLL != COLL_MRT) && (p.feat & FEAT_LES);
+  if (les) om = les_omega<L>(p, x, y, z, c, solid);
+  const Real rho = collide<L, Real, COLL>(p, d, solid, om, les);
+  guard_rho(p, rho, step_now);
+  S *Pn = static_cast<S *>(p.Pn);
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    SO::template store<i, L>(Pn, elem(p, i, c), d[i]);
+  });
+}
+
 // One full step: state of step n from P_n, scalar step, collision -> P_{n+1}.
 // FROM_STATE: P holds a state (deviations) to be collided as is (used after
 // the host sets f, and to start from an initial state).
@@ -776,54 +879,265 @@ __global__ void __launch_bounds__(kStepBlock, sizeof(typename StoreOps<S>::Real)
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z;
   if (x >= p.nx) return;
-  const uint32_t c = cell_index(p, x, y, z);
-  const bool solid = p.solid[c];
-  Real d[L::Q];
-  ScalarCtx<Real> sc;
-  int64_t step_now = 0;
   if constexpr (FROM_STATE) {
+    const uint32_t c = cell_index(p, x, y, z);
+    const bool solid = p.flags[c] & FLAG_SOLID;
+    Real d[L::Q];
     const S *P = static_cast<const S *>(p.P);
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
       d[i] = SO::template load<i, L>(P, elem(p, i, c));
     });
+    Real om = p.omega;
+    const bool les = (COLL != COLL_MRT) && (p.feat & FEAT_LES);
+    if (les) om = les_omega<L>(p, x, y, z, c, solid);
+    collide<L, Real, COLL>(p, d, solid, om, les);
+    S *Pn = static_cast<S *>(p.Pn);
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      SO::template store<i, L>(Pn, elem(p, i, c), d[i]);
+    });
   } else {
-    step_now = *p.step;
-    full_state<L, S, Real>(p, x, y, z, step_now, d, p.prevn, &sc);
-    if (p.feat & FEAT_OBSTACLE_BB) {
-      const int64_t slot = link_slot(p, x, y, z);
-      if (slot >= 0) link_cell_forces<L, S, Real>(p, x, y, z, c, slot, d);
+    step_cell<L, S, COLL>(p, x, y, z, *p.step, GlobalGather<L, S, Real>{p, y, z});
+  }
+}
+
+// --------------------------------------------------------------------------
+// Row-tiled step.  A tile is `tile_rows` consecutive y rows of one z plane
+// (whole x rows).  For direction i the cells of a tile pull from the source
+// rows (y - ey, z - ez), which are contiguous in plane i of P (one run, or
+// two when the y range wraps), so one thread of the block brings them into
+// a shared-memory slab with bulk async copies (cp.async.bulk, completion
+// counted in bytes on an mbarrier).  Blocks are persistent, walk the tiles
+// with a grid stride and keep two stages: the next tile's rows are in
+// flight while the current tile is computed.  Every element of P is read
+// from HBM once per step and the gather costs no global-load latency in the
+// issue path.  The host uses this kernel when a row fits a slab
+// (nx <= TileCfg::cap) and rows start 16-byte aligned (nx * sizeof(S) a
+// multiple of 16, P 16-byte aligned); otherwise it launches k_step.  With
+// NS stages the block keeps NS - 1 tiles in flight while it computes one.
+// --------------------------------------------------------------------------
+// Tile shape: one cell per thread, so a slab holds `threads` cells and a row
+// of up to that many cells fits one tile (at most kMaxTileRows rows).  A
+// stage holds Q population slabs, the tile's flag bytes (copied from a
+// 16-byte-aligned superset of the tile's cells, hence cap + 32 bytes) and
+// the rows' convective outlet state (kMaxTileRows x QP values).  Every block
+// gets the same shared-memory budget (two blocks per SM fit), spent on as
+// many stages (two to four) as it holds.
+#ifndef AERO_TILE_BLOCK_SMEM
+#define AERO_TILE_BLOCK_SMEM 100352
+#endif
+constexpr uint64_t kWaitNs = 1000000000ull;  // a stage not complete after 1 s is declared lost
+constexpr int kMaxTileRows = 16;
+
+template <class L, class S>
+struct TileCfg {
+  using Real = typename StoreOps<S>::Real;
+  static constexpr int threads = sizeof(S) == 8 ? 256 : 512;
+  static constexpr int min_blocks = 2;
+  static constexpr int cap = threads;  // cells per slab
+  static constexpr int stage_elems = L::Q * cap;
+  static constexpr int pop_bytes = stage_elems * (int)sizeof(S);
+  static constexpr int flag_bytes = cap + 32;
+  static constexpr int prev_bytes = kMaxTileRows * L::QP * (int)sizeof(Real);
+  static constexpr int stage_bytes = pop_bytes + flag_bytes + prev_bytes;
+  static constexpr int stages_fit = AERO_TILE_BLOCK_SMEM / stage_bytes;
+  static constexpr int stages = stages_fit > 4 ? 4 : (stages_fit < 2 ? 2 : stages_fit);
+  static constexpr int smem_bytes = stages * stage_bytes + 8 * stages;  // stages + one mbarrier per stage
+  static_assert(pop_bytes % 16 == 0 && flag_bytes % 16 == 0 && prev_bytes % 16 == 0, "16-byte stage parts");
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void *ptr) {
+  return (uint32_t)__cvta_generic_to_shared(ptr);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred pw;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 pw, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, pw;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait: false when the phase did not complete within kWaitNs.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    for (int k = 0; k < 64; ++k)
+      if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > kWaitNs) return false;
+  }
+}
+// Generic-proxy accesses to shared memory before async-proxy writes to it.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// Bulk copy global -> shared (no multicast), completion counted on bar.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+struct TileCoord {
+  int z, y0, rows;
+};
+
+template <class Real>
+__device__ __forceinline__ TileCoord tile_coord(const StepParams<Real> &p, int tile) {
+  TileCoord t;
+  t.z = tile / p.tiles_per_plane;
+  t.y0 = (tile - t.z * p.tiles_per_plane) * p.tile_rows;
+  t.rows = p.ny - t.y0 < p.tile_rows ? p.ny - t.y0 : p.tile_rows;
+  return t;
+}
+
+// Byte offset of the tile's first cell in its flag copy (the copy starts at
+// the 16-byte boundary at or below that cell).
+template <class Real>
+__device__ __forceinline__ uint32_t tile_flag_skew(const StepParams<Real> &p, const TileCoord &t) {
+  return (uint32_t)((((int64_t)t.z * p.ny + t.y0) * p.nx) & 15);
+}
+
+// Issued by one thread: the source rows of every direction of a tile, its
+// flag bytes and (convective outlet) its rows' outlet state into one stage.
+// The byte count announced on the barrier is exactly what the copies
+// deliver.  Every copy starts and ends on a 16-byte boundary: rows because
+// nx * sizeof(S) and the plane stride are multiples of 16, flags because
+// the copy is widened to 16-byte boundaries (the flag buffer has slack past
+// the last cell), outlet rows because QP * sizeof(Real) is.
+template <class L, class S, class Real>
+__device__ __forceinline__ void issue_tile(const StepParams<Real> &p, int tile, unsigned char *stage,
+                                           uint64_t *bar) {
+  using Cfg = TileCfg<L, S>;
+  constexpr int CAP = Cfg::cap;
+  const TileCoord t = tile_coord(p, tile);
+  const uint32_t row_bytes = (uint32_t)p.nx * (uint32_t)sizeof(S);
+  const int64_t c0 = ((int64_t)t.z * p.ny + t.y0) * p.nx;  // first cell of the tile
+  const int64_t fa = c0 & ~(int64_t)15;
+  const uint32_t fbytes = (uint32_t)(((c0 + (int64_t)t.rows * p.nx + 15) & ~(int64_t)15) - fa);
+  const bool conv = (p.feat & FEAT_OPEN) && p.outlet == OUTLET_CONVECTIVE;
+  const uint32_t pbytes = conv ? (uint32_t)t.rows * (uint32_t)(L::QP * sizeof(Real)) : 0u;
+  mbar_arrive_expect_tx(bar, (uint32_t)L::Q * (uint32_t)t.rows * row_bytes + fbytes + pbytes);
+  const char *P = static_cast<const char *>(p.P);
+  S *slab0 = reinterpret_cast<S *>(stage);
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    constexpr int ey = Dir<L, i>::y, ez = Dir<L, i>::z;
+    const int zs = L::DIMS == 3 ? wrap_n(t.z - ez, p.nz) : 0;
+    const int ys = wrap_n(t.y0 - ey, p.ny);               // first source row
+    const int n1 = p.ny - ys < t.rows ? p.ny - ys : t.rows;  // rows before the y wrap
+    char *dst = reinterpret_cast<char *>(slab0 + i * CAP);
+    const int64_t base = (int64_t)i * p.cs + (int64_t)zs * p.ny * p.nx;
+    bulk_g2s(dst, P + (base + (int64_t)ys * p.nx) * (int64_t)sizeof(S), (uint32_t)n1 * row_bytes, bar);
+    if (n1 < t.rows)
+      bulk_g2s(dst + (size_t)n1 * row_bytes, P + base * (int64_t)sizeof(S), (uint32_t)(t.rows - n1) * row_bytes,
+               bar);
+  });
+  bulk_g2s(stage + Cfg::pop_bytes, p.flags + fa, fbytes, bar);
+  if (conv)
+    bulk_g2s(stage + Cfg::pop_bytes + Cfg::flag_bytes, p.prev + ((int64_t)t.z * p.ny + t.y0) * L::QP, pbytes, bar);
+}
+
+// Warps never wait for one another: each one waits only for the stage it
+// needs to be full, computes its cells of the tile, and counts itself done
+// with the stage on a shared-memory counter; the warp that completes the
+// count refills the stage with the tile NS tiles ahead.  A slow warp (inlet,
+// outlet or link cells) therefore delays only the refill of one stage, not
+// the other warps, which may run up to NS - 1 tiles ahead.
+template <class L, class S, int COLL>
+__global__ void __launch_bounds__(TileCfg<L, S>::threads, TileCfg<L, S>::min_blocks)
+    k_step_tiled(const StepParams<typename StoreOps<S>::Real> p) {
+  using Real = typename StoreOps<S>::Real;
+  using Cfg = TileCfg<L, S>;
+  constexpr int NS = Cfg::stages;
+  constexpr int NW = Cfg::threads / 32;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char *stage0 = smem_raw;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + NS * Cfg::stage_bytes);
+  __shared__ uint32_t done[NS];  // warps finished with each stage (monotonic)
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int G = gridDim.x, nt = p.ntiles;
+  if (tid == 0) {
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      mbar_init(&bar[k], 1);
+      done[k] = 0;
     }
-    if (p.feat & FEAT_THERMAL) {
-      if (p.feat & FEAT_SCALAR_REDUCED) {
-        using G = typename ScalarReduced<L>::Lat;
-        scalar_step<L, G>(p, x, y, z, c, solid, sc, Real(G::cs2inv));
-      } else {
-        scalar_step<L, L>(p, x, y, z, c, solid, sc, Real(3));
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (tid == 0) {
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      const int tk = blockIdx.x + k * G;
+      if (tk < nt) issue_tile<L, S>(p, tk, stage0 + k * Cfg::stage_bytes, &bar[k]);
+    }
+  }
+  const int64_t step_now = *p.step;
+  int tile = blockIdx.x;
+  for (int it = 0; tile < nt; ++it, tile += G) {
+    const int s = it % NS;
+    const uint32_t use = (uint32_t)(it / NS);
+    if (!mbar_wait(&bar[s], use & 1u)) {
+      // the stage never completed: report and stop this warp; the stage is
+      // not refilled, so the other warps stop at their next wait.  Copies
+      // still in flight are waited for (bounded again) so that none lands
+      // after the block has exited.
+      if (lane == 0) atomicOr(p.status, STATUS_WAIT_TIMEOUT);
+      for (int k = 1; k < NS; k++) {
+        const int jt = it + k;
+        if (tile + k * G < nt) mbar_wait(&bar[jt % NS], (uint32_t)(jt / NS) & 1u);
+      }
+      return;
+    }
+    const unsigned char *sb = stage0 + s * Cfg::stage_bytes;
+    const S *st = reinterpret_cast<const S *>(sb);
+    const TileCoord t = tile_coord(p, tile);
+    const uint8_t *fl = sb + Cfg::pop_bytes + tile_flag_skew(p, t);
+    const Real *pv = reinterpret_cast<const Real *>(sb + Cfg::pop_bytes + Cfg::flag_bytes);
+    const int ncell = t.rows * p.nx;
+    int r = 0, x = tid;
+    while (x >= p.nx) { x -= p.nx; ++r; }
+    for (int k = tid; k < ncell; k += Cfg::threads) {
+      const uint32_t row = (uint32_t)(r * p.nx);
+      step_cell<L, S, COLL>(p, x, t.y0 + r, t.z, step_now,
+                            SmemGather<L, S, Real, Cfg::cap>{st, row, p.nx, fl + row, pv + r * L::QP});
+      x += Cfg::threads;
+      while (x >= p.nx) { x -= p.nx; ++r; }
+    }
+    // this warp's reads of stage s are complete (their values have been
+    // used); the last warp to get here refills the stage
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence_block();
+      const uint32_t before = atomicAdd(&done[s], 1u);
+      if (before == (use + 1) * NW - 1 && tile + NS * G < nt) {
+        fence_proxy_async_smem();
+        issue_tile<L, S>(p, tile + NS * G, stage0 + s * Cfg::stage_bytes, &bar[s]);
       }
     }
   }
-  Real om = p.omega;
-  const bool les = (COLL != COLL_MRT) && (p.feat & FEAT_LES);
-  if (les) om = les_omega<L>(p, x, y, z, c, solid);
-  const Real rho = collide<L, Real, COLL>(p, d, solid, om, les);
-  if constexpr (!FROM_STATE) {
-    // divergence guard (diagnostics.py:32-71): non-finite or non-positive rho
-    // of the state; one lane per warp reports, and only until it is recorded
-    const bool bad = !(rho > Real(0)) || !isfinite(rho);
-    const unsigned badm = __ballot_sync(__activemask(), bad);
-    if (bad && (threadIdx.x & 31) == __ffs(badm) - 1) {
-      if (!(*(volatile uint32_t *)p.status & STATUS_NONFINITE_OR_NONPOSITIVE_RHO))
-        atomicOr(p.status, STATUS_NONFINITE_OR_NONPOSITIVE_RHO);
-      if (*(volatile unsigned long long *)p.first_bad_step > (unsigned long long)(step_now + 1))
-        atomicMin(p.first_bad_step, (unsigned long long)(step_now + 1));
-    }
-  }
-  S *Pn = static_cast<S *>(p.Pn);
-  static_for<L::Q>([&](auto ic) {
-    constexpr int i = decltype(ic)::value;
-    SO::template store<i, L>(Pn, elem(p, i, c), d[i]);
-  });
 }
 
 // LES side pass: velocity of the current state (les.py:288 / :325 use

@@ -25,6 +25,7 @@ AERO_HD void static_for(F &&f) {
 
 struct D2Q9 {
   static constexpr int Q = 9, DIMS = 2, NP = 4;
+  static constexpr int QP = 12;  // Q rounded up to a multiple of 4 (16-byte rows of outlet state)
   static constexpr int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
   static constexpr int ey[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
   static constexpr int ez[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -39,6 +40,7 @@ struct D2Q9 {
 
 struct D3Q19 {
   static constexpr int Q = 19, DIMS = 3, NP = 9;
+  static constexpr int QP = 20;  // Q rounded up to a multiple of 4 (16-byte rows of outlet state)
   static constexpr int ex[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
   static constexpr int ey[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
   static constexpr int ez[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};

@@ -25,9 +25,16 @@ enum Feature : uint32_t {
   FEAT_OBSTACLE_BB = 1u << 10,    // obstacle bounce-back active (links present)
 };
 
+// Per-cell flag byte.
+enum CellFlag : uint8_t {
+  FLAG_SOLID = 1u << 0,
+  FLAG_LINK = 1u << 1,  // the cell has at least one obstacle link
+};
+
 // Status bits raised by the kernels (atomicOr into a device word).
 enum Status : uint32_t {
   STATUS_NONFINITE_OR_NONPOSITIVE_RHO = 1u << 0,
+  STATUS_WAIT_TIMEOUT = 1u << 1,  // a bounded device-side wait gave up (the step's output is incomplete)
 };
 
 // MRT operator in the even/odd pair basis (see lbm_mrt.cpp).  For D3Q19:
@@ -62,11 +69,13 @@ struct StepParams {
   int32_t inlet, outlet, wall;
   int32_t sponge_start; // first sponge x plane (>= nx when off)
   int32_t sponge_thickness;
+  // row tiles of the tiled step kernel: tile_rows y rows of one z plane
+  int32_t tile_rows, tiles_per_plane, ntiles;
 
   // populations (deviation from the rest weights, see Store<>)
   const void *P;        // current post-collision populations (read)
   void *Pn;             // next post-collision populations (written)
-  const uint8_t *solid; // (cells) 1 = solid
+  const uint8_t *flags; // (cells) CellFlag bits; the buffer has 32 bytes of slack past cs
   const uint32_t *lbits;  // per 32-cell word: bit k set when cell k of the word has links
   const int32_t *loff;    // per 32-cell word: index of its first link cell
   const uint32_t *lc_mask;  // per link cell: bit i set when direction i is a link
@@ -74,7 +83,7 @@ struct StepParams {
   const int64_t *lc_cell;   // per link cell: cell index
   int64_t n_lc;
 
-  const Real *prev;     // convective outlet state (Q, nz, ny), deviations
+  const Real *prev;     // convective outlet state (nz, ny, QP), deviations
   Real *prevn;
   const Real *g;        // scalar state (Qg, cells) -- populations, not deviations
   Real *gn;

@@ -8,7 +8,8 @@
 //   __nv_bfloat16  : d_i as is (8-bit exponent, no scaling needed)
 // Arithmetic is always done in Real (float, or double for double storage).
 // load/store take the base of one direction plane (a warp-uniform pointer)
-// and a 32-bit cell index, so each access is one wide multiply-add.
+// and a 32-bit cell index, so each access is one wide multiply-add; lds
+// reads the same format from a shared-memory tile.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -24,6 +25,8 @@ template <> struct StoreOps<float> {
   template <int I, class L>
   static __device__ __forceinline__ float load(const float *p, uint32_t o) { return __ldg(p + o); }
   template <int I, class L>
+  static __device__ __forceinline__ float lds(const float *p, uint32_t o) { return p[o]; }
+  template <int I, class L>
   static __device__ __forceinline__ void store(float *p, uint32_t o, float v) { p[o] = v; }
 };
 
@@ -31,6 +34,8 @@ template <> struct StoreOps<double> {
   using Real = double;
   template <int I, class L>
   static __device__ __forceinline__ double load(const double *p, uint32_t o) { return __ldg(p + o); }
+  template <int I, class L>
+  static __device__ __forceinline__ double lds(const double *p, uint32_t o) { return p[o]; }
   template <int I, class L>
   static __device__ __forceinline__ void store(double *p, uint32_t o, double v) { p[o] = v; }
 };
@@ -41,6 +46,11 @@ template <> struct StoreOps<__half> {
   static __device__ __forceinline__ float load(const __half *p, uint32_t o) {
     constexpr float s = float(L::w[I] / 64.0);
     return __half2float(__ldg(p + o)) * s;
+  }
+  template <int I, class L>
+  static __device__ __forceinline__ float lds(const __half *p, uint32_t o) {
+    constexpr float s = float(L::w[I] / 64.0);
+    return __half2float(p[o]) * s;
   }
   template <int I, class L>
   static __device__ __forceinline__ void store(__half *p, uint32_t o, float v) {
@@ -54,6 +64,10 @@ template <> struct StoreOps<__nv_bfloat16> {
   template <int I, class L>
   static __device__ __forceinline__ float load(const __nv_bfloat16 *p, uint32_t o) {
     return __bfloat162float(__ldg(p + o));
+  }
+  template <int I, class L>
+  static __device__ __forceinline__ float lds(const __nv_bfloat16 *p, uint32_t o) {
+    return __bfloat162float(p[o]);
   }
   template <int I, class L>
   static __device__ __forceinline__ void store(__nv_bfloat16 *p, uint32_t o, float v) {

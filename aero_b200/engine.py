@@ -157,6 +157,12 @@ class Engine:
             check("aero_first_bad_step", self.lib.aero_first_bad_step(self.h, ctypes.byref(v), self.stream()))
         return int(v.value)
 
+    def step_plan(self) -> dict:
+        """Step kernel in use: {"tiled": bool, "tile_rows": r, "blocks": b}."""
+        t, r, b = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        check("aero_step_plan", self.lib.aero_step_plan(self.h, ctypes.byref(t), ctypes.byref(r), ctypes.byref(b)))
+        return {"tiled": bool(t.value), "tile_rows": int(r.value), "blocks": int(b.value)}
+
     # ------------------------------------------------------------------ timing
     def enable_timing(self, on: bool = True) -> None:
         check("aero_enable_timing", self.lib.aero_enable_timing(self.h, 1 if on else 0))

@@ -247,7 +247,14 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--collision", default=None, choices=["bgk", "trt", "mrt"],
                     help="override the workload's collision operator (profiling)")
+    ap.add_argument("--kernel", default="rowgather", choices=["rowgather", "tiled"],
+                    help="step kernel: per-cell global gather (default) or rows staged in shared "
+                         "memory by bulk async copies")
     args = ap.parse_args()
+    if args.kernel == "tiled":
+        os.environ["AERO_B200_TILES"] = "1"
+    else:
+        os.environ.pop("AERO_B200_TILES", None)
     w = dict(WORKLOADS[args.workload])
     if args.collision:
         w["kwargs"] = dict(w["kwargs"], collision=args.collision)
@@ -331,9 +338,13 @@ def main():
     # DRAM bytes per launch from the committed ncu capture summary of this
     # kernel and precision (a smaller case scaled by cells where the summary
     # says so); None when no capture covers the workload
+    plan = eng.step_plan()
+    kname = "k_step_tiled" if plan["tiled"] else "k_step"
     traffic = None
     pat = re.compile(rf"^- {re.escape(args.workload)}: dram bytes per launch = (\d+)\s*$", re.M)
-    for md in sorted((ROOT / "profiles").glob(f"k_step_*_{args.precision}.md")):
+    for md in sorted((ROOT / "profiles").glob(f"{kname}_*_{args.precision}.md")):
+        if kname == "k_step" and md.name.startswith("k_step_tiled"):
+            continue
         m = pat.search(md.read_text())
         if m:
             traffic = int(m.group(1))
@@ -395,7 +406,11 @@ def main():
         "gpu_launches": launches_per_step * args.steps + 1,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": traffic, "kernel": "k_step (fused stream/BC/collide)",
+                     "traffic": traffic,
+                     "kernel": f"{kname} (fused stream/BC/collide"
+                               + (", source rows staged in shared memory by bulk async copies)"
+                                  if plan["tiled"] else ", per-cell global gather)"),
+                     "step_plan": plan,
                      "alg_bytes_per_launch": alg_bytes, "bytes_per_cell": bytes_per_cell,
                      "kernel_ms": k_ms, "finalize_ms": force_ms / max(nt, 1)},
         "clocks": clk.summary(),

@@ -135,14 +135,25 @@ AERO_API int aero_read_forces(AeroLattice *lat, double *out, int64_t max_steps, 
  * spanwise_force_profile_3d, forces3d.py:148-171); host memory, synchronous. */
 AERO_API int aero_read_profile(AeroLattice *lat, double *out, void *stream);
 
-/* Divergence flags raised on the device since creation (bit 0: a cell had a
+/* Status flags raised on the device since creation (bit 0: a cell had a
  * non-finite or non-positive density; the test of check_stability,
- * diagnostics.py:32-71).  Synchronous. */
+ * diagnostics.py:32-71.  Bit 1: a bounded device-side wait gave up, so a
+ * step's output is incomplete; no counterpart in the reference).
+ * Synchronous. */
 AERO_API int aero_status(AeroLattice *lat, uint32_t *status, void *stream);
 
 /* The first step (1-based, as counted by step_count) whose state had a
  * non-finite or non-positive density, or -1 if none has.  Synchronous. */
 AERO_API int aero_first_bad_step(AeroLattice *lat, int64_t *step, void *stream);
+
+/* Which step kernel aero_step launches (no counterpart in the reference):
+ * *tiled = 0 for the default kernel, in which each cell gathers its pulled
+ * populations from global memory; 1 for the row-tiled kernel, in which each
+ * block stages the source rows of its tile in shared memory with bulk async
+ * copies (selected by AERO_B200_TILES=1 in the environment at bind time,
+ * where rows fit a tile and start 16-byte aligned), with the rows per tile
+ * and the persistent grid size.  Valid after binding. */
+AERO_API int aero_step_plan(const AeroLattice *lat, int32_t *tiled, int32_t *tile_rows, int32_t *blocks);
 
 /* Steps taken (host mirror of the reference's step_count). */
 AERO_API int aero_step_count(const AeroLattice *lat, int64_t *steps);
