@@ -13,7 +13,7 @@ raise instead of falling back to a CPU path.
 from .geometry import Box, Cylinder, Rectangle, Sphere
 from .links import build_surface_links, build_surface_links_3d
 
-__all__ = ["Solver", "Solver3D", "Cylinder", "Rectangle", "Sphere", "Box", "build_surface_links",
+__all__ = ["Solver", "Solver3D", "Batch", "Cylinder", "Rectangle", "Sphere", "Box", "build_surface_links",
            "build_surface_links_3d", "build"]
 
 
@@ -30,4 +30,7 @@ def __getattr__(name):
     if name == "Solver3D":
         from .solver3d import Solver3D
         return Solver3D
+    if name == "Batch":
+        from .batch import Batch
+        return Batch
     raise AttributeError(name)

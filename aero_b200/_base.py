@@ -285,6 +285,12 @@ class LatticeSolverBase:
         c = self._coefficients(raw)
         return self._step_return(c, 0)
 
+    def _drag_norm(self) -> float:
+        """Force that makes Cd = 1: 0.5 rho0 u0^2 D (2D, forces.py:78-103) or
+        0.5 rho0 u0^2 D^2 (3D, forces3d.py:70-101)."""
+        fdyn = 0.5 * self.rho0 * self.u0 * self.u0 * self.D * (self.D if self.dims == 3 else 1.0)
+        return fdyn if fdyn > 0.0 else 1.0
+
     def status(self) -> int:
         """Device divergence flags (bit 0: non-finite or non-positive density seen)."""
         return self._engine.status()

@@ -70,6 +70,15 @@ SIGNATURES = {
                                 ctypes.c_int),
     "aero_kernel_times": ([_VP, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_I64), _VP],
                           ctypes.c_int),
+    "aero_batch_create": ([_I32, ctypes.POINTER(_VP)], ctypes.c_int),
+    "aero_batch_workspace_size": ([_VP, ctypes.POINTER(_U64)], ctypes.c_int),
+    "aero_batch_bind_workspace": ([_VP, _VP, _U64], ctypes.c_int),
+    "aero_batch_add": ([_VP, _VP, _D], ctypes.c_int),
+    "aero_batch_remove": ([_VP, _VP], ctypes.c_int),
+    "aero_batch_size": ([_VP, ctypes.POINTER(_I32)], ctypes.c_int),
+    "aero_batch_step": ([_VP, _I64, _VP], ctypes.c_int),
+    "aero_batch_converge": ([_VP, _I32, _D, _VP, _VP], ctypes.c_int),
+    "aero_batch_destroy": ([_VP], ctypes.c_int),
 }
 
 

@@ -96,6 +96,8 @@ int aero::set_error(int code, const char *msg) {
   return code;
 }
 
+struct AeroBatch;
+
 struct AeroLattice {
   AeroParams prm;
   int Q = 0, QP = 0, Qg = 0;
@@ -127,6 +129,8 @@ struct AeroLattice {
   cudaGraphExec_t pair_exec[2] = {nullptr, nullptr};
   bool use_graphs = true;
   int device = -1;  // device of the bound workspace
+  AeroBatch *batch = nullptr;  // batch this lattice is a member of (stepped only by it)
+  double cd_norm = 1.0;        // drag normalisation given when it joined the batch
   // row-tiled step plan (k_step_tiled), fixed at bind time
   bool tiled = false;
   int tile_blocks = 0, tile_rows = 0, tiles_per_plane = 0, ntiles = 0;
@@ -733,6 +737,7 @@ int aero_bind_workspace(AeroLattice *L, void *dptr, uint64_t bytes, void *stream
 int aero_set_state(AeroLattice *L, const double *f, const double *prev, const double *g, int64_t steps,
                    void *stream) {
   if (!L || !f) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (L->batch) return fail(AERO_ERR_STATE, "the lattice is a batch member; remove it from the batch first");
   if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
   if (steps < 0) return fail(AERO_ERR_INVALID, "negative step count");
   if (!L->state_set && !prev && (L->prm.outlet_bc == AERO_OUTLET_CONVECTIVE))
@@ -793,6 +798,7 @@ int aero_kernel_times(AeroLattice *L, double *step_ms, double *forces_ms, int64_
 
 int aero_step(AeroLattice *L, int64_t n, void *stream) {
   if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (L->batch) return fail(AERO_ERR_STATE, "the lattice is a batch member; it advances with aero_batch_step");
   if (!L->state_set) return fail(AERO_ERR_STATE, "aero_set_state must come first");
   if (n < 0) return fail(AERO_ERR_INVALID, "negative step count");
   if (L->step_count + n - L->read_upto > L->hist_cap)
@@ -878,6 +884,7 @@ int aero_step_plan(const AeroLattice *L, int32_t *tiled, int32_t *tile_rows, int
 
 int aero_destroy(AeroLattice *L) {
   if (!L) return AERO_OK;
+  if (L->batch) return fail(AERO_ERR_STATE, "the lattice is a batch member; remove it from the batch first");
   for (auto &e : L->pair_exec)
     if (e) cudaGraphExecDestroy(e);
   if (L->cap_stream) cudaStreamDestroy(L->cap_stream);
@@ -923,6 +930,475 @@ int aero_mrt_operator(int32_t dims, double omega, double *A, double *B) {
   if ((dims != 2 && dims != 3) || !A || !B) return fail(AERO_ERR_INVALID, "bad argument");
   MrtCoeffs<double> tmp;
   if (!build_mrt(dims, omega, tmp, A, B)) return fail(AERO_ERR_INVALID, "MRT operator not block diagonal");
+  return AERO_OK;
+}
+
+}  // extern "C"
+
+// ==========================================================================
+// Batches: many lattices advanced together, one launch per lattice class
+// (dimensions, storage, collision) and per step kernel (moments pass, step,
+// force finalisation).  The batch owns no device memory either: the caller
+// binds a workspace for its plan (parameter arrays, block prefixes, the
+// convergence items and results).
+// ==========================================================================
+namespace {
+
+// Rolling convergence of the drag coefficient on the device, with the rule
+// of analyze_convergence (diagnostics.py:87-120): over the last `window`
+// steps of Cd = Fx / cd_norm, ratio = std / mean|Cd| (population std);
+// converged when ratio < tol, or when mean|Cd| < 1e-12.  One block per
+// lattice; out receives (ratio, mean|Cd|, std, converged, steps) doubles and
+// converged = 0 while fewer than `window` steps are in the ring.
+struct ConvergeItem {
+  const double *hist;
+  const int64_t *step;
+  const int64_t *hist_base;
+  double *out;
+  double cd_norm;
+  int32_t hist_cap;
+};
+
+__global__ void __launch_bounds__(kFinalizeBlock) k_converge(const ConvergeItem *__restrict__ items, int n, int W,
+                                                              double tol) {
+  __shared__ double red[3][kFinalizeBlock / 32];
+  if ((int)blockIdx.x >= n) return;
+  const ConvergeItem it = items[blockIdx.x];
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  const int64_t steps = *it.step, hb = *it.hist_base;
+  if (steps - hb < W || W > it.hist_cap || W < 1) {
+    if (t == 0) {
+      it.out[0] = __longlong_as_double(0x7ff0000000000000ll);  // +inf
+      it.out[1] = 0.0;
+      it.out[2] = 0.0;
+      it.out[3] = 0.0;
+      it.out[4] = (double)steps;
+    }
+    return;
+  }
+  auto block_sum = [&](double v, int j) -> double {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (lane == 0) red[j][wid] = v;
+    __syncthreads();
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < kFinalizeBlock / 32; w++) s += red[j][w];
+    __syncthreads();
+    return s;
+  };
+  double sa = 0.0, sv = 0.0;
+  for (int k = t; k < W; k += kFinalizeBlock) {
+    const int64_t slot = (steps - W + k - hb) % it.hist_cap;
+    const double cd = it.hist[slot * 12] / it.cd_norm;
+    sa += fabs(cd);
+    sv += cd;
+  }
+  const double mean_abs = block_sum(sa, 0) / W;
+  const double mean = block_sum(sv, 1) / W;
+  double sq = 0.0;
+  for (int k = t; k < W; k += kFinalizeBlock) {
+    const int64_t slot = (steps - W + k - hb) % it.hist_cap;
+    const double dv = it.hist[slot * 12] / it.cd_norm - mean;
+    sq += dv * dv;
+  }
+  const double sd = sqrt(block_sum(sq, 2) / W);
+  if (t == 0) {
+    const bool tiny = mean_abs < 1e-12;
+    const double ratio = tiny ? 0.0 : sd / mean_abs;
+    it.out[0] = ratio;
+    it.out[1] = mean_abs;
+    it.out[2] = sd;
+    it.out[3] = (tiny || ratio < tol) ? 1.0 : 0.0;
+    it.out[4] = (double)steps;
+  }
+}
+
+
+__global__ void k_set_profile_steps(int64_t *const *ctrs, int n, int64_t delta) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) ctrs[k][4] = ctrs[k][0] + delta;  // profile_step = step + delta
+}
+
+struct ClassKey {
+  int dims, storage, coll;
+  bool operator==(const ClassKey &o) const { return dims == o.dims && storage == o.storage && coll == o.coll; }
+};
+
+struct ClassPlan {
+  ClassKey key;
+  bool f64;
+  int n = 0, n_les = 0;
+  int64_t blocks = 0, blocks_les = 0;
+  uint64_t params[2] = {0, 0}, first = 0, params_les[2] = {0, 0}, first_les = 0;
+};
+
+struct FinPlan {
+  int n = 0;
+  int64_t blocks = 0;
+  uint64_t params[2] = {0, 0}, first = 0;
+};
+
+ClassKey class_of(const AeroLattice *L) { return {L->prm.dims, L->prm.storage, L->prm.collision}; }
+
+}  // namespace
+
+struct AeroBatch {
+  int max_members = 0;
+  std::vector<AeroLattice *> members;
+  int device = -1;
+  char *ws = nullptr;
+  uint64_t ws_bytes = 0;
+  bool bound = false, dirty = true;
+  int phase = 0;  // parity of the steps taken since the plan was built
+  // plan (device offsets into ws)
+  std::vector<ClassPlan> classes;
+  FinPlan fin[2];  // [0] float members, [1] double members
+  uint64_t ctr_ptrs = 0, conv_items = 0, conv_out = 0;
+  std::vector<char> host_plan;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [steps - 1][phase]
+};
+
+namespace {
+
+void batch_drop_graphs(AeroBatch *B) {
+  for (auto &row : B->graph)
+    for (auto &g : row)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+}
+
+uint64_t batch_bytes(int max_members) {
+  // Upper bound of batch_build's plan: every member in the step, LES and
+  // finalisation lists with the largest parameter block (two parities plus
+  // a block prefix each); the one-entry minimum of the LES lists of up to
+  // 24 classes and of the two finalisation lists; counters pointers,
+  // convergence items and results; 256-byte alignment of every array.
+  const uint64_t m = (uint64_t)std::max(max_members, 1);
+  const uint64_t sp = sizeof(StepParams<double>);
+  const uint64_t kClasses = 2 * 4 * 3;
+  uint64_t b = 3 * m * (2 * sp + 8);
+  b += (kClasses + 2) * (2 * sp + 8);
+  b += m * (8 + sizeof(ConvergeItem) + 5 * 8);
+  b += kAlign * (6 * kClasses + 6 + 3 + 1);
+  return align_up(b);
+}
+
+template <class Real>
+void put_params(std::vector<char> &buf, uint64_t off, const AeroLattice *L, int parity) {
+  const StepParams<Real> p = make_params<Real>(L, parity);
+  std::memcpy(buf.data() + off, &p, sizeof(p));
+}
+
+// Builds the plan for the current members on the host and uploads it.  The
+// parameter array used by step j of a graph is [(phase + j) % 2], and holds
+// each member's buffers for its own parity at that step.
+int batch_build(AeroBatch *B, cudaStream_t st) {
+  B->classes.clear();
+  B->fin[0] = FinPlan{};
+  B->fin[1] = FinPlan{};
+  for (AeroLattice *L : B->members) {
+    const ClassKey k = class_of(L);
+    auto it = std::find_if(B->classes.begin(), B->classes.end(), [&](const ClassPlan &c) { return c.key == k; });
+    if (it == B->classes.end()) {
+      ClassPlan c;
+      c.key = k;
+      c.f64 = is_f64(L);
+      B->classes.push_back(c);
+      it = B->classes.end() - 1;
+    }
+    it->n++;
+    if (les_active(L)) it->n_les++;
+    B->fin[is_f64(L) ? 1 : 0].n++;
+  }
+  std::vector<char> &h = B->host_plan;
+  h.assign(B->ws_bytes, 0);
+  uint64_t o = 0;
+  auto take = [&](uint64_t bytes) {
+    const uint64_t at = o;
+    o = align_up(o + std::max<uint64_t>(bytes, 1));
+    return at;
+  };
+  auto cell_blocks = [](const AeroLattice *L) {
+    return (int64_t)blocks_for(L->prm.nx, kStepBlock) * L->prm.ny * L->prm.nz;
+  };
+  for (ClassPlan &c : B->classes) {
+    const uint64_t sp = c.f64 ? sizeof(StepParams<double>) : sizeof(StepParams<float>);
+    c.params[0] = take(sp * c.n);
+    c.params[1] = take(sp * c.n);
+    c.first = take(8 * (uint64_t)c.n);
+    c.params_les[0] = take(sp * std::max(c.n_les, 1));
+    c.params_les[1] = take(sp * std::max(c.n_les, 1));
+    c.first_les = take(8 * (uint64_t)std::max(c.n_les, 1));
+    int k = 0, kl = 0;
+    int64_t blocks = 0, blocks_les = 0;
+    for (AeroLattice *L : B->members) {
+      if (!(class_of(L) == c.key)) continue;
+      for (int j = 0; j < 2; j++) {
+        const int par = (L->cur + j) & 1;  // parity at steps with (phase + j') % 2 == j, phase = 0 after a build
+        if (c.f64) put_params<double>(h, c.params[j] + sp * k, L, par);
+        else put_params<float>(h, c.params[j] + sp * k, L, par);
+      }
+      std::memcpy(h.data() + c.first + 8 * k, &blocks, 8);
+      blocks += cell_blocks(L);
+      k++;
+      if (les_active(L)) {
+        for (int j = 0; j < 2; j++) {
+          const int par = (L->cur + j) & 1;
+          if (c.f64) put_params<double>(h, c.params_les[j] + sp * kl, L, par);
+          else put_params<float>(h, c.params_les[j] + sp * kl, L, par);
+        }
+        std::memcpy(h.data() + c.first_les + 8 * kl, &blocks_les, 8);
+        blocks_les += cell_blocks(L);
+        kl++;
+      }
+    }
+    c.blocks = blocks;
+    c.blocks_les = blocks_les;
+  }
+  for (int r = 0; r < 2; r++) {
+    FinPlan &f = B->fin[r];
+    const uint64_t sp = r ? sizeof(StepParams<double>) : sizeof(StepParams<float>);
+    f.params[0] = take(sp * std::max(f.n, 1));
+    f.params[1] = take(sp * std::max(f.n, 1));
+    f.first = take(8 * (uint64_t)std::max(f.n, 1));
+    int k = 0;
+    int64_t blocks = 0;
+    for (AeroLattice *L : B->members) {
+      if ((is_f64(L) ? 1 : 0) != r) continue;
+      for (int j = 0; j < 2; j++) {
+        const int par = (L->cur + j) & 1;
+        if (r) put_params<double>(h, f.params[j] + sp * k, L, par);
+        else put_params<float>(h, f.params[j] + sp * k, L, par);
+      }
+      std::memcpy(h.data() + f.first + 8 * k, &blocks, 8);
+      blocks += r ? make_params<double>(L, L->cur).fin_blocks : make_params<float>(L, L->cur).fin_blocks;
+      k++;
+    }
+    f.blocks = blocks;
+  }
+  const int n = (int)B->members.size();
+  B->ctr_ptrs = take(8 * (uint64_t)std::max(n, 1));
+  B->conv_items = take(sizeof(ConvergeItem) * std::max(n, 1));
+  B->conv_out = take(5 * 8 * (uint64_t)std::max(n, 1));
+  if (o > B->ws_bytes) return fail(AERO_ERR_CAPACITY, "batch plan needs %llu bytes, workspace has %llu",
+                                   (unsigned long long)o, (unsigned long long)B->ws_bytes);
+  for (int k = 0; k < n; k++) {
+    AeroLattice *L = B->members[k];
+    int64_t *ctr = reinterpret_cast<int64_t *>(L->ws + L->lay.counters);
+    std::memcpy(h.data() + B->ctr_ptrs + 8 * k, &ctr, 8);
+    ConvergeItem ci;
+    ci.hist = reinterpret_cast<const double *>(L->ws + L->lay.hist);
+    ci.step = ctr;
+    ci.hist_base = ctr + 1;
+    ci.out = reinterpret_cast<double *>(B->ws + B->conv_out) + 5 * k;
+    ci.cd_norm = L->cd_norm;
+    ci.hist_cap = L->hist_cap;
+    std::memcpy(h.data() + B->conv_items + sizeof(ConvergeItem) * k, &ci, sizeof(ci));
+  }
+  // pageable source: the call returns once the data is staged, so the host
+  // plan may be rebuilt afterwards
+  CUDA_TRY(cudaMemcpyAsync(B->ws, h.data(), o, cudaMemcpyHostToDevice, st));
+  batch_drop_graphs(B);
+  B->phase = 0;
+  B->dirty = false;
+  return AERO_OK;
+}
+
+// Launches one step of every member; `j` selects the parameter arrays.
+int batch_launch_step(AeroBatch *B, int j, cudaStream_t st) {
+  char *ws = B->ws;
+  for (const ClassPlan &c : B->classes) {
+    if (c.f64) {
+      const Ops<double> *ops = ops_f64(c.key.dims, c.key.coll);
+      auto *P = reinterpret_cast<const StepParams<double> *>(ws + c.params[j]);
+      auto *PL = reinterpret_cast<const StepParams<double> *>(ws + c.params_les[j]);
+      if (c.n_les) CUDA_TRY(ops->moments_batch(PL, reinterpret_cast<const int64_t *>(ws + c.first_les), c.n_les,
+                                               c.blocks_les, st));
+      CUDA_TRY(ops->step_batch(P, reinterpret_cast<const int64_t *>(ws + c.first), c.n, c.blocks, st));
+    } else {
+      const Ops<float> *ops = c.key.storage == AERO_STORE_F32   ? ops_f32(c.key.dims, c.key.coll)
+                              : c.key.storage == AERO_STORE_F16 ? ops_f16(c.key.dims, c.key.coll)
+                                                                : ops_bf16(c.key.dims, c.key.coll);
+      auto *P = reinterpret_cast<const StepParams<float> *>(ws + c.params[j]);
+      auto *PL = reinterpret_cast<const StepParams<float> *>(ws + c.params_les[j]);
+      if (c.n_les) CUDA_TRY(ops->moments_batch(PL, reinterpret_cast<const int64_t *>(ws + c.first_les), c.n_les,
+                                               c.blocks_les, st));
+      CUDA_TRY(ops->step_batch(P, reinterpret_cast<const int64_t *>(ws + c.first), c.n, c.blocks, st));
+    }
+  }
+  // the finalisation kernels do not depend on the lattice class, so any
+  // table of the right arithmetic type launches them
+  if (B->fin[0].n)
+    CUDA_TRY(ops_f32(2, 0)->finalize_batch(reinterpret_cast<const StepParams<float> *>(ws + B->fin[0].params[j]),
+                                           reinterpret_cast<const int64_t *>(ws + B->fin[0].first), B->fin[0].n,
+                                           B->fin[0].blocks, st));
+  if (B->fin[1].n)
+    CUDA_TRY(ops_f64(2, 0)->finalize_batch(reinterpret_cast<const StepParams<double> *>(ws + B->fin[1].params[j]),
+                                           reinterpret_cast<const int64_t *>(ws + B->fin[1].first), B->fin[1].n,
+                                           B->fin[1].blocks, st));
+  return AERO_OK;
+}
+
+// Graph of `steps` (1 or 2) consecutive steps starting at `phase`.
+int batch_graph(AeroBatch *B, int steps, int phase, cudaGraphExec_t *out) {
+  cudaGraphExec_t &g = B->graph[steps - 1][phase];
+  if (!g) {
+    if (!B->cap_stream) CUDA_TRY(cudaStreamCreateWithFlags(&B->cap_stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaStreamBeginCapture(B->cap_stream, cudaStreamCaptureModeThreadLocal));
+    int rc = AERO_OK;
+    for (int j = 0; j < steps && rc == AERO_OK; j++) rc = batch_launch_step(B, (phase + j) & 1, B->cap_stream);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(B->cap_stream, &graph);
+    if (rc != AERO_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (e != cudaSuccess) return fail(AERO_ERR_CUDA, "batch capture: %s", cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(&g, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return fail(AERO_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(ei));
+  }
+  *out = g;
+  return AERO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int aero_batch_create(int32_t max_members, AeroBatch **out) {
+  if (!out) return fail(AERO_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  if (max_members < 1 || max_members > 65536) return fail(AERO_ERR_INVALID, "max_members must be in 1..65536");
+  AeroBatch *B = new AeroBatch();
+  B->max_members = max_members;
+  B->ws_bytes = batch_bytes(max_members);
+  *out = B;
+  return AERO_OK;
+}
+
+int aero_batch_workspace_size(const AeroBatch *B, uint64_t *bytes) {
+  if (!B || !bytes) return fail(AERO_ERR_INVALID, "NULL argument");
+  *bytes = B->ws_bytes;
+  return AERO_OK;
+}
+
+int aero_batch_bind_workspace(AeroBatch *B, void *dptr, uint64_t bytes) {
+  if (!B || !dptr) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (B->bound) return fail(AERO_ERR_STATE, "batch workspace already bound");
+  if (bytes < B->ws_bytes) return fail(AERO_ERR_INVALID, "batch workspace too small: %llu < %llu",
+                                       (unsigned long long)bytes, (unsigned long long)B->ws_bytes);
+  if (reinterpret_cast<uintptr_t>(dptr) % kAlign) return fail(AERO_ERR_INVALID, "workspace must be 256-byte aligned");
+  cudaPointerAttributes attr;
+  CUDA_TRY(cudaPointerGetAttributes(&attr, dptr));
+  if (attr.type != cudaMemoryTypeDevice) return fail(AERO_ERR_INVALID, "workspace is not device memory");
+  B->device = attr.device;
+  B->ws = static_cast<char *>(dptr);
+  B->bound = true;
+  return AERO_OK;
+}
+
+int aero_batch_add(AeroBatch *B, AeroLattice *L, double cd_norm) {
+  if (!B || !L) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!B->bound) return fail(AERO_ERR_STATE, "batch workspace not bound");
+  if (!L->state_set) return fail(AERO_ERR_STATE, "the lattice needs a state (aero_set_state) before joining");
+  if (L->batch) return fail(AERO_ERR_STATE, "the lattice is already a batch member");
+  if (L->device != B->device) return fail(AERO_ERR_INVALID, "the lattice is on another device than the batch");
+  if ((int)B->members.size() >= B->max_members) return fail(AERO_ERR_CAPACITY, "batch holds %d members", B->max_members);
+  if (!(cd_norm > 0.0) || !std::isfinite(cd_norm)) return fail(AERO_ERR_INVALID, "cd_norm must be > 0");
+  L->batch = B;
+  L->cd_norm = cd_norm;
+  B->members.push_back(L);
+  B->dirty = true;
+  return AERO_OK;
+}
+
+int aero_batch_remove(AeroBatch *B, AeroLattice *L) {
+  if (!B || !L) return fail(AERO_ERR_INVALID, "NULL argument");
+  auto it = std::find(B->members.begin(), B->members.end(), L);
+  if (it == B->members.end()) return fail(AERO_ERR_INVALID, "the lattice is not a member of this batch");
+  B->members.erase(it);
+  L->batch = nullptr;
+  B->dirty = true;
+  return AERO_OK;
+}
+
+int aero_batch_size(const AeroBatch *B, int32_t *n) {
+  if (!B || !n) return fail(AERO_ERR_INVALID, "NULL argument");
+  *n = (int32_t)B->members.size();
+  return AERO_OK;
+}
+
+int aero_batch_step(AeroBatch *B, int64_t n, void *stream) {
+  if (!B) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!B->bound) return fail(AERO_ERR_STATE, "batch workspace not bound");
+  if (n < 0) return fail(AERO_ERR_INVALID, "negative step count");
+  if (n == 0 || B->members.empty()) return AERO_OK;
+  CUDA_TRY(cudaSetDevice(B->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (B->dirty) {
+    const int rc = batch_build(B, st);
+    if (rc != AERO_OK) return rc;
+  }
+  const int nm = (int)B->members.size();
+  // only the last step of the call sums the force profiles
+  k_set_profile_steps<<<blocks_for(nm, 128), 128, 0, st>>>(reinterpret_cast<int64_t *const *>(B->ws + B->ctr_ptrs),
+                                                          nm, n);
+  CUDA_TRY(cudaGetLastError());
+  int64_t left = n;
+  while (left > 0) {
+    const int steps = left >= 2 ? 2 : 1;
+    cudaGraphExec_t g = nullptr;
+    const int rc = batch_graph(B, steps, B->phase, &g);
+    if (rc != AERO_OK) return rc;
+    CUDA_TRY(cudaGraphLaunch(g, st));
+    B->phase = (B->phase + steps) & 1;
+    left -= steps;
+  }
+  for (AeroLattice *L : B->members) {
+    L->cur ^= (int)(n & 1);
+    L->step_count += n;
+    L->old_is_state = false;
+    // a member's history is a rolling window: unread steps older than the
+    // ring are dropped
+    L->read_upto = std::max(L->read_upto, L->step_count - (int64_t)L->hist_cap);
+  }
+  return AERO_OK;
+}
+
+int aero_batch_converge(AeroBatch *B, int32_t window, double tol, double *out, void *stream) {
+  if (!B || !out) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!B->bound) return fail(AERO_ERR_STATE, "batch workspace not bound");
+  if (window < 1) return fail(AERO_ERR_INVALID, "window must be >= 1");
+  for (AeroLattice *L : B->members)
+    if (window > L->hist_cap) return fail(AERO_ERR_INVALID, "window %d exceeds a member's history ring (%d steps)",
+                                          window, L->hist_cap);
+  const int nm = (int)B->members.size();
+  if (nm == 0) return AERO_OK;
+  CUDA_TRY(cudaSetDevice(B->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (B->dirty) {
+    const int rc = batch_build(B, st);
+    if (rc != AERO_OK) return rc;
+  }
+  k_converge<<<nm, kFinalizeBlock, 0, st>>>(reinterpret_cast<const ConvergeItem *>(B->ws + B->conv_items), nm,
+                                            window, tol);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(out, B->ws + B->conv_out, 5 * 8 * (size_t)nm, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return AERO_OK;
+}
+
+int aero_batch_destroy(AeroBatch *B) {
+  if (!B) return AERO_OK;
+  for (AeroLattice *L : B->members) L->batch = nullptr;
+  batch_drop_graphs(B);
+  if (B->cap_stream) cudaStreamDestroy(B->cap_stream);
+  delete B;
   return AERO_OK;
 }
 

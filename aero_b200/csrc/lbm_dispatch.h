@@ -21,6 +21,14 @@ struct Ops {
   // on the current device: raises the kernel's dynamic shared-memory limit and
   // reports resident blocks per SM and the cells one row slab holds
   cudaError_t (*tiled_setup)(int *blocks_per_sm, int *cap_cells);
+  // batched kernels over `n` members of one class: params and first (block
+  // prefix, n entries) are device arrays; blocks = total grid size
+  cudaError_t (*step_batch)(const StepParams<Real> *params, const int64_t *first, int n, int64_t blocks,
+                            cudaStream_t);
+  cudaError_t (*moments_batch)(const StepParams<Real> *params, const int64_t *first, int n, int64_t blocks,
+                               cudaStream_t);
+  cudaError_t (*finalize_batch)(const StepParams<Real> *params, const int64_t *first, int n, int64_t blocks,
+                                cudaStream_t);
   int store_bytes;
 };
 

@@ -60,8 +60,24 @@ struct Launch {
     *cap_cells = TileCfg<L, S>::cap;
     return e;
   }
-  static constexpr Ops<Real> table = {&step,       &moments,     &finalize,     &state_out, &load_state,
-                                      &step_tiled, &tiled_setup, (int)sizeof(S)};
+  static cudaError_t step_batch(const StepParams<Real> *params, const int64_t *first, int n, int64_t blocks,
+                                cudaStream_t st) {
+    k_step_batch<L, S, COLL><<<(unsigned)blocks, kStepBlock, 0, st>>>(params, first, n);
+    return cudaGetLastError();
+  }
+  static cudaError_t moments_batch(const StepParams<Real> *params, const int64_t *first, int n, int64_t blocks,
+                                   cudaStream_t st) {
+    k_moments_batch<L, S><<<(unsigned)blocks, kStepBlock, 0, st>>>(params, first, n);
+    return cudaGetLastError();
+  }
+  static cudaError_t finalize_batch(const StepParams<Real> *params, const int64_t *first, int n, int64_t blocks,
+                                    cudaStream_t st) {
+    k_finalize_batch<Real><<<(unsigned)blocks, kFinalizeBlock, 0, st>>>(params, first, n);
+    return cudaGetLastError();
+  }
+  static constexpr Ops<Real> table = {&step,       &moments,     &finalize,   &state_out,     &load_state,
+                                      &step_tiled, &tiled_setup, &step_batch, &moments_batch, &finalize_batch,
+                                      (int)sizeof(S)};
 };
 
 template <class S>

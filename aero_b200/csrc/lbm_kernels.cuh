@@ -1143,12 +1143,9 @@ __global__ void __launch_bounds__(TileCfg<L, S>::threads, TileCfg<L, S>::min_blo
 // LES side pass: velocity of the current state (les.py:288 / :325 use
 // compute_macroscopic of the pre-collision state, solids not zeroed).
 template <class L, class S, bool FROM_STATE>
-__global__ void __launch_bounds__(kStepBlock) k_moments(const StepParams<typename StoreOps<S>::Real> p) {
+__device__ __forceinline__ void moments_cell(const StepParams<typename StoreOps<S>::Real> &p, int x, int y, int z) {
   using Real = typename StoreOps<S>::Real;
   using SO = StoreOps<S>;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y, z = blockIdx.z;
-  if (x >= p.nx) return;
   const uint32_t c = cell_index(p, x, y, z);
   Real d[L::Q];
   if constexpr (FROM_STATE) {
@@ -1175,19 +1172,27 @@ __global__ void __launch_bounds__(kStepBlock) k_moments(const StepParams<typenam
   p.Uw[2 * p.cs + c] = jz * inv;
 }
 
+template <class L, class S, bool FROM_STATE>
+__global__ void __launch_bounds__(kStepBlock) k_moments(const StepParams<typename StoreOps<S>::Real> p) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= p.nx) return;
+  moments_cell<L, S, FROM_STATE>(p, x, (int)blockIdx.y, (int)blockIdx.z);
+}
+
 // Sums the per-link-cell contributions plus the constant rest-weight part
 // into the device history ring, sums the profile segments when this step's
 // profile is the one that can be read, then advances the step counter.
 // Block b adds link cells [b * fin_chunk, (b + 1) * fin_chunk) in a fixed
 // order and stores 12 partial sums; the block that finishes last adds the
 // partials in block order, so the result does not depend on block timing.
+// Block `bid` of `nblocks` finalisation blocks of one lattice.
 template <class Real>
-__global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const StepParams<Real> p) {
+__device__ __forceinline__ void finalize_block(const StepParams<Real> &p, int bid, int nblocks) {
   __shared__ double sm[12][kFinalizeBlock / 32];
   __shared__ bool last;
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   const int64_t n = p.n_lc;
-  const int64_t k0 = (int64_t)blockIdx.x * p.fin_chunk;
+  const int64_t k0 = (int64_t)bid * p.fin_chunk;
   const int64_t k1 = k0 + p.fin_chunk < n ? k0 + p.fin_chunk : n;
   double a[12];
 #pragma unroll
@@ -1208,11 +1213,11 @@ __global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const StepParams<Re
     double v = 0.0;
 #pragma unroll
     for (int w = 0; w < kFinalizeBlock / 32; w++) v += sm[t][w];
-    p.fin_partial[blockIdx.x * 12 + t] = v;
+    p.fin_partial[bid * 12 + t] = v;
     __threadfence();
   }
   __syncthreads();
-  if (t == 0) last = atomicAdd(p.fin_ticket, 1u) == gridDim.x - 1;
+  if (t == 0) last = atomicAdd(p.fin_ticket, 1u) == (unsigned)nblocks - 1;
   __syncthreads();
   if (!last) return;
   __threadfence();
@@ -1220,7 +1225,7 @@ __global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const StepParams<Re
   const int64_t slot = (step - *p.hist_base) % p.hist_cap;
   if (t < 12) {
     double v = p.force_const[t];
-    for (int b = 0; b < (int)gridDim.x; b++) v += __ldcg(p.fin_partial + b * 12 + t);
+    for (int b = 0; b < nblocks; b++) v += __ldcg(p.fin_partial + b * 12 + t);
     p.hist[slot * 12 + t] = v;
   }
   if (p.want_profile && step + 1 == *p.profile_step) {
@@ -1241,6 +1246,80 @@ __global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const StepParams<Re
     *p.fin_ticket = 0u;
     *p.step = step + 1;
   }
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const StepParams<Real> p) {
+  finalize_block(p, (int)blockIdx.x, (int)gridDim.x);
+}
+
+// --------------------------------------------------------------------------
+// Batched stepping: many lattices of one class (lattice, storage format,
+// collision) advance in one launch.  Member m owns blocks [first[m],
+// first[m + 1]) of the grid, with the same cell mapping as the single-lattice
+// kernel (one block per kStepBlock-cell x segment of a row, or per
+// finalisation block); each block copies its member's parameters into shared
+// memory, then runs the same per-cell code.  The parameter arrays live in
+// device memory, so a captured launch stays valid while the members advance.
+// --------------------------------------------------------------------------
+__device__ __forceinline__ int find_member(const int64_t *__restrict__ first, int n, int64_t b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(first + mid) <= b) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <class Real>
+__device__ __forceinline__ void params_to_smem(StepParams<Real> &dst, const StepParams<Real> *src) {
+  static_assert(sizeof(StepParams<Real>) % 8 == 0, "parameter block in 8-byte words");
+  constexpr int W = (int)(sizeof(StepParams<Real>) / 8);
+  uint64_t *d = reinterpret_cast<uint64_t *>(&dst);
+  const uint64_t *s = reinterpret_cast<const uint64_t *>(src);
+  for (int k = threadIdx.x; k < W; k += blockDim.x) d[k] = __ldg(s + k);
+  __syncthreads();
+}
+
+template <class L, class S, int COLL>
+__global__ void __launch_bounds__(kStepBlock, sizeof(typename StoreOps<S>::Real) == 4 ? kStepMinBlocks : 4)
+    k_step_batch(const StepParams<typename StoreOps<S>::Real> *__restrict__ params,
+                 const int64_t *__restrict__ first, int nmembers) {
+  using Real = typename StoreOps<S>::Real;
+  __shared__ StepParams<Real> sp;
+  const int m = find_member(first, nmembers, blockIdx.x);
+  params_to_smem(sp, params + m);
+  const int64_t b = (int64_t)blockIdx.x - __ldg(first + m);
+  const int nxb = (sp.nx + kStepBlock - 1) / kStepBlock;
+  const int64_t row = b / nxb;
+  const int x = (int)(b - row * nxb) * kStepBlock + threadIdx.x;
+  const int y = (int)(row % sp.ny), z = (int)(row / sp.ny);
+  if (x >= sp.nx) return;
+  step_cell<L, S, COLL>(sp, x, y, z, *sp.step, GlobalGather<L, S, Real>{sp, y, z});
+}
+
+template <class L, class S>
+__global__ void __launch_bounds__(kStepBlock) k_moments_batch(const StepParams<typename StoreOps<S>::Real> *__restrict__ params,
+                                                              const int64_t *__restrict__ first, int nmembers) {
+  using Real = typename StoreOps<S>::Real;
+  __shared__ StepParams<Real> sp;
+  const int m = find_member(first, nmembers, blockIdx.x);
+  params_to_smem(sp, params + m);
+  const int64_t b = (int64_t)blockIdx.x - __ldg(first + m);
+  const int nxb = (sp.nx + kStepBlock - 1) / kStepBlock;
+  const int64_t row = b / nxb;
+  const int x = (int)(b - row * nxb) * kStepBlock + threadIdx.x;
+  if (x >= sp.nx) return;
+  moments_cell<L, S, false>(sp, x, (int)(row % sp.ny), (int)(row / sp.ny));
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kFinalizeBlock) k_finalize_batch(const StepParams<Real> *__restrict__ params,
+                                                                   const int64_t *__restrict__ first, int nmembers) {
+  __shared__ StepParams<Real> sp;
+  const int m = find_member(first, nmembers, blockIdx.x);
+  params_to_smem(sp, params + m);
+  finalize_block(sp, (int)((int64_t)blockIdx.x - __ldg(first + m)), sp.fin_blocks);
 }
 
 // State of the step that produced P (f as the reference stores it), written

@@ -211,6 +211,47 @@ AERO_API int aero_link_forces_static(int32_t dims, int32_t nx, int32_t ny, int32
                                      const double *f_post, const int32_t *links, int64_t n_links,
                                      const double *center, double *out, double *profile, void *stream);
 
+/* ---- Batches: many lattices advanced together -------------------------
+ * No counterpart in the reference, which advances one Solver at a time from
+ * Python (Solver.run, solver.py:517-570).  A batch steps all its member
+ * lattices with one launch per lattice class (dimensions, storage,
+ * collision) and step kernel, replayed as CUDA graphs; lattices of any size,
+ * geometry and parameters mix.  Members keep their own device state, force
+ * history and read functions (aero_read_forces, aero_get_state, ...); while a
+ * member, a lattice is advanced only by aero_batch_step (aero_step,
+ * aero_set_state and aero_destroy on it return AERO_ERR_STATE) and its force
+ * history is a rolling window of its ring: unread steps older than the ring
+ * are dropped.  The caller allocates the batch's device workspace, as for a
+ * lattice.  Not thread-safe: one host thread per batch and its members. */
+typedef struct AeroBatch AeroBatch;
+
+/* A batch for up to max_members lattices. */
+AERO_API int aero_batch_create(int32_t max_members, AeroBatch **out);
+/* Device bytes of the batch's plan; the caller allocates them. */
+AERO_API int aero_batch_workspace_size(const AeroBatch *batch, uint64_t *bytes);
+/* Binds the caller's device workspace (256-byte aligned). */
+AERO_API int aero_batch_bind_workspace(AeroBatch *batch, void *device_ptr, uint64_t bytes);
+/* Adds a bound lattice whose state is set.  cd_norm is the drag
+ * normalisation used by aero_batch_converge: Cd = Fx / cd_norm (the
+ * reference's 0.5 rho0 u0^2 D in 2D, forces.py:78-103, and 0.5 rho0 u0^2 D^2
+ * in 3D, forces3d.py:70-101). */
+AERO_API int aero_batch_add(AeroBatch *batch, AeroLattice *lat, double cd_norm);
+/* Removes a member; it can then be stepped, read or destroyed on its own. */
+AERO_API int aero_batch_remove(AeroBatch *batch, AeroLattice *lat);
+AERO_API int aero_batch_size(const AeroBatch *batch, int32_t *n);
+/* Advances every member n_steps steps, forces included.  Asynchronous. */
+AERO_API int aero_batch_step(AeroBatch *batch, int64_t n_steps, void *stream);
+/* Rolling drag convergence of every member on the device, by the rule of
+ * analyze_convergence (diagnostics.py:87-120): over the last `window`
+ * steps, ratio = std(Cd) / mean|Cd|, converged when ratio < tol (or mean|Cd|
+ * < 1e-12).  out (host) receives 5 doubles per member, in the order the
+ * members joined: ratio, mean|Cd|, std, converged (0/1), steps taken; ratio
+ * is +inf and converged 0 while fewer than `window` steps are in the ring.
+ * Synchronous. */
+AERO_API int aero_batch_converge(AeroBatch *batch, int32_t window, double tol, double *out, void *stream);
+/* Releases the batch (members stay valid and leave it). */
+AERO_API int aero_batch_destroy(AeroBatch *batch);
+
 /* sizeof(AeroParams), so bindings can check their struct layout. */
 AERO_API int aero_params_size(void);
 

@@ -1,0 +1,205 @@
+"""Batched stepping (aero_batch_*): members of mixed class advance in the
+batch exactly as they do alone, join and leave between steps, and the
+device convergence detector follows analyze_convergence
+(aero/diagnostics.py:87-120).  The CPU tests cover argument checking of
+the C ABI without a GPU."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+
+def _lib():
+    from aero_b200 import _lib
+    return _lib.load(build_if_missing=False)
+
+
+def test_batch_create_checks_arguments():
+    lib = _lib()
+    h = ctypes.c_void_p()
+    assert lib.aero_batch_create(0, ctypes.byref(h)) != 0
+    assert lib.aero_batch_create(4, ctypes.byref(h)) == 0
+    n = ctypes.c_uint64()
+    assert lib.aero_batch_workspace_size(h, ctypes.byref(n)) == 0 and n.value > 0
+    assert lib.aero_batch_bind_workspace(h, None, n.value) != 0
+    out = np.zeros(5)
+    assert lib.aero_batch_converge(h, 10, 1e-3, out.ctypes.data, None) != 0  # not bound
+    assert lib.aero_batch_step(h, 1, None) != 0  # not bound
+    size = ctypes.c_int32(-1)
+    assert lib.aero_batch_size(h, ctypes.byref(size)) == 0 and size.value == 0
+    assert lib.aero_batch_destroy(h) == 0
+
+
+def _cases():
+    """Solver constructors of mixed class: 2D/3D, BGK/TRT/MRT, LES (moments
+    pass), thermal scalar, fp32/fp64/fp16s/bf16s, Bouzidi, uneven sizes."""
+    from aero_b200 import Box, Cylinder, Rectangle, Solver, Solver3D, Sphere
+
+    def c2d(ny, nx, geo, **kw):
+        solid = geo.mark_solid(ny, nx)
+        phi = geo.sdf_field(ny, nx) if kw.get("bouzidi") else None
+        return lambda: Solver(Ny=ny, Nx=nx, solid=solid, D=geo.reference_length(), phi=phi, **kw)
+
+    def c3d(nz, ny, nx, geo, **kw):
+        solid = geo.mark_solid(nz, ny, nx)
+        phi = geo.sdf_field(nz, ny, nx) if kw.get("bouzidi") else None
+        return lambda: Solver3D(Nz=nz, Ny=ny, Nx=nx, solid=solid, D=geo.reference_length(), phi=phi, **kw)
+
+    return [
+        c2d(40, 96, Cylinder(radius=6, cx_frac=0.3, cy_frac=0.5), omega=1 / 0.56, u0=0.05,
+            wall_bc="noslip", outlet_bc="zerogradient", bouzidi=True, precision="fp32"),
+        c2d(34, 70, Rectangle(width=10, height=8, cx_frac=0.3, cy_frac=0.5), omega=1 / 0.8, u0=0.05,
+            collision="trt", wall_bc="slip", outlet_bc="convective", les=True, les_cs=0.15, precision="fp32"),
+        c2d(30, 64, Cylinder(radius=4, cx_frac=0.3, cy_frac=0.5), omega=1 / 0.6, u0=0.04,
+            collision="mrt", wall_bc="noslip", sponge_thickness=8, precision="fp64"),
+        c3d(16, 18, 40, Sphere(radius=4, cx_frac=0.3, cy_frac=0.5, cz_frac=0.5), omega=1 / 0.6, u0=0.05,
+            collision="mrt", bouzidi=True, wall_bc="slip", outlet_bc="convective", sponge_thickness=6,
+            precision="fp32"),
+        c3d(12, 14, 30, Sphere(radius=3, cx_frac=0.3, cy_frac=0.5, cz_frac=0.5), omega=1 / 0.7, u0=0.05,
+            collision="bgk", les=True, les_cs=0.1, wall_bc="noslip", precision="fp16s"),
+        c3d(12, 16, 24, Box(width=4, height=4, depth=12, cx_frac=0.3, cy_frac=0.25, cz_frac=0.5),
+            omega=1 / 0.8, u0=0.05, collision="trt", trt_lambda=0.25, wall_bc="noslip", streamwise_bc="periodic",
+            body_force_x=1e-6, thermal=True, alpha_T=0.02, buoyancy=True, g_gravity=1e-4, beta=1.0,
+            T_ref=0.5, precision="bf16s"),
+    ]
+
+
+def _alone(make, steps):
+    s = make()
+    r = s.run(steps, check_every=steps + 1, verbose=False)
+    return s.f, np.array(r["Cd_history"])
+
+
+# The batch kernels run the per-cell code of the single-lattice kernels, but
+# they are separate compilations, so floating-point contraction may differ in
+# the last bit: the batch agrees with the single-lattice API to these
+# fractions of max|f| (and of max|Cd|) per storage format.
+TOL = {"fp64": 1e-12, "fp32": 1e-6, "fp16s": 2e-3, "bf16s": 2e-3}
+
+
+def _close(s, f, f_ref, cd=None, cd_ref=None):
+    tol = TOL[s.precision]
+    np.testing.assert_allclose(f, f_ref, rtol=0, atol=tol * np.abs(f_ref).max())
+    if cd is not None:
+        np.testing.assert_allclose(cd, cd_ref, rtol=0, atol=tol * max(np.abs(cd_ref).max(), 1e-3))
+
+
+@pytest.mark.gpu
+def test_batch_members_match_alone():
+    from aero_b200 import Batch
+    makes = _cases()
+    steps = 31  # odd: the batch ends on the other buffer parity
+    ref = [_alone(m, steps) for m in makes]
+    b = Batch(max_members=8)
+    solvers = [m() for m in makes]
+    for s in solvers:
+        b.add(s)
+    b.step(steps)
+    for s, (f_ref, cd_ref) in zip(solvers, ref):
+        cd = s._coefficients(s._engine.read_forces())["Cd"]
+        b.remove(s)
+        _close(s, s.f, f_ref, cd, cd_ref)
+    b.close()
+
+
+@pytest.mark.gpu
+def test_batch_result_same_alone_and_in_the_mix():
+    """Each case gives bit-identical populations and forces whether it runs
+    alone in a batch or in a batch with every other case: the members of a
+    batch share launches but no data."""
+    from aero_b200 import Batch
+    makes = _cases()
+    steps = 24
+    alone = []
+    for m in makes:
+        b = Batch(max_members=1)
+        s = m()
+        b.add(s)
+        b.step(steps)
+        alone.append((s._engine.read_forces(), s._engine.get_state()[0]))
+        b.remove(s)
+        b.close()
+    b = Batch(max_members=8)
+    mix = [m() for m in makes]
+    for s in mix:
+        b.add(s)
+    b.step(10)
+    b.step(steps - 10)
+    for s, (raw, f) in zip(mix, alone):
+        np.testing.assert_array_equal(s._engine.read_forces(), raw)
+        np.testing.assert_array_equal(s._engine.get_state()[0], f)
+    b.close()
+
+
+@pytest.mark.gpu
+def test_batch_join_and_leave_between_steps():
+    """Continuous batching: members join and leave at different steps and
+    end in the same state as when run alone for the same number of steps."""
+    from aero_b200 import Batch
+    makes = _cases()[:4]
+    b = Batch(max_members=4)
+    s = [m() for m in makes]
+    b.add(s[0])
+    b.step(7)
+    b.add(s[1])
+    b.add(s[2])
+    b.step(10)
+    b.remove(s[0])      # 17 steps
+    b.add(s[3])
+    b.step(5)
+    b.remove(s[2])      # 15 steps
+    b.step(4)           # s[1]: 19, s[3]: 9
+    done = {0: 17, 1: 19, 2: 15, 3: 9}
+    b.remove(s[1])
+    b.remove(s[3])
+    for k, n in done.items():
+        f_ref, _ = _alone(makes[k], n)
+        assert s[k].step_count == n
+        _close(s[k], s[k].f, f_ref)
+    # a solver that left the batch steps on its own again
+    s[0].run(3, check_every=10, verbose=False)
+    f_ref, _ = _alone(makes[0], 20)
+    _close(s[0], s[0].f, f_ref)
+    b.close()
+
+
+@pytest.mark.gpu
+def test_member_cannot_step_alone():
+    from aero_b200 import Batch
+    from aero_b200._lib import AeroError
+    s = _cases()[0]()
+    b = Batch(max_members=2)
+    b.add(s)
+    with pytest.raises(AeroError, match="batch member"):
+        s._engine.step(1)
+    b.remove(s)
+    s._engine.step(1)
+    b.close()
+
+
+@pytest.mark.gpu
+def test_device_convergence_matches_analyze_convergence():
+    from aero_b200 import Batch
+    from aero_b200.diagnostics import analyze_convergence
+    makes = _cases()
+    b = Batch(max_members=8)
+    solvers = [makes[0](), makes[3]()]
+    for s in solvers:
+        b.add(s)
+    W = 60
+    out = b.converge(W, 1e-3)
+    assert np.all(out[:, 3] == 0) and np.all(np.isinf(out[:, 0]))  # too few steps yet
+    b.step(100)
+    out = b.converge(W, 0.05)
+    for s, row in zip(solvers, out):
+        raw = s._engine.read_forces()
+        cd = s._coefficients(raw)["Cd"]
+        assert len(cd) == 100
+        rep = analyze_convergence(list(cd), window=W, tol=0.05)
+        np.testing.assert_allclose(row[0], rep.ratio, rtol=1e-9, atol=1e-15)
+        np.testing.assert_allclose(row[1], rep.mean_abs, rtol=1e-12)
+        np.testing.assert_allclose(row[2], rep.std, rtol=1e-9, atol=1e-15)
+        assert bool(row[3]) == rep.converged
+        assert row[4] == 100
+    b.close()
