@@ -25,7 +25,7 @@ import numpy as np
 from . import _lib
 from ._lib import check
 
-CONVERGE_FIELDS = ("ratio", "mean_abs", "std", "converged", "steps")
+CONVERGE_FIELDS = ("ratio", "mean_abs", "std", "converged", "steps", "status", "mean")
 
 
 class Batch:
@@ -76,8 +76,9 @@ class Batch:
             s.step_count += int(n)
 
     def converge(self, window: int, tol: float) -> np.ndarray:
-        """(members, 5) array: ratio, mean|Cd|, std, converged, steps (join order)."""
-        out = np.zeros((max(len(self.members), 1), 5), dtype=np.float64)
+        """(members, 7) array, join order: ratio, mean|Cd|, std, converged,
+        steps, status word, mean Cd (CONVERGE_FIELDS)."""
+        out = np.zeros((max(len(self.members), 1), len(CONVERGE_FIELDS)), dtype=np.float64)
         with self.torch.cuda.device(self.device):
             check("aero_batch_converge", self.lib.aero_batch_converge(
                 self.h, int(window), float(tol), out.ctypes.data, self._stream()))

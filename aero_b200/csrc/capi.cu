@@ -948,12 +948,16 @@ namespace {
 // of analyze_convergence (diagnostics.py:87-120): over the last `window`
 // steps of Cd = Fx / cd_norm, ratio = std / mean|Cd| (population std);
 // converged when ratio < tol, or when mean|Cd| < 1e-12.  One block per
-// lattice; out receives (ratio, mean|Cd|, std, converged, steps) doubles and
-// converged = 0 while fewer than `window` steps are in the ring.
+// lattice; out receives (ratio, mean|Cd|, std, converged, steps, status,
+// mean Cd) doubles, with ratio = +inf and converged = 0 while fewer than
+// `window` steps are in the ring.  status is the lattice's device status word.
+constexpr int kConvergeValues = AERO_CONVERGE_VALUES;
+
 struct ConvergeItem {
   const double *hist;
   const int64_t *step;
   const int64_t *hist_base;
+  const uint32_t *status;
   double *out;
   double cd_norm;
   int32_t hist_cap;
@@ -973,6 +977,8 @@ __global__ void __launch_bounds__(kFinalizeBlock) k_converge(const ConvergeItem 
       it.out[2] = 0.0;
       it.out[3] = 0.0;
       it.out[4] = (double)steps;
+      it.out[5] = (double)*it.status;
+      it.out[6] = 0.0;
     }
     return;
   }
@@ -1011,6 +1017,8 @@ __global__ void __launch_bounds__(kFinalizeBlock) k_converge(const ConvergeItem 
     it.out[2] = sd;
     it.out[3] = (tiny || ratio < tol) ? 1.0 : 0.0;
     it.out[4] = (double)steps;
+    it.out[5] = (double)*it.status;
+    it.out[6] = mean;
   }
 }
 
@@ -1082,7 +1090,7 @@ uint64_t batch_bytes(int max_members) {
   const uint64_t kClasses = 2 * 4 * 3;
   uint64_t b = 3 * m * (2 * sp + 8);
   b += (kClasses + 2) * (2 * sp + 8);
-  b += m * (8 + sizeof(ConvergeItem) + 5 * 8);
+  b += m * (8 + sizeof(ConvergeItem) + kConvergeValues * 8);
   b += kAlign * (6 * kClasses + 6 + 3 + 1);
   return align_up(b);
 }
@@ -1183,7 +1191,7 @@ int batch_build(AeroBatch *B, cudaStream_t st) {
   const int n = (int)B->members.size();
   B->ctr_ptrs = take(8 * (uint64_t)std::max(n, 1));
   B->conv_items = take(sizeof(ConvergeItem) * std::max(n, 1));
-  B->conv_out = take(5 * 8 * (uint64_t)std::max(n, 1));
+  B->conv_out = take(kConvergeValues * 8 * (uint64_t)std::max(n, 1));
   if (o > B->ws_bytes) return fail(AERO_ERR_CAPACITY, "batch plan needs %llu bytes, workspace has %llu",
                                    (unsigned long long)o, (unsigned long long)B->ws_bytes);
   for (int k = 0; k < n; k++) {
@@ -1194,7 +1202,8 @@ int batch_build(AeroBatch *B, cudaStream_t st) {
     ci.hist = reinterpret_cast<const double *>(L->ws + L->lay.hist);
     ci.step = ctr;
     ci.hist_base = ctr + 1;
-    ci.out = reinterpret_cast<double *>(B->ws + B->conv_out) + 5 * k;
+    ci.status = reinterpret_cast<const uint32_t *>(ctr + 2);
+    ci.out = reinterpret_cast<double *>(B->ws + B->conv_out) + kConvergeValues * k;
     ci.cd_norm = L->cd_norm;
     ci.hist_cap = L->hist_cap;
     std::memcpy(h.data() + B->conv_items + sizeof(ConvergeItem) * k, &ci, sizeof(ci));
@@ -1388,7 +1397,7 @@ int aero_batch_converge(AeroBatch *B, int32_t window, double tol, double *out, v
   k_converge<<<nm, kFinalizeBlock, 0, st>>>(reinterpret_cast<const ConvergeItem *>(B->ws + B->conv_items), nm,
                                             window, tol);
   CUDA_TRY(cudaGetLastError());
-  CUDA_TRY(cudaMemcpyAsync(out, B->ws + B->conv_out, 5 * 8 * (size_t)nm, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaMemcpyAsync(out, B->ws + B->conv_out, kConvergeValues * 8 * (size_t)nm, cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
   return AERO_OK;
 }

@@ -1,0 +1,304 @@
+"""Continuous-batching request loop for wind-tunnel cases on one GPU.
+
+Requests (``Case``) arrive over time.  The server admits each one as soon as
+its device footprint fits under an HBM cap and a batch slot is free, builds
+its solver (geometry, links, initial equilibrium state on the device) and
+adds it to the running ``Batch``; every member then advances with the
+others in ``chunk``-step rounds.  After each round the batch evaluates the
+reference's drag-convergence rule (``analyze_convergence``,
+aero/diagnostics.py:87-120: std / mean|Cd| over a trailing window) for all
+members on the device, and the server retires the members that converged,
+reached their step limit or diverged (the device status word, the test of
+``check_stability``, aero/diagnostics.py:32-71), freeing their memory for
+waiting requests.  Populations and force histories stay on the device for
+the whole life of a case; per round the host reads only the convergence
+table.
+
+``run_plain`` solves the same cases one after another through the plain
+single-solver API with the same stopping rule (checked at the same step
+counts), which is the sequential baseline the serving throughput is
+compared with.
+
+Case construction follows the reference CLI defaults (cli.py:43-170,
+cli3d.py:36-174: velocity inlet, convective outlet, slip walls, LES
+constant 0.16) and derives nu = u0 D / Re, omega = 1 / (3 nu + 1/2)
+(cli.py:191-204).  There is no serving loop in the reference.
+"""
+
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import asdict, dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from .batch import CONVERGE_FIELDS, Batch
+
+_F = {k: i for i, k in enumerate(CONVERGE_FIELDS)}
+STATUS_DIVERGED = 1  # bit 0 of the device status word
+
+
+@dataclass
+class Case:
+    """One wind-tunnel request."""
+    id: int
+    dims: int
+    nx: int
+    ny: int
+    nz: int = 1
+    shape: str = "cylinder"     # cylinder | rectangle (2D), sphere | box (3D)
+    size: float = 8.0           # radius, or half-width, in cells
+    Re: float = 100.0
+    u0: float = 0.05
+    collision: str = "bgk"
+    les: bool = False
+    precision: str = "fp32"
+    arrival: float = 0.0        # seconds after the start of the trace
+    max_steps: int = 50000
+
+
+@dataclass
+class Result:
+    id: int
+    status: str                 # converged | max_steps | diverged | rejected
+    steps: int
+    cd_mean: float
+    ratio: float
+    arrival: float
+    admitted: float
+    done: float
+    cells: int
+    footprint: int
+
+    @property
+    def latency(self) -> float:
+        return self.done - self.arrival
+
+
+def geometry(case: Case):
+    from .geometry import Box, Cylinder, Rectangle, Sphere
+    h = float(case.size)
+    if case.dims == 2:
+        if case.shape == "rectangle":
+            return Rectangle(width=2 * h, height=2 * h, cx_frac=0.25, cy_frac=0.5)
+        return Cylinder(radius=h, cx_frac=0.25, cy_frac=0.5)
+    if case.shape == "box":
+        return Box(width=2 * h, height=2 * h, depth=2 * h, cx_frac=0.25, cy_frac=0.5, cz_frac=0.5)
+    return Sphere(radius=h, cx_frac=0.25, cy_frac=0.5, cz_frac=0.5)
+
+
+def omega_of(case: Case, D: float) -> float:
+    nu = case.u0 * D / case.Re
+    return 1.0 / (3.0 * nu + 0.5)
+
+
+def make_solver(case: Case, device=None, hist_capacity: int = 4096):
+    """The solver of a case, with the reference CLI's boundary conditions."""
+    from .solver import Solver
+    from .solver3d import Solver3D
+    geo = geometry(case)
+    D = geo.reference_length()
+    kw = dict(omega=omega_of(case, D), u0=case.u0, D=D, wall_bc="slip", inlet_bc="velocity",
+              outlet_bc="convective", collision=case.collision, les=case.les, les_cs=0.16,
+              precision=case.precision, device=device, hist_capacity=hist_capacity)
+    if case.dims == 2:
+        solid = geo.mark_solid(case.ny, case.nx)
+        return Solver(Ny=case.ny, Nx=case.nx, solid=solid, **kw)
+    solid = geo.mark_solid(case.nz, case.ny, case.nx)
+    return Solver3D(Nz=case.nz, Ny=case.ny, Nx=case.nx, solid=solid, **kw)
+
+
+def footprint(case: Case, hist_capacity: int = 4096) -> int:
+    """Upper bound of the device bytes a case holds while admitted: the
+    population buffers, flags, LES velocities and outlet state of its
+    workspace, the force ring, plus the FP64 initial state built during set-up."""
+    Q = 9 if case.dims == 2 else 19
+    cells = case.nx * case.ny * case.nz
+    cs = (cells + 63) // 64 * 64
+    sb = {"fp32": 4, "fp64": 8, "fp16s": 2, "bf16s": 2}[case.precision]
+    rb = 8 if case.precision == "fp64" else 4
+    ws = 2 * Q * cs * sb + cs + 32 + 8 * (cs // 32 + 64)
+    ws += (3 * cs * rb if case.les and case.collision != "mrt" else 0)
+    ws += 2 * 20 * case.ny * case.nz * rb + 96 * hist_capacity + (1 << 20)
+    staging = Q * cells * 8 * 2
+    return int(ws + staging)
+
+
+def _cells(case: Case) -> int:
+    return case.nx * case.ny * case.nz
+
+
+class Server:
+    """Continuous batching of wind-tunnel cases on one device."""
+
+    def __init__(self, hbm_cap: float = 150e9, max_members: int = 256, chunk: int = 200,
+                 window: int = 2000, tol: float = 1e-3, device=None, hist_capacity: int = 4096):
+        if window > hist_capacity:
+            raise ValueError("the convergence window must fit the force history ring")
+        self.hbm_cap = float(hbm_cap)
+        self.max_members = int(max_members)
+        self.chunk = int(chunk)
+        self.window = int(window)
+        self.tol = float(tol)
+        self.device = device
+        self.hist_capacity = int(hist_capacity)
+        self.batch = Batch(max_members=max_members, device=device)
+        self.stats: Dict[str, float] = {}
+
+    def run(self, cases: List[Case], clock=time.perf_counter, sleep=time.sleep) -> List[Result]:
+        """Serves the cases (arrival times relative to the call) and returns
+        one Result per case, in completion order."""
+        import torch
+        pending = sorted(cases, key=lambda c: (c.arrival, c.id))
+        queue: List[Case] = []
+        active: List[tuple] = []     # (case, solver, admitted, bytes), join order = batch order
+        results: List[Result] = []
+        used = 0
+        cell_steps = 0
+        t0 = clock()
+        rounds = 0
+        while pending or queue or active:
+            now = clock() - t0
+            while pending and pending[0].arrival <= now:
+                queue.append(pending.pop(0))
+            # admission, first come first served, by device footprint
+            while queue and len(active) < self.max_members:
+                c = queue[0]
+                need = footprint(c, self.hist_capacity)
+                if need > self.hbm_cap:
+                    queue.pop(0)
+                    t = clock() - t0
+                    results.append(Result(c.id, "rejected", 0, math.nan, math.nan, c.arrival, t, t,
+                                          _cells(c), need))
+                    continue
+                if used + need > self.hbm_cap:
+                    break
+                queue.pop(0)
+                s = make_solver(c, self.device, self.hist_capacity)
+                self.batch.add(s)
+                used += need
+                active.append((c, s, clock() - t0, need))
+            if not active:
+                if pending:
+                    sleep(max(0.0, pending[0].arrival - (clock() - t0)))
+                continue
+            self.batch.step(self.chunk)
+            cell_steps += self.chunk * sum(_cells(a[0]) for a in active)
+            table = self.batch.converge(self.window, self.tol)  # synchronises the stream
+            rounds += 1
+            t = clock() - t0
+            keep = []
+            for (c, s, t_adm, need), row in zip(active, table):
+                steps = int(row[_F["steps"]])
+                status = int(row[_F["status"]])
+                if status & STATUS_DIVERGED:
+                    verdict = "diverged"
+                elif row[_F["converged"]] > 0.5:
+                    verdict = "converged"
+                elif steps >= c.max_steps:
+                    verdict = "max_steps"
+                else:
+                    keep.append((c, s, t_adm, need))
+                    continue
+                self.batch.remove(s)
+                used -= need
+                results.append(Result(c.id, verdict, steps, float(row[_F["mean"]]), float(row[_F["ratio"]]),
+                                      c.arrival, t_adm, t, _cells(c), need))
+                del s
+            active = keep
+        torch.cuda.synchronize(self.batch.device)
+        wall = clock() - t0
+        self.stats = {"wall_s": wall, "rounds": rounds, "cell_steps": float(cell_steps),
+                      "mlups": cell_steps / wall / 1e6 if wall > 0 else 0.0}
+        return results
+
+    def close(self):
+        self.batch.close()
+
+
+def run_plain(cases: List[Case], chunk: int = 200, window: int = 2000, tol: float = 1e-3, device=None,
+              hist_capacity: int = 4096, clock=time.perf_counter) -> List[Result]:
+    """Solves the cases one after another through the plain solver API, with
+    the serving rule checked at the same step counts; arrival times are
+    ignored (the queue is full from the start)."""
+    from .diagnostics import analyze_convergence
+    results = []
+    t0 = clock()
+    for c in cases:
+        t_adm = clock() - t0
+        s = make_solver(c, device, hist_capacity)
+        cd: List[float] = []
+        verdict = "max_steps"
+        ratio = math.inf
+        while True:
+            r = s.run(chunk, check_every=chunk + 1, verbose=False)
+            cd = list(r["Cd_history"])  # run() returns the solver's whole history
+            if s.status() & STATUS_DIVERGED:
+                verdict = "diverged"
+                break
+            rep = analyze_convergence(cd, window=window, tol=tol)
+            ratio = rep.ratio
+            if rep.converged:
+                verdict = "converged"
+                break
+            if len(cd) >= c.max_steps:
+                break
+        mean = float(np.mean(cd[-window:])) if len(cd) >= window else 0.0
+        results.append(Result(c.id, verdict, len(cd), mean, float(ratio), 0.0, t_adm, clock() - t0,
+                              _cells(c), footprint(c, hist_capacity)))
+        del s
+    return results
+
+
+def trace(n: int, seed: int = 0, rate: float = 1.0, frac_2d: float = 0.7, nx2=(256, 1024), nx3=(96, 320),
+          size_frac=(0.04, 0.12), re=(50.0, 500.0), collisions=("bgk", "trt", "mrt"), les_above_re: float = 200.0,
+          precision: str = "fp32", max_steps: int = 50000, tau_min: float = 0.51, u0_max: float = 0.1,
+          step2: int = 64, step3: int = 32) -> List[Case]:
+    """A seeded request trace: Poisson arrivals at `rate` per second; 2D
+    (ny = nx/2) or 3D (ny = nz = nx/2) lattices, geometry sized a fraction
+    of ny, Re log-uniform, collision drawn uniformly, Smagorinsky above
+    `les_above_re`, u0 = max(0.05, the smallest value giving tau >= tau_min),
+    capped at u0_max (Re is then lowered to keep tau >= tau_min)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(n):
+        t += float(rng.exponential(1.0 / rate)) if rate > 0 else 0.0
+        dims = 2 if rng.random() < frac_2d else 3
+        lo, hi = (nx2 if dims == 2 else nx3)
+        step = step2 if dims == 2 else step3
+        nx = int(rng.integers(lo // step, hi // step + 1)) * step
+        ny = nx // 2
+        nz = ny if dims == 3 else 1
+        shape = (["cylinder", "rectangle"] if dims == 2 else ["sphere", "box"])[int(rng.integers(0, 2))]
+        size = max(2.0, round(float(rng.uniform(*size_frac)) * ny / 2.0))
+        Re = float(np.exp(rng.uniform(np.log(re[0]), np.log(re[1]))))
+        D = 2.0 * size
+        u0 = max(0.05, (tau_min - 0.5) * Re / (3.0 * D))
+        if u0 > u0_max:
+            u0 = u0_max
+            Re = min(Re, 3.0 * u0 * D / (tau_min - 0.5))
+        coll = collisions[int(rng.integers(0, len(collisions)))]
+        out.append(Case(id=k, dims=dims, nx=nx, ny=ny, nz=nz, shape=shape, size=size, Re=Re, u0=u0,
+                        collision=coll, les=Re > les_above_re, precision=precision, arrival=t,
+                        max_steps=max_steps))
+    return out
+
+
+def summarize(results: List[Result], wall_s: float) -> dict:
+    done = [r for r in results if r.status != "rejected"]
+    lat = np.array([r.latency for r in done]) if done else np.zeros(1)
+    return {
+        "solves": len(done),
+        "solves_per_s": len(done) / wall_s if wall_s > 0 else 0.0,
+        "p50_latency_s": float(np.percentile(lat, 50)),
+        "p99_latency_s": float(np.percentile(lat, 99)),
+        "status": {k: sum(1 for r in results if r.status == k)
+                   for k in ("converged", "max_steps", "diverged", "rejected")},
+    }
+
+
+def case_dict(c: Case) -> dict:
+    return asdict(c)

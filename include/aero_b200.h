@@ -244,10 +244,12 @@ AERO_API int aero_batch_step(AeroBatch *batch, int64_t n_steps, void *stream);
 /* Rolling drag convergence of every member on the device, by the rule of
  * analyze_convergence (diagnostics.py:87-120): over the last `window`
  * steps, ratio = std(Cd) / mean|Cd|, converged when ratio < tol (or mean|Cd|
- * < 1e-12).  out (host) receives 5 doubles per member, in the order the
- * members joined: ratio, mean|Cd|, std, converged (0/1), steps taken; ratio
- * is +inf and converged 0 while fewer than `window` steps are in the ring.
+ * < 1e-12).  out (host) receives AERO_CONVERGE_VALUES doubles per member, in
+ * the order the members joined: ratio, mean|Cd|, std, converged (0/1),
+ * steps taken, the member's status word (aero_status), mean Cd; ratio is
+ * +inf and converged 0 while fewer than `window` steps are in the ring.
  * Synchronous. */
+#define AERO_CONVERGE_VALUES 7
 AERO_API int aero_batch_converge(AeroBatch *batch, int32_t window, double tol, double *out, void *stream);
 /* Releases the batch (members stay valid and leave it). */
 AERO_API int aero_batch_destroy(AeroBatch *batch);

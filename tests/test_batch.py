@@ -23,7 +23,7 @@ def test_batch_create_checks_arguments():
     n = ctypes.c_uint64()
     assert lib.aero_batch_workspace_size(h, ctypes.byref(n)) == 0 and n.value > 0
     assert lib.aero_batch_bind_workspace(h, None, n.value) != 0
-    out = np.zeros(5)
+    out = np.zeros(7)
     assert lib.aero_batch_converge(h, 10, 1e-3, out.ctypes.data, None) != 0  # not bound
     assert lib.aero_batch_step(h, 1, None) != 0  # not bound
     size = ctypes.c_int32(-1)
@@ -201,5 +201,6 @@ def test_device_convergence_matches_analyze_convergence():
         np.testing.assert_allclose(row[1], rep.mean_abs, rtol=1e-12)
         np.testing.assert_allclose(row[2], rep.std, rtol=1e-9, atol=1e-15)
         assert bool(row[3]) == rep.converged
-        assert row[4] == 100
+        assert row[4] == 100 and row[5] == 0
+        np.testing.assert_allclose(row[6], np.mean(cd[-W:]), rtol=1e-12)
     b.close()

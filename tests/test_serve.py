@@ -1,0 +1,157 @@
+"""Continuous-batching server (aero_b200.serve): trace generation and the
+footprint bound on CPU; on the GPU, served results equal sequential plain
+solves with the same stopping rule, each case gives the same result alone
+and in the mix, and requests that arrive while others run are admitted
+before those finish."""
+
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+from aero_b200 import serve
+
+
+def test_trace_is_seeded_and_respects_the_rules():
+    a = serve.trace(200, seed=3, rate=5.0)
+    b = serve.trace(200, seed=3, rate=5.0)
+    assert [serve.case_dict(c) for c in a] == [serve.case_dict(c) for c in b]
+    arr = [c.arrival for c in a]
+    assert all(x < y for x, y in zip(arr, arr[1:]))
+    n2 = sum(c.dims == 2 for c in a)
+    assert 0.55 < n2 / len(a) < 0.85
+    for c in a:
+        assert c.ny == c.nx // 2 and (c.nz == (c.ny if c.dims == 3 else 1))
+        assert (256 <= c.nx <= 1024) if c.dims == 2 else (96 <= c.nx <= 320)
+        D = serve.geometry(c).reference_length()
+        tau = 1.0 / serve.omega_of(c, D)
+        assert tau >= 0.51 - 1e-12 and c.u0 <= 0.1 + 1e-12
+        assert c.les == (c.Re > 200.0)
+        assert c.collision in ("bgk", "trt", "mrt")
+
+
+def test_footprint_bounds_the_workspace():
+    """footprint() is at least the workspace aero_workspace_size reports
+    (computed through the C ABI, no GPU needed)."""
+    from aero_b200 import _lib
+    from aero_b200.links import build_surface_links
+    lib = _lib.load(build_if_missing=False)
+    for c in serve.trace(12, seed=5, rate=0.0, nx2=(64, 192), nx3=(32, 64)):
+        c.les = True
+        geo = serve.geometry(c)
+        shape = (c.ny, c.nx) if c.dims == 2 else (c.nz, c.ny, c.nx)
+        solid = geo.mark_solid(*shape)
+        links, q = build_surface_links(solid, None)
+        P = _lib.AeroParams()
+        P.abi_version, P.dims = _lib.ABI_VERSION, c.dims
+        P.nx, P.ny, P.nz = c.nx, c.ny, c.nz
+        P.storage = _lib.STORE[c.precision]
+        P.collision = _lib.COLLISION["bgk"]
+        P.inlet_bc, P.outlet_bc, P.wall_bc = 1, 1, 1
+        P.streamwise_open, P.les = 1, 1
+        P.omega, P.u0, P.rho0 = 1.0 / 0.6, c.u0, 1.0
+        h = ctypes.c_void_p()
+        assert lib.aero_create(ctypes.byref(P), ctypes.byref(h)) == 0
+        s8 = np.ascontiguousarray(solid, dtype=np.uint8)
+        links = np.ascontiguousarray(links, dtype=np.int32)
+        q = np.ascontiguousarray(q, dtype=np.float32)
+        assert lib.aero_set_geometry(h, s8.ctypes.data, links.ctypes.data if len(links) else None,
+                                     q.ctypes.data if len(q) else None, len(links), None) == 0
+        nb = ctypes.c_uint64()
+        assert lib.aero_workspace_size(h, ctypes.byref(nb)) == 0
+        assert serve.footprint(c) >= nb.value
+        lib.aero_destroy(h)
+
+
+def _small_cases():
+    """Mixed 2D/3D cases at stable relaxation times (tau 0.55; TRT at tau
+    0.86, where the reference's TRT parameters are stable), so that no
+    verdict depends on when a divergence is detected."""
+    cs = [
+        serve.Case(0, 2, 96, 48, shape="cylinder", size=5, Re=30, collision="bgk", arrival=0.0),
+        serve.Case(1, 2, 80, 40, shape="rectangle", size=4, Re=24, collision="mrt", arrival=0.0),
+        serve.Case(2, 3, 48, 24, 24, shape="sphere", size=3, Re=18, collision="mrt", arrival=0.0),
+        serve.Case(3, 2, 64, 32, shape="cylinder", size=4, Re=24, collision="bgk", les=True, arrival=0.0),
+        serve.Case(4, 3, 40, 20, 20, shape="box", size=3, Re=18, collision="bgk", arrival=0.0),
+        serve.Case(5, 2, 128, 64, shape="cylinder", size=6, Re=5, collision="trt", arrival=0.0),
+    ]
+    for c in cs:
+        c.max_steps = 600
+    return cs
+
+
+KW = dict(chunk=50, window=100, tol=2e-3)
+
+
+@pytest.mark.gpu
+def test_served_results_equal_plain_sequential_solves():
+    plain = {r.id: r for r in serve.run_plain(_small_cases(), **KW)}
+    srv = serve.Server(hbm_cap=8e9, max_members=8, **KW)
+    served = {r.id: r for r in srv.run(_small_cases())}
+    srv.close()
+    assert set(plain) == set(served)
+    for k, p in plain.items():
+        s = served[k]
+        assert s.status == p.status and s.steps == p.steps, (k, s, p)
+        if p.status in ("converged", "max_steps") and math.isfinite(p.cd_mean) and p.cd_mean != 0.0:
+            # batch and single-lattice kernels differ only in FP32 rounding
+            assert abs(s.cd_mean - p.cd_mean) <= 1e-5 * abs(p.cd_mean), (k, s.cd_mean, p.cd_mean)
+
+
+@pytest.mark.gpu
+def test_each_result_same_alone_and_in_the_mix():
+    mix = serve.Server(hbm_cap=8e9, max_members=8, **KW)
+    together = {r.id: r for r in mix.run(_small_cases())}
+    mix.close()
+    for c in _small_cases():
+        one = serve.Server(hbm_cap=8e9, max_members=1, **KW)
+        (r,) = one.run([c])
+        one.close()
+        t = together[c.id]
+        assert (r.status, r.steps) == (t.status, t.steps)
+        assert r.cd_mean == t.cd_mean or (math.isnan(r.cd_mean) and math.isnan(t.cd_mean))
+
+
+@pytest.mark.gpu
+def test_late_requests_join_while_others_run():
+    cs = _small_cases()
+    for c in cs:
+        c.max_steps = 2000
+    # half the requests arrive after the first ones are running
+    for c in cs[3:]:
+        c.arrival = 0.3
+    # simulated clock: every reading advances 10 ms, so the late requests
+    # arrive after a few rounds whatever the speed of the GPU
+    t = [0.0]
+
+    def clock():
+        t[0] += 0.01
+        return t[0]
+
+    def sleep(dt):
+        t[0] += dt
+
+    srv = serve.Server(hbm_cap=8e9, max_members=8, chunk=50, window=2000, tol=0.0)
+    res = {r.id: r for r in srv.run(cs, clock=clock, sleep=sleep)}
+    srv.close()
+    first_done = min(res[c.id].done for c in cs[:3])
+    late_admitted = max(res[c.id].admitted for c in cs[3:])
+    assert late_admitted < first_done        # admitted while the first cases were still running
+    assert all(r.status == "max_steps" and r.steps == 2000 for r in res.values())
+
+
+def test_oversized_request_is_rejected_without_gpu_work(monkeypatch):
+    """A request larger than the HBM cap is rejected at admission."""
+    class FakeBatch:
+        def __init__(self, *a, **k):
+            self.device = None
+        def close(self):
+            pass
+    monkeypatch.setattr(serve, "Batch", FakeBatch)
+    import sys, types
+    fake_torch = types.SimpleNamespace(cuda=types.SimpleNamespace(synchronize=lambda d=None: None))
+    monkeypatch.setitem(sys.modules, "torch", fake_torch)
+    srv = serve.Server(hbm_cap=1e6, max_members=4, chunk=10, window=10)
+    (r,) = srv.run([serve.Case(0, 3, 128, 64, 64)])
+    assert r.status == "rejected" and r.steps == 0
