@@ -1131,7 +1131,8 @@ int batch_build(AeroBatch *B, cudaStream_t st) {
     return at;
   };
   auto cell_blocks = [](const AeroLattice *L) {
-    return (int64_t)blocks_for(L->prm.nx, kStepBlock) * L->prm.ny * L->prm.nz;
+    const int64_t rows = (int64_t)L->prm.ny * L->prm.nz;
+    return (int64_t)blocks_for(L->prm.nx, kStepBlock) * ((rows + kBatchRows - 1) / kBatchRows);
   };
   for (ClassPlan &c : B->classes) {
     const uint64_t sp = c.f64 ? sizeof(StepParams<double>) : sizeof(StepParams<float>);

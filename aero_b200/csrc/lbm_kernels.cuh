@@ -1257,18 +1257,39 @@ __global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const StepParams<Re
 // Batched stepping: many lattices of one class (lattice, storage format,
 // collision) advance in one launch.  Member m owns blocks [first[m],
 // first[m + 1]) of the grid, with the same cell mapping as the single-lattice
-// kernel (one block per kStepBlock-cell x segment of a row, or per
+// kernel (one block per kStepBlock-cell x segment of kBatchRows rows, or per
 // finalisation block); each block copies its member's parameters into shared
 // memory, then runs the same per-cell code.  The parameter arrays live in
 // device memory, so a captured launch stays valid while the members advance.
 // --------------------------------------------------------------------------
+// Member owning block b: the last m with first[m] <= b (first[0] = 0).
+// Up to 1024 members the search takes two dependent loads: every lane of
+// the first warp tests one of 32 evenly spaced entries, then one entry of
+// the chosen stretch; larger batches bisect.  The result is broadcast
+// through shared memory, so the caller must reach this with the whole block.
 __device__ __forceinline__ int find_member(const int64_t *__restrict__ first, int n, int64_t b) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(first + mid) <= b) lo = mid; else hi = mid - 1;
+  __shared__ int found;
+  if (n <= 1024) {
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      const int S = (n + 31) >> 5;  // stretch length, <= 32
+      const int c0 = lane * S;
+      const unsigned coarse = __ballot_sync(0xffffffffu, c0 < n && __ldg(first + c0) <= b);
+      const int c = (31 - __clz(coarse)) * S;  // start of the stretch holding b (bit 0 is always set)
+      const int f = c + lane;
+      const unsigned fine = __ballot_sync(0xffffffffu, lane < S && f < n && __ldg(first + f) <= b);
+      if (lane == 0) found = c + (31 - __clz(fine));
+    }
+  } else if (threadIdx.x == 0) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(first + mid) <= b) lo = mid; else hi = mid - 1;
+    }
+    found = lo;
   }
-  return lo;
+  __syncthreads();
+  return found;
 }
 
 template <class Real>
@@ -1281,6 +1302,11 @@ __device__ __forceinline__ void params_to_smem(StepParams<Real> &dst, const Step
   __syncthreads();
 }
 
+// A block of a batched cell kernel covers one kStepBlock-cell x segment of
+// kBatchRows consecutive rows (y, then z) of its member, so the member
+// lookup and the parameter copy are paid once per kBatchRows segments.
+constexpr int kBatchRows = 4;
+
 template <class L, class S, int COLL>
 __global__ void __launch_bounds__(kStepBlock, sizeof(typename StoreOps<S>::Real) == 4 ? kStepMinBlocks : 4)
     k_step_batch(const StepParams<typename StoreOps<S>::Real> *__restrict__ params,
@@ -1291,11 +1317,15 @@ __global__ void __launch_bounds__(kStepBlock, sizeof(typename StoreOps<S>::Real)
   params_to_smem(sp, params + m);
   const int64_t b = (int64_t)blockIdx.x - __ldg(first + m);
   const int nxb = (sp.nx + kStepBlock - 1) / kStepBlock;
-  const int64_t row = b / nxb;
-  const int x = (int)(b - row * nxb) * kStepBlock + threadIdx.x;
-  const int y = (int)(row % sp.ny), z = (int)(row / sp.ny);
+  const int64_t rg = b / nxb;
+  const int x = (int)(b - rg * nxb) * kStepBlock + threadIdx.x;
   if (x >= sp.nx) return;
-  step_cell<L, S, COLL>(sp, x, y, z, *sp.step, GlobalGather<L, S, Real>{sp, y, z});
+  const int64_t nrows = (int64_t)sp.ny * sp.nz;
+  const int64_t step_now = *sp.step;
+  for (int64_t row = rg * kBatchRows; row < nrows && row < (rg + 1) * kBatchRows; ++row) {
+    const int y = (int)(row % sp.ny), z = (int)(row / sp.ny);
+    step_cell<L, S, COLL>(sp, x, y, z, step_now, GlobalGather<L, S, Real>{sp, y, z});
+  }
 }
 
 template <class L, class S>
@@ -1307,10 +1337,12 @@ __global__ void __launch_bounds__(kStepBlock) k_moments_batch(const StepParams<t
   params_to_smem(sp, params + m);
   const int64_t b = (int64_t)blockIdx.x - __ldg(first + m);
   const int nxb = (sp.nx + kStepBlock - 1) / kStepBlock;
-  const int64_t row = b / nxb;
-  const int x = (int)(b - row * nxb) * kStepBlock + threadIdx.x;
+  const int64_t rg = b / nxb;
+  const int x = (int)(b - rg * nxb) * kStepBlock + threadIdx.x;
   if (x >= sp.nx) return;
-  moments_cell<L, S, false>(sp, x, (int)(row % sp.ny), (int)(row / sp.ny));
+  const int64_t nrows = (int64_t)sp.ny * sp.nz;
+  for (int64_t row = rg * kBatchRows; row < nrows && row < (rg + 1) * kBatchRows; ++row)
+    moments_cell<L, S, false>(sp, x, (int)(row % sp.ny), (int)(row / sp.ny));
 }
 
 template <class Real>

@@ -17,35 +17,51 @@ import numpy as np
 from .lattice import E, E3
 
 
-def _shift_clipped(a: np.ndarray, axis: int, step: int) -> np.ndarray:
-    """b[..., k, ...] = a[..., clip(k + step), ...] along one axis (step in -1, 0, 1)."""
-    if step == 0:
-        return a
-    n = a.shape[axis]
-    if step > 0:
-        idx = np.concatenate([np.arange(1, n), [n - 1]])
-    else:
-        idx = np.concatenate([[0], np.arange(0, n - 1)])
-    return np.take(a, idx, axis=axis)
-
-
 def build_surface_links(solid: np.ndarray, phi: Optional[np.ndarray] = None
                         ) -> Tuple[np.ndarray, np.ndarray]:
+    """Links are only possible in the solid's bounding box grown by one cell,
+    so the search runs on that box: padded by one more cell on every side,
+    with the edge value repeated where the box meets the grid edge (the
+    reference's clipped neighbour) and fluid elsewhere (no solid lies outside
+    the box).  Within one direction the C order of the box's cells is the C
+    order of the grid's, so the list is the reference's, entry for entry."""
     solid = np.asarray(solid, dtype=bool)
     dims = solid.ndim
     e = E if dims == 2 else E3
-    fluid = ~solid
+    empty = (np.empty((0, dims + 1), dtype=np.int32), np.empty(0, dtype=np.float32))
+    idx = np.nonzero(solid)
+    if idx[0].size == 0:
+        return empty
+    lo = [max(int(a.min()) - 1, 0) for a in idx]
+    hi = [min(int(a.max()) + 2, n) for a, n in zip(idx, solid.shape)]
+    box = solid[tuple(slice(l, h) for l, h in zip(lo, hi))]
+    # pad by one: repeat the edge at the grid boundary, fluid inside the grid
+    pad = np.pad(box, 1, mode="constant", constant_values=False)
+    for ax in range(dims):
+        n = solid.shape[ax]
+        if lo[ax] == 0:
+            src = [slice(None)] * dims
+            dst = [slice(None)] * dims
+            src[ax], dst[ax] = slice(1, 2), slice(0, 1)
+            pad[tuple(dst)] = pad[tuple(src)]
+        if hi[ax] == n:
+            src = [slice(None)] * dims
+            dst = [slice(None)] * dims
+            src[ax], dst[ax] = slice(-2, -1), slice(-1, None)
+            pad[tuple(dst)] = pad[tuple(src)]
+    fluid = ~box
+    shape = box.shape
     parts = []
     for i in range(1, len(e)):
-        nb = solid
         # array axes are ([z,] y, x); e is (ex, ey[, ez])
-        for comp in range(dims):
-            nb = _shift_clipped(nb, dims - 1 - comp, int(e[i, comp]))
-        idx = np.nonzero(fluid & nb)
-        if idx[0].size:
-            parts.append(np.stack([np.full(idx[0].size, i, dtype=np.int64), *idx], axis=1))
+        sl = tuple(slice(1 + int(e[i, dims - 1 - ax]), 1 + int(e[i, dims - 1 - ax]) + shape[ax])
+                   for ax in range(dims))
+        hit = np.nonzero(fluid & pad[sl])
+        if hit[0].size:
+            parts.append(np.stack([np.full(hit[0].size, i, dtype=np.int64)] +
+                                  [h + l for h, l in zip(hit, lo)], axis=1))
     if not parts:
-        return np.empty((0, dims + 1), dtype=np.int32), np.empty(0, dtype=np.float32)
+        return empty
     links = np.concatenate(parts).astype(np.int32)
     if phi is not None:
         cells = tuple(links[:, 1 + a] for a in range(dims))

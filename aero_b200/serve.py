@@ -149,22 +149,36 @@ class Server:
 
     def run(self, cases: List[Case], clock=time.perf_counter, sleep=time.sleep) -> List[Result]:
         """Serves the cases (arrival times relative to the call) and returns
-        one Result per case, in completion order."""
+        one Result per case, in completion order.
+
+        One round: launch the next chunk of steps for the members (the call
+        returns at once), build the solvers of the requests admitted now on
+        a side stream while that chunk runs, evaluate convergence (this
+        waits for the chunk), retire finished members, then let the new
+        solvers join."""
         import torch
+        side = torch.cuda.Stream(self.batch.device)
         pending = sorted(cases, key=lambda c: (c.arrival, c.id))
         queue: List[Case] = []
         active: List[tuple] = []     # (case, solver, admitted, bytes), join order = batch order
         results: List[Result] = []
         used = 0
         cell_steps = 0
+        setup_s = 0.0
+        wait_s = 0.0
         t0 = clock()
         rounds = 0
         while pending or queue or active:
+            stepped = bool(active)
+            if stepped:
+                self.batch.step(self.chunk)
+                cell_steps += self.chunk * sum(_cells(a[0]) for a in active)
             now = clock() - t0
             while pending and pending[0].arrival <= now:
                 queue.append(pending.pop(0))
             # admission, first come first served, by device footprint
-            while queue and len(active) < self.max_members:
+            joining = []
+            while queue and len(active) + len(joining) < self.max_members:
                 c = queue[0]
                 need = footprint(c, self.hist_capacity)
                 if need > self.hbm_cap:
@@ -176,42 +190,47 @@ class Server:
                 if used + need > self.hbm_cap:
                     break
                 queue.pop(0)
-                s = make_solver(c, self.device, self.hist_capacity)
-                self.batch.add(s)
+                ts = clock()
+                with torch.cuda.stream(side):
+                    s = make_solver(c, self.device, self.hist_capacity)
+                setup_s += clock() - ts
                 used += need
-                active.append((c, s, clock() - t0, need))
-            if not active:
-                if pending:
-                    sleep(max(0.0, pending[0].arrival - (clock() - t0)))
-                continue
-            self.batch.step(self.chunk)
-            cell_steps += self.chunk * sum(_cells(a[0]) for a in active)
-            table = self.batch.converge(self.window, self.tol)  # synchronises the stream
-            rounds += 1
-            t = clock() - t0
-            keep = []
-            for (c, s, t_adm, need), row in zip(active, table):
-                steps = int(row[_F["steps"]])
-                status = int(row[_F["status"]])
-                if status & STATUS_DIVERGED:
-                    verdict = "diverged"
-                elif row[_F["converged"]] > 0.5:
-                    verdict = "converged"
-                elif steps >= c.max_steps:
-                    verdict = "max_steps"
-                else:
-                    keep.append((c, s, t_adm, need))
-                    continue
-                self.batch.remove(s)
-                used -= need
-                results.append(Result(c.id, verdict, steps, float(row[_F["mean"]]), float(row[_F["ratio"]]),
-                                      c.arrival, t_adm, t, _cells(c), need))
-                del s
-            active = keep
+                joining.append((c, s, clock() - t0, need))
+            if stepped:
+                tw = clock()
+                table = self.batch.converge(self.window, self.tol)  # waits for the chunk
+                wait_s += clock() - tw
+                rounds += 1
+                t = clock() - t0
+                keep = []
+                for (c, s, t_adm, need), row in zip(active, table):
+                    steps = int(row[_F["steps"]])
+                    status = int(row[_F["status"]])
+                    if status & STATUS_DIVERGED:
+                        verdict = "diverged"
+                    elif row[_F["converged"]] > 0.5:
+                        verdict = "converged"
+                    elif steps >= c.max_steps:
+                        verdict = "max_steps"
+                    else:
+                        keep.append((c, s, t_adm, need))
+                        continue
+                    self.batch.remove(s)
+                    used -= need
+                    results.append(Result(c.id, verdict, steps, float(row[_F["mean"]]), float(row[_F["ratio"]]),
+                                          c.arrival, t_adm, t, _cells(c), need))
+                    del s
+                active = keep
+            for j in joining:
+                self.batch.add(j[1])
+                active.append(j)
+            if not active and not joining and pending and not queue:
+                sleep(max(0.0, pending[0].arrival - (clock() - t0)))
         torch.cuda.synchronize(self.batch.device)
         wall = clock() - t0
         self.stats = {"wall_s": wall, "rounds": rounds, "cell_steps": float(cell_steps),
-                      "mlups": cell_steps / wall / 1e6 if wall > 0 else 0.0}
+                      "mlups": cell_steps / wall / 1e6 if wall > 0 else 0.0,
+                      "setup_s": setup_s, "gpu_wait_s": wait_s}
         return results
 
     def close(self):
@@ -219,16 +238,19 @@ class Server:
 
 
 def run_plain(cases: List[Case], chunk: int = 200, window: int = 2000, tol: float = 1e-3, device=None,
-              hist_capacity: int = 4096, clock=time.perf_counter) -> List[Result]:
+              hist_capacity: int = 4096, clock=time.perf_counter, stats: Optional[dict] = None) -> List[Result]:
     """Solves the cases one after another through the plain solver API, with
     the serving rule checked at the same step counts; arrival times are
-    ignored (the queue is full from the start)."""
+    ignored (the queue is full from the start).  `stats`, if given, receives
+    the time spent building solvers."""
     from .diagnostics import analyze_convergence
     results = []
     t0 = clock()
+    setup_s = 0.0
     for c in cases:
         t_adm = clock() - t0
         s = make_solver(c, device, hist_capacity)
+        setup_s += clock() - t0 - t_adm
         cd: List[float] = []
         verdict = "max_steps"
         ratio = math.inf
@@ -249,6 +271,9 @@ def run_plain(cases: List[Case], chunk: int = 200, window: int = 2000, tol: floa
         results.append(Result(c.id, verdict, len(cd), mean, float(ratio), 0.0, t_adm, clock() - t0,
                               _cells(c), footprint(c, hist_capacity)))
         del s
+    if stats is not None:
+        stats["setup_s"] = setup_s
+        stats["wall_s"] = clock() - t0
     return results
 
 

@@ -235,13 +235,186 @@ def run_reference(args, w):
     return 0
 
 
+# ----------------------------------------------------------------------------
+# Batched workloads: a sweep of many cases in one batch, and a served trace
+# ----------------------------------------------------------------------------
+def sweep_cases(seed=96, precision="fp32"):
+    """The 96-case sweep: 64 D2Q9 cases (nx 256..1024 step 64, ny = nx/2,
+    cylinder or rectangle, radius / half-width 8..32, Re 40..200) and 32
+    D3Q19 spheres (nx 96..256 step 32, ny = nz = nx/2, radius 6..16, Re
+    50..300), TRT, u0 = max(0.05, the value giving tau >= 0.51), seeded."""
+    import numpy as np
+    from aero_b200.serve import Case
+    rng = np.random.default_rng(seed)
+    cases = []
+    for k in range(96):
+        if k < 64:
+            dims, nx = 2, int(rng.integers(4, 17)) * 64
+            shape = "cylinder" if rng.random() < 0.5 else "rectangle"
+            size, Re = float(rng.integers(8, 33)), float(rng.uniform(40, 200))
+        else:
+            dims, nx = 3, int(rng.integers(3, 9)) * 32
+            shape, size, Re = "sphere", float(rng.integers(6, 17)), float(rng.uniform(50, 300))
+        ny = nx // 2
+        size = min(size, ny / 4)
+        u0 = min(max(0.05, 0.01 * Re / (3.0 * 2.0 * size)), 0.1)
+        cases.append(Case(id=k, dims=dims, nx=nx, ny=ny, nz=ny if dims == 3 else 1, shape=shape, size=size,
+                          Re=Re, u0=u0, collision="trt", precision=precision))
+    return cases
+
+
+def _bench_line(metric, value, unit, args, ms_per_step, dtype, config, **extra):
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": config}
+    line.update(extra)
+    return line
+
+
+def run_batch96(args):
+    """All 96 sweep cases advance together in one batch for --steps steps
+    (timed with CUDA events, state resident); then each case alone through
+    the plain API for a bounded sample of steps, whose per-case rate gives
+    the time the same sweep takes as sequential plain solves."""
+    import torch
+    from aero_b200 import Batch
+    from aero_b200.serve import make_solver
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    cases = sweep_cases(precision=args.precision)
+    t0 = time.perf_counter()
+    solvers = [make_solver(c, dev) for c in cases]
+    setup_s = time.perf_counter() - t0
+    cells = [c.nx * c.ny * c.nz for c in cases]
+    b = Batch(max_members=len(solvers), device=dev)
+    for s in solvers:
+        b.add(s)
+    b.step(max(args.warmup, 3))
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clk:
+        e0.record(stream)
+        b.step(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    conv = b.converge(min(args.steps, 1000), 1e-3)
+    diverged = int(sum(1 for r in conv if int(r[5]) & 1))
+    for s in list(b.members):
+        b.remove(s)
+    b.close()
+    # sequential plain solves: each case alone, its rate measured on a bounded sample
+    sample = min(200, args.steps)
+    seq_s = 0.0
+    per_case = []
+    for s, n in zip(solvers, cells):
+        s.run(10, check_every=11, verbose=False)
+        torch.cuda.synchronize(dev)
+        t1 = time.perf_counter()
+        s.run(sample, check_every=sample + 1, verbose=False)
+        torch.cuda.synchronize(dev)
+        dt = (time.perf_counter() - t1) / sample
+        per_case.append(n / dt / 1e6)
+        seq_s += dt * args.steps
+    total = sum(cells)
+    mlups = total * args.steps / (ms / 1e3) / 1e6
+    batch_s = ms / 1e3
+    line = _bench_line(
+        "batched sweep MLUPS", mlups, "MLUPS", args, ms / args.steps,
+        {"fp32": "f32", "fp64": "f64", "fp16s": "f16 storage / f32 compute",
+         "bf16s": "bf16 storage / f32 compute"}[args.precision],
+        {"workload": "batch96", "cases": len(cases), "cells_per_step": total, "precision": args.precision,
+         "desc": "64 D2Q9 (nx 256..1024) + 32 D3Q19 spheres (nx 96..256), TRT, one batch"},
+        gpu_launches=None,
+        batch={"solves_per_s": len(cases) / batch_s, "seconds": batch_s, "setup_s": setup_s,
+               "diverged_members": diverged},
+        sequential_plain={"solves_per_s": len(cases) / seq_s, "seconds_estimated": seq_s,
+                          "sample_steps_per_case": sample,
+                          "median_case_mlups": float(sorted(per_case)[len(per_case) // 2])},
+        speedup_vs_sequential=seq_s / batch_s,
+        clocks=clk.summary())
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serve(args):
+    """A served trace: seeded requests with Poisson arrivals at 80% of the
+    capacity measured on the same trace with every request queued at t = 0;
+    requests run until the drag converges (window, tolerance) or their step
+    limit; then the same requests as sequential plain solves."""
+    import numpy as np
+    import torch
+    from aero_b200 import serve
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    kw = dict(chunk=args.serve_chunk, window=args.serve_window, tol=args.serve_tol)
+    mk = dict(n=args.serve_requests, seed=5, nx2=(256, 512), nx3=(96, 160), max_steps=args.steps,
+              precision=args.precision, tau_min=args.serve_tau_min)
+    # capacity: the whole trace queued at once
+    cal = serve.trace(rate=0.0, **mk)
+    srv = serve.Server(hbm_cap=args.serve_hbm_gb * 1e9, max_members=256, device=dev, **kw)
+    res_cal = srv.run(cal)
+    cap = len([r for r in res_cal if r.status != "rejected"]) / srv.stats["wall_s"]
+    srv.close()
+    # the served trace at 80% of capacity
+    cases = serve.trace(rate=0.8 * cap, **mk)
+    srv = serve.Server(hbm_cap=args.serve_hbm_gb * 1e9, max_members=256, device=dev, **kw)
+    with ClockSampler(dev.index) as clk:
+        res = srv.run(cases)
+    stats = dict(srv.stats)
+    srv.close()
+    span = max(r.done for r in res)
+    summ = serve.summarize(res, span)
+    # sequential plain solves of the same requests (plain FP32 storage)
+    plain_cases = serve.trace(rate=0.0, **dict(mk, precision="fp32"))
+    t0 = time.perf_counter()
+    pstats = {}
+    plain = serve.run_plain(plain_cases, device=dev, stats=pstats, **kw)
+    torch.cuda.synchronize(dev)
+    plain_s = time.perf_counter() - t0
+    pmap = {r.id: r for r in plain}
+
+    def rel_dcd(kind):
+        return [abs(r.cd_mean - pmap[r.id].cd_mean) / abs(pmap[r.id].cd_mean) for r in res
+                if r.status == kind and pmap[r.id].status == kind
+                and np.isfinite(pmap[r.id].cd_mean) and pmap[r.id].cd_mean != 0.0]
+    dcd_conv, dcd_max = rel_dcd("converged"), rel_dcd("max_steps")
+    same_verdict = sum(1 for r in res if pmap[r.id].status == r.status)
+    line = _bench_line(
+        "served solves/s", summ["solves_per_s"], "solves/s", args, None,
+        {"fp32": "f32", "fp64": "f64", "fp16s": "f16 storage / f32 compute",
+         "bf16s": "bf16 storage / f32 compute"}[args.precision],
+        {"workload": "serve", "requests": len(cases), "arrivals": "Poisson at 0.8 x measured capacity",
+         "capacity_solves_per_s": cap, "chunk": args.serve_chunk, "window": args.serve_window,
+         "tol": args.serve_tol, "max_steps": args.steps, "hbm_cap_gb": args.serve_hbm_gb,
+         "tau_min": args.serve_tau_min,
+         "desc": "70% D2Q9 (nx 256..512) / 30% D3Q19 (nx 96..160), cylinder/rectangle/sphere/box, "
+                 "Re log-uniform 50..500, BGK/TRT/MRT, Smagorinsky above Re 200"},
+        latency={"p50_s": summ["p50_latency_s"], "p99_s": summ["p99_latency_s"]},
+        status=summ["status"], aggregate_mlups=stats["cell_steps"] / span / 1e6,
+        served_time={"setup_s": stats["setup_s"], "gpu_wait_s": stats["gpu_wait_s"], "rounds": stats["rounds"]},
+        sequential_plain={"solves_per_s": len(plain) / plain_s, "seconds": plain_s, "setup_s": pstats["setup_s"],
+                          "status": {k: sum(1 for r in plain if r.status == k)
+                                     for k in ("converged", "max_steps", "diverged")}},
+        speedup_vs_sequential=summ["solves_per_s"] / (len(plain) / plain_s),
+        cd_vs_plain={"same_verdict": same_verdict,
+                     "converged_compared": len(dcd_conv),
+                     "converged_max_rel_diff": max(dcd_conv) if dcd_conv else None,
+                     "max_steps_compared": len(dcd_max),
+                     "max_steps_max_rel_diff": max(dcd_max) if dcd_max else None},
+        clocks=clk.summary())
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="sphere512", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="sphere512", choices=sorted(WORKLOADS) + ["batch96", "serve"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16s", "bf16s", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -250,7 +423,18 @@ def main():
     ap.add_argument("--kernel", default="rowgather", choices=["rowgather", "tiled"],
                     help="step kernel: per-cell global gather (default) or rows staged in shared "
                          "memory by bulk async copies")
+    ap.add_argument("--serve-requests", type=int, default=64)
+    ap.add_argument("--serve-chunk", type=int, default=250)
+    ap.add_argument("--serve-window", type=int, default=1000)
+    ap.add_argument("--serve-tol", type=float, default=1e-3)
+    ap.add_argument("--serve-hbm-gb", type=float, default=150.0)
+    ap.add_argument("--serve-tau-min", type=float, default=0.51,
+                    help="smallest relaxation time of a request (u0 raised, then Re lowered, to reach it)")
     args = ap.parse_args()
+    if args.workload == "batch96":
+        return run_batch96(args)
+    if args.workload == "serve":
+        return run_serve(args)
     if args.kernel == "tiled":
         os.environ["AERO_B200_TILES"] = "1"
     else:

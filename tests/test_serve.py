@@ -150,7 +150,8 @@ def test_oversized_request_is_rejected_without_gpu_work(monkeypatch):
             pass
     monkeypatch.setattr(serve, "Batch", FakeBatch)
     import sys, types
-    fake_torch = types.SimpleNamespace(cuda=types.SimpleNamespace(synchronize=lambda d=None: None))
+    fake_torch = types.SimpleNamespace(cuda=types.SimpleNamespace(synchronize=lambda d=None: None,
+                                                                  Stream=lambda d=None: None))
     monkeypatch.setitem(sys.modules, "torch", fake_torch)
     srv = serve.Server(hbm_cap=1e6, max_members=4, chunk=10, window=10)
     (r,) = srv.run([serve.Case(0, 3, 128, 64, 64)])
