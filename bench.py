@@ -281,7 +281,7 @@ def run_batch96(args):
     from aero_b200.serve import make_solver
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    cases = sweep_cases(precision=args.precision)
+    cases = sweep_cases(precision=args.precision)[::max(args.batch_every, 1)]
     t0 = time.perf_counter()
     solvers = [make_solver(c, dev) for c in cases]
     setup_s = time.perf_counter() - t0
@@ -324,7 +324,8 @@ def run_batch96(args):
         "batched sweep MLUPS", mlups, "MLUPS", args, ms / args.steps,
         {"fp32": "f32", "fp64": "f64", "fp16s": "f16 storage / f32 compute",
          "bf16s": "bf16 storage / f32 compute"}[args.precision],
-        {"workload": "batch96", "cases": len(cases), "cells_per_step": total, "precision": args.precision,
+        {"workload": "batch96", "cases": len(cases), "every": args.batch_every, "cells_per_step": total,
+         "precision": args.precision,
          "desc": "64 D2Q9 (nx 256..1024) + 32 D3Q19 spheres (nx 96..256), TRT, one batch"},
         gpu_launches=None,
         batch={"solves_per_s": len(cases) / batch_s, "seconds": batch_s, "setup_s": setup_s,
@@ -423,6 +424,8 @@ def main():
     ap.add_argument("--kernel", default="rowgather", choices=["rowgather", "tiled"],
                     help="step kernel: per-cell global gather (default) or rows staged in shared "
                          "memory by bulk async copies")
+    ap.add_argument("--batch-every", type=int, default=1,
+                    help="batch96: keep every k-th case (a smaller batch for profiling captures)")
     ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--serve-chunk", type=int, default=250)
     ap.add_argument("--serve-window", type=int, default=1000)
