@@ -53,8 +53,6 @@ class LatticeSolverBase:
             raise ValueError("scalar_lattice must be 'full' or 'reduced'.")
         if ibm_enabled:
             raise NotImplementedError("ibm_enabled: immersed-boundary forcing is not part of the b200 engine")
-        if synthetic_inflow:
-            raise NotImplementedError("synthetic_inflow is not part of the b200 engine yet")
         self.backend = "b200"
         self.solid = np.ascontiguousarray(solid, dtype=np.bool_)
         if self.solid.shape != tuple(shape):
@@ -84,8 +82,9 @@ class LatticeSolverBase:
         self.van_driest_A = float(van_driest_A)
         self.wall_velocity_top = float(wall_velocity_top)
         self.wall_velocity_bottom = float(wall_velocity_bottom)
-        self.synthetic_inflow = False
+        self.synthetic_inflow = bool(synthetic_inflow)
         self.synthetic_inflow_intensity = float(synthetic_inflow_intensity)
+        self.synthetic_inflow_seed = int(synthetic_inflow_seed)
         self.thermal = bool(thermal)
         self.T_hot = float(T_hot)
         self.T_cold = float(T_cold)
@@ -146,6 +145,17 @@ class LatticeSolverBase:
         P.alpha_T, P.T_hot, P.T_cold = self.alpha_T, self.T_hot, self.T_cold
         P.g_gravity, P.beta, P.T_ref = self.g_gravity, self.beta, self.T_ref
         P.center[:] = self._ref_center
+        # synthetic inflow only drives an open velocity inlet (solver.py:385-392,
+        # solver3d.py:432-445); the fields come from the reference's random stream
+        self._inflow = None
+        if self.synthetic_inflow and inlet_bc == "velocity" and (self.dims == 2 or streamwise_bc == "open"):
+            from .inflow import SyntheticInflow
+            nz_ = shape[0] if self.dims == 3 else 1
+            self._inflow = SyntheticInflow(self.dims, shape[-2], nz_, self.u0, self.synthetic_inflow_intensity,
+                                           self.synthetic_inflow_seed)
+            P.inflow_field = 1
+            P.inflow_ring = 64
+        P.recycling = 1 if (self.dims == 3 and streamwise_bc == "recycling") else 0
         self._params = P
         self._engine = Engine(P, self.solid, self.surface_links, self.q_vals,
                               phi if (self.van_driest and phi is not None) else None, device)
@@ -269,8 +279,11 @@ class LatticeSolverBase:
         rows = []
         left = int(n)
         cap = self._engine.hist_capacity
+        ring = self._params.inflow_ring if self._inflow is not None else cap
         while left > 0:
-            k = min(left, cap)
+            k = min(left, cap, ring)
+            if self._inflow is not None:
+                self._engine.set_inflow(self._inflow.fields(k), self.step_count + int(n) - left)
             self._engine.step(k)
             rows.append(self._engine.read_forces(k))
             left -= k

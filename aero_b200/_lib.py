@@ -12,7 +12,7 @@ import pathlib
 
 from . import _build
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 FORCE_VALUES = 12
 
 STORE = {"fp32": 0, "fp64": 1, "fp16s": 2, "bf16s": 3}
@@ -40,7 +40,8 @@ class AeroParams(ctypes.Structure):
             "wall_velocity_bottom")] + [
         ("body_force", _D * 3)] + [
         (n, _D) for n in ("alpha_T", "T_hot", "T_cold", "g_gravity", "beta", "T_ref")] + [
-        ("center", _D * 3)]
+        ("center", _D * 3)] + [
+        (n, _I32) for n in ("recycling", "inflow_field", "inflow_ring")]
 
 
 SIGNATURES = {
@@ -61,6 +62,7 @@ SIGNATURES = {
     "aero_status": ([_VP, ctypes.POINTER(ctypes.c_uint32), _VP], ctypes.c_int),
     "aero_step_count": ([_VP, ctypes.POINTER(_I64)], ctypes.c_int),
     "aero_step_plan": ([_VP, ctypes.POINTER(_I32), ctypes.POINTER(_I32), ctypes.POINTER(_I32)], ctypes.c_int),
+    "aero_set_inflow": ([_VP, _VP, _I64, _I64, _VP], ctypes.c_int),
     "aero_first_bad_step": ([_VP, ctypes.POINTER(_I64), _VP], ctypes.c_int),
     "aero_destroy": ([_VP], ctypes.c_int),
     "aero_mrt_operator": ([_I32, _D, _VP, _VP], ctypes.c_int),

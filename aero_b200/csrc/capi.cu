@@ -47,7 +47,7 @@ uint64_t align_up(uint64_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
 struct Layout {
   uint64_t P[2], flags, lbits, loff, lc_mask, lc_q, lc_cell, lc_contrib, fin_partial, prof_off, force_const, prof_const,
-      prev[2], g[2], U, cs_cell, hist, prof_out, counters, total;
+      prev[2], g[2], U, cs_cell, inflow, recycle, hist, prof_out, counters, total;
 };
 
 struct WTab {
@@ -129,6 +129,9 @@ struct AeroLattice {
   cudaGraphExec_t pair_exec[2] = {nullptr, nullptr};
   bool use_graphs = true;
   int device = -1;  // device of the bound workspace
+  int inflow_ring = 0;            // steps of inflow fields the device holds
+  int64_t inflow_upto = 0;        // inflow fields are on the device for steps < inflow_upto
+  int recycle_blocks = 0;
   AeroBatch *batch = nullptr;  // batch this lattice is a member of (stepped only by it)
   double cd_norm = 1.0;        // drag normalisation given when it joined the batch
   // row-tiled step plan (k_step_tiled), fixed at bind time
@@ -198,6 +201,12 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   p.U = reinterpret_cast<const Real *>(ws + L->lay.U);
   p.Uw = reinterpret_cast<Real *>(ws + L->lay.U);
   p.cs_cell = reinterpret_cast<const Real *>(ws + L->lay.cs_cell);
+  p.inflow = reinterpret_cast<const Real *>(ws + L->lay.inflow);
+  p.inflow_ring = std::max(L->inflow_ring, 1);
+  p.recycle_partial = reinterpret_cast<double *>(ws + L->lay.recycle);
+  p.recycle_mean = reinterpret_cast<double *>(ws + L->lay.recycle) + L->recycle_blocks;
+  p.recycle_ticket = reinterpret_cast<uint32_t *>(p.recycle_mean + 1);
+  p.recycle_blocks = L->recycle_blocks;
   p.lc_contrib = reinterpret_cast<double *>(ws + L->lay.lc_contrib);
   p.fin_partial = reinterpret_cast<double *>(ws + L->lay.fin_partial);
   {
@@ -297,6 +306,7 @@ int launch_step(AeroLattice *L, int cur, cudaStream_t st, bool timed = false) {
     e = &L->ev[3 * (size_t)L->timed_steps];
     CUDA_TRY(cudaEventRecord(e[0], st));
   }
+  if (L->feat & FEAT_RECYCLE) CUDA_TRY(ops->recycle_mean(p, st));
   if (les_active(L)) CUDA_TRY(ops->moments(p, false, grid, st));
   if (L->tiled)
     CUDA_TRY(ops->step_tiled(p, L->tile_blocks, st));
@@ -385,6 +395,7 @@ int do_set_state(AeroLattice *L, const double *f, const double *prev, const doub
   L->old_is_state = true;
   L->step_count = steps;
   L->read_upto = steps;
+  L->inflow_upto = steps;  // inflow fields are uploaded again from the new step count
   L->state_set = true;
   return AERO_OK;
 }
@@ -466,6 +477,10 @@ int check_params(const AeroParams *a) {
   if (a->dims == 3 && (a->inlet_bc == AERO_INLET_PRESSURE || a->outlet_bc == AERO_OUTLET_PRESSURE))
     return fail(AERO_ERR_UNSUPPORTED, "pressure inlet/outlet exist only in 2D");
   if (a->sponge_thickness < 0) return fail(AERO_ERR_INVALID, "sponge_thickness < 0");
+  if (a->recycling && (a->dims != 3 || a->streamwise_open))
+    return fail(AERO_ERR_INVALID, "recycling is a 3D streamwise mode (streamwise_open must be 0)");
+  if (a->inflow_field && a->recycling) return fail(AERO_ERR_INVALID, "inflow_field needs an open inlet");
+  if (a->inflow_ring < 0 || a->inflow_ring > 65536) return fail(AERO_ERR_INVALID, "inflow_ring must be in 0..65536");
   if (a->hist_capacity < 0) return fail(AERO_ERR_INVALID, "hist_capacity < 0");
   return AERO_OK;
 }
@@ -515,6 +530,14 @@ int aero_create(const AeroParams *params, AeroLattice **out) {
   if (a.les && a.collision != AERO_MRT) {
     f |= FEAT_LES;
     if (a.les_model == AERO_LES_WALE) f |= FEAT_LES_WALE;
+  }
+  if (a.inflow_field && (a.dims == 2 || a.streamwise_open) && a.inlet_bc == AERO_INLET_VELOCITY) {
+    f |= FEAT_INFLOW_FIELD;
+    L->inflow_ring = a.inflow_ring > 0 ? a.inflow_ring : 64;
+  }
+  if (a.recycling) {
+    f |= FEAT_RECYCLE;
+    L->recycle_blocks = (int)((L->prev_plane + kRecycleBlock - 1) / kRecycleBlock);
   }
   if (a.thermal) {
     f |= FEAT_THERMAL;
@@ -669,6 +692,8 @@ int aero_set_geometry(AeroLattice *L, const uint8_t *solid, const int32_t *links
   y.g[1] = take(L->Qg ? rb * L->Qg * L->cs : 0);
   y.U = take((L->feat & FEAT_LES) ? rb * 3 * L->cs : 0);
   y.cs_cell = take(L->cs_cell.empty() ? 0 : rb * L->cs);
+  y.inflow = take((L->feat & FEAT_INFLOW_FIELD) ? rb * (uint64_t)L->inflow_ring * (a.dims - 1) * L->prev_plane : 0);
+  y.recycle = take((L->feat & FEAT_RECYCLE) ? 8 * (uint64_t)(L->recycle_blocks + 2) : 0);
   y.hist = take(8 * 12 * (uint64_t)L->hist_cap);
   y.prof_out = take(24 * (uint64_t)L->nprof);
   y.counters = take(64);
@@ -803,6 +828,9 @@ int aero_step(AeroLattice *L, int64_t n, void *stream) {
   if (n < 0) return fail(AERO_ERR_INVALID, "negative step count");
   if (L->step_count + n - L->read_upto > L->hist_cap)
     return fail(AERO_ERR_CAPACITY, "force history holds %d steps; read it before stepping further", L->hist_cap);
+  if ((L->feat & FEAT_INFLOW_FIELD) && L->step_count + n > L->inflow_upto)
+    return fail(AERO_ERR_STATE, "inflow fields are on the device up to step %lld; upload them with aero_set_inflow",
+                (long long)L->inflow_upto);
   CUDA_TRY(cudaSetDevice(L->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (n == 0) return AERO_OK;
@@ -870,6 +898,35 @@ int aero_first_bad_step(AeroLattice *L, int64_t *step, void *stream) {
 int aero_step_count(const AeroLattice *L, int64_t *steps) {
   if (!L || !steps) return fail(AERO_ERR_INVALID, "NULL argument");
   *steps = L->step_count;
+  return AERO_OK;
+}
+
+int aero_set_inflow(AeroLattice *L, const double *fields, int64_t first, int64_t n, void *stream) {
+  if (!L || (n > 0 && !fields)) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
+  if (!(L->feat & FEAT_INFLOW_FIELD)) return fail(AERO_ERR_STATE, "the lattice has no inflow field inlet");
+  if (n < 0 || first < L->step_count) return fail(AERO_ERR_INVALID, "fields for steps already taken, or n < 0");
+  if (first > L->inflow_upto) return fail(AERO_ERR_INVALID, "inflow fields must be uploaded without gaps");
+  if (first + n - L->step_count > L->inflow_ring)
+    return fail(AERO_ERR_CAPACITY, "the device holds inflow fields for %d steps ahead", L->inflow_ring);
+  if (n == 0) return AERO_OK;
+  CUDA_TRY(cudaSetDevice(L->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t per = (int64_t)(L->prm.dims - 1) * L->prev_plane;  // values per step
+  const size_t rb = is_f64(L) ? 8 : 4;
+  std::vector<char> host((size_t)(per * n) * rb);
+  for (int64_t k = 0; k < per * n; k++) {
+    if (rb == 8) reinterpret_cast<double *>(host.data())[k] = fields[k];
+    else reinterpret_cast<float *>(host.data())[k] = (float)fields[k];
+  }
+  char *ring = L->ws + L->lay.inflow;
+  for (int64_t k = 0; k < n; k++) {
+    const int64_t slot = (first + k) % L->inflow_ring;
+    CUDA_TRY(cudaMemcpyAsync(ring + (size_t)(slot * per) * rb, host.data() + (size_t)(k * per) * rb,
+                             (size_t)per * rb, cudaMemcpyHostToDevice, st));
+  }
+  CUDA_TRY(cudaStreamSynchronize(st));  // the staging vector goes out of scope
+  L->inflow_upto = std::max(L->inflow_upto, first + n);
   return AERO_OK;
 }
 
@@ -1320,6 +1377,8 @@ int aero_batch_add(AeroBatch *B, AeroLattice *L, double cd_norm) {
   if (L->device != B->device) return fail(AERO_ERR_INVALID, "the lattice is on another device than the batch");
   if ((int)B->members.size() >= B->max_members) return fail(AERO_ERR_CAPACITY, "batch holds %d members", B->max_members);
   if (!(cd_norm > 0.0) || !std::isfinite(cd_norm)) return fail(AERO_ERR_INVALID, "cd_norm must be > 0");
+  if (L->feat & (FEAT_INFLOW_FIELD | FEAT_RECYCLE))
+    return fail(AERO_ERR_UNSUPPORTED, "lattices with synthetic inflow or a recycling inlet step only on their own");
   L->batch = B;
   L->cd_norm = cd_norm;
   B->members.push_back(L);

@@ -29,6 +29,8 @@ struct Ops {
                                cudaStream_t);
   cudaError_t (*finalize_batch)(const StepParams<Real> *params, const int64_t *first, int n, int64_t blocks,
                                 cudaStream_t);
+  // mean ux of the recycle plane (3D recycling inlet), before the step kernel
+  cudaError_t (*recycle_mean)(const StepParams<Real> &, cudaStream_t);
   int store_bytes;
 };
 

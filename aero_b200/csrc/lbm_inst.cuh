@@ -75,9 +75,16 @@ struct Launch {
     k_finalize_batch<Real><<<(unsigned)blocks, kFinalizeBlock, 0, st>>>(params, first, n);
     return cudaGetLastError();
   }
+  static cudaError_t recycle_mean(const StepParams<Real> &p, cudaStream_t st) {
+    if constexpr (L::DIMS == 3) {
+      k_recycle_mean<L, S><<<p.recycle_blocks, kRecycleBlock, 0, st>>>(p);
+      return cudaGetLastError();
+    }
+    return cudaErrorInvalidValue;  // recycling exists in 3D only
+  }
   static constexpr Ops<Real> table = {&step,       &moments,     &finalize,   &state_out,     &load_state,
                                       &step_tiled, &tiled_setup, &step_batch, &moments_batch, &finalize_batch,
-                                      (int)sizeof(S)};
+                                      &recycle_mean, (int)sizeof(S)};
 };
 
 template <class S>

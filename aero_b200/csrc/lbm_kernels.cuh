@@ -124,6 +124,39 @@ __device__ __forceinline__ void inlet_velocity(const StepParams<Real> &p, Real (
   }
 }
 
+// Zou-He velocity inlet with per-row target velocities (ux = u0, transverse
+// components from the inflow ring slot of this step): 2D boundary.py:48-65,
+// 3D boundary3d.py:71-93, as the synthetic inflow calls them
+// (solver.py:386-392, solver3d.py:436-445).  Unlike the uniform inlet these
+// carry no transverse correction from the incoming populations.
+template <class L, class Real>
+__device__ __forceinline__ void inlet_velocity_field(const StepParams<Real> &p, Real (&d)[L::Q], int y, int z,
+                                                     int64_t step_now) {
+  const int64_t plane = (int64_t)p.nz * p.ny;
+  const Real *slot = p.inflow + (step_now % p.inflow_ring) * (L::DIMS - 1) * plane;
+  const int64_t r = (int64_t)z * p.ny + y;
+  const Real ux = p.u0;
+  const Real den = Real(1) - ux > Real(1e-8) ? Real(1) - ux : Real(1e-8);
+  if constexpr (L::DIMS == 2) {
+    const Real rho_in = (Real(1) + (d[0] + d[2] + d[4]) + Real(2) * (d[3] + d[6] + d[7])) / den;
+    const Real cy = rho_in * slot[r];
+    d[1] = d[3] + Real(2.0 / 3.0) * rho_in * ux;
+    d[5] = d[7] - Real(0.5) * cy + Real(1.0 / 6.0) * rho_in * ux;
+    d[8] = d[6] + Real(0.5) * cy + Real(1.0 / 6.0) * rho_in * ux;
+  } else {
+    const Real Fm = d[2] + d[8] + d[10] + d[12] + d[14];
+    const Real Fn = d[0] + d[3] + d[4] + d[5] + d[6] + d[15] + d[16] + d[17] + d[18];
+    const Real rho_in = (Real(1) + Real(2) * Fm + Fn) / den;
+    const Real cy = rho_in * slot[r], cz = rho_in * slot[plane + r];
+    const Real r6 = Real(1.0 / 6.0) * rho_in * ux;
+    d[1] = d[2] + Real(1.0 / 3.0) * rho_in * ux;
+    d[7] = d[10] + r6 - Real(0.5) * cy;
+    d[9] = d[8] + r6 + Real(0.5) * cy;
+    d[11] = d[14] + r6 - Real(0.5) * cz;
+    d[13] = d[12] + r6 + Real(0.5) * cz;
+  }
+}
+
 // Zou-He pressure inlet (2D): boundary.py:116-136
 template <class Real>
 __device__ __forceinline__ void inlet_pressure_2d(const StepParams<Real> &p, Real (&d)[9]) {
@@ -337,7 +370,10 @@ __device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, 
   }
   if ((p.feat & FEAT_OPEN) && x == 0) {
     if (p.inlet == INLET_VELOCITY) {
-      inlet_velocity<L>(p, d, y, z, step_now);
+      if (p.feat & FEAT_INFLOW_FIELD)
+        inlet_velocity_field<L>(p, d, y, z, step_now);
+      else
+        inlet_velocity<L>(p, d, y, z, step_now);
     } else if constexpr (L::DIMS == 2) {
       if (p.inlet == INLET_PRESSURE) inlet_pressure_2d(p, d);
     }
@@ -373,6 +409,35 @@ __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int
     }
   } else if constexpr (L::DIMS == 2) {
     if (open && x == p.nx - 1 && p.outlet == OUTLET_PRESSURE) outlet_pressure_2d(p, d);
+  }
+  if constexpr (L::DIMS == 3) {
+    // recycling inlet (boundary3d.py:172-198, applied after bounce-back as in
+    // solver3d.py:460-461): the inlet plane takes the equilibrium of the
+    // x = nx-2 cell's post-bounce-back state with its velocity scaled so that
+    // the plane's mean ux becomes u0
+    if ((p.feat & FEAT_RECYCLE) && x == 0) {
+      Real r[L::Q];
+      partial_state<L, S, Real>(p, p.nx - 2, y, z, step_now, r, gather);
+      Real drho = 0, jx = 0, jy = 0, jz = 0;
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        drho += r[i];
+        if (Dir<L, i>::x) jx += Dir<L, i>::x * r[i];
+        if (Dir<L, i>::y) jy += Dir<L, i>::y * r[i];
+        if (Dir<L, i>::z) jz += Dir<L, i>::z * r[i];
+      });
+      const Real rho = Real(1) + drho;
+      const Real inv = rho > Real(0) ? Real(1) / rho : Real(0);
+      const double mean = *p.recycle_mean;
+      const Real scale = fabs(mean) < 1e-12 ? Real(1) : (Real)((double)p.u0 / mean);
+      const Real ux = jx * inv * scale, uy = jy * inv * scale, uz = jz * inv * scale;
+      const Real usq = ux * ux + uy * uy + uz * uz;
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        const Real eu = Dir<L, i>::x * ux + Dir<L, i>::y * uy + Dir<L, i>::z * uz;
+        d[i] = Real(Dir<L, i>::w) * (drho + rho * (Real(3) * eu + Real(4.5) * eu * eu - Real(1.5) * usq));
+      });
+    }
   }
   // sponge (sponge.py:8-70)
   if ((p.feat & FEAT_SPONGE) && x >= p.sponge_start) {
@@ -1177,6 +1242,55 @@ __global__ void __launch_bounds__(kStepBlock) k_moments(const StepParams<typenam
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= p.nx) return;
   moments_cell<L, S, FROM_STATE>(p, x, (int)blockIdx.y, (int)blockIdx.z);
+}
+
+// Mean ux of the recycle plane x = nx-2 of the current step's post-bounce-
+// back state (boundary3d.py:186-188: compute_macroscopic_3d, 0 where rho <=
+// 0, mean over every cell of the plane).  One thread per (z, y) row; blocks
+// sum in a fixed order, the last block adds the block sums in block order.
+constexpr int kRecycleBlock = 256;
+
+template <class L, class S>
+__global__ void __launch_bounds__(kRecycleBlock) k_recycle_mean(const StepParams<typename StoreOps<S>::Real> p) {
+  using Real = typename StoreOps<S>::Real;
+  __shared__ double red[kRecycleBlock / 32];
+  __shared__ bool last;
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  const int64_t k = (int64_t)blockIdx.x * kRecycleBlock + t;
+  const int64_t plane = (int64_t)p.ny * p.nz;
+  double v = 0.0;
+  if (k < plane) {
+    const int y = (int)(k % p.ny), z = (int)(k / p.ny);
+    Real d[L::Q];
+    partial_state<L, S, Real>(p, p.nx - 2, y, z, *p.step, d, GlobalGather<L, S, Real>{p, y, z});
+    Real drho = 0, jx = 0;
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      drho += d[i];
+      if (Dir<L, i>::x) jx += Dir<L, i>::x * d[i];
+    });
+    const Real rho = Real(1) + drho;
+    v = rho > Real(0) ? (double)(jx * (Real(1) / rho)) : 0.0;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  if (t == 0) {
+    double b = 0.0;
+    for (int w = 0; w < kRecycleBlock / 32; w++) b += red[w];
+    p.recycle_partial[blockIdx.x] = b;
+    __threadfence();
+    last = atomicAdd(p.recycle_ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && t == 0) {
+    __threadfence();
+    double sum = 0.0;
+    for (int b = 0; b < (int)gridDim.x; b++) sum += __ldcg(p.recycle_partial + b);
+    *p.recycle_mean = sum / (double)plane;
+    *p.recycle_ticket = 0u;
+  }
 }
 
 // Sums the per-link-cell contributions plus the constant rest-weight part

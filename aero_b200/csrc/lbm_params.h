@@ -23,6 +23,8 @@ enum Feature : uint32_t {
   FEAT_SCALAR_REDUCED = 1u << 8,  // D2Q5 / D3Q7 scalar lattice
   FEAT_OPEN = 1u << 9,            // streamwise open: inlet/outlet active
   FEAT_OBSTACLE_BB = 1u << 10,    // obstacle bounce-back active (links present)
+  FEAT_INFLOW_FIELD = 1u << 11,   // velocity inlet from per-step transverse fields (synthetic inflow)
+  FEAT_RECYCLE = 1u << 12,        // 3D recycling inlet (rescaled equilibrium of plane nx-2)
 };
 
 // Per-cell flag byte.
@@ -90,6 +92,12 @@ struct StepParams {
   const Real *U;        // LES velocities (3, cells) of the current state
   Real *Uw;             // LES velocity side output (written by the moments pass)
   const Real *cs_cell;  // per-cell LES constant (van Driest), optional
+  const Real *inflow;   // inflow ring: inflow_ring steps x (dims-1) x (nz*ny) transverse velocities
+  int32_t inflow_ring;
+  double *recycle_partial;  // per k_recycle_mean block: sum of ux over its cells
+  double *recycle_mean;     // mean ux of the recycle plane of the current step
+  uint32_t *recycle_ticket;
+  int32_t recycle_blocks;
 
   // force reduction
   double *lc_contrib;   // 12 x n_lc doubles, component-major: deviation part of each link cell's forces

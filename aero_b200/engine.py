@@ -126,6 +126,13 @@ class Engine:
                 self.h, int(z0), int(nzs), out.data_ptr(), self.stream()))
         return out
 
+    def set_inflow(self, fields: np.ndarray, first_step: int) -> None:
+        """Uploads the transverse inlet velocities of steps first_step.. (n, dims-1, nz*ny)."""
+        a = np.ascontiguousarray(fields, dtype=np.float64)
+        with self.torch.cuda.device(self.device):
+            check("aero_set_inflow", self.lib.aero_set_inflow(
+                self.h, a.ctypes.data, int(first_step), int(a.shape[0]), self.stream()))
+
     def step(self, n: int) -> None:
         with self.torch.cuda.device(self.device):
             check("aero_step", self.lib.aero_step(self.h, int(n), self.stream()))

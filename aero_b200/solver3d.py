@@ -5,9 +5,9 @@ Drop-in for the reference ``aero.lbm.solver3d.Solver3D``
 ``_step()`` returning (Cd, Cl_y, Cl_z), ``run()`` with the same result dict,
 host-visible ``f`` / ``g`` / ``_f_outlet_prev`` and .npz checkpoints.  Extra
 options as for the 2D Solver (``precision``, ``scalar_lattice`` with
-"reduced" = D3Q7, ``device``, ``hist_capacity``).  Streamwise "recycling",
-the SEM inlet and synthetic inflow are not part of the engine and raise
-NotImplementedError.
+"reduced" = D3Q7, ``device``, ``hist_capacity``).  Streamwise "recycling"
+and synthetic inflow run in the engine; the SEM inlet is not part of it and
+raises NotImplementedError.
 """
 
 from __future__ import annotations
@@ -42,8 +42,6 @@ class Solver3D(LatticeSolverBase):
         if streamwise_bc not in ("open", "periodic", "recycling"):
             raise ValueError(
                 f"Unknown streamwise_bc '{streamwise_bc}'. Choose 'open', 'periodic', or 'recycling'.")
-        if streamwise_bc == "recycling":
-            raise NotImplementedError("streamwise_bc='recycling' is not part of the b200 engine yet")
         if sem_inlet:
             raise NotImplementedError("sem_inlet is not part of the b200 engine yet")
         self.Nz, self.Ny, self.Nx = int(Nz), int(Ny), int(Nx)

@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define AERO_ABI_VERSION 1
+#define AERO_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define AERO_API __attribute__((visibility("default")))
@@ -78,6 +78,11 @@ typedef struct AeroParams {
   double body_force[3];     /* (fx, fy, fz); 3D only */
   double alpha_T, T_hot, T_cold, g_gravity, beta, T_ref;
   double center[3];         /* moment reference point (x, y, z): mean solid cell */
+  int32_t recycling;        /* 3D streamwise "recycling": the inlet plane is the rescaled
+                               equilibrium of plane x = nx-2 (needs streamwise_open = 0) */
+  int32_t inflow_field;     /* velocity inlet driven by per-step transverse velocity fields
+                               (synthetic inflow), uploaded with aero_set_inflow */
+  int32_t inflow_ring;      /* steps of inflow fields held on the device (0 = 64) */
 } AeroParams;
 
 typedef struct AeroLattice AeroLattice;
@@ -154,6 +159,19 @@ AERO_API int aero_first_bad_step(AeroLattice *lat, int64_t *step, void *stream);
  * where rows fit a tile and start 16-byte aligned), with the rows per tile
  * and the persistent grid size.  Valid after binding. */
 AERO_API int aero_step_plan(const AeroLattice *lat, int32_t *tiled, int32_t *tile_rows, int32_t *blocks);
+
+/* Transverse inlet velocities of steps first_step .. first_step+n_steps-1
+ * for a lattice with inflow_field set: `fields` (host) holds n_steps blocks
+ * of (dims-1) planes of nz*ny doubles, (z, y) order: uy in 2D; uy then uz in
+ * 3D.  The inlet of such a step is the Zou-He velocity-field inlet of
+ * apply_inlet_velocity_field(_3d) (boundary.py:48-65, boundary3d.py:71-93)
+ * with ux = u0, as the reference's synthetic inflow calls it
+ * (solver.py:386-392, solver3d.py:436-445).  The device holds inflow_ring
+ * steps: first_step must not precede the next step to run, and the fields
+ * must not reach beyond inflow_ring steps past it; aero_step refuses steps
+ * whose fields are missing.  Synchronous. */
+AERO_API int aero_set_inflow(AeroLattice *lat, const double *fields, int64_t first_step, int64_t n_steps,
+                             void *stream);
 
 /* Steps taken (host mirror of the reference's step_count). */
 AERO_API int aero_step_count(const AeroLattice *lat, int64_t *steps);

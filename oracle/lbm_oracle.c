@@ -332,7 +332,19 @@ static void bounce_back(const OracleLattice *s, const Lat *L, double *f, const d
 static void inlet_outlet_2d(OracleLattice *s, double *f) {
   const int nx = s->nx, ny = s->ny, nz = 1;
   const double u0 = s->u0;
-  if (s->inlet_bc == ORACLE_INLET_VELOCITY) {
+  if (s->inlet_bc == ORACLE_INLET_VELOCITY && s->inflow) {
+    /* per-row field inlet, boundary.py:48-65, with ux = u0 (solver.py:386-392) */
+    for (int y = 0; y < ny; y++) {
+#define F(i) f[IDX(i, 0, y, 0)]
+      double den = 1.0 - u0 > 1e-8 ? 1.0 - u0 : 1e-8;
+      double rho_in = ((F(0) + F(2) + F(4)) + 2.0 * (F(3) + F(6) + F(7))) / den;
+      double cy = rho_in * s->inflow[y];
+      F(1) = F(3) + (2.0 / 3.0) * rho_in * u0;
+      F(5) = F(7) - 0.5 * cy + (1.0 / 6.0) * rho_in * u0;
+      F(8) = F(6) + 0.5 * cy + (1.0 / 6.0) * rho_in * u0;
+#undef F
+    }
+  } else if (s->inlet_bc == ORACLE_INLET_VELOCITY) {
     const int64_t step = s->step_count + 1;
     for (int y = 0; y < ny; y++) {
 #define F(i) f[IDX(i, 0, y, 0)]
@@ -391,8 +403,65 @@ static void inlet_outlet_2d(OracleLattice *s, double *f) {
 static void inlet_outlet_3d(OracleLattice *s, double *f) {
   const int nx = s->nx, ny = s->ny, nz = s->nz;
   const double u0 = s->u0;
+  if (s->streamwise_bc == ORACLE_STREAM_RECYCLING) {
+    /* boundary3d.py:172-198: macroscopic state of plane x = nx-2, its mean ux
+     * over the plane, then the inlet plane = feq(rho, scale * u) */
+    const int64_t plane = (int64_t)nz * ny;
+    double *rho = malloc(sizeof(double) * plane * 4);
+    double *ux = rho + plane, *uy = ux + plane, *uz = uy + plane;
+    double sum = 0.0;
+    for (int z = 0; z < nz; z++)
+      for (int y = 0; y < ny; y++) {
+        const int64_t r = (int64_t)z * ny + y;
+        double m = 0.0, jx = 0.0, jy = 0.0, jz = 0.0;
+        for (int i = 0; i < 19; i++) {
+          double v = f[IDX(i, z, y, nx - 2)];
+          m += v;
+          jx += E3[i][0] * v;
+          jy += E3[i][1] * v;
+          jz += E3[i][2] * v;
+        }
+        double inv = m > 0.0 ? 1.0 / m : 0.0;
+        rho[r] = m;
+        ux[r] = inv * jx;
+        uy[r] = inv * jy;
+        uz[r] = inv * jz;
+      }
+    for (int64_t r = 0; r < plane; r++) sum += ux[r];
+    const double mean = sum / (double)plane;
+    const double scale = fabs(mean) < 1e-12 ? 1.0 : u0 / mean;
+    Lat L;
+    lat_init(&L, 3);
+    for (int z = 0; z < nz; z++)
+      for (int y = 0; y < ny; y++) {
+        const int64_t r = (int64_t)z * ny + y;
+        for (int i = 0; i < 19; i++)
+          f[IDX(i, z, y, 0)] = feq_i(&L, i, rho[r], ux[r] * scale, uy[r] * scale, uz[r] * scale);
+      }
+    free(rho);
+    return;
+  }
   if (s->streamwise_bc != ORACLE_STREAM_OPEN) return;
-  if (s->inlet_bc == ORACLE_INLET_VELOCITY) {
+  if (s->inlet_bc == ORACLE_INLET_VELOCITY && s->inflow) {
+    /* per-cell field inlet, boundary3d.py:71-93, ux = u0 (solver3d.py:436-445) */
+    const int64_t plane = (int64_t)nz * ny;
+    for (int z = 0; z < nz; z++)
+      for (int y = 0; y < ny; y++) {
+#define F(i) f[IDX(i, z, y, 0)]
+        const int64_t r = (int64_t)z * ny + y;
+        double Fm = F(2) + F(8) + F(10) + F(12) + F(14);
+        double Fn = F(0) + F(3) + F(4) + F(5) + F(6) + F(15) + F(16) + F(17) + F(18);
+        double den = 1.0 - u0 > 1e-8 ? 1.0 - u0 : 1e-8;
+        double rho_in = (2.0 * Fm + Fn) / den;
+        double cy = rho_in * s->inflow[r], cz = rho_in * s->inflow[plane + r];
+        F(1) = F(2) + (1.0 / 3.0) * rho_in * u0;
+        F(7) = F(10) + (1.0 / 6.0) * rho_in * u0 - 0.5 * cy;
+        F(9) = F(8) + (1.0 / 6.0) * rho_in * u0 + 0.5 * cy;
+        F(11) = F(14) + (1.0 / 6.0) * rho_in * u0 - 0.5 * cz;
+        F(13) = F(12) + (1.0 / 6.0) * rho_in * u0 + 0.5 * cz;
+#undef F
+      }
+  } else if (s->inlet_bc == ORACLE_INLET_VELOCITY) {
     const int64_t step = s->step_count + 1;
 #pragma omp parallel for collapse(2)
     for (int z = 0; z < nz; z++)

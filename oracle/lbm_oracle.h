@@ -19,7 +19,7 @@ enum {
   ORACLE_OUTLET_ZEROGRAD = 2,
   ORACLE_OUTLET_PRESSURE = 3
 };
-enum { ORACLE_STREAM_OPEN = 0, ORACLE_STREAM_PERIODIC = 1 };
+enum { ORACLE_STREAM_OPEN = 0, ORACLE_STREAM_PERIODIC = 1, ORACLE_STREAM_RECYCLING = 2 };
 
 typedef struct OracleLattice {
   int32_t dims, nx, ny, nz;
@@ -44,6 +44,9 @@ typedef struct OracleLattice {
   const float *q_vals;   /* (n_links,) */
   const double *mrt_M, *mrt_Minv, *mrt_s;
   double *work_a, *work_b, *work_om, *work_g;
+  /* synthetic inflow of the step about to run: (dims-1, nz, ny) transverse
+   * inlet velocities (uy; 3D then uz), or NULL for the uniform inlet */
+  const double *inflow;
 } OracleLattice;
 
 int oracle_step(OracleLattice *s, double *out_forces, double *out_profile);

@@ -132,7 +132,7 @@ class _OracleLattice(ctypes.Structure):
     ] + [("center", ctypes.c_double * 3)] + [
         (n, ctypes.c_void_p) for n in (
             "f", "g", "f_outlet_prev", "solid", "phi", "links", "q_vals", "mrt_M", "mrt_Minv",
-            "mrt_s", "work_a", "work_b", "work_om", "work_g")]
+            "mrt_s", "work_a", "work_b", "work_om", "work_g", "inflow")]
 
 
 def build(force: bool = False) -> pathlib.Path:
@@ -187,7 +187,8 @@ class OracleSolver:
                  T_hot: float = 1.0, T_cold: float = 0.0, alpha_T: float = 1e-3,
                  buoyancy: bool = False, g_gravity: float = 0.0, beta: float = 1e-3,
                  T_ref: float = 0.5, scalar_lattice: str = "full", threads: Optional[int] = None,
-                 **_ignored):
+                 synthetic_inflow: bool = False, synthetic_inflow_intensity: float = 0.03,
+                 synthetic_inflow_seed: int = 12345, **_ignored):
         solid = np.ascontiguousarray(solid, dtype=np.bool_)
         self.dims = solid.ndim
         if self.dims == 2:
@@ -244,7 +245,16 @@ class OracleSolver:
         s.wall_bc = _WALL.get(wall_bc, 0)
         s.inlet_bc = _INLET.get(inlet_bc, 0)
         s.outlet_bc = _OUTLET.get(outlet_bc, 2)
-        s.streamwise_bc = 0 if streamwise_bc == "open" else 1
+        s.streamwise_bc = {"open": 0, "periodic": 1, "recycling": 2}[streamwise_bc]
+        # synthetic inflow (solver.py:259-270, solver3d.py:297-321): transverse
+        # inlet velocities drawn step by step from the seeded generator
+        self._inflow_on = bool(synthetic_inflow) and inlet_bc == "velocity" and (
+            self.dims == 2 or streamwise_bc == "open")
+        self._inflow_target = float(synthetic_inflow_intensity) * float(u0)
+        self._inflow_rng = np.random.default_rng(int(synthetic_inflow_seed))
+        plane = (self.ny,) if self.dims == 2 else (self.nz, self.ny)
+        self._inflow_u = [np.zeros(plane) for _ in range(self.dims - 1)]
+        self._inflow_buf = None
         s.sponge_thickness = int(sponge_thickness)
         s.thermal = int(bool(thermal))
         s.buoyancy = int(bool(buoyancy))
@@ -291,9 +301,37 @@ class OracleSolver:
         s.work_om, s.work_g = _ptr(self._work_om), _ptr(self._work_g)
         s.step_count = self.step_count
 
+    def _next_inflow(self):
+        """The next step's transverse inlet velocities, as the reference draws them."""
+        rng, t = self._inflow_rng, self._inflow_target
+        if self.dims == 2:
+            n = rng.standard_normal(self.ny)
+            filt = (n + np.roll(n, 1) + np.roll(n, -1)) / 3.0
+            u = 0.75 * self._inflow_u[0] + 0.25 * filt
+            u = u - float(np.mean(u))
+            rms = float(np.sqrt(np.mean(u ** 2)))
+            if rms > 1e-12 and t > 0.0:
+                u = u * (t / rms)
+            self._inflow_u = [u]
+        else:
+            raw = [rng.standard_normal((self.nz, self.ny)), rng.standard_normal((self.nz, self.ny))]
+            new = []
+            for prev, n in zip(self._inflow_u, raw):
+                sm = (n + np.roll(n, 1, 0) + np.roll(n, -1, 0) + np.roll(n, 1, 1) + np.roll(n, -1, 1)) / 5.0
+                u = 0.8 * prev + 0.2 * sm
+                new.append(u - float(np.mean(u)))
+            rms = float(np.sqrt(np.mean(new[0] ** 2 + new[1] ** 2)))
+            if rms > 1e-12 and t > 0.0:
+                new = [u * (t / rms) for u in new]
+            self._inflow_u = new
+        return np.ascontiguousarray(np.stack(self._inflow_u), dtype=np.float64)
+
     def step_raw(self):
         """One step; returns (raw 12-vector of forces/moments, profile (nprof, 3))."""
         self._bind()
+        if self._inflow_on:
+            self._inflow_buf = self._next_inflow()
+            self._s_struct.inflow = self._inflow_buf.ctypes.data
         out = np.zeros(12)
         prof = np.zeros((self.nprof, 3))
         rc = lib().oracle_step(ctypes.byref(self._s_struct), out.ctypes.data, prof.ctypes.data)

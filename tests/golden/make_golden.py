@@ -71,6 +71,9 @@ CASES_2D = [
     ("c2d_mrt_smag_bouzidi_noslip", ("cyl", 5.0, 0.3, 0.45),
      dict(collision="mrt", wall_bc="noslip", outlet_bc="zerogradient", bouzidi=True,
           les=True), 40),
+    ("c2d_bgk_synthetic_inflow", ("cyl", 4.5, 0.3, 0.5),
+     dict(collision="bgk", wall_bc="noslip", outlet_bc="convective", synthetic_inflow=True,
+          synthetic_inflow_intensity=0.05, synthetic_inflow_seed=77), 40),
 ]
 
 CASES_3D = [
@@ -95,6 +98,12 @@ CASES_3D = [
     ("c3d_bgk_smag_bodyforce_open", ("sph", 3.0, 0.3, 0.5, 0.5),
      dict(collision="bgk", wall_bc="slip", outlet_bc="convective", les=True, les_cs=0.16,
           body_force_x=2e-5, body_force_y=-1e-5), 12),
+    ("c3d_bgk_synthetic_inflow", ("sph", 3.0, 0.3, 0.5, 0.5),
+     dict(collision="bgk", wall_bc="slip", outlet_bc="convective", synthetic_inflow=True,
+          synthetic_inflow_intensity=0.05, synthetic_inflow_seed=91), 12),
+    ("c3d_mrt_recycling_sponge_bodyforce", ("sph", 3.0, 0.3, 0.5, 0.5),
+     dict(collision="mrt", wall_bc="noslip", streamwise_bc="recycling", sponge_thickness=4,
+          body_force_x=1e-5, bouzidi=True), 12),
 ]
 
 
