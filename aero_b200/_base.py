@@ -298,6 +298,12 @@ class LatticeSolverBase:
         c = self._coefficients(raw)
         return self._step_return(c, 0)
 
+    def autotune(self, steps: int = 20) -> dict:
+        """Selects the fastest step kernel for this lattice by timing each one
+        (see aero_b200.autotune); call before the first step."""
+        from .autotune import autotune
+        return autotune(self, steps=steps)
+
     def _drag_norm(self) -> float:
         """Force that makes Cd = 1: 0.5 rho0 u0^2 D (2D, forces.py:78-103) or
         0.5 rho0 u0^2 D^2 (3D, forces3d.py:70-101)."""

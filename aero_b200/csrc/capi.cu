@@ -134,7 +134,9 @@ struct AeroLattice {
   int recycle_blocks = 0;
   AeroBatch *batch = nullptr;  // batch this lattice is a member of (stepped only by it)
   double cd_norm = 1.0;        // drag normalisation given when it joined the batch
-  // row-tiled step plan (k_step_tiled), fixed at bind time
+  // step kernel: block shape of k_step (kStepShapeXY), or the row-tiled
+  // k_step_tiled with its plan
+  int step_shape = 0;
   bool tiled = false;
   int tile_blocks = 0, tile_rows = 0, tiles_per_plane = 0, ntiles = 0;
   // optional per-kernel event timing (eager launches only)
@@ -310,6 +312,8 @@ int launch_step(AeroLattice *L, int cur, cudaStream_t st, bool timed = false) {
   if (les_active(L)) CUDA_TRY(ops->moments(p, false, grid, st));
   if (L->tiled)
     CUDA_TRY(ops->step_tiled(p, L->tile_blocks, st));
+  else if (L->step_shape != 0)
+    CUDA_TRY(ops->step_shaped(p, L->step_shape, st));
   else
     CUDA_TRY(ops->step(p, false, grid, st));
   if (timed) CUDA_TRY(cudaEventRecord(e[1], st));
@@ -433,11 +437,11 @@ int do_get_state(AeroLattice *L, double *f, double *prev, double *g, int z0, int
 // 16-byte boundary (the bulk-copy alignment): tiles of tile_rows rows, a
 // persistent grid of resident blocks.
 template <class Real>
-int plan_tiles(AeroLattice *L) {
+int plan_tiles(AeroLattice *L, bool force = false) {
   L->tiled = false;
   L->tile_blocks = L->tile_rows = L->tiles_per_plane = L->ntiles = 0;
   const char *want = std::getenv("AERO_B200_TILES");
-  if (!(want && want[0] == '1')) return AERO_OK;
+  if (!force && !(want && want[0] == '1')) return AERO_OK;
   const Ops<Real> *ops = get_ops<Real>(L);
   const AeroParams &a = L->prm;
   const int sb = ops->store_bytes;
@@ -927,6 +931,34 @@ int aero_set_inflow(AeroLattice *L, const double *fields, int64_t first, int64_t
   }
   CUDA_TRY(cudaStreamSynchronize(st));  // the staging vector goes out of scope
   L->inflow_upto = std::max(L->inflow_upto, first + n);
+  return AERO_OK;
+}
+
+int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
+  if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
+  if (kernel < 0 || kernel > kStepShapes) return fail(AERO_ERR_INVALID, "kernel must be 0..%d", kStepShapes);
+  CUDA_TRY(cudaSetDevice(L->device));
+  if (kernel == kStepShapes) {
+    const int rc = is_f64(L) ? plan_tiles<double>(L, true) : plan_tiles<float>(L, true);
+    if (rc != AERO_OK) return rc;
+    if (!L->tiled) return fail(AERO_ERR_UNSUPPORTED, "rows of this lattice do not fit the row-tiled kernel");
+  } else {
+    L->tiled = false;
+    L->step_shape = kernel;
+  }
+  // captured step sequences launch the previous kernel
+  for (auto &e : L->pair_exec)
+    if (e) {
+      cudaGraphExecDestroy(e);
+      e = nullptr;
+    }
+  return AERO_OK;
+}
+
+int aero_get_step_kernel(const AeroLattice *L, int32_t *kernel) {
+  if (!L || !kernel) return fail(AERO_ERR_INVALID, "NULL argument");
+  *kernel = L->tiled ? kStepShapes : L->step_shape;
   return AERO_OK;
 }
 

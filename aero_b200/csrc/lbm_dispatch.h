@@ -10,6 +10,8 @@ template <class Real>
 struct Ops {
   // grid covers (ceil(nx / kStepBlock), ny, nz)
   cudaError_t (*step)(const StepParams<Real> &, bool from_state, dim3 grid, cudaStream_t);
+  // regular step with block shape `shape` (kStepShapes); grid from step_grid
+  cudaError_t (*step_shaped)(const StepParams<Real> &, int shape, cudaStream_t);
   cudaError_t (*moments)(const StepParams<Real> &, bool from_state, dim3 grid, cudaStream_t);
   cudaError_t (*finalize)(const StepParams<Real> &, cudaStream_t);
   // grid.z = planes written, starting at plane z0; out holds (Q, grid.z, ny, nx)
@@ -38,6 +40,16 @@ const Ops<float> *ops_f32(int dims, int coll);
 const Ops<double> *ops_f64(int dims, int coll);
 const Ops<float> *ops_f16(int dims, int coll);
 const Ops<float> *ops_bf16(int dims, int coll);
+
+// Block shapes of the per-cell step kernel an autotuner can choose from:
+// {threads along x, rows}.  Shape 0 is the default.
+constexpr int kStepShapes = 3;
+constexpr int kStepShapeXY[kStepShapes][2] = {{128, 1}, {256, 1}, {32, 4}};
+
+inline dim3 step_grid(int shape, int nx, int ny, int nz) {
+  const int bx = kStepShapeXY[shape][0], by = kStepShapeXY[shape][1];
+  return dim3((unsigned)((nx + bx - 1) / bx), (unsigned)((ny + by - 1) / by), (unsigned)nz);
+}
 
 bool build_mrt(int dims, double omega, MrtCoeffs<double> &out, double *A_full, double *B_full);
 bool build_mrt3_adapted(double omega, Mrt3Adapted<double> &out);

@@ -17,6 +17,20 @@ struct Launch {
       k_step<L, S, COLL, false><<<grid, kStepBlock, 0, st>>>(p);
     return cudaGetLastError();
   }
+  static cudaError_t step_shaped(const StepParams<Real> &p, int shape, cudaStream_t st) {
+    const dim3 grid = step_grid(shape, p.nx, p.ny, p.nz);
+    switch (shape) {
+      case 1:
+        k_step<L, S, COLL, false, 256, 1><<<grid, dim3(256, 1), 0, st>>>(p);
+        break;
+      case 2:
+        k_step<L, S, COLL, false, 32, 4><<<grid, dim3(32, 4), 0, st>>>(p);
+        break;
+      default:
+        k_step<L, S, COLL, false, 128, 1><<<grid, dim3(128, 1), 0, st>>>(p);
+    }
+    return cudaGetLastError();
+  }
   static cudaError_t moments(const StepParams<Real> &p, bool from_state, dim3 grid, cudaStream_t st) {
     if (from_state)
       k_moments<L, S, true><<<grid, kStepBlock, 0, st>>>(p);
@@ -82,7 +96,7 @@ struct Launch {
     }
     return cudaErrorInvalidValue;  // recycling exists in 3D only
   }
-  static constexpr Ops<Real> table = {&step,       &moments,     &finalize,   &state_out,     &load_state,
+  static constexpr Ops<Real> table = {&step,       &step_shaped, &moments,    &finalize,      &state_out,     &load_state,
                                       &step_tiled, &tiled_setup, &step_batch, &moments_batch, &finalize_batch,
                                       &recycle_mean, (int)sizeof(S)};
 };

@@ -936,14 +936,24 @@ __device__ __forceinline__ void step_cell(const StepParams<typename StoreOps<S>:
 // One full step: state of step n from P_n, scalar step, collision -> P_{n+1}.
 // FROM_STATE: P holds a state (deviations) to be collided as is (used after
 // the host sets f, and to start from an initial state).
-template <class L, class S, int COLL, bool FROM_STATE>
-__global__ void __launch_bounds__(kStepBlock, sizeof(typename StoreOps<S>::Real) == 4 ? kStepMinBlocks : 4)
+// Block shapes of the per-cell kernel: BX threads along x times BY rows
+// (y).  Every shape keeps 64 registers per thread: 8 blocks of 128 threads,
+// 4 of 256 (4-byte arithmetic; FP64 takes half the blocks).
+template <int BX, int BY>
+struct StepShape {
+  static constexpr int threads = BX * BY;
+  static constexpr int min_blocks4 = 1024 / (BX * BY);
+};
+
+template <class L, class S, int COLL, bool FROM_STATE, int BX = kStepBlock, int BY = 1>
+__global__ void __launch_bounds__(BX *BY, sizeof(typename StoreOps<S>::Real) == 4 ? StepShape<BX, BY>::min_blocks4
+                                                                                  : StepShape<BX, BY>::min_blocks4 / 2)
     k_step(const StepParams<typename StoreOps<S>::Real> p) {
   using Real = typename StoreOps<S>::Real;
   using SO = StoreOps<S>;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y, z = blockIdx.z;
-  if (x >= p.nx) return;
+  const int x = blockIdx.x * BX + threadIdx.x;
+  const int y = BY == 1 ? (int)blockIdx.y : (int)(blockIdx.y * BY + threadIdx.y), z = blockIdx.z;
+  if (x >= p.nx || y >= p.ny) return;
   if constexpr (FROM_STATE) {
     const uint32_t c = cell_index(p, x, y, z);
     const bool solid = p.flags[c] & FLAG_SOLID;

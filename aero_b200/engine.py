@@ -164,6 +164,14 @@ class Engine:
             check("aero_first_bad_step", self.lib.aero_first_bad_step(self.h, ctypes.byref(v), self.stream()))
         return int(v.value)
 
+    def set_step_kernel(self, kernel: int) -> None:
+        check("aero_set_step_kernel", self.lib.aero_set_step_kernel(self.h, int(kernel)))
+
+    def get_step_kernel(self) -> int:
+        k = ctypes.c_int32()
+        check("aero_get_step_kernel", self.lib.aero_get_step_kernel(self.h, ctypes.byref(k)))
+        return int(k.value)
+
     def step_plan(self) -> dict:
         """Step kernel in use: {"tiled": bool, "tile_rows": r, "blocks": b}."""
         t, r, b = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()

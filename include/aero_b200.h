@@ -160,6 +160,14 @@ AERO_API int aero_first_bad_step(AeroLattice *lat, int64_t *step, void *stream);
  * and the persistent grid size.  Valid after binding. */
 AERO_API int aero_step_plan(const AeroLattice *lat, int32_t *tiled, int32_t *tile_rows, int32_t *blocks);
 
+/* Step kernel choice for an autotuner (no counterpart in the reference):
+ * 0, 1, 2 = the per-cell-gather kernel with blocks of 128x1, 256x1 or 32x4
+ * cells (x by y); 3 = the row-tiled kernel (AERO_ERR_UNSUPPORTED where rows
+ * do not fit it).  Results are the same for every choice up to FP rounding
+ * of the compiled variant.  Takes effect at the next aero_step. */
+AERO_API int aero_set_step_kernel(AeroLattice *lat, int32_t kernel);
+AERO_API int aero_get_step_kernel(const AeroLattice *lat, int32_t *kernel);
+
 /* Transverse inlet velocities of steps first_step .. first_step+n_steps-1
  * for a lattice with inflow_field set: `fields` (host) holds n_steps blocks
  * of (dims-1) planes of nz*ny doubles, (z, y) order: uy in 2D; uy then uz in

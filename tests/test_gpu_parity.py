@@ -261,3 +261,44 @@ def test_tiled_kernel_equals_rowgather_kernel(precision, monkeypatch):
     (fa, cda), (fb, cdb) = runs["tiled"], runs["rowgather"]
     np.testing.assert_allclose(fa, fb, rtol=0, atol=1e-6 * np.abs(fb).max())
     np.testing.assert_allclose(cda, cdb, rtol=0, atol=1e-5 * np.abs(cdb).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", [1, 2, 3])
+@pytest.mark.parametrize("name", ["c3d_mrt_smag_bouzidi_sponge", "c2d_trt_bouzidi_moving",
+                                  "c3d_mrt_recycling_sponge_bodyforce"])
+def test_step_kernel_variants_agree(name, kernel):
+    """Every step kernel an autotuner may pick (256x1 and 32x4 blocks of the
+    per-cell kernel, the row-tiled kernel) reproduces the default kernel's
+    FP64 result to 1e-12 of max|f|."""
+    from aero_b200._lib import AeroError
+    c = load_case(name)
+    a = _solver(c, precision="fp64")
+    b = _solver(c, precision="fp64")
+    try:
+        b._engine.set_step_kernel(kernel)
+    except AeroError:
+        assert kernel == 3  # only the tiled kernel can be unavailable (row alignment)
+        pytest.skip("rows do not fit the row-tiled kernel")
+    assert b._engine.get_step_kernel() == kernel
+    for _ in range(c["steps"]):
+        a._step()
+        b._step()
+    np.testing.assert_allclose(b.f, a.f, rtol=0, atol=1e-12 * np.abs(a.f).max())
+
+
+@pytest.mark.gpu
+def test_autotune_restores_the_state():
+    """autotune() times the kernels, keeps the fastest and restores the
+    initial state: the tuned run is bit-identical to a run that selects the
+    same kernel without tuning."""
+    c = load_case("c3d_bgk_synthetic_inflow")
+    a = _solver(c, precision="fp32")
+    rep = a.autotune(steps=5)
+    assert set(rep["ms_per_step"]) >= {0, 1, 2} and rep["kernel"] in rep["ms_per_step"]
+    b = _solver(c, precision="fp32")
+    b._engine.set_step_kernel(rep["kernel"])
+    ra = a.run(c["steps"], check_every=c["steps"] + 1, verbose=False)
+    rb = b.run(c["steps"], check_every=c["steps"] + 1, verbose=False)
+    assert np.array_equal(a.f, b.f)
+    assert ra["Cd_history"] == rb["Cd_history"]
