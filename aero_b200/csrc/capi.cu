@@ -185,6 +185,7 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   p.sponge_thickness = a.sponge_thickness;
   p.sponge_start = std::max(a.nx - a.sponge_thickness, 0);
   p.tile_rows = L->tile_rows;
+  p.batch_rows = L->ncells < kBatchSmallCells ? 1 : kBatchRows;
   p.tiles_per_plane = L->tiles_per_plane;
   p.ntiles = L->ntiles;
   p.P = ws + L->lay.P[cur];
@@ -945,6 +946,7 @@ int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
     if (!L->tiled) return fail(AERO_ERR_UNSUPPORTED, "rows of this lattice do not fit the row-tiled kernel");
   } else {
     L->tiled = false;
+    L->tile_blocks = L->tile_rows = L->tiles_per_plane = L->ntiles = 0;
     L->step_shape = kernel;
   }
   // captured step sequences launch the previous kernel
@@ -1155,6 +1157,11 @@ struct AeroBatch {
   std::vector<char> host_plan;
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [steps - 1][phase]
+  // branch streams and events of a captured step: the lattice classes run
+  // as parallel branches of the graph, joined before the force finalisation
+  std::vector<cudaStream_t> branch;
+  std::vector<cudaEvent_t> branch_done;
+  cudaEvent_t fork = nullptr;
 };
 
 namespace {
@@ -1221,7 +1228,8 @@ int batch_build(AeroBatch *B, cudaStream_t st) {
   };
   auto cell_blocks = [](const AeroLattice *L) {
     const int64_t rows = (int64_t)L->prm.ny * L->prm.nz;
-    return (int64_t)blocks_for(L->prm.nx, kStepBlock) * ((rows + kBatchRows - 1) / kBatchRows);
+    const int64_t R = L->ncells < kBatchSmallCells ? 1 : kBatchRows;  // as make_params' batch_rows
+    return (int64_t)blocks_for(L->prm.nx, kStepBlock) * ((rows + R - 1) / R);
   };
   for (ClassPlan &c : B->classes) {
     const uint64_t sp = c.f64 ? sizeof(StepParams<double>) : sizeof(StepParams<float>);
@@ -1308,16 +1316,37 @@ int batch_build(AeroBatch *B, cudaStream_t st) {
 }
 
 // Launches one step of every member; `j` selects the parameter arrays.
-int batch_launch_step(AeroBatch *B, int j, cudaStream_t st) {
+// With `branches`, every lattice class runs on its own stream forked from st
+// and joined back before the finalisation (during capture this makes the
+// classes parallel branches of the graph: they touch disjoint lattices).
+int batch_launch_step(AeroBatch *B, int j, cudaStream_t st, bool branches = false) {
   char *ws = B->ws;
-  for (const ClassPlan &c : B->classes) {
+  if (branches) {
+    while (B->branch.size() < B->classes.size()) {
+      cudaStream_t bs;
+      cudaEvent_t ev;
+      CUDA_TRY(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
+      CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      B->branch.push_back(bs);
+      B->branch_done.push_back(ev);
+    }
+    if (!B->fork) CUDA_TRY(cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventRecord(B->fork, st));
+  }
+  for (size_t ci = 0; ci < B->classes.size(); ci++) {
+    const ClassPlan &c = B->classes[ci];
+    cudaStream_t cs = st;
+    if (branches) {
+      cs = B->branch[ci];
+      CUDA_TRY(cudaStreamWaitEvent(cs, B->fork, 0));
+    }
     if (c.f64) {
       const Ops<double> *ops = ops_f64(c.key.dims, c.key.coll);
       auto *P = reinterpret_cast<const StepParams<double> *>(ws + c.params[j]);
       auto *PL = reinterpret_cast<const StepParams<double> *>(ws + c.params_les[j]);
       if (c.n_les) CUDA_TRY(ops->moments_batch(PL, reinterpret_cast<const int64_t *>(ws + c.first_les), c.n_les,
-                                               c.blocks_les, st));
-      CUDA_TRY(ops->step_batch(P, reinterpret_cast<const int64_t *>(ws + c.first), c.n, c.blocks, st));
+                                               c.blocks_les, cs));
+      CUDA_TRY(ops->step_batch(P, reinterpret_cast<const int64_t *>(ws + c.first), c.n, c.blocks, cs));
     } else {
       const Ops<float> *ops = c.key.storage == AERO_STORE_F32   ? ops_f32(c.key.dims, c.key.coll)
                               : c.key.storage == AERO_STORE_F16 ? ops_f16(c.key.dims, c.key.coll)
@@ -1325,8 +1354,12 @@ int batch_launch_step(AeroBatch *B, int j, cudaStream_t st) {
       auto *P = reinterpret_cast<const StepParams<float> *>(ws + c.params[j]);
       auto *PL = reinterpret_cast<const StepParams<float> *>(ws + c.params_les[j]);
       if (c.n_les) CUDA_TRY(ops->moments_batch(PL, reinterpret_cast<const int64_t *>(ws + c.first_les), c.n_les,
-                                               c.blocks_les, st));
-      CUDA_TRY(ops->step_batch(P, reinterpret_cast<const int64_t *>(ws + c.first), c.n, c.blocks, st));
+                                               c.blocks_les, cs));
+      CUDA_TRY(ops->step_batch(P, reinterpret_cast<const int64_t *>(ws + c.first), c.n, c.blocks, cs));
+    }
+    if (branches) {
+      CUDA_TRY(cudaEventRecord(B->branch_done[ci], cs));
+      CUDA_TRY(cudaStreamWaitEvent(st, B->branch_done[ci], 0));
     }
   }
   // the finalisation kernels do not depend on the lattice class, so any
@@ -1349,7 +1382,9 @@ int batch_graph(AeroBatch *B, int steps, int phase, cudaGraphExec_t *out) {
     if (!B->cap_stream) CUDA_TRY(cudaStreamCreateWithFlags(&B->cap_stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaStreamBeginCapture(B->cap_stream, cudaStreamCaptureModeThreadLocal));
     int rc = AERO_OK;
-    for (int j = 0; j < steps && rc == AERO_OK; j++) rc = batch_launch_step(B, (phase + j) & 1, B->cap_stream);
+    const bool branches = B->classes.size() > 1;
+    for (int j = 0; j < steps && rc == AERO_OK; j++)
+      rc = batch_launch_step(B, (phase + j) & 1, B->cap_stream, branches);
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(B->cap_stream, &graph);
     if (rc != AERO_OK) {
@@ -1499,6 +1534,9 @@ int aero_batch_destroy(AeroBatch *B) {
   for (AeroLattice *L : B->members) L->batch = nullptr;
   batch_drop_graphs(B);
   if (B->cap_stream) cudaStreamDestroy(B->cap_stream);
+  for (auto bs : B->branch) cudaStreamDestroy(bs);
+  for (auto ev : B->branch_done) cudaEventDestroy(ev);
+  if (B->fork) cudaEventDestroy(B->fork);
   delete B;
   return AERO_OK;
 }

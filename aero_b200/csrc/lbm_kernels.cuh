@@ -1427,9 +1427,12 @@ __device__ __forceinline__ void params_to_smem(StepParams<Real> &dst, const Step
 }
 
 // A block of a batched cell kernel covers one kStepBlock-cell x segment of
-// kBatchRows consecutive rows (y, then z) of its member, so the member
-// lookup and the parameter copy are paid once per kBatchRows segments.
+// batch_rows consecutive rows (y, then z) of its member: kBatchRows for
+// large members, so the member lookup and the parameter copy are paid once
+// per kBatchRows segments, and 1 for members below kBatchSmallCells, so a
+// few small members still spread over the whole GPU.
 constexpr int kBatchRows = 4;
+constexpr int64_t kBatchSmallCells = 1 << 16;
 
 template <class L, class S, int COLL>
 __global__ void __launch_bounds__(kStepBlock, sizeof(typename StoreOps<S>::Real) == 4 ? kStepMinBlocks : 4)
@@ -1446,7 +1449,8 @@ __global__ void __launch_bounds__(kStepBlock, sizeof(typename StoreOps<S>::Real)
   if (x >= sp.nx) return;
   const int64_t nrows = (int64_t)sp.ny * sp.nz;
   const int64_t step_now = *sp.step;
-  for (int64_t row = rg * kBatchRows; row < nrows && row < (rg + 1) * kBatchRows; ++row) {
+  const int R = sp.batch_rows;
+  for (int64_t row = rg * R; row < nrows && row < (rg + 1) * R; ++row) {
     const int y = (int)(row % sp.ny), z = (int)(row / sp.ny);
     step_cell<L, S, COLL>(sp, x, y, z, step_now, GlobalGather<L, S, Real>{sp, y, z});
   }
@@ -1465,7 +1469,8 @@ __global__ void __launch_bounds__(kStepBlock) k_moments_batch(const StepParams<t
   const int x = (int)(b - rg * nxb) * kStepBlock + threadIdx.x;
   if (x >= sp.nx) return;
   const int64_t nrows = (int64_t)sp.ny * sp.nz;
-  for (int64_t row = rg * kBatchRows; row < nrows && row < (rg + 1) * kBatchRows; ++row)
+  const int R = sp.batch_rows;
+  for (int64_t row = rg * R; row < nrows && row < (rg + 1) * R; ++row)
     moments_cell<L, S, false>(sp, x, (int)(row % sp.ny), (int)(row / sp.ny));
 }
 

@@ -73,6 +73,7 @@ struct StepParams {
   int32_t sponge_thickness;
   // row tiles of the tiled step kernel: tile_rows y rows of one z plane
   int32_t tile_rows, tiles_per_plane, ntiles;
+  int32_t batch_rows;   // rows per block in the batched cell kernels
 
   // populations (deviation from the rest weights, see Store<>)
   const void *P;        // current post-collision populations (read)

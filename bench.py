@@ -421,9 +421,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--collision", default=None, choices=["bgk", "trt", "mrt"],
                     help="override the workload's collision operator (profiling)")
-    ap.add_argument("--kernel", default="rowgather", choices=["rowgather", "tiled"],
-                    help="step kernel: per-cell global gather (default) or rows staged in shared "
-                         "memory by bulk async copies")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "rowgather", "tiled"],
+                    help="step kernel: chosen by the autotuner (default), the per-cell global gather, or "
+                         "rows staged in shared memory by bulk async copies")
     ap.add_argument("--batch-every", type=int, default=1,
                     help="batch96: keep every k-th case (a smaller batch for profiling captures)")
     ap.add_argument("--serve-requests", type=int, default=64)
@@ -483,6 +483,11 @@ def main():
     del ux0
     eng.set_state(f0, prev0, g0, 0)
     stream = torch.cuda.current_stream(dev)
+    tune = None
+    if args.kernel == "auto":
+        # set-up, outside the timed region: time each step kernel on this
+        # lattice, keep the fastest, restore the initial state
+        tune = s.autotune(steps=10)
 
     # ---------------- device-timed region --------------------------------
     eng.enable_timing(True)
@@ -526,6 +531,9 @@ def main():
     # kernel and precision (a smaller case scaled by cells where the summary
     # says so); None when no capture covers the workload
     plan = eng.step_plan()
+    plan["kernel_id"] = eng.get_step_kernel()
+    if tune is not None:
+        plan["autotune_ms_per_step"] = {str(k): v for k, v in tune["ms_per_step"].items()}
     kname = "k_step_tiled" if plan["tiled"] else "k_step"
     traffic = None
     pat = re.compile(rf"^- {re.escape(args.workload)}: dram bytes per launch = (\d+)\s*$", re.M)
@@ -596,7 +604,8 @@ def main():
                      "traffic": traffic,
                      "kernel": f"{kname} (fused stream/BC/collide"
                                + (", source rows staged in shared memory by bulk async copies)"
-                                  if plan["tiled"] else ", per-cell global gather)"),
+                                  if plan["tiled"] else ", per-cell global gather, blocks "
+                                  + ("128x1", "256x1", "32x4")[plan["kernel_id"]] + ")"),
                      "step_plan": plan,
                      "alg_bytes_per_launch": alg_bytes, "bytes_per_cell": bytes_per_cell,
                      "kernel_ms": k_ms, "finalize_ms": force_ms / max(nt, 1)},
