@@ -40,7 +40,7 @@ class LatticeSolverBase:
                bouzidi, van_driest, van_driest_A, body_force, wall_velocity_top,
                wall_velocity_bottom, synthetic_inflow, synthetic_inflow_intensity,
                synthetic_inflow_seed, thermal, T_hot, T_cold, alpha_T, buoyancy, g_gravity, beta,
-               T_ref, precision, scalar_lattice, device, hist_capacity, rho_in=1.0, rho_out=1.0):
+               T_ref, precision, scalar_lattice, device, hist_capacity, rho_in=1.0, rho_out=1.0, sem=None):
         if backend not in BACKENDS:
             raise ValueError(f"Unknown backend '{backend}'. Choose 'b200' or 'auto'.")
         if collision not in ("bgk", "mrt", "trt"):
@@ -148,7 +148,13 @@ class LatticeSolverBase:
         # synthetic inflow only drives an open velocity inlet (solver.py:385-392,
         # solver3d.py:432-445); the fields come from the reference's random stream
         self._inflow = None
-        if self.synthetic_inflow and inlet_bc == "velocity" and (self.dims == 2 or streamwise_bc == "open"):
+        if sem is not None and self.dims == 3 and inlet_bc == "velocity" and streamwise_bc == "open":
+            # SEM takes precedence over synthetic inflow (solver3d.py:433-445)
+            from .inflow import SEMInflow
+            self._inflow = SEMInflow(shape[-2], shape[0], self.u0, sem[0], sem[1], sem[2])
+            P.inflow_field = 2
+            P.inflow_ring = 64
+        elif self.synthetic_inflow and inlet_bc == "velocity" and (self.dims == 2 or streamwise_bc == "open"):
             from .inflow import SyntheticInflow
             nz_ = shape[0] if self.dims == 3 else 1
             self._inflow = SyntheticInflow(self.dims, shape[-2], nz_, self.u0, self.synthetic_inflow_intensity,

@@ -48,7 +48,8 @@ def autotune(solver, steps: int = 20, warmup: int = 2) -> Dict:
         eng.set_state(f, prev, g, 0)
         if inflow is not None:
             plane = int(np.prod(solver.solid.shape[:-1]))  # nz * ny (3D) or ny (2D)
-            zeros = np.zeros((min(n_total, ring), solver.dims - 1, plane))
+            comps = 3 if solver._params.inflow_field == 2 else solver.dims - 1
+            zeros = np.zeros((min(n_total, ring), comps, plane))
         done = 0
         ms = None
         stream = torch.cuda.current_stream(eng.device)

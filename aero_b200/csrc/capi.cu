@@ -290,6 +290,10 @@ dim3 cell_grid(const AeroLattice *L) {
 
 bool les_active(const AeroLattice *L) { return (L->feat & FEAT_LES) != 0; }
 
+// values per inlet cell and step in the inflow ring: the transverse
+// velocities of synthetic inflow (dims - 1), or SEM's (u', v', w')
+int inflow_components(const AeroLattice *L) { return (L->feat & FEAT_INFLOW_SEM) ? 3 : L->prm.dims - 1; }
+
 // Launches one step with buffer parity `cur` on stream st.  With timing on,
 // events bracket the fused step (moments pass + step kernel, which also
 // computes the link-cell force contributions) and the force finalisation.
@@ -485,6 +489,8 @@ int check_params(const AeroParams *a) {
   if (a->recycling && (a->dims != 3 || a->streamwise_open))
     return fail(AERO_ERR_INVALID, "recycling is a 3D streamwise mode (streamwise_open must be 0)");
   if (a->inflow_field && a->recycling) return fail(AERO_ERR_INVALID, "inflow_field needs an open inlet");
+  if (a->inflow_field < 0 || a->inflow_field > 2 || (a->inflow_field == 2 && a->dims != 3))
+    return fail(AERO_ERR_INVALID, "inflow_field is 0, 1 (synthetic inflow) or 2 (SEM, 3D)");
   if (a->inflow_ring < 0 || a->inflow_ring > 65536) return fail(AERO_ERR_INVALID, "inflow_ring must be in 0..65536");
   if (a->hist_capacity < 0) return fail(AERO_ERR_INVALID, "hist_capacity < 0");
   return AERO_OK;
@@ -538,6 +544,7 @@ int aero_create(const AeroParams *params, AeroLattice **out) {
   }
   if (a.inflow_field && (a.dims == 2 || a.streamwise_open) && a.inlet_bc == AERO_INLET_VELOCITY) {
     f |= FEAT_INFLOW_FIELD;
+    if (a.inflow_field == 2) f |= FEAT_INFLOW_SEM;
     L->inflow_ring = a.inflow_ring > 0 ? a.inflow_ring : 64;
   }
   if (a.recycling) {
@@ -697,7 +704,8 @@ int aero_set_geometry(AeroLattice *L, const uint8_t *solid, const int32_t *links
   y.g[1] = take(L->Qg ? rb * L->Qg * L->cs : 0);
   y.U = take((L->feat & FEAT_LES) ? rb * 3 * L->cs : 0);
   y.cs_cell = take(L->cs_cell.empty() ? 0 : rb * L->cs);
-  y.inflow = take((L->feat & FEAT_INFLOW_FIELD) ? rb * (uint64_t)L->inflow_ring * (a.dims - 1) * L->prev_plane : 0);
+  y.inflow = take((L->feat & FEAT_INFLOW_FIELD) ? rb * (uint64_t)L->inflow_ring * inflow_components(L) * L->prev_plane
+                                                 : 0);
   y.recycle = take((L->feat & FEAT_RECYCLE) ? 8 * (uint64_t)(L->recycle_blocks + 2) : 0);
   y.hist = take(8 * 12 * (uint64_t)L->hist_cap);
   y.prof_out = take(24 * (uint64_t)L->nprof);
@@ -917,7 +925,7 @@ int aero_set_inflow(AeroLattice *L, const double *fields, int64_t first, int64_t
   if (n == 0) return AERO_OK;
   CUDA_TRY(cudaSetDevice(L->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int64_t per = (int64_t)(L->prm.dims - 1) * L->prev_plane;  // values per step
+  const int64_t per = (int64_t)inflow_components(L) * L->prev_plane;  // values per step
   const size_t rb = is_f64(L) ? 8 : 4;
   std::vector<char> host((size_t)(per * n) * rb);
   for (int64_t k = 0; k < per * n; k++) {

@@ -129,10 +129,33 @@ __device__ __forceinline__ void inlet_velocity(const StepParams<Real> &p, Real (
 // 3D boundary3d.py:71-93, as the synthetic inflow calls them
 // (solver.py:386-392, solver3d.py:436-445).  Unlike the uniform inlet these
 // carry no transverse correction from the incoming populations.
+// With FEAT_INFLOW_SEM (3D) the slot holds the SEM fluctuations (u', v', w')
+// and the inlet is apply_inlet_sem_3d (boundary3d.py:96-137): ux = u0 + u',
+// the uniform inlet's transverse corrections minus rho (v', w').
 template <class L, class Real>
 __device__ __forceinline__ void inlet_velocity_field(const StepParams<Real> &p, Real (&d)[L::Q], int y, int z,
                                                      int64_t step_now) {
   const int64_t plane = (int64_t)p.nz * p.ny;
+  if constexpr (L::DIMS == 3) {
+    if (p.feat & FEAT_INFLOW_SEM) {
+      const Real *slot = p.inflow + (step_now % p.inflow_ring) * 3 * plane;
+      const int64_t r = (int64_t)z * p.ny + y;
+      const Real ux = p.u0 + slot[r];
+      const Real den = Real(1) - ux > Real(1e-10) ? Real(1) - ux : Real(1e-10);
+      const Real Fm = d[2] + d[8] + d[10] + d[12] + d[14];
+      const Real Fn = d[0] + d[3] + d[4] + d[5] + d[6] + d[15] + d[16] + d[17] + d[18];
+      const Real rho_in = (Real(1) + Real(2) * Fm + Fn) / den;
+      const Real cy = (d[3] - d[4] + d[15] - d[16] + d[17] - d[18]) - rho_in * slot[plane + r];
+      const Real cz = (d[5] - d[6] + d[15] + d[16] - d[17] - d[18]) - rho_in * slot[2 * plane + r];
+      const Real r6 = Real(1.0 / 6.0) * rho_in * ux;
+      d[1] = d[2] + Real(1.0 / 3.0) * rho_in * ux;
+      d[7] = d[10] + r6 - Real(0.5) * cy;
+      d[9] = d[8] + r6 + Real(0.5) * cy;
+      d[11] = d[14] + r6 - Real(0.5) * cz;
+      d[13] = d[12] + r6 + Real(0.5) * cz;
+      return;
+    }
+  }
   const Real *slot = p.inflow + (step_now % p.inflow_ring) * (L::DIMS - 1) * plane;
   const int64_t r = (int64_t)z * p.ny + y;
   const Real ux = p.u0;

@@ -25,6 +25,7 @@ enum Feature : uint32_t {
   FEAT_OBSTACLE_BB = 1u << 10,    // obstacle bounce-back active (links present)
   FEAT_INFLOW_FIELD = 1u << 11,   // velocity inlet from per-step transverse fields (synthetic inflow)
   FEAT_RECYCLE = 1u << 12,        // 3D recycling inlet (rescaled equilibrium of plane nx-2)
+  FEAT_INFLOW_SEM = 1u << 13,     // with FEAT_INFLOW_FIELD: SEM fluctuations (u', v', w') per step
 };
 
 // Per-cell flag byte.
@@ -93,7 +94,7 @@ struct StepParams {
   const Real *U;        // LES velocities (3, cells) of the current state
   Real *Uw;             // LES velocity side output (written by the moments pass)
   const Real *cs_cell;  // per-cell LES constant (van Driest), optional
-  const Real *inflow;   // inflow ring: inflow_ring steps x (dims-1) x (nz*ny) transverse velocities
+  const Real *inflow;   // inflow ring: inflow_ring steps x components x (nz*ny) inlet velocities
   int32_t inflow_ring;
   double *recycle_partial;  // per k_recycle_mean block: sum of ux over its cells
   double *recycle_mean;     // mean ux of the recycle plane of the current step

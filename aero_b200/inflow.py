@@ -58,3 +58,84 @@ class SyntheticInflow:
         for k in range(int(n)):
             out[k] = self._next().reshape(self.dims - 1, -1)
         return out
+
+
+class SEMInflow:
+    """Synthetic-eddy inlet fluctuations, step by step.
+
+    Restates the reference's SEMInlet (aero/lbm/sem_inlet.py:15-136, after
+    Jarrin et al. 2006) with its random stream: N eddies with random
+    positions in a box of half-width 3 sigma around the inlet plane and
+    random signs per component, advected by u0 per step and re-drawn when
+    they leave; the fluctuations are sums of tent kernels
+    max(0, 1 - r / sigma) / sqrt(N) at the plane's cell centres; (v, w) are
+    made divergence-free in the plane by a Fourier projection (Nyquist modes
+    removed first); u, and (v, w) jointly, are rescaled to RMS Tu u0.  The
+    solver calls step() then fluctuation() once per time step
+    (solver3d.py:433-438); the reference constructs it without a seed, so
+    the stream starts from default_rng(0)."""
+
+    def __init__(self, ny: int, nz: int, u0: float, Tu: float, L_int: float, N: int, seed: int = 0):
+        self.ny, self.nz = int(ny), int(nz)
+        self.u0, self.Tu, self.sigma, self.N = float(u0), float(Tu), float(L_int), int(N)
+        self.half = 3.0 * self.sigma
+        self.rng = np.random.default_rng(seed)
+        self.x = self.rng.uniform(-self.half, self.half, self.N)
+        self.y = self.rng.uniform(0.0, float(self.ny), self.N)
+        self.z = self.rng.uniform(0.0, float(self.nz), self.N)
+        self.sign = self.rng.choice(np.array([-1.0, 1.0]), size=(3, self.N)).astype(np.float64)
+
+    def _advect(self):
+        self.x += self.u0
+        out = self.x > self.half
+        k = int(np.sum(out))
+        if k > 0:
+            self.x[out] = -self.half
+            self.y[out] = self.rng.uniform(0.0, float(self.ny), k)
+            self.z[out] = self.rng.uniform(0.0, float(self.nz), k)
+            self.sign[:, out] = self.rng.choice(np.array([-1.0, 1.0]), size=(3, k)).astype(np.float64)
+
+    def _fluctuation(self) -> np.ndarray:
+        shape = (self.nz, self.ny)
+        if self.Tu <= 0.0 or self.sigma <= 0.0 or self.N == 0:
+            return np.zeros((3,) + shape)
+        zc = np.arange(self.nz, dtype=np.float64) + 0.5
+        yc = np.arange(self.ny, dtype=np.float64) + 0.5
+        Z, Y = np.meshgrid(zc, yc, indexing="ij")
+        r = np.sqrt(self.x[:, None, None] ** 2 + (Y[None] - self.y[:, None, None]) ** 2
+                    + (Z[None] - self.z[:, None, None]) ** 2)
+        tent = np.maximum(0.0, 1.0 - r / self.sigma)
+        norm = 1.0 / np.sqrt(float(self.N))
+        raw = [norm * (self.sign[c, :, None, None] * tent).sum(axis=0) for c in range(3)]
+        vh, wh = np.fft.fft2(raw[1]), np.fft.fft2(raw[2])
+        if self.nz % 2 == 0:
+            vh[self.nz // 2, :] = 0.0
+            wh[self.nz // 2, :] = 0.0
+        if self.ny % 2 == 0:
+            vh[:, self.ny // 2] = 0.0
+            wh[:, self.ny // 2] = 0.0
+        kz = (np.fft.fftfreq(self.nz) * 2.0 * np.pi)[:, None]
+        ky = (np.fft.fftfreq(self.ny) * 2.0 * np.pi)[None, :]
+        k2 = kz ** 2 + ky ** 2
+        k2[0, 0] = 1.0
+        div = ky * vh + kz * wh
+        vh -= ky / k2 * div
+        wh -= kz / k2 * div
+        v, w = np.real(np.fft.ifft2(vh)), np.real(np.fft.ifft2(wh))
+        target = self.Tu * self.u0
+        su = float(np.std(raw[0]))
+        svw = float(np.sqrt(np.mean(v ** 2 + w ** 2) / 2.0))
+        u = raw[0] * (target / su) if su > 1e-14 else np.zeros(shape)
+        if svw > 1e-14:
+            v, w = v * (target / svw), w * (target / svw)
+        else:
+            v, w = np.zeros(shape), np.zeros(shape)
+        return np.stack([u, v, w])
+
+    def fields(self, n: int) -> np.ndarray:
+        """The next n steps' fluctuations: (n, 3, nz*ny) doubles (u', v', w'), (z, y) order."""
+        out = np.empty((int(n), 3, self.nz * self.ny), dtype=np.float64)
+        for k in range(int(n)):
+            self._advect()
+            out[k] = self._fluctuation().reshape(3, -1)
+        return out

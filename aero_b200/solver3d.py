@@ -5,9 +5,8 @@ Drop-in for the reference ``aero.lbm.solver3d.Solver3D``
 ``_step()`` returning (Cd, Cl_y, Cl_z), ``run()`` with the same result dict,
 host-visible ``f`` / ``g`` / ``_f_outlet_prev`` and .npz checkpoints.  Extra
 options as for the 2D Solver (``precision``, ``scalar_lattice`` with
-"reduced" = D3Q7, ``device``, ``hist_capacity``).  Streamwise "recycling"
-and synthetic inflow run in the engine; the SEM inlet is not part of it and
-raises NotImplementedError.
+"reduced" = D3Q7, ``device``, ``hist_capacity``).  Streamwise "recycling",
+synthetic inflow and the SEM inlet run in the engine.
 """
 
 from __future__ import annotations
@@ -42,10 +41,8 @@ class Solver3D(LatticeSolverBase):
         if streamwise_bc not in ("open", "periodic", "recycling"):
             raise ValueError(
                 f"Unknown streamwise_bc '{streamwise_bc}'. Choose 'open', 'periodic', or 'recycling'.")
-        if sem_inlet:
-            raise NotImplementedError("sem_inlet is not part of the b200 engine yet")
         self.Nz, self.Ny, self.Nx = int(Nz), int(Ny), int(Nx)
-        self.sem_inlet = False
+        self.sem_inlet = bool(sem_inlet)
         self._setup(
             shape=(self.Nz, self.Ny, self.Nx), solid=solid, omega=omega, u0=u0, D=D, rho0=rho0,
             wall_bc=wall_bc, inlet_bc=inlet_bc, outlet_bc=outlet_bc, streamwise_bc=streamwise_bc,
@@ -56,7 +53,8 @@ class Solver3D(LatticeSolverBase):
             van_driest_A=van_driest_A, body_force=(body_force_x, body_force_y, body_force_z),
             wall_velocity_top=wall_velocity_top, wall_velocity_bottom=wall_velocity_bottom,
             synthetic_inflow=synthetic_inflow, synthetic_inflow_intensity=synthetic_inflow_intensity,
-            synthetic_inflow_seed=synthetic_inflow_seed, thermal=thermal, T_hot=T_hot,
+            synthetic_inflow_seed=synthetic_inflow_seed, sem=(float(sem_Tu), float(sem_L_int), int(sem_N))
+            if sem_inlet else None, thermal=thermal, T_hot=T_hot,
             T_cold=T_cold, alpha_T=alpha_T, buoyancy=buoyancy, g_gravity=g_gravity, beta=beta,
             T_ref=T_ref, precision=precision, scalar_lattice=scalar_lattice, device=device,
             hist_capacity=hist_capacity)

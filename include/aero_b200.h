@@ -80,8 +80,9 @@ typedef struct AeroParams {
   double center[3];         /* moment reference point (x, y, z): mean solid cell */
   int32_t recycling;        /* 3D streamwise "recycling": the inlet plane is the rescaled
                                equilibrium of plane x = nx-2 (needs streamwise_open = 0) */
-  int32_t inflow_field;     /* velocity inlet driven by per-step transverse velocity fields
-                               (synthetic inflow), uploaded with aero_set_inflow */
+  int32_t inflow_field;     /* velocity inlet driven by per-step fields uploaded with
+                               aero_set_inflow: 1 = synthetic inflow (transverse velocities),
+                               2 = SEM fluctuations (u', v', w'; 3D) */
   int32_t inflow_ring;      /* steps of inflow fields held on the device (0 = 64) */
 } AeroParams;
 
@@ -168,13 +169,14 @@ AERO_API int aero_step_plan(const AeroLattice *lat, int32_t *tiled, int32_t *til
 AERO_API int aero_set_step_kernel(AeroLattice *lat, int32_t kernel);
 AERO_API int aero_get_step_kernel(const AeroLattice *lat, int32_t *kernel);
 
-/* Transverse inlet velocities of steps first_step .. first_step+n_steps-1
- * for a lattice with inflow_field set: `fields` (host) holds n_steps blocks
- * of (dims-1) planes of nz*ny doubles, (z, y) order: uy in 2D; uy then uz in
- * 3D.  The inlet of such a step is the Zou-He velocity-field inlet of
+/* Inlet fields of steps first_step .. first_step+n_steps-1 for a lattice
+ * with inflow_field set: `fields` (host) holds n_steps blocks of planes of
+ * nz*ny doubles, (z, y) order.  Synthetic inflow: uy in 2D, uy then uz in
+ * 3D; the inlet is the Zou-He velocity-field inlet of
  * apply_inlet_velocity_field(_3d) (boundary.py:48-65, boundary3d.py:71-93)
  * with ux = u0, as the reference's synthetic inflow calls it
- * (solver.py:386-392, solver3d.py:436-445).  The device holds inflow_ring
+ * (solver.py:386-392, solver3d.py:436-445).  SEM: u', v', w'; the inlet is
+ * apply_inlet_sem_3d (boundary3d.py:96-137, solver3d.py:433-438).  The device holds inflow_ring
  * steps: first_step must not precede the next step to run, and the fields
  * must not reach beyond inflow_ring steps past it; aero_step refuses steps
  * whose fields are missing.  Synchronous. */

@@ -442,7 +442,28 @@ static void inlet_outlet_3d(OracleLattice *s, double *f) {
     return;
   }
   if (s->streamwise_bc != ORACLE_STREAM_OPEN) return;
-  if (s->inlet_bc == ORACLE_INLET_VELOCITY && s->inflow) {
+  if (s->inlet_bc == ORACLE_INLET_VELOCITY && s->sem) {
+    /* apply_inlet_sem_3d, boundary3d.py:96-137 */
+    const int64_t plane = (int64_t)nz * ny;
+    for (int z = 0; z < nz; z++)
+      for (int y = 0; y < ny; y++) {
+#define F(i) f[IDX(i, z, y, 0)]
+        const int64_t r = (int64_t)z * ny + y;
+        double ux = u0 + s->sem[r];
+        double den = 1.0 - ux > 1e-10 ? 1.0 - ux : 1e-10;
+        double Fm = F(2) + F(8) + F(10) + F(12) + F(14);
+        double Fn = F(0) + F(3) + F(4) + F(5) + F(6) + F(15) + F(16) + F(17) + F(18);
+        double rho_in = (2.0 * Fm + Fn) / den;
+        double cy = F(3) - F(4) + F(15) - F(16) + F(17) - F(18) - rho_in * s->sem[plane + r];
+        double cz = F(5) - F(6) + F(15) + F(16) - F(17) - F(18) - rho_in * s->sem[2 * plane + r];
+        F(1) = F(2) + (1.0 / 3.0) * rho_in * ux;
+        F(7) = F(10) + (1.0 / 6.0) * rho_in * ux - 0.5 * cy;
+        F(9) = F(8) + (1.0 / 6.0) * rho_in * ux + 0.5 * cy;
+        F(11) = F(14) + (1.0 / 6.0) * rho_in * ux - 0.5 * cz;
+        F(13) = F(12) + (1.0 / 6.0) * rho_in * ux + 0.5 * cz;
+#undef F
+      }
+  } else if (s->inlet_bc == ORACLE_INLET_VELOCITY && s->inflow) {
     /* per-cell field inlet, boundary3d.py:71-93, ux = u0 (solver3d.py:436-445) */
     const int64_t plane = (int64_t)nz * ny;
     for (int z = 0; z < nz; z++)

@@ -47,6 +47,9 @@ typedef struct OracleLattice {
   /* synthetic inflow of the step about to run: (dims-1, nz, ny) transverse
    * inlet velocities (uy; 3D then uz), or NULL for the uniform inlet */
   const double *inflow;
+  /* SEM fluctuations of the step about to run: (3, nz, ny) u', v', w'
+   * (3D), or NULL; takes precedence over `inflow` */
+  const double *sem;
 } OracleLattice;
 
 int oracle_step(OracleLattice *s, double *out_forces, double *out_profile);

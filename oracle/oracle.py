@@ -132,7 +132,7 @@ class _OracleLattice(ctypes.Structure):
     ] + [("center", ctypes.c_double * 3)] + [
         (n, ctypes.c_void_p) for n in (
             "f", "g", "f_outlet_prev", "solid", "phi", "links", "q_vals", "mrt_M", "mrt_Minv",
-            "mrt_s", "work_a", "work_b", "work_om", "work_g", "inflow")]
+            "mrt_s", "work_a", "work_b", "work_om", "work_g", "inflow", "sem")]
 
 
 def build(force: bool = False) -> pathlib.Path:
@@ -188,7 +188,8 @@ class OracleSolver:
                  buoyancy: bool = False, g_gravity: float = 0.0, beta: float = 1e-3,
                  T_ref: float = 0.5, scalar_lattice: str = "full", threads: Optional[int] = None,
                  synthetic_inflow: bool = False, synthetic_inflow_intensity: float = 0.03,
-                 synthetic_inflow_seed: int = 12345, **_ignored):
+                 synthetic_inflow_seed: int = 12345, sem_inlet: bool = False, sem_Tu: float = 0.05,
+                 sem_L_int: float = 10.0, sem_N: int = 200, **_ignored):
         solid = np.ascontiguousarray(solid, dtype=np.bool_)
         self.dims = solid.ndim
         if self.dims == 2:
@@ -255,6 +256,19 @@ class OracleSolver:
         plane = (self.ny,) if self.dims == 2 else (self.nz, self.ny)
         self._inflow_u = [np.zeros(plane) for _ in range(self.dims - 1)]
         self._inflow_buf = None
+        # SEM inlet (sem_inlet.py:15-136, used first when enabled, solver3d.py:433-438);
+        # the reference builds it without a seed: default_rng(0)
+        self._sem_on = bool(sem_inlet) and self.dims == 3 and inlet_bc == "velocity" and streamwise_bc == "open"
+        if self._sem_on:
+            self._inflow_on = False
+            g = np.random.default_rng(0)
+            self._sem = dict(Tu=float(sem_Tu), sig=float(sem_L_int), N=int(sem_N), rng=g)
+            r = 3.0 * float(sem_L_int)
+            n = int(sem_N)
+            self._sem["x"] = g.uniform(-r, r, n)
+            self._sem["y"] = g.uniform(0.0, float(self.ny), n)
+            self._sem["z"] = g.uniform(0.0, float(self.nz), n)
+            self._sem["eps"] = g.choice(np.array([-1.0, 1.0]), size=(3, n)).astype(np.float64)
         s.sponge_thickness = int(sponge_thickness)
         s.thermal = int(bool(thermal))
         s.buoyancy = int(bool(buoyancy))
@@ -326,9 +340,53 @@ class OracleSolver:
             self._inflow_u = new
         return np.ascontiguousarray(np.stack(self._inflow_u), dtype=np.float64)
 
+    def _next_sem(self):
+        """Advance the eddies one step and return (u', v', w') as (3, nz, ny)."""
+        S = self._sem
+        g, sig, N, r = S["rng"], S["sig"], S["N"], 3.0 * S["sig"]
+        S["x"] = S["x"] + self.u0
+        out = S["x"] > r
+        k = int(out.sum())
+        if k:
+            S["x"][out] = -r
+            S["y"][out] = g.uniform(0.0, float(self.ny), k)
+            S["z"][out] = g.uniform(0.0, float(self.nz), k)
+            S["eps"][:, out] = g.choice(np.array([-1.0, 1.0]), size=(3, k)).astype(np.float64)
+        shape = (self.nz, self.ny)
+        if S["Tu"] <= 0.0 or sig <= 0.0 or N == 0:
+            return np.zeros((3,) + shape)
+        zz, yy = np.meshgrid(np.arange(self.nz) + 0.5, np.arange(self.ny) + 0.5, indexing="ij")
+        dist = np.sqrt(S["x"][:, None, None] ** 2 + (yy[None] - S["y"][:, None, None]) ** 2
+                       + (zz[None] - S["z"][:, None, None]) ** 2)
+        tent = np.maximum(0.0, 1.0 - dist / sig)
+        comp = [(S["eps"][c][:, None, None] * tent).sum(axis=0) / np.sqrt(float(N)) for c in range(3)]
+        vh, wh = np.fft.fft2(comp[1]), np.fft.fft2(comp[2])
+        if self.nz % 2 == 0:
+            vh[self.nz // 2, :] = 0.0
+            wh[self.nz // 2, :] = 0.0
+        if self.ny % 2 == 0:
+            vh[:, self.ny // 2] = 0.0
+            wh[:, self.ny // 2] = 0.0
+        kz = (np.fft.fftfreq(self.nz) * 2 * np.pi)[:, None]
+        ky = (np.fft.fftfreq(self.ny) * 2 * np.pi)[None, :]
+        k2 = kz ** 2 + ky ** 2
+        k2[0, 0] = 1.0
+        dv = ky * vh + kz * wh
+        v = np.real(np.fft.ifft2(vh - ky / k2 * dv))
+        w = np.real(np.fft.ifft2(wh - kz / k2 * dv))
+        t = S["Tu"] * self.u0
+        su = float(np.std(comp[0]))
+        svw = float(np.sqrt(np.mean(v ** 2 + w ** 2) / 2.0))
+        u = comp[0] * (t / su) if su > 1e-14 else np.zeros(shape)
+        v, w = ((v * (t / svw), w * (t / svw)) if svw > 1e-14 else (np.zeros(shape), np.zeros(shape)))
+        return np.stack([u, v, w])
+
     def step_raw(self):
         """One step; returns (raw 12-vector of forces/moments, profile (nprof, 3))."""
         self._bind()
+        if self._sem_on:
+            self._sem_buf = np.ascontiguousarray(self._next_sem(), dtype=np.float64)
+            self._s_struct.sem = self._sem_buf.ctypes.data
         if self._inflow_on:
             self._inflow_buf = self._next_inflow()
             self._s_struct.inflow = self._inflow_buf.ctypes.data

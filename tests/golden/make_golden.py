@@ -101,6 +101,9 @@ CASES_3D = [
     ("c3d_bgk_synthetic_inflow", ("sph", 3.0, 0.3, 0.5, 0.5),
      dict(collision="bgk", wall_bc="slip", outlet_bc="convective", synthetic_inflow=True,
           synthetic_inflow_intensity=0.05, synthetic_inflow_seed=91), 12),
+    ("c3d_bgk_sem_inlet", ("sph", 3.0, 0.3, 0.5, 0.5),
+     dict(collision="bgk", wall_bc="slip", outlet_bc="convective", sem_inlet=True, sem_Tu=0.05,
+          sem_L_int=3.0, sem_N=40), 12),
     ("c3d_mrt_recycling_sponge_bodyforce", ("sph", 3.0, 0.3, 0.5, 0.5),
      dict(collision="mrt", wall_bc="noslip", streamwise_bc="recycling", sponge_thickness=4,
           body_force_x=1e-5, bouzidi=True), 12),
