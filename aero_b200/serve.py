@@ -134,7 +134,8 @@ class Server:
     """Continuous batching of wind-tunnel cases on one device."""
 
     def __init__(self, hbm_cap: float = 150e9, max_members: int = 256, chunk: int = 200,
-                 window: int = 2000, tol: float = 1e-3, device=None, hist_capacity: int = 4096):
+                 window: int = 2000, tol: float = 1e-3, device=None, hist_capacity: int = 4096,
+                 on_admit=None, admit_per_round: int = 8):
         if window > hist_capacity:
             raise ValueError("the convergence window must fit the force history ring")
         self.hbm_cap = float(hbm_cap)
@@ -146,6 +147,12 @@ class Server:
         self.hist_capacity = int(hist_capacity)
         self.batch = Batch(max_members=max_members, device=device)
         self.stats: Dict[str, float] = {}
+        # optional callback(case, solver) run before a new solver joins the
+        # batch, e.g. to set a state of its own
+        self.on_admit = on_admit
+        # requests set up per round: the rest wait for the next round, so a
+        # burst of arrivals does not hold the GPU idle behind serial set-up
+        self.admit_per_round = max(int(admit_per_round), 1)
 
     def run(self, cases: List[Case], clock=time.perf_counter, sleep=time.sleep) -> List[Result]:
         """Serves the cases (arrival times relative to the call) and returns
@@ -178,7 +185,8 @@ class Server:
                 queue.append(pending.pop(0))
             # admission, first come first served, by device footprint
             joining = []
-            while queue and len(active) + len(joining) < self.max_members:
+            while (queue and len(active) + len(joining) < self.max_members
+                   and len(joining) < self.admit_per_round):
                 c = queue[0]
                 need = footprint(c, self.hist_capacity)
                 if need > self.hbm_cap:
@@ -193,6 +201,9 @@ class Server:
                 ts = clock()
                 with torch.cuda.stream(side):
                     s = make_solver(c, self.device, self.hist_capacity)
+                    if self.on_admit is not None:
+                        self.on_admit(c, s)
+                        s._flush_host_state()
                 setup_s += clock() - ts
                 used += need
                 joining.append((c, s, clock() - t0, need))
@@ -285,12 +296,14 @@ def trace(n: int, seed: int = 0, rate: float = 1.0, frac_2d: float = 0.7, nx2=(2
     (ny = nx/2) or 3D (ny = nz = nx/2) lattices, geometry sized a fraction
     of ny, Re log-uniform, collision drawn uniformly, Smagorinsky above
     `les_above_re`, u0 = max(0.05, the smallest value giving tau >= tau_min),
-    capped at u0_max (Re is then lowered to keep tau >= tau_min)."""
-    rng = np.random.default_rng(seed)
+    capped at u0_max (Re is then lowered to keep tau >= tau_min).  Arrival
+    times come from a stream of their own, so the cases of a trace do not
+    depend on `rate`."""
+    rng, arrivals = (np.random.default_rng(s) for s in np.random.SeedSequence(seed).spawn(2))
     t = 0.0
     out = []
     for k in range(n):
-        t += float(rng.exponential(1.0 / rate)) if rate > 0 else 0.0
+        t += float(arrivals.exponential(1.0 / rate)) if rate > 0 else 0.0
         dims = 2 if rng.random() < frac_2d else 3
         lo, hi = (nx2 if dims == 2 else nx3)
         step = step2 if dims == 2 else step3

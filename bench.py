@@ -426,7 +426,7 @@ def main():
                          "rows staged in shared memory by bulk async copies")
     ap.add_argument("--batch-every", type=int, default=1,
                     help="batch96: keep every k-th case (a smaller batch for profiling captures)")
-    ap.add_argument("--serve-requests", type=int, default=64)
+    ap.add_argument("--serve-requests", type=int, default=128)
     ap.add_argument("--serve-chunk", type=int, default=250)
     ap.add_argument("--serve-window", type=int, default=1000)
     ap.add_argument("--serve-tol", type=float, default=1e-3)

@@ -31,6 +31,14 @@ def test_trace_is_seeded_and_respects_the_rules():
         assert c.collision in ("bgk", "trt", "mrt")
 
 
+def test_trace_cases_do_not_depend_on_the_arrival_rate():
+    a = serve.trace(50, seed=9, rate=0.0)
+    b = serve.trace(50, seed=9, rate=7.0)
+    strip = lambda c: {k: v for k, v in serve.case_dict(c).items() if k != "arrival"}
+    assert [strip(c) for c in a] == [strip(c) for c in b]
+    assert all(c.arrival == 0.0 for c in a) and b[-1].arrival > 0.0
+
+
 def test_footprint_bounds_the_workspace():
     """footprint() is at least the workspace aero_workspace_size reports
     (computed through the C ABI, no GPU needed)."""
@@ -156,3 +164,29 @@ def test_oversized_request_is_rejected_without_gpu_work(monkeypatch):
     srv = serve.Server(hbm_cap=1e6, max_members=4, chunk=10, window=10)
     (r,) = srv.run([serve.Case(0, 3, 128, 64, 64)])
     assert r.status == "rejected" and r.steps == 0
+
+
+@pytest.mark.gpu
+def test_diverged_request_is_retired_and_others_finish():
+    """A request whose state goes bad (a NaN injected into its initial state
+    on the host) is retired as 'diverged' after its first round, from the
+    device status word; the other requests in the same batch run to their
+    normal end with the same results as without the faulty one."""
+    def poison(case, solver):
+        if case.id == 1:
+            f = solver.f
+            f[:, 3, 5] = np.nan
+            solver.f = f
+
+    srv = serve.Server(hbm_cap=8e9, max_members=8, on_admit=poison, **KW)
+    res = {r.id: r for r in srv.run(_small_cases())}
+    srv.close()
+    clean = serve.Server(hbm_cap=8e9, max_members=8, **KW)
+    ref = {r.id: r for r in clean.run(_small_cases())}
+    clean.close()
+    assert res[1].status == "diverged" and res[1].steps == KW["chunk"]
+    for k in ref:
+        if k == 1:
+            continue
+        assert (res[k].status, res[k].steps) == (ref[k].status, ref[k].steps)
+        assert res[k].cd_mean == ref[k].cd_mean or (math.isnan(res[k].cd_mean) and math.isnan(ref[k].cd_mean))
