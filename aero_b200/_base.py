@@ -30,6 +30,18 @@ PRECISIONS = tuple(_lib.STORE)
 _PRISTINE_LIMIT = 1 << 28  # elements; above this a handed-out array is always re-uploaded
 
 
+def _open_checkpoint(path: str):
+    """np.load of a checkpoint, with a truncated or corrupt file reported as
+    ValueError (before anything touches the GPU)."""
+    import zipfile
+    import zlib
+    try:
+        with np.load(path, allow_pickle=False) as npz:
+            return {k: npz[k] for k in npz.files}
+    except (OSError, ValueError, EOFError, KeyError, zipfile.BadZipFile, zlib.error) as e:
+        raise ValueError(f"corrupt or unreadable checkpoint {path}: {e}") from e
+
+
 class LatticeSolverBase:
     dims = 2
 
@@ -338,7 +350,13 @@ class LatticeSolverBase:
         np.savez_compressed(path, **kwargs)
 
     def load_checkpoint(self, path: str) -> None:
-        data = np.load(path, allow_pickle=False)
+        data = _open_checkpoint(path)
+        for key in ("f", "f_outlet_prev", "step_count"):
+            if key not in data:
+                raise ValueError(f"checkpoint {path} has no '{key}' entry")
+        if tuple(data["f"].shape) != (self.Q,) + tuple(self.solid.shape):
+            raise ValueError(f"checkpoint {path}: f has shape {tuple(data['f'].shape)}, "
+                             f"the solver needs {(self.Q,) + tuple(self.solid.shape)}")
         for k in self._history_keys():
             if k in data:
                 setattr(self, k, list(data[k]))
@@ -355,8 +373,14 @@ class LatticeSolverBase:
 
     @classmethod
     def from_checkpoint(cls, path: str, backend: Optional[str] = None, **overrides):
-        data = np.load(path, allow_pickle=False)
-        params = json.loads(str(data["params_json"]))
+        data = _open_checkpoint(path)
+        for key in ("params_json", "solid"):
+            if key not in data:
+                raise ValueError(f"checkpoint {path} has no '{key}' entry")
+        try:
+            params = json.loads(str(data["params_json"]))
+        except json.JSONDecodeError as e:
+            raise ValueError(f"checkpoint {path}: unreadable params_json ({e})") from e
         params["backend"] = "b200"
         params.update(overrides)
         solid = data["solid"]

@@ -139,6 +139,7 @@ struct AeroLattice {
   int step_shape = 0;
   bool tiled = false;
   int tile_blocks = 0, tile_rows = 0, tiles_per_plane = 0, ntiles = 0;
+  uint32_t tile_extra_tx = 0;  // AERO_B200_TEST_STALL_TILES=1 at bind: stages never complete
   // optional per-kernel event timing (eager launches only)
   bool timing = false;
   std::vector<cudaEvent_t> ev;  // 4 events per timed step
@@ -186,6 +187,7 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   p.sponge_start = std::max(a.nx - a.sponge_thickness, 0);
   p.tile_rows = L->tile_rows;
   p.batch_rows = L->ncells < kBatchSmallCells ? 1 : kBatchRows;
+  p.tile_extra_tx = L->tile_extra_tx;
   p.tiles_per_plane = L->tiles_per_plane;
   p.ntiles = L->ntiles;
   p.P = ws + L->lay.P[cur];
@@ -768,6 +770,11 @@ int aero_bind_workspace(AeroLattice *L, void *dptr, uint64_t bytes, void *stream
   CUDA_TRY(cudaStreamSynchronize(st));
   const int rc = is_f64(L) ? plan_tiles<double>(L) : plan_tiles<float>(L);
   if (rc != AERO_OK) return rc;
+  // Test of the bounded waits of the row-tiled kernel: every stage announces
+  // 16 bytes more than its copies deliver, so no stage completes; the waits
+  // give up after their limit, raise status bit 1 and the kernel returns.
+  const char *stall = std::getenv("AERO_B200_TEST_STALL_TILES");
+  L->tile_extra_tx = (stall && stall[0] == '1') ? 16u : 0u;
   L->bound = true;
   return AERO_OK;
 }

@@ -1136,7 +1136,7 @@ __device__ __forceinline__ void issue_tile(const StepParams<Real> &p, int tile, 
   const uint32_t fbytes = (uint32_t)(((c0 + (int64_t)t.rows * p.nx + 15) & ~(int64_t)15) - fa);
   const bool conv = (p.feat & FEAT_OPEN) && p.outlet == OUTLET_CONVECTIVE;
   const uint32_t pbytes = conv ? (uint32_t)t.rows * (uint32_t)(L::QP * sizeof(Real)) : 0u;
-  mbar_arrive_expect_tx(bar, (uint32_t)L::Q * (uint32_t)t.rows * row_bytes + fbytes + pbytes);
+  mbar_arrive_expect_tx(bar, (uint32_t)L::Q * (uint32_t)t.rows * row_bytes + fbytes + pbytes + p.tile_extra_tx);
   const char *P = static_cast<const char *>(p.P);
   S *slab0 = reinterpret_cast<S *>(stage);
   static_for<L::Q>([&](auto ic) {

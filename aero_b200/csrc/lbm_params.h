@@ -75,6 +75,8 @@ struct StepParams {
   // row tiles of the tiled step kernel: tile_rows y rows of one z plane
   int32_t tile_rows, tiles_per_plane, ntiles;
   int32_t batch_rows;   // rows per block in the batched cell kernels
+  uint32_t tile_extra_tx;  // bytes announced on a tile stage beyond its copies (0; > 0 only to test
+                           // that the bounded stage waits give up)
 
   // populations (deviation from the rest weights, see Store<>)
   const void *P;        // current post-collision populations (read)

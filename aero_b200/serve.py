@@ -62,7 +62,7 @@ class Case:
 @dataclass
 class Result:
     id: int
-    status: str                 # converged | max_steps | diverged | rejected
+    status: str                 # converged | max_steps | diverged | rejected | cancelled
     steps: int
     cd_mean: float
     ratio: float
@@ -135,7 +135,7 @@ class Server:
 
     def __init__(self, hbm_cap: float = 150e9, max_members: int = 256, chunk: int = 200,
                  window: int = 2000, tol: float = 1e-3, device=None, hist_capacity: int = 4096,
-                 on_admit=None, admit_per_round: int = 8):
+                 on_admit=None, admit_per_round: int = 8, on_round=None):
         if window > hist_capacity:
             raise ValueError("the convergence window must fit the force history ring")
         self.hbm_cap = float(hbm_cap)
@@ -153,6 +153,14 @@ class Server:
         # requests set up per round: the rest wait for the next round, so a
         # burst of arrivals does not hold the GPU idle behind serial set-up
         self.admit_per_round = max(int(admit_per_round), 1)
+        # optional callback(server, round) after each round, e.g. to cancel requests
+        self.on_round = on_round
+        self.cancelled = set()
+
+    def cancel(self, case_id: int) -> None:
+        """Cancels a request: a waiting one is dropped, a running one leaves the
+        batch at the end of the current round; either reports 'cancelled'."""
+        self.cancelled.add(int(case_id))
 
     def run(self, cases: List[Case], clock=time.perf_counter, sleep=time.sleep) -> List[Result]:
         """Serves the cases (arrival times relative to the call) and returns
@@ -183,6 +191,11 @@ class Server:
             now = clock() - t0
             while pending and pending[0].arrival <= now:
                 queue.append(pending.pop(0))
+            for lst in (pending, queue):
+                for c in [c for c in lst if c.id in self.cancelled]:
+                    lst.remove(c)
+                    results.append(Result(c.id, "cancelled", 0, math.nan, math.nan, c.arrival, now, now,
+                                          _cells(c), 0))
             # admission, first come first served, by device footprint
             joining = []
             while (queue and len(active) + len(joining) < self.max_members
@@ -217,7 +230,9 @@ class Server:
                 for (c, s, t_adm, need), row in zip(active, table):
                     steps = int(row[_F["steps"]])
                     status = int(row[_F["status"]])
-                    if status & STATUS_DIVERGED:
+                    if c.id in self.cancelled:
+                        verdict = "cancelled"
+                    elif status & STATUS_DIVERGED:
                         verdict = "diverged"
                     elif row[_F["converged"]] > 0.5:
                         verdict = "converged"
@@ -235,6 +250,8 @@ class Server:
             for j in joining:
                 self.batch.add(j[1])
                 active.append(j)
+            if self.on_round is not None and stepped:
+                self.on_round(self, rounds)
             if not active and not joining and pending and not queue:
                 sleep(max(0.0, pending[0].arrival - (clock() - t0)))
         torch.cuda.synchronize(self.batch.device)
@@ -334,7 +351,7 @@ def summarize(results: List[Result], wall_s: float) -> dict:
         "p50_latency_s": float(np.percentile(lat, 50)),
         "p99_latency_s": float(np.percentile(lat, 99)),
         "status": {k: sum(1 for r in results if r.status == k)
-                   for k in ("converged", "max_steps", "diverged", "rejected")},
+                   for k in ("converged", "max_steps", "diverged", "rejected", "cancelled")},
     }
 
 

@@ -172,3 +172,27 @@ def test_mrt_operator_matches_reference_basis(dims):
         B_ref = Minv @ np.diag(s) @ M
         np.testing.assert_allclose(A, A_ref, rtol=0, atol=1e-13)
         np.testing.assert_allclose(B, B_ref, rtol=0, atol=1e-13)
+
+
+def test_corrupt_checkpoint_is_rejected_before_gpu_work(tmp_path):
+    """A truncated or incomplete checkpoint raises ValueError when it is
+    opened, before any solver (or device memory) is created."""
+    from aero_b200.solver import Solver
+    from aero_b200.solver3d import Solver3D
+    good = tmp_path / "ok.npz"
+    np.savez(good, f=np.zeros((9, 4, 6)), f_outlet_prev=np.zeros((9, 4)), step_count=np.array(3),
+             solid=np.zeros((4, 6), bool), params_json=np.array('{"omega": 1.0}'))
+    raw = good.read_bytes()
+    trunc = tmp_path / "trunc.npz"
+    trunc.write_bytes(raw[: len(raw) // 2])
+    for cls in (Solver, Solver3D):
+        with pytest.raises(ValueError, match="corrupt or unreadable checkpoint"):
+            cls.from_checkpoint(str(trunc))
+    nokeys = tmp_path / "nokeys.npz"
+    np.savez(nokeys, f=np.zeros(3))
+    with pytest.raises(ValueError, match="no 'params_json' entry"):
+        Solver.from_checkpoint(str(nokeys))
+    badjson = tmp_path / "badjson.npz"
+    np.savez(badjson, solid=np.zeros((4, 6), bool), params_json=np.array("{not json"))
+    with pytest.raises(ValueError, match="unreadable params_json"):
+        Solver.from_checkpoint(str(badjson))

@@ -190,3 +190,28 @@ def test_diverged_request_is_retired_and_others_finish():
             continue
         assert (res[k].status, res[k].steps) == (ref[k].status, ref[k].steps)
         assert res[k].cd_mean == ref[k].cd_mean or (math.isnan(res[k].cd_mean) and math.isnan(ref[k].cd_mean))
+
+
+@pytest.mark.gpu
+def test_cancelled_requests_leave_and_others_finish():
+    """A running request cancelled after two rounds leaves the batch with
+    status 'cancelled'; a queued one is dropped before it starts; the rest
+    finish as they would without them."""
+    cs = _small_cases()
+    cs[4].arrival = 1e9  # never arrives before it is cancelled
+
+    def on_round(srv, k):
+        if k == 2:
+            srv.cancel(1)
+            srv.cancel(4)
+
+    srv = serve.Server(hbm_cap=8e9, max_members=8, on_round=on_round, **KW)
+    res = {r.id: r for r in srv.run(cs)}
+    srv.close()
+    assert res[1].status == "cancelled" and res[1].steps == 3 * KW["chunk"]
+    assert res[4].status == "cancelled" and res[4].steps == 0
+    clean = serve.Server(hbm_cap=8e9, max_members=8, **KW)
+    ref = {r.id: r for r in clean.run(_small_cases())}
+    clean.close()
+    for k in (0, 2, 3, 5):
+        assert (res[k].status, res[k].steps, res[k].cd_mean) == (ref[k].status, ref[k].steps, ref[k].cd_mean)
