@@ -190,13 +190,15 @@ class LatticeSolverBase:
         del f0, prev0, g0
         self._init_histories()
 
-    def _uniform_state_device(self, ux=None):
-        """Equilibrium populations for rho0 and velocity (ux, 0, 0) as device
-        tensors; ux defaults to u0 everywhere.  Also returns the matching
-        outlet column and the scalar at T_ref."""
+    def _uniform_state_device(self, ux=None, uy=None):
+        """Equilibrium populations for rho0 and velocity (ux, uy, 0) as device
+        tensors; ux defaults to u0 and uy to 0 everywhere.  Also returns the
+        matching outlet column and the scalar at T_ref."""
         import torch
         dev = self._engine.device
         shape = self.solid.shape
+        if ux is None and uy is not None:
+            ux = torch.full(tuple(shape), self.u0, dtype=torch.float64, device=dev)
         if ux is None:
             vec = feq(self.dims, np.array(self.rho0), np.array(self.u0), np.array(0.0),
                       np.array(0.0) if self.dims == 3 else None)
@@ -205,7 +207,7 @@ class LatticeSolverBase:
         else:
             rho = torch.full(tuple(shape), self.rho0, dtype=torch.float64, device=dev)
             zero = torch.zeros_like(rho)
-            f0 = feq(self.dims, rho, ux, zero, zero if self.dims == 3 else None, xp=torch)
+            f0 = feq(self.dims, rho, ux, zero if uy is None else uy, zero if self.dims == 3 else None, xp=torch)
         prev0 = f0[..., -1].contiguous()
         g0 = None
         if self.thermal:

@@ -11,15 +11,19 @@ stored in FP32 (``--precision``).  A "step" is one full solver step: the fused
 stream/BC/collide kernel plus the momentum-exchange force reduction.
 
 One JSON line on stdout (rank 0):
-  value   : whole-job MLUPS from CUDA events around K steps with the state
-            resident in HBM (two 2.5 GB population buffers, larger than L2,
-            so no flush is needed), max over ranks;
+  value   : whole-job MLUPS from CUDA events around K steps run as the
+            engine runs them (CUDA graphs), state resident in HBM (two 2.5 GB
+            population buffers, larger than L2, so no flush is needed), max
+            over ranks;
   e2e     : MLUPS through the public API, Solver3D.run(K), timed on the host,
             including the upload of the initial state from pinned host memory
             and the read-back of forces, stability plane and final fields;
   roofline: the fused step kernel's algorithmic bytes per launch
-            (2 Q bytes-per-population + 1 flag byte per cell) over its
-            average CUDA-event duration, against the measured HBM copy rate;
+            (2 Q bytes-per-population + 1 flag byte per cell, plus the scalar
+            lattice and the LES side pass where present) over its average
+            CUDA-event duration, measured in a separate phase of up to 200
+            steps with events around each kernel, against the measured HBM
+            copy rate;
   cpu_baseline: the FP64 oracle (C/OpenMP restatement of the reference step)
             on a bounded slab of the same workload, on this host's cores.
 
@@ -59,6 +63,12 @@ WORKLOADS = {
                     sponge_thickness=16, sponge_strength=0.1),
         u0=0.05, nu=0.0016, perturb=0.01,
         desc="half-size sphere512 (256x128x128, r8), for profiling captures"),
+    "channel400": dict(
+        dims=2, nx=400, ny=200, nz=1, shape=("cylinder", 20.0, 0.25, 0.5),
+        kwargs=dict(collision="bgk", wall_bc="noslip", outlet_bc="zerogradient", inlet_bc="velocity"),
+        u0=0.05, nu=0.02, perturb=0.0, perturb_uy=1e-4,
+        desc="D2Q9 BGK cylinder channel 400x200, r20 at (100,100), Re 100 (tau 0.56), no-slip walls, "
+             "zero-gradient outlet, uy seeded +-1e-4"),
     "box256": dict(
         dims=3, nx=256, ny=128, nz=128, shape=("box", 24.0, 24.0, 128.0, 76 / 256, 12 / 128, 0.5),
         kwargs=dict(collision="trt", trt_lambda=3 / 16, les=True, les_model="wale", les_cs=0.5,
@@ -101,8 +111,10 @@ def _peak_hbm():
 
 
 def _geometry(w):
-    from aero_b200 import Box, Sphere
+    from aero_b200 import Box, Cylinder, Sphere
     s = w["shape"]
+    if s[0] == "cylinder":
+        return Cylinder(radius=s[1], cx_frac=s[2], cy_frac=s[3])
     if s[0] == "sphere":
         g = Sphere(radius=s[1], cx_frac=s[2], cy_frac=s[3], cz_frac=s[4])
     else:
@@ -165,7 +177,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(mhz)}
 
 
-def cpu_oracle_sample(w, target_s=15.0, max_steps=50, nz_sample=32, threads=None):
+def cpu_oracle_sample(w, target_s=15.0, max_steps=None, nz_sample=32, threads=None):
     """Times the FP64 oracle on a slab (nz_sample planes) of the workload."""
     import numpy as np
     from oracle.oracle import OracleSolver
@@ -173,8 +185,9 @@ def cpu_oracle_sample(w, target_s=15.0, max_steps=50, nz_sample=32, threads=None
     os.environ["OMP_NUM_THREADS"] = str(threads)
     g = _geometry(w)
     nz = min(nz_sample, w["nz"])
-    solid = g.mark_solid(nz, w["ny"], w["nx"])
-    phi = g.sdf_field(nz, w["ny"], w["nx"])
+    shp = (w["ny"], w["nx"]) if w["dims"] == 2 else (nz, w["ny"], w["nx"])
+    solid = g.mark_solid(*shp)
+    phi = g.sdf_field(*shp)
     D = g.reference_length()
     omega = 1.0 / (3.0 * w["nu"] + 0.5)
     kw = dict(w["kwargs"])
@@ -182,6 +195,8 @@ def cpu_oracle_sample(w, target_s=15.0, max_steps=50, nz_sample=32, threads=None
     o = OracleSolver(solid=solid, omega=omega, u0=w["u0"], D=D, phi=phi, threads=threads, **kw)
     o.step()  # warm-up (page-in, OpenMP start)
     cells = solid.size
+    if max_steps is None:
+        max_steps = max(50, int(2e8 // cells))
     t0 = time.perf_counter()
     n = 0
     while n < max_steps:
@@ -192,7 +207,9 @@ def cpu_oracle_sample(w, target_s=15.0, max_steps=50, nz_sample=32, threads=None
     dt = time.perf_counter() - t0
     return {"value": cells * n / dt / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
             "sample": f"{n} FP64 oracle steps of a {w['nx']}x{w['ny']}x{nz} slab of the workload "
-                      f"({cells} cells, same physics options), {dt:.1f} s"}
+                      f"({cells} cells, same physics options), {dt:.1f} s"
+            if w["dims"] == 3 else f"{n} FP64 oracle steps of the whole {w['nx']}x{w['ny']} workload, "
+                                   f"{dt:.1f} s"}
 
 
 def run_reference(args, w):
@@ -206,8 +223,9 @@ def run_reference(args, w):
     g = _geometry(w)
     # each step is a bounded sample: a slab sized so that W + K steps stay near a minute
     nz = 16 if args.steps <= 20 else 4
-    solid = g.mark_solid(nz, w["ny"], w["nx"])
-    phi = g.sdf_field(nz, w["ny"], w["nx"])
+    shp = (w["ny"], w["nx"]) if w["dims"] == 2 else (nz, w["ny"], w["nx"])
+    solid = g.mark_solid(*shp)
+    phi = g.sdf_field(*shp)
     kw = dict(w["kwargs"])
     kw.pop("scalar_lattice", None)
     o = OracleSolver(solid=solid, omega=1.0 / (3.0 * w["nu"] + 0.5), u0=w["u0"],
@@ -222,7 +240,8 @@ def run_reference(args, w):
     sample = (f"each step: FP64 oracle step of a {w['nx']}x{w['ny']}x{nz} slab of the workload "
               f"({solid.size} cells), {args.steps} steps in {dt:.1f} s")
     line = {
-        "impl": "reference", "metric": "D3Q19 MLUPS", "value": v, "unit": "MLUPS",
+        "impl": "reference", "metric": "D2Q9 MLUPS" if w["dims"] == 2 else "D3Q19 MLUPS", "value": v,
+        "unit": "MLUPS",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -461,26 +480,31 @@ def main():
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
 
-    from aero_b200 import Solver3D
+    from aero_b200 import Solver, Solver3D
     g = _geometry(w)
+    dims = w["dims"]
     nz, ny, nx = w["nz"], w["ny"], w["nx"]
-    solid = g.mark_solid(nz, ny, nx)
-    phi = g.sdf_field(nz, ny, nx) if w["kwargs"].get("bouzidi") else None
+    shp = (ny, nx) if dims == 2 else (nz, ny, nx)
+    solid = g.mark_solid(*shp)
+    phi = g.sdf_field(*shp) if w["kwargs"].get("bouzidi") else None
     D = g.reference_length()
     omega = 1.0 / (3.0 * w["nu"] + 0.5)
     cap = max(4096, args.steps + args.warmup + 8)
-    s = Solver3D(Nz=nz, Ny=ny, Nx=nx, solid=solid, omega=omega, u0=w["u0"], D=D, phi=phi,
-                 precision=args.precision, device=dev, hist_capacity=cap, **w["kwargs"])
+    common = dict(solid=solid, omega=omega, u0=w["u0"], D=D, phi=phi, precision=args.precision, device=dev,
+                  hist_capacity=cap, **w["kwargs"])
+    s = Solver(Ny=ny, Nx=nx, **common) if dims == 2 else Solver3D(Nz=nz, Ny=ny, Nx=nx, **common)
     del phi
     eng = s._engine
     ncells = nx * ny * nz
     # seeded +-1% uniform perturbation of the initial streamwise velocity
     gen = torch.Generator(device=dev)
     gen.manual_seed(1234 + rank)
-    ux0 = w["u0"] * (1.0 + w["perturb"] * (2.0 * torch.rand((nz, ny, nx), generator=gen, device=dev,
+    ux0 = w["u0"] * (1.0 + w["perturb"] * (2.0 * torch.rand(shp, generator=gen, device=dev,
                                                             dtype=torch.float64) - 1.0))
-    f0, prev0, g0 = s._uniform_state_device(ux=ux0)
-    del ux0
+    uy0 = (w["perturb_uy"] * (2.0 * torch.rand(shp, generator=gen, device=dev, dtype=torch.float64) - 1.0)
+           if w.get("perturb_uy") else None)
+    f0, prev0, g0 = s._uniform_state_device(ux=ux0, uy=uy0)
+    del ux0, uy0
     eng.set_state(f0, prev0, g0, 0)
     stream = torch.cuda.current_stream(dev)
     tune = None
@@ -490,10 +514,11 @@ def main():
         tune = s.autotune(steps=10)
 
     # ---------------- device-timed region --------------------------------
-    eng.enable_timing(True)
+    # steps run as the engine runs them (CUDA graphs); the split between the
+    # step kernel and the force kernel comes from a separate phase in which
+    # CUDA events bracket every kernel (which needs eager launches)
     eng.step(args.warmup)
     eng.read_forces()
-    eng.kernel_times()  # reset
     if dist:
         dist.barrier()
     torch.cuda.synchronize(dev)
@@ -506,10 +531,15 @@ def main():
     if dist:
         dist.barrier()
     ms = e0.elapsed_time(e1)
-    step_ms, force_ms, nt = eng.kernel_times()
     raw = eng.read_forces()
-    s.step_count += args.warmup + args.steps
+    n_split = max(min(args.steps, 200), 20)
+    eng.enable_timing(True)
+    eng.kernel_times()  # reset
+    eng.step(n_split)
+    step_ms, force_ms, nt = eng.kernel_times()
     eng.enable_timing(False)
+    eng.read_forces()
+    s.step_count += args.warmup + args.steps + n_split
     status = eng.status()
     first_bad = eng.first_bad_step()
     ms = max_over_ranks(ms, dist, dev)
@@ -519,11 +549,16 @@ def main():
     # roofline of the fused step kernel
     peak, peak_kind = _peak_hbm()
     sb = {"fp32": 4, "fp64": 8, "fp16s": 2, "bf16s": 2}[args.precision]
-    Q = 19
+    Q = 9 if dims == 2 else 19
     bytes_per_cell = 2 * Q * sb + 1
+    rb = 8 if args.precision == "fp64" else 4
     if s.thermal:
-        qg = 7 if s.scalar_lattice == "reduced" else 19
-        bytes_per_cell += 2 * qg * (8 if args.precision == "fp64" else 4)
+        qg = (5 if dims == 2 else 7) if s.scalar_lattice == "reduced" else Q
+        bytes_per_cell += 2 * qg * rb
+    if s.les and s.collision != "mrt":
+        # the LES side pass reads the populations once more and writes the
+        # velocity buffer, which the step kernel reads back
+        bytes_per_cell += Q * sb + 2 * 3 * rb
     alg_bytes = bytes_per_cell * ncells
     k_ms = step_ms / max(nt, 1)
     achieved = alg_bytes / (k_ms / 1e3) / 1e9
@@ -566,11 +601,11 @@ def main():
         dt = time.perf_counter() - t0
         dt = max_over_ranks(dt, dist, dev)
         h2d = f0_host.numel() * 8 + prev_host.numel() * 8 + (0 if g_host is None else g_host.numel() * 8)
-        d2h = (args.steps * 12 * 8 + nz * 3 * 8 + Q * ny * nx * 8 + 4 * ncells * 8
+        d2h = (args.steps * 12 * 8 + (nz if dims == 3 else ny) * 3 * 8 + Q * ny * nx * 8 + 4 * ncells * 8
                + (ncells * 8 if s.thermal else 0))
         e2e = {"value": whole_job_mlups(ncells, world, args.steps, dt), "unit": "MLUPS",
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "call": "Solver3D.run(K) after uploading the initial state from pinned host memory",
+               "call": f"{type(s).__name__}.run(K) after uploading the initial state from pinned host memory",
                "Cd_mean": r["Cd_mean"]}
     else:
         del f0, prev0, g0
@@ -584,9 +619,10 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    cd = raw[:, 0] / (0.5 * s.rho0 * s.u0 ** 2 * D * D) if len(raw) else np.zeros(1)
+    cd = raw[:, 0] / s._drag_norm() if len(raw) else np.zeros(1)
     line = {
-        "metric": "D3Q19 MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world,
+        "metric": "D2Q9 MLUPS" if dims == 2 else "D3Q19 MLUPS", "value": value, "unit": "MLUPS",
+        "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": {"fp32": "f32", "fp64": "f64", "fp16s": "f16 storage / f32 compute",
