@@ -30,6 +30,18 @@ PRECISIONS = tuple(_lib.STORE)
 _PRISTINE_LIMIT = 1 << 28  # elements; above this a handed-out array is always re-uploaded
 
 
+def _check_layout(layout: str) -> None:
+    """Population layout: "ab" (two buffers, the engine's) is the only one
+    built.  The in-place "aa" pattern is not: several boundary conditions of
+    the fused step read other cells' values of the same step (the outlet and
+    recycling planes, Bouzidi neighbours, link-cell forces), which an in-place
+    update would overwrite."""
+    if layout == "aa":
+        raise NotImplementedError("layout='aa' (in-place AA pattern) is not part of the b200 engine")
+    if layout != "ab":
+        raise ValueError(f"Unknown layout '{layout}'. Choose 'ab'.")
+
+
 def _open_checkpoint(path: str):
     """np.load of a checkpoint, with a truncated or corrupt file reported as
     ValueError (before anything touches the GPU)."""

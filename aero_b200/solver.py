@@ -16,7 +16,7 @@ from typing import Optional
 
 import numpy as np
 
-from ._base import LatticeSolverBase
+from ._base import LatticeSolverBase, _check_layout
 from .diagnostics import check_stability, coefficient_spectrum
 
 
@@ -37,7 +37,8 @@ class Solver(LatticeSolverBase):
                  T_cold: float = 0.0, alpha_T: float = 1e-3, buoyancy: bool = False,
                  g_gravity: float = 0.0, beta: float = 1e-3, T_ref: float = 0.5,
                  precision: str = "fp32", scalar_lattice: str = "full", device=None,
-                 hist_capacity: int = 4096):
+                 hist_capacity: int = 4096, layout: str = "ab"):
+        _check_layout(layout)
         self.Ny, self.Nx = int(Ny), int(Nx)
         self._setup(
             shape=(self.Ny, self.Nx), solid=solid, omega=omega, u0=u0, D=D, rho0=rho0,

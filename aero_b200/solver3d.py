@@ -15,7 +15,7 @@ from typing import Optional
 
 import numpy as np
 
-from ._base import LatticeSolverBase
+from ._base import LatticeSolverBase, _check_layout
 from .diagnostics import check_stability, coefficient_spectrum
 
 
@@ -37,7 +37,9 @@ class Solver3D(LatticeSolverBase):
                  sem_N: int = 200, thermal: bool = False, T_hot: float = 1.0, T_cold: float = 0.0,
                  alpha_T: float = 1e-3, buoyancy: bool = False, g_gravity: float = 0.0,
                  beta: float = 1e-3, T_ref: float = 0.5, precision: str = "fp32",
-                 scalar_lattice: str = "full", device=None, hist_capacity: int = 4096):
+                 scalar_lattice: str = "full", device=None, hist_capacity: int = 4096,
+                 layout: str = "ab"):
+        _check_layout(layout)
         if streamwise_bc not in ("open", "periodic", "recycling"):
             raise ValueError(
                 f"Unknown streamwise_bc '{streamwise_bc}'. Choose 'open', 'periodic', or 'recycling'.")

@@ -196,3 +196,16 @@ def test_corrupt_checkpoint_is_rejected_before_gpu_work(tmp_path):
     np.savez(badjson, solid=np.zeros((4, 6), bool), params_json=np.array("{not json"))
     with pytest.raises(ValueError, match="unreadable params_json"):
         Solver.from_checkpoint(str(badjson))
+
+
+def test_layout_option():
+    """layout='ab' is the engine's; 'aa' is refused before any device work."""
+    from aero_b200.solver import Solver
+    from aero_b200.solver3d import Solver3D
+    solid = np.zeros((8, 16), bool)
+    with pytest.raises(NotImplementedError, match="AA pattern"):
+        Solver(Ny=8, Nx=16, solid=solid, omega=1.0, u0=0.05, D=4.0, layout="aa")
+    with pytest.raises(NotImplementedError, match="AA pattern"):
+        Solver3D(Nz=4, Ny=8, Nx=16, solid=np.zeros((4, 8, 16), bool), omega=1.0, u0=0.05, D=4.0, layout="aa")
+    with pytest.raises(ValueError, match="Unknown layout"):
+        Solver(Ny=8, Nx=16, solid=solid, omega=1.0, u0=0.05, D=4.0, layout="soa")
