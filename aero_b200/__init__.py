@@ -11,10 +11,10 @@ raise instead of falling back to a CPU path.
 """
 
 from .geometry import Box, Cylinder, Rectangle, Sphere
-from .links import build_surface_links, build_surface_links_3d
+from .links import build_surface_links, build_surface_links_3d, build_surface_links_device
 
 __all__ = ["Solver", "Solver3D", "Batch", "Cylinder", "Rectangle", "Sphere", "Box", "build_surface_links",
-           "build_surface_links_3d", "build"]
+           "build_surface_links_3d", "build_surface_links_device", "build"]
 
 
 def build(force: bool = False):

@@ -24,6 +24,7 @@ LES_MODEL = {"smagorinsky": 0, "wale": 1}
 
 ERRORS = {0: "AERO_OK", -1: "AERO_ERR_INVALID", -2: "AERO_ERR_CUDA", -3: "AERO_ERR_STATE",
           -4: "AERO_ERR_UNSUPPORTED", -5: "AERO_ERR_CAPACITY"}
+ERRORS_BY_NAME = {v: k for k, v in ERRORS.items()}
 
 # exported entry points with their argument types
 _I32, _I64, _U64, _D, _VP = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double, ctypes.c_void_p
@@ -83,6 +84,9 @@ SIGNATURES = {
     "aero_batch_step": ([_VP, _I64, _VP], ctypes.c_int),
     "aero_batch_converge": ([_VP, _I32, _D, _VP, _VP], ctypes.c_int),
     "aero_batch_destroy": ([_VP], ctypes.c_int),
+    "aero_surface_links_scratch_size": ([_I32, _I32, _I32, _I32, ctypes.POINTER(_U64)], ctypes.c_int),
+    "aero_surface_links_device": ([_I32, _I32, _I32, _I32, _VP, _VP, _VP, _U64, _VP, _VP, _I64,
+                                   ctypes.POINTER(_I64), _VP], ctypes.c_int),
 }
 
 

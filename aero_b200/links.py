@@ -74,3 +74,57 @@ def build_surface_links(solid: np.ndarray, phi: Optional[np.ndarray] = None
 def build_surface_links_3d(solid: np.ndarray, phi: Optional[np.ndarray] = None
                            ) -> Tuple[np.ndarray, np.ndarray]:
     return build_surface_links(solid, phi)
+
+
+def build_surface_links_device(solid, phi=None, stream=None, capacity: int = 1 << 16):
+    """The same list built on the GPU (aero_surface_links_device in
+    libaero_b200.so): solid is a ([nz,] ny, nx) torch CUDA tensor (bool or
+    uint8) and phi an optional float64 tensor of the same shape; returns
+    (links int32 (n, dims+1), q float32 (n,)) as CUDA tensors, equal entry for
+    entry to build_surface_links(solid, phi).  `capacity` is the first guess
+    of the list length; a longer list costs one more counting pass."""
+    import ctypes
+
+    import torch
+
+    from . import _lib
+    from ._lib import AeroError, check
+
+    if not isinstance(solid, torch.Tensor) or solid.device.type != "cuda":
+        raise ValueError("build_surface_links_device takes a CUDA tensor; use build_surface_links for host arrays")
+    dims = solid.dim()
+    if dims not in (2, 3):
+        raise ValueError(f"solid must be 2D or 3D, got shape {tuple(solid.shape)}")
+    dev = solid.device
+    s = solid.to(torch.uint8).contiguous()
+    p = None
+    if phi is not None:
+        if tuple(phi.shape) != tuple(solid.shape):
+            raise ValueError("phi must have the shape of solid")
+        p = phi.to(device=dev, dtype=torch.float64).contiguous()
+    nz, ny, nx = (1,) + tuple(s.shape) if dims == 2 else tuple(s.shape)
+    lib = _lib.load()
+    nbytes = ctypes.c_uint64()
+    check("aero_surface_links_scratch_size",
+          lib.aero_surface_links_scratch_size(dims, nx, ny, nz, ctypes.byref(nbytes)))
+    with torch.cuda.device(dev):
+        st = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+        scratch = torch.empty((int(nbytes.value) + 7) // 8, dtype=torch.int64, device=dev)
+        n = ctypes.c_int64()
+        cap = max(int(capacity), 1)
+        for _ in range(2):
+            links = torch.empty((cap, dims + 1), dtype=torch.int32, device=dev)
+            q = torch.empty(cap, dtype=torch.float32, device=dev)
+            rc = lib.aero_surface_links_device(
+                dims, nx, ny, nz, s.data_ptr(), None if p is None else p.data_ptr(), scratch.data_ptr(),
+                nbytes.value, links.data_ptr(), q.data_ptr(), cap, ctypes.byref(n), st)
+            if rc == _lib.ERRORS_BY_NAME["AERO_ERR_CAPACITY"] and n.value > cap:
+                cap = int(n.value)
+                continue
+            check("aero_surface_links_device", rc)
+            if stream is not None:
+                # the kernels ran on a stream the allocator does not order with
+                # the current one: keep the inputs and scratch alive until they end
+                torch.cuda.ExternalStream(st).synchronize()
+            return links[: n.value], q[: n.value]
+    raise AeroError("aero_surface_links_device", -5, "link count changed between passes")

@@ -291,6 +291,27 @@ AERO_API int aero_params_size(void);
  * the mid plane, solver3d.py:608-615). */
 AERO_API int aero_get_state_slab(AeroLattice *lat, int32_t z0, int32_t nzs, double *f, void *stream);
 
+/* ---- Surface links built on the device --------------------------------
+ * Replaces build_surface_links (boundary.py:232-280) and
+ * build_surface_links_3d (boundary3d.py:279-329) for geometry that already
+ * lives on the GPU.  Same list, entry for entry: rows [i, (z,) y, x] int32
+ * for every fluid cell whose neighbour in direction i (1..Q-1, the index
+ * clipped to the grid) is solid, direction-major, cells in C order within a
+ * direction; q = clip(float32(phi), 1e-4, 1) when phi is given, else 0.5.
+ * dims 2 (nz = 1, D2Q9) or 3 (D3Q19).  The caller provides the scratch:
+ * aero_surface_links_scratch_size gives its bytes (8-byte aligned). */
+AERO_API int aero_surface_links_scratch_size(int32_t dims, int32_t nx, int32_t ny, int32_t nz, uint64_t *bytes);
+/* solid (nz*ny*nx bytes, nonzero = solid), phi (float64 per cell or NULL),
+ * links (capacity rows of dims+1 int32) and q (capacity floats) are DEVICE
+ * arrays.  Counts the links, writes the count to *n_links (host), then writes
+ * the list; when the count exceeds capacity nothing is written and the call
+ * returns AERO_ERR_CAPACITY with *n_links set, so a caller can size the
+ * output from a first call with capacity 0.  Synchronises the stream once
+ * (to read the count). */
+AERO_API int aero_surface_links_device(int32_t dims, int32_t nx, int32_t ny, int32_t nz, const uint8_t *solid,
+                                       const double *phi, void *scratch, uint64_t scratch_size, int32_t *links,
+                                       float *q, int64_t capacity, int64_t *n_links, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
