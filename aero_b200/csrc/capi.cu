@@ -134,10 +134,11 @@ struct AeroLattice {
   int recycle_blocks = 0;
   AeroBatch *batch = nullptr;  // batch this lattice is a member of (stepped only by it)
   double cd_norm = 1.0;        // drag normalisation given when it joined the batch
-  // step kernel: block shape of k_step (kStepShapeXY), or the row-tiled
-  // k_step_tiled with its plan
+  // step kernel: block shape of k_step (kStepShapeXY), the row-tiled
+  // k_step_tiled with its plan, or the two-cells-per-thread k_step_pair
   int step_shape = 0;
   bool tiled = false;
+  bool pair = false;
   int tile_blocks = 0, tile_rows = 0, tiles_per_plane = 0, ntiles = 0;
   uint32_t tile_extra_tx = 0;  // AERO_B200_TEST_STALL_TILES=1 at bind: stages never complete
   // optional per-kernel event timing (eager launches only)
@@ -319,6 +320,8 @@ int launch_step(AeroLattice *L, int cur, cudaStream_t st, bool timed = false) {
   if (les_active(L)) CUDA_TRY(ops->moments(p, false, grid, st));
   if (L->tiled)
     CUDA_TRY(ops->step_tiled(p, L->tile_blocks, st));
+  else if (L->pair)
+    CUDA_TRY(ops->step_pair(p, st));
   else if (L->step_shape != 0)
     CUDA_TRY(ops->step_shaped(p, L->step_shape, st));
   else
@@ -953,16 +956,25 @@ int aero_set_inflow(AeroLattice *L, const double *fields, int64_t first, int64_t
 int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
   if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
   if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
-  if (kernel < 0 || kernel > kStepShapes) return fail(AERO_ERR_INVALID, "kernel must be 0..%d", kStepShapes);
+  if (kernel < 0 || kernel > kStepPair) return fail(AERO_ERR_INVALID, "kernel must be 0..%d", kStepPair);
   CUDA_TRY(cudaSetDevice(L->device));
+  if (kernel == kStepPair) {
+    if (is_f64(L) || L->prm.dims != 3 || L->prm.collision != AERO_MRT)
+      return fail(AERO_ERR_UNSUPPORTED, "the two-cell kernel covers D3Q19 MRT with 4- or 2-byte storage");
+    if (L->prm.nx % 2 != 0) return fail(AERO_ERR_UNSUPPORTED, "the two-cell kernel needs an even nx");
+    if (L->feat & (FEAT_BODY_FORCE | FEAT_THERMAL))
+      return fail(AERO_ERR_UNSUPPORTED, "the two-cell kernel has no body force or scalar lattice");
+  }
   if (kernel == kStepShapes) {
     const int rc = is_f64(L) ? plan_tiles<double>(L, true) : plan_tiles<float>(L, true);
     if (rc != AERO_OK) return rc;
     if (!L->tiled) return fail(AERO_ERR_UNSUPPORTED, "rows of this lattice do not fit the row-tiled kernel");
+    L->pair = false;
   } else {
     L->tiled = false;
     L->tile_blocks = L->tile_rows = L->tiles_per_plane = L->ntiles = 0;
-    L->step_shape = kernel;
+    L->pair = kernel == kStepPair;
+    L->step_shape = L->pair ? 0 : kernel;
   }
   // captured step sequences launch the previous kernel
   for (auto &e : L->pair_exec)
@@ -975,7 +987,7 @@ int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
 
 int aero_get_step_kernel(const AeroLattice *L, int32_t *kernel) {
   if (!L || !kernel) return fail(AERO_ERR_INVALID, "NULL argument");
-  *kernel = L->tiled ? kStepShapes : L->step_shape;
+  *kernel = L->tiled ? kStepShapes : (L->pair ? kStepPair : L->step_shape);
   return AERO_OK;
 }
 

@@ -33,6 +33,9 @@ struct Ops {
                                 cudaStream_t);
   // mean ux of the recycle plane (3D recycling inlet), before the step kernel
   cudaError_t (*recycle_mean)(const StepParams<Real> &, cudaStream_t);
+  // regular step, two cells per thread (k_step_pair; D3Q19 MRT, 4-byte
+  // arithmetic); cudaErrorNotSupported for other classes
+  cudaError_t (*step_pair)(const StepParams<Real> &, cudaStream_t);
   int store_bytes;
 };
 
@@ -45,6 +48,10 @@ const Ops<float> *ops_bf16(int dims, int coll);
 // {threads along x, rows}.  Shape 0 is the default.
 constexpr int kStepShapes = 3;
 constexpr int kStepShapeXY[kStepShapes][2] = {{128, 1}, {256, 1}, {32, 4}};
+
+// Step kernel ids beyond the shapes: kStepShapes = the row-tiled kernel,
+// kStepPair = the two-cells-per-thread kernel.
+constexpr int kStepPair = kStepShapes + 1;
 
 inline dim3 step_grid(int shape, int nx, int ny, int nz) {
   const int bx = kStepShapeXY[shape][0], by = kStepShapeXY[shape][1];

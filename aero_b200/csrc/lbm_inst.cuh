@@ -1,8 +1,11 @@
 // lbm_inst.cuh -- explicit instantiation of the kernels for one storage type.
 // Included by lbm_inst_<storage>.cu with AERO_STORE / AERO_OPS_FN defined.
 #pragma once
+#include <type_traits>
+
 #include "lbm_dispatch.h"
 #include "lbm_kernels.cuh"
+#include "lbm_pair.cuh"
 
 namespace aero {
 namespace inst {
@@ -96,9 +99,19 @@ struct Launch {
     }
     return cudaErrorInvalidValue;  // recycling exists in 3D only
   }
+  static cudaError_t step_pair(const StepParams<Real> &p, cudaStream_t st) {
+    if constexpr (std::is_same<Real, float>::value && L::DIMS == 3 && COLL == COLL_MRT) {
+      k_step_pair<L, S, COLL><<<pair_blocks(p), kPairBlock, 0, st>>>(p);
+      return cudaGetLastError();
+    } else {
+      (void)p;
+      (void)st;
+      return cudaErrorNotSupported;
+    }
+  }
   static constexpr Ops<Real> table = {&step,       &step_shaped, &moments,    &finalize,      &state_out,     &load_state,
                                       &step_tiled, &tiled_setup, &step_batch, &moments_batch, &finalize_batch,
-                                      &recycle_mean, (int)sizeof(S)};
+                                      &recycle_mean, &step_pair, (int)sizeof(S)};
 };
 
 template <class S>

@@ -616,66 +616,72 @@ __device__ __forceinline__ Real les_omega(const StepParams<Real> &p, int x, int 
 // remaining odd edge combinations (the directions the rank-16 basis projects
 // out).  The host derives the block entries from the dense operator and
 // checks that nothing outside them is non-zero.
+// 1 / rho for rho > 0, else 0 (the reference's guard in compute_macroscopic)
 template <class Real>
-AERO_HD Real mrt3_adapted(const StepParams<Real> &p, Real (&d)[19], bool solid, Real drho_in) {
-  const Mrt3Adapted<Real> &m = p.mrt3;
+AERO_HD Real pos_recip(Real rho) {
+  return rho > Real(0) ? Real(1) / rho : Real(0);
+}
+
+// The operator on the values V of one cell (V = Real), or of two cells at
+// once (V = F2, lbm_pair.cuh: every operation one packed FP32 instruction).
+template <class Real, class V>
+AERO_HD V mrt3_core(const Mrt3Adapted<Real> &m, V (&d)[19], bool solid) {
   // pair sums (even) and differences (odd)
-  const Real X = d[1] + d[2], Y = d[3] + d[4], Z = d[5] + d[6];
-  const Real p710 = d[7] + d[10], p89 = d[8] + d[9], p1114 = d[11] + d[14], p1213 = d[12] + d[13];
-  const Real p1518 = d[15] + d[18], p1617 = d[16] + d[17];
-  const Real t1 = d[1] - d[2], t2 = d[3] - d[4], t3 = d[5] - d[6];
-  const Real q710 = d[7] - d[10], q89 = d[8] - d[9], q1114 = d[11] - d[14], q1213 = d[12] - d[13];
-  const Real q1518 = d[15] - d[18], q1617 = d[16] - d[17];
+  const V X = d[1] + d[2], Y = d[3] + d[4], Z = d[5] + d[6];
+  const V p710 = d[7] + d[10], p89 = d[8] + d[9], p1114 = d[11] + d[14], p1213 = d[12] + d[13];
+  const V p1518 = d[15] + d[18], p1617 = d[16] + d[17];
+  const V t1 = d[1] - d[2], t2 = d[3] - d[4], t3 = d[5] - d[6];
+  const V q710 = d[7] - d[10], q89 = d[8] - d[9], q1114 = d[11] - d[14], q1213 = d[12] - d[13];
+  const V q1518 = d[15] - d[18], q1617 = d[16] - d[17];
   // even adapted coordinates
-  const Real Pxy = p710 + p89, Pxz = p1114 + p1213, Pyz = p1518 + p1617;
-  const Real g0 = d[0], g1 = X + Y + Z, g2 = Pxy + Pxz + Pyz;
-  const Real g3 = Real(2) * X - Y - Z, g4 = Y - Z;
-  const Real g5 = Real(2) * Pyz - Pxz - Pxy, g6 = Pxz - Pxy;
-  const Real g7 = p710 - p89, g8 = p1114 - p1213, g9 = p1518 - p1617;
+  const V Pxy = p710 + p89, Pxz = p1114 + p1213, Pyz = p1518 + p1617;
+  const V g0 = d[0], g1 = X + Y + Z, g2 = Pxy + Pxz + Pyz;
+  const V g3 = Real(2) * X - Y - Z, g4 = Y - Z;
+  const V g5 = Real(2) * Pyz - Pxz - Pxy, g6 = Pxz - Pxy;
+  const V g7 = p710 - p89, g8 = p1114 - p1213, g9 = p1518 - p1617;
   // odd adapted coordinates (momentum-like edge sums)
-  const Real Wx = (q710 - q89) + (q1114 - q1213);
-  const Real Wy = (q710 + q89) + (q1518 - q1617);
-  const Real Wz = (q1114 + q1213) + (q1518 + q1617);
+  const V Wx = (q710 - q89) + (q1114 - q1213);
+  const V Wy = (q710 + q89) + (q1518 - q1617);
+  const V Wz = (q1114 + q1213) + (q1518 + q1617);
   // moments
-  const Real drho = g0 + g1 + g2;
-  (void)drho_in;
-  const Real jx = t1 + Wx, jy = t2 + Wy, jz = t3 + Wz;
-  const Real rho = Real(1) + drho;
-  const Real inv = rho > Real(0) ? Real(1) / rho : Real(0);
-  Real ux = jx * inv, uy = jy * inv, uz = jz * inv;
-  if (solid) ux = uy = uz = Real(0);
-  const Real rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
-  const Real kxx = rux * ux, kyy = ruy * uy, kzz = ruz * uz;
-  const Real ru2 = kxx + kyy + kzz;
-  const Real mE1 = Real(2) * kxx - kyy - kzz, mE2 = kyy - kzz;
+  const V drho = g0 + g1 + g2;
+  const V jx = t1 + Wx, jy = t2 + Wy, jz = t3 + Wz;
+  const V rho = Real(1) + drho;
+  const V inv = pos_recip(rho);
+  V ux = jx * inv, uy = jy * inv, uz = jz * inv;
+  if (solid) ux = uy = uz = V(Real(0));
+  const V rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
+  const V kxx = rux * ux, kyy = ruy * uy, kzz = ruz * uz;
+  const V ru2 = kxx + kyy + kzz;
+  const V mE1 = Real(2) * kxx - kyy - kzz, mE2 = kyy - kzz;
   // blocks
-  const Real h0 = m.a1[0] * g0 + m.a1[1] * g1 + m.a1[2] * g2 + m.ca1[0] * drho + m.ca1[1] * ru2;
-  const Real h1 = m.a1[3] * g0 + m.a1[4] * g1 + m.a1[5] * g2 + m.ca1[2] * drho + m.ca1[3] * ru2;
-  const Real h2 = m.a1[6] * g0 + m.a1[7] * g1 + m.a1[8] * g2 + m.ca1[4] * drho + m.ca1[5] * ru2;
-  const Real h3 = m.e[0] * g3 + m.e[1] * g5 + m.ce[0] * mE1;
-  const Real h5 = m.e[2] * g3 + m.e[3] * g5 + m.ce[1] * mE1;
-  const Real h4 = m.e[0] * g4 + m.e[1] * g6 + m.ce[0] * mE2;
-  const Real h6 = m.e[2] * g4 + m.e[3] * g6 + m.ce[1] * mE2;
-  const Real h7 = m.t2 * g7 + m.ct2 * (rux * uy);
-  const Real h8 = m.t2 * g8 + m.ct2 * (rux * uz);
-  const Real h9 = m.t2 * g9 + m.ct2 * (ruy * uz);
-  const Real vx = m.v[0] * t1 + m.v[1] * Wx + m.cv[0] * rux;
-  const Real Vx = m.v[2] * t1 + m.v[3] * Wx + m.cv[1] * rux;
-  const Real vy = m.v[0] * t2 + m.v[1] * Wy + m.cv[0] * ruy;
-  const Real Vy = m.v[2] * t2 + m.v[3] * Wy + m.cv[1] * ruy;
-  const Real vz = m.v[0] * t3 + m.v[1] * Wz + m.cv[0] * ruz;
-  const Real Vz = m.v[2] * t3 + m.v[3] * Wz + m.cv[1] * ruz;
+  const V h0 = m.a1[0] * g0 + m.a1[1] * g1 + m.a1[2] * g2 + m.ca1[0] * drho + m.ca1[1] * ru2;
+  const V h1 = m.a1[3] * g0 + m.a1[4] * g1 + m.a1[5] * g2 + m.ca1[2] * drho + m.ca1[3] * ru2;
+  const V h2 = m.a1[6] * g0 + m.a1[7] * g1 + m.a1[8] * g2 + m.ca1[4] * drho + m.ca1[5] * ru2;
+  const V h3 = m.e[0] * g3 + m.e[1] * g5 + m.ce[0] * mE1;
+  const V h5 = m.e[2] * g3 + m.e[3] * g5 + m.ce[1] * mE1;
+  const V h4 = m.e[0] * g4 + m.e[1] * g6 + m.ce[0] * mE2;
+  const V h6 = m.e[2] * g4 + m.e[3] * g6 + m.ce[1] * mE2;
+  const V h7 = m.t2 * g7 + m.ct2 * (rux * uy);
+  const V h8 = m.t2 * g8 + m.ct2 * (rux * uz);
+  const V h9 = m.t2 * g9 + m.ct2 * (ruy * uz);
+  const V vx = m.v[0] * t1 + m.v[1] * Wx + m.cv[0] * rux;
+  const V Vx = m.v[2] * t1 + m.v[3] * Wx + m.cv[1] * rux;
+  const V vy = m.v[0] * t2 + m.v[1] * Wy + m.cv[0] * ruy;
+  const V Vy = m.v[2] * t2 + m.v[3] * Wy + m.cv[1] * ruy;
+  const V vz = m.v[0] * t3 + m.v[1] * Wz + m.cv[0] * ruz;
+  const V Vz = m.v[2] * t3 + m.v[3] * Wz + m.cv[1] * ruz;
   // back to populations
-  const Real Xn = (h1 + h3) * Real(1.0 / 3.0);
-  const Real Yn = Real(0.5) * (h1 - Xn + h4), Zn = Real(0.5) * (h1 - Xn - h4);
-  const Real Pyzn = (h2 + h5) * Real(1.0 / 3.0);
-  const Real Pxzn = Real(0.5) * (h2 - Pyzn + h6), Pxyn = Real(0.5) * (h2 - Pyzn - h6);
-  const Real p710n = Real(0.5) * (Pxyn + h7), p89n = Real(0.5) * (Pxyn - h7);
-  const Real p1114n = Real(0.5) * (Pxzn + h8), p1213n = Real(0.5) * (Pxzn - h8);
-  const Real p1518n = Real(0.5) * (Pyzn + h9), p1617n = Real(0.5) * (Pyzn - h9);
-  const Real q710n = Real(0.25) * (Vx + Vy), q89n = Real(0.25) * (Vy - Vx);
-  const Real q1114n = Real(0.25) * (Vx + Vz), q1213n = Real(0.25) * (Vz - Vx);
-  const Real q1518n = Real(0.25) * (Vy + Vz), q1617n = Real(0.25) * (Vz - Vy);
+  const V Xn = (h1 + h3) * Real(1.0 / 3.0);
+  const V Yn = Real(0.5) * (h1 - Xn + h4), Zn = Real(0.5) * (h1 - Xn - h4);
+  const V Pyzn = (h2 + h5) * Real(1.0 / 3.0);
+  const V Pxzn = Real(0.5) * (h2 - Pyzn + h6), Pxyn = Real(0.5) * (h2 - Pyzn - h6);
+  const V p710n = Real(0.5) * (Pxyn + h7), p89n = Real(0.5) * (Pxyn - h7);
+  const V p1114n = Real(0.5) * (Pxzn + h8), p1213n = Real(0.5) * (Pxzn - h8);
+  const V p1518n = Real(0.5) * (Pyzn + h9), p1617n = Real(0.5) * (Pyzn - h9);
+  const V q710n = Real(0.25) * (Vx + Vy), q89n = Real(0.25) * (Vy - Vx);
+  const V q1114n = Real(0.25) * (Vx + Vz), q1213n = Real(0.25) * (Vz - Vx);
+  const V q1518n = Real(0.25) * (Vy + Vz), q1617n = Real(0.25) * (Vz - Vy);
   d[0] = h0;
   d[1] = Real(0.5) * (Xn + vx);
   d[2] = Real(0.5) * (Xn - vx);
@@ -696,6 +702,12 @@ AERO_HD Real mrt3_adapted(const StepParams<Real> &p, Real (&d)[19], bool solid, 
   d[16] = Real(0.5) * (p1617n + q1617n);
   d[17] = Real(0.5) * (p1617n - q1617n);
   return rho;
+}
+
+template <class Real>
+AERO_HD Real mrt3_adapted(const StepParams<Real> &p, Real (&d)[19], bool solid, Real drho_in) {
+  (void)drho_in;
+  return mrt3_core<Real, Real>(p.mrt3, d, solid);
 }
 
 template <class L, class Real, int COLL>
@@ -908,8 +920,7 @@ __device__ __forceinline__ void link_cell_forces(const StepParams<Real> &p, int 
 // Divergence guard (diagnostics.py:32-71): non-finite or non-positive rho of
 // the state; one lane per warp reports, and only until it is recorded.
 template <class Real>
-__device__ __forceinline__ void guard_rho(const StepParams<Real> &p, Real rho, int64_t step_now) {
-  const bool bad = !(rho > Real(0)) || !isfinite(rho);
+__device__ __forceinline__ void guard_bad(const StepParams<Real> &p, bool bad, int64_t step_now) {
   const unsigned badm = __ballot_sync(__activemask(), bad);
   if (bad && (threadIdx.x & 31) == __ffs(badm) - 1) {
     if (!(*(volatile uint32_t *)p.status & STATUS_NONFINITE_OR_NONPOSITIVE_RHO))
@@ -917,6 +928,11 @@ __device__ __forceinline__ void guard_rho(const StepParams<Real> &p, Real rho, i
     if (*(volatile unsigned long long *)p.first_bad_step > (unsigned long long)(step_now + 1))
       atomicMin(p.first_bad_step, (unsigned long long)(step_now + 1));
   }
+}
+
+template <class Real>
+__device__ __forceinline__ void guard_rho(const StepParams<Real> &p, Real rho, int64_t step_now) {
+  guard_bad(p, !(rho > Real(0)) || !isfinite(rho), step_now);
 }
 
 // One regular step of cell (x, y, z): state of step n from P_n (gathered by
@@ -965,7 +981,7 @@ __device__ __forceinline__ void step_cell(const StepParams<typename StoreOps<S>:
 template <int BX, int BY>
 struct StepShape {
   static constexpr int threads = BX * BY;
-  static constexpr int min_blocks4 = 1024 / (BX * BY);
+  static constexpr int min_blocks4 = kStepMinBlocks * 128 / (BX * BY);
 };
 
 template <class L, class S, int COLL, bool FROM_STATE, int BX = kStepBlock, int BY = 1>

@@ -440,9 +440,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--collision", default=None, choices=["bgk", "trt", "mrt"],
                     help="override the workload's collision operator (profiling)")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "rowgather", "tiled"],
-                    help="step kernel: chosen by the autotuner (default), the per-cell global gather, or "
-                         "rows staged in shared memory by bulk async copies")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "rowgather", "tiled", "pair"],
+                    help="step kernel: chosen by the autotuner (default), the per-cell global gather, "
+                         "rows staged in shared memory by bulk async copies, or two cells per thread "
+                         "on packed FP32 arithmetic")
     ap.add_argument("--batch-every", type=int, default=1,
                     help="batch96: keep every k-th case (a smaller batch for profiling captures)")
     ap.add_argument("--serve-requests", type=int, default=128)
@@ -512,6 +513,8 @@ def main():
         # set-up, outside the timed region: time each step kernel on this
         # lattice, keep the fastest, restore the initial state
         tune = s.autotune(steps=10)
+    elif args.kernel == "pair":
+        eng.set_step_kernel(4)
 
     # ---------------- device-timed region --------------------------------
     # steps run as the engine runs them (CUDA graphs); the split between the
@@ -569,11 +572,11 @@ def main():
     plan["kernel_id"] = eng.get_step_kernel()
     if tune is not None:
         plan["autotune_ms_per_step"] = {str(k): v for k, v in tune["ms_per_step"].items()}
-    kname = "k_step_tiled" if plan["tiled"] else "k_step"
+    kname = "k_step_tiled" if plan["tiled"] else ("k_step_pair" if plan["kernel_id"] == 4 else "k_step")
     traffic = None
     pat = re.compile(rf"^- {re.escape(args.workload)}: dram bytes per launch = (\d+)\s*$", re.M)
     for md in sorted((ROOT / "profiles").glob(f"{kname}_*_{args.precision}.md")):
-        if kname == "k_step" and md.name.startswith("k_step_tiled"):
+        if kname == "k_step" and md.name.startswith(("k_step_tiled", "k_step_pair")):
             continue
         m = pat.search(md.read_text())
         if m:
@@ -638,10 +641,11 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic,
-                     "kernel": f"{kname} (fused stream/BC/collide"
-                               + (", source rows staged in shared memory by bulk async copies)"
-                                  if plan["tiled"] else ", per-cell global gather, blocks "
-                                  + ("128x1", "256x1", "32x4")[plan["kernel_id"]] + ")"),
+                     "kernel": f"{kname} (fused stream/BC/collide" + (
+                         ", source rows staged in shared memory by bulk async copies)" if plan["tiled"]
+                         else ", two cells per thread on packed FP32 arithmetic)" if plan["kernel_id"] == 4
+                         else ", per-cell global gather, blocks "
+                         + ("128x1", "256x1", "32x4")[plan["kernel_id"]] + ")"),
                      "step_plan": plan,
                      "alg_bytes_per_launch": alg_bytes, "bytes_per_cell": bytes_per_cell,
                      "kernel_ms": k_ms, "finalize_ms": force_ms / max(nt, 1)},

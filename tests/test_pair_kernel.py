@@ -1,0 +1,112 @@
+"""The two-cells-per-thread D3Q19 MRT step kernel (step kernel 4, packed FP32
+arithmetic) against the per-cell kernel, the reference fixtures and the FP64
+oracle.
+
+Tolerances: each lane runs the per-cell step's operations in the same order;
+only the fusion of a product into a sum may differ, an FP32 rounding per
+operation.  After 60 steps the states agree to 1e-6 of max|f| with FP32
+storage, and to the storage's own resolution with 16-bit storage, where one
+such rounding can move a value by one 16-bit step: 1e-4 (FP16, 11-bit
+significand of the scaled deviation) and 1e-3 (BF16, 8 bits) of max|f|."""
+
+import numpy as np
+import pytest
+
+from tests.golden_cases import load_case
+
+pytestmark = pytest.mark.gpu
+
+PAIR = 4
+TOL = {"fp32": 1e-6, "fp16s": 1e-4, "bf16s": 1e-3}
+
+
+def _sphere(precision, kernel, nz=20, ny=22, nx=64, steps=60):
+    from aero_b200 import Solver3D, Sphere
+    sph = Sphere(radius=4, cx_frac=0.3, cy_frac=0.5, cz_frac=0.5)
+    solid, phi = sph.mark_solid(nz, ny, nx), sph.sdf_field(nz, ny, nx)
+    kw = dict(omega=1 / 0.6, u0=0.05, D=sph.reference_length(), collision="mrt", bouzidi=True, phi=phi,
+              wall_bc="slip", outlet_bc="convective", sponge_thickness=6, inlet_perturbation=0.05)
+    s = Solver3D(Nz=nz, Ny=ny, Nx=nx, solid=solid, precision=precision, **kw)
+    s._engine.set_step_kernel(kernel)
+    assert s._engine.get_step_kernel() == kernel
+    r = s.run(steps, check_every=steps + 1, verbose=False)
+    return s.f, np.array(r["Cd_history"])
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16s", "bf16s"])
+def test_pair_kernel_equals_per_cell_kernel(precision):
+    """3D MRT + Bouzidi sphere with slip walls (wall rows), sponge and
+    convective outlet (per-cell fallback columns), y and z wrap."""
+    fa, cda = _sphere(precision, PAIR)
+    fb, cdb = _sphere(precision, 0)
+    np.testing.assert_allclose(fa, fb, rtol=0, atol=TOL[precision] * np.abs(fb).max())
+    np.testing.assert_allclose(cda, cdb, rtol=0, atol=10 * TOL[precision] * np.abs(cdb).max())
+
+
+def test_pair_kernel_sphere_matches_oracle_300_steps():
+    """The acceptance bound of the plain FP32 form through the pair kernel:
+    rel-L2(rho, u) <= 1e-5 after 300 steps against the FP64 oracle."""
+    from aero_b200 import Solver3D, Sphere
+    from oracle.oracle import OracleSolver
+    from tests.test_gpu_parity import _macro, rel_l2
+    nz, ny, nx = 40, 40, 96
+    sph = Sphere(radius=6, cx_frac=0.25, cy_frac=0.5, cz_frac=0.5)
+    solid, phi = sph.mark_solid(nz, ny, nx), sph.sdf_field(nz, ny, nx)
+    kw = dict(omega=1 / 0.6, u0=0.05, D=sph.reference_length(), collision="mrt", bouzidi=True,
+              phi=phi, wall_bc="slip", outlet_bc="convective", sponge_thickness=8)
+    s = Solver3D(Nz=nz, Ny=ny, Nx=nx, solid=solid, precision="fp32", **kw)
+    s._engine.set_step_kernel(PAIR)
+    o = OracleSolver(solid=solid, **kw)
+    s.run(300, check_every=301, verbose=False)
+    for _ in range(300):
+        o.step_raw()
+    got, ref = _macro(s.f, 3), _macro(o.f, 3)
+    assert rel_l2(got[0], ref[0]) <= 1e-5
+    assert rel_l2(np.stack(got[1:]), np.stack(ref[1:])) <= 1e-5
+
+
+@pytest.mark.parametrize("name", ["c3d_mrt_noslip_zerograd", "c3d_mrt_smag_bouzidi_sponge"])
+def test_pair_kernel_close_to_reference_fixture(name):
+    from tests.test_gpu_parity import _macro, _solver, rel_l2
+    c = load_case(name)
+    s = _solver(c, precision="fp32")
+    s._engine.set_step_kernel(PAIR)
+    cd = [s._step()[0] for _ in range(c["steps"])]
+    got, ref = _macro(s.f, 3), _macro(c["f"], 3)
+    assert rel_l2(got[0], ref[0]) <= 1e-5
+    assert rel_l2(np.stack(got[1:]), np.stack(ref[1:])) <= 1e-5
+    np.testing.assert_allclose(cd, c["hist"]["Cd"], rtol=0, atol=1e-4 * np.abs(c["hist"]["Cd"]).max())
+
+
+def test_pair_kernel_nan_guard():
+    """A NaN planted in plain fluid cells is caught by the divergence guard."""
+    from tests.test_gpu_parity import _solver
+    c = load_case("c3d_mrt_noslip_zerograd")
+    s = _solver(c, precision="fp32")
+    s._engine.set_step_kernel(PAIR)
+    s._step()
+    assert s.status() == 0
+    f = s.f
+    f[:, 4, 5, 8] = np.nan  # x = 8, an interior row
+    s.f = f
+    s._step()
+    s._step()
+    assert s.status() & 1
+
+
+def test_pair_kernel_refused_outside_its_cover():
+    from aero_b200 import Solver3D, Sphere
+    from aero_b200._lib import AeroError
+
+    def make(nx=32, **kw):
+        sph = Sphere(radius=3, cx_frac=0.3, cy_frac=0.5, cz_frac=0.5)
+        solid = sph.mark_solid(12, 12, nx)
+        args = dict(omega=1 / 0.6, u0=0.05, D=sph.reference_length(), collision="mrt")
+        args.update(kw)
+        return Solver3D(Nz=12, Ny=12, Nx=nx, solid=solid, **args)
+
+    for s in (make(nx=33), make(collision="bgk"), make(precision="fp64"),
+              make(body_force_x=1e-6, streamwise_bc="periodic")):
+        with pytest.raises(AeroError, match="AERO_ERR_UNSUPPORTED"):
+            s._engine.set_step_kernel(PAIR)
+        assert s._engine.get_step_kernel() == 0
