@@ -63,11 +63,11 @@ template <class S> struct PairOps;
 template <> struct PairOps<float> {
   template <int I, class L>
   static __device__ __forceinline__ F2 aligned(const float *p, uint32_t o) {
-    return F2(__ldg(reinterpret_cast<const float2 *>(p + o)));
+    return F2(ld_pop64(p + o));
   }
   template <int I, class L>
   static __device__ __forceinline__ F2 split(const float *p, uint32_t o) {
-    return F2(make_float2(__ldg(p + o), __ldg(p + o + 1)));
+    return F2(make_float2(ld_pop(p + o), ld_pop(p + o + 1)));
   }
   template <int I, class L>
   static __device__ __forceinline__ void store(float *p, uint32_t o, F2 v) {
@@ -83,11 +83,13 @@ template <> struct PairOps<__half> {
   }
   template <int I, class L>
   static __device__ __forceinline__ F2 aligned(const __half *p, uint32_t o) {
-    return scaled<I, L>(__half22float2(__ldg(reinterpret_cast<const __half2 *>(p + o))));
+    const unsigned int u = ld_pop32(p + o);
+    return scaled<I, L>(__half22float2(*reinterpret_cast<const __half2 *>(&u)));
   }
   template <int I, class L>
   static __device__ __forceinline__ F2 split(const __half *p, uint32_t o) {
-    return scaled<I, L>(make_float2(__half2float(__ldg(p + o)), __half2float(__ldg(p + o + 1))));
+    return scaled<I, L>(make_float2(__half2float(__ushort_as_half(ld_pop16(p + o))),
+                                    __half2float(__ushort_as_half(ld_pop16(p + o + 1)))));
   }
   template <int I, class L>
   static __device__ __forceinline__ void store(__half *p, uint32_t o, F2 v) {
@@ -99,11 +101,13 @@ template <> struct PairOps<__half> {
 template <> struct PairOps<__nv_bfloat16> {
   template <int I, class L>
   static __device__ __forceinline__ F2 aligned(const __nv_bfloat16 *p, uint32_t o) {
-    return F2(__bfloat1622float2(__ldg(reinterpret_cast<const __nv_bfloat162 *>(p + o))));
+    const unsigned int u = ld_pop32(p + o);
+    return F2(__bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u)));
   }
   template <int I, class L>
   static __device__ __forceinline__ F2 split(const __nv_bfloat16 *p, uint32_t o) {
-    return F2(make_float2(__bfloat162float(__ldg(p + o)), __bfloat162float(__ldg(p + o + 1))));
+    return F2(make_float2(__bfloat162float(__ushort_as_bfloat16(ld_pop16(p + o))),
+                          __bfloat162float(__ushort_as_bfloat16(ld_pop16(p + o + 1)))));
   }
   template <int I, class L>
   static __device__ __forceinline__ void store(__nv_bfloat16 *p, uint32_t o, F2 v) {

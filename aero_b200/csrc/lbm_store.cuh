@@ -18,12 +18,57 @@
 
 namespace aero {
 
+// Read-only population loads.  With AERO_L2_256B the load asks L2 to fetch
+// the whole 256-byte block around a miss (PTX ld.global.nc.L2::256B): a warp
+// reads 64-128 contiguous bytes of a direction plane and its neighbour warp
+// the next ones, so one DRAM access serves both.
+#ifndef AERO_L2_256B
+#define AERO_L2_256B 1
+#endif
+__device__ __forceinline__ float ld_pop(const float *p) {
+#if AERO_L2_256B
+  float v;
+  asm("ld.global.nc.L2::256B.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+#else
+  return __ldg(p);
+#endif
+}
+__device__ __forceinline__ double ld_pop(const double *p) { return __ldg(p); }
+__device__ __forceinline__ unsigned short ld_pop16(const void *p) {
+#if AERO_L2_256B
+  unsigned short v;
+  asm("ld.global.nc.L2::256B.b16 %0, [%1];" : "=h"(v) : "l"(p));
+  return v;
+#else
+  return __ldg(static_cast<const unsigned short *>(p));
+#endif
+}
+__device__ __forceinline__ unsigned int ld_pop32(const void *p) {
+#if AERO_L2_256B
+  unsigned int v;
+  asm("ld.global.nc.L2::256B.b32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+#else
+  return __ldg(static_cast<const unsigned int *>(p));
+#endif
+}
+__device__ __forceinline__ float2 ld_pop64(const float *p) {
+#if AERO_L2_256B
+  float2 v;
+  asm("ld.global.nc.L2::256B.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+#else
+  return __ldg(reinterpret_cast<const float2 *>(p));
+#endif
+}
+
 template <class S> struct StoreOps;
 
 template <> struct StoreOps<float> {
   using Real = float;
   template <int I, class L>
-  static __device__ __forceinline__ float load(const float *p, uint32_t o) { return __ldg(p + o); }
+  static __device__ __forceinline__ float load(const float *p, uint32_t o) { return ld_pop(p + o); }
   template <int I, class L>
   static __device__ __forceinline__ float lds(const float *p, uint32_t o) { return p[o]; }
   template <int I, class L>
@@ -45,7 +90,7 @@ template <> struct StoreOps<__half> {
   template <int I, class L>
   static __device__ __forceinline__ float load(const __half *p, uint32_t o) {
     constexpr float s = float(L::w[I] / 64.0);
-    return __half2float(__ldg(p + o)) * s;
+    return __half2float(__ushort_as_half(ld_pop16(p + o))) * s;
   }
   template <int I, class L>
   static __device__ __forceinline__ float lds(const __half *p, uint32_t o) {
@@ -63,7 +108,7 @@ template <> struct StoreOps<__nv_bfloat16> {
   using Real = float;
   template <int I, class L>
   static __device__ __forceinline__ float load(const __nv_bfloat16 *p, uint32_t o) {
-    return __bfloat162float(__ldg(p + o));
+    return __bfloat162float(__ushort_as_bfloat16(ld_pop16(p + o)));
   }
   template <int I, class L>
   static __device__ __forceinline__ float lds(const __nv_bfloat16 *p, uint32_t o) {
