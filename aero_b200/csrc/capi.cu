@@ -962,6 +962,8 @@ int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
     if (is_f64(L) || L->prm.dims != 3 || L->prm.collision != AERO_MRT)
       return fail(AERO_ERR_UNSUPPORTED, "the two-cell kernel covers D3Q19 MRT with 4- or 2-byte storage");
     if (L->prm.nx % 2 != 0) return fail(AERO_ERR_UNSUPPORTED, "the two-cell kernel needs an even nx");
+    if (((int64_t)L->prm.ny * L->prm.nz + 31) / 32 > 65535)
+      return fail(AERO_ERR_UNSUPPORTED, "the two-cell kernel takes at most 65535 * 32 rows (ny * nz)");
     if (L->feat & (FEAT_BODY_FORCE | FEAT_THERMAL))
       return fail(AERO_ERR_UNSUPPORTED, "the two-cell kernel has no body force or scalar lattice");
   }

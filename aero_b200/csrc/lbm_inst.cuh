@@ -101,7 +101,7 @@ struct Launch {
   }
   static cudaError_t step_pair(const StepParams<Real> &p, cudaStream_t st) {
     if constexpr (std::is_same<Real, float>::value && L::DIMS == 3 && COLL == COLL_MRT) {
-      k_step_pair<L, S, COLL><<<pair_blocks(p), kPairBlock, 0, st>>>(p);
+      k_step_pair<L, S, COLL><<<pair_grid(p), kPairBlock, 0, st>>>(p);
       return cudaGetLastError();
     } else {
       (void)p;

@@ -178,10 +178,11 @@ constexpr int kPairMinBlocks = AERO_PAIR_MINB;
 // Work split of the pair step.  The pairs (x, x+1), x even, of columns
 // [2, xb), xb = nx - 2 -- clear of the inlet column and of the outlet column
 // with the column it copies -- take two cells per thread; the edge columns 0,
-// 1 and [xb, nx) one cell per thread.  The grid is flat: per group of
-// kPairRows rows, the pair blocks of each row, then one edge block holding
-// the group's edge cells (so a warp of edge cells spans eight rows instead of
-// leaving most of its lanes idle, and edge blocks run among pair blocks).
+// 1 and [xb, nx) one cell per thread.  Grid: x = pair block of a row, y = row
+// of a group of kPairRows rows, z = group; y = kPairRows is the group's edge
+// block (x = 0 only), which holds the edge cells of all its rows, so a warp
+// of edge cells spans eight rows instead of leaving most of its lanes idle,
+// and edge blocks run among pair blocks.
 constexpr int kPairRows = kPairBlock / 4;
 
 struct PairSplit {
@@ -209,22 +210,19 @@ template <class L, class S, int COLL>
 __global__ void __launch_bounds__(kPairBlock, kPairMinBlocks) k_step_pair(const StepParams<float> p) {
   static_assert(L::DIMS == 3 && COLL == COLL_MRT, "the pair kernel covers the D3Q19 MRT step");
   const PairSplit sp = pair_split(p);
-  const uint32_t per_group = (uint32_t)(kPairRows * sp.row_blocks + 1);
-  const uint32_t g = blockIdx.x / per_group;
-  const uint32_t w = blockIdx.x - g * per_group;
   const int64_t step_now = *p.step;
-  if (w == per_group - 1) {
-    // edge block: cell k of row g * kPairRows + threadIdx.x / 4
+  if (blockIdx.y == kPairRows) {
+    // edge block: cell k of row blockIdx.z * kPairRows + threadIdx.x / 4
+    if (blockIdx.x != 0) return;
     const int k = threadIdx.x & 3;
-    const int r = (int)(g * kPairRows + (threadIdx.x >> 2));
+    const int r = (int)(blockIdx.z * kPairRows + (threadIdx.x >> 2));
     if (k >= sp.nedge || r >= sp.rows) return;
     const int y = r % p.ny, z = r / p.ny;
     step_cell<L, S, COLL>(p, k < 2 ? k : sp.xb + (k - 2), y, z, step_now, GlobalGather<L, S, float>{p, y, z});
     return;
   }
-  const uint32_t rb = w / (uint32_t)sp.row_blocks;
-  const int r = (int)(g * kPairRows + rb);
-  const int t = (int)(w - rb * (uint32_t)sp.row_blocks) * kPairBlock + (int)threadIdx.x;
+  const int r = (int)(blockIdx.z * kPairRows + blockIdx.y);
+  const int t = (int)(blockIdx.x * kPairBlock + threadIdx.x);
   if (r >= sp.rows || t >= sp.npairs) return;
   const int x = 2 + 2 * t, y = r % p.ny, z = r / p.ny;
   const uint32_t c = cell_index(p, x, y, z);
@@ -249,9 +247,9 @@ __global__ void __launch_bounds__(kPairBlock, kPairMinBlocks) k_step_pair(const 
 }
 
 template <class Real>
-inline unsigned pair_blocks(const StepParams<Real> &p) {
+inline dim3 pair_grid(const StepParams<Real> &p) {
   const PairSplit sp = pair_split(p);
-  return (unsigned)(sp.groups * ((int64_t)kPairRows * sp.row_blocks + 1));
+  return dim3((unsigned)(sp.row_blocks > 0 ? sp.row_blocks : 1), (unsigned)(kPairRows + 1), (unsigned)sp.groups);
 }
 
 }  // namespace aero
