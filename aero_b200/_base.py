@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import json
 import pathlib
+import threading
 import time
 import warnings
 from typing import Optional
@@ -416,6 +417,11 @@ class LatticeSolverBase:
             warnings.warn("hdf5_path is ignored by the b200 backend (h5py output is not part of the "
                           "engine)", RuntimeWarning)
         t0 = time.perf_counter()
+        if self.dims == 3:
+            # host arrays for the result's fields, their pages touched by a
+            # helper thread while the GPU steps (a gigabyte of fresh pages
+            # otherwise costs as long as the copy itself)
+            self._field_host = _HostBuffer((4,) + tuple(self.solid.shape))
         avg_window = max(1, steps // 5)
         stop_reason = "max_steps"
         last_conv = last_st = None
@@ -465,29 +471,34 @@ class LatticeSolverBase:
         _, _, g = self._engine.get_state_device(want_prev=False, want_g=True)
         return g.sum(dim=0).cpu().numpy()
 
-    def _macroscopic_device(self):
-        """rho, u of the current state, computed slab by slab on the GPU."""
+    def _macroscopic_host(self):
+        """rho, u of the current state as host arrays: computed on the GPU from
+        the population buffers (aero_get_macroscopic) and copied into the
+        arrays run() prepared, or fresh ones."""
         import torch
-        e, _, _ = tables(self.dims)
-        et = torch.tensor(e.astype(np.float64), device=self._engine.device)
-        if self.dims == 2:
-            f = self._engine.get_slab_device(0, 1)[:, 0]
-            return _moments_torch(f, et, 2)
-        nz = self.solid.shape[0]
-        plane = int(np.prod(self.solid.shape[1:]))
-        slab = max(1, min(nz, (1 << 27) // max(plane * self.Q, 1)))
-        outs = [[] for _ in range(4)]
-        for z0 in range(0, nz, slab):
-            nzs = min(slab, nz - z0)
-            f = self._engine.get_slab_device(z0, nzs)
-            for k, a in enumerate(_moments_torch(f, et, 3)):
-                outs[k].append(a)
-        return tuple(torch.cat(o) for o in outs)
+        dev = self._engine.macroscopic_device()
+        buf = getattr(self, "_field_host", None)
+        self._field_host = None
+        host = buf.get() if buf is not None and buf.shape == tuple(dev.shape) else np.empty(tuple(dev.shape))
+        torch.from_numpy(host).copy_(dev)
+        return tuple(host[k] for k in range(host.shape[0]))
 
 
-def _moments_torch(f, et, dims):
-    import torch
-    rho = f.sum(dim=0)
-    inv = torch.where(rho > 0, 1.0 / torch.where(rho > 0, rho, torch.ones_like(rho)), torch.zeros_like(rho))
-    u = [inv * torch.tensordot(et[:, a], f, dims=([0], [0])) for a in range(dims)]
-    return (rho, *u)
+class _HostBuffer:
+    """A float64 host array whose pages a daemon thread touches in the
+    background; get() waits for the thread and hands the array over."""
+
+    def __init__(self, shape):
+        self.shape = tuple(shape)
+        self._a = None
+        self._t = threading.Thread(target=self._fill, daemon=True)
+        self._t.start()
+
+    def _fill(self):
+        a = np.empty(self.shape)
+        a.reshape(-1)[::512] = 0.0  # one write per 4 KiB page
+        self._a = a
+
+    def get(self):
+        self._t.join()
+        return self._a

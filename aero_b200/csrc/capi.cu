@@ -815,6 +815,22 @@ int aero_get_state_slab(AeroLattice *L, int32_t z0, int32_t nzs, double *f, void
                     : do_get_state<float>(L, f, nullptr, nullptr, z0, nzs, st);
 }
 
+int aero_get_macroscopic(AeroLattice *L, double *out, void *stream) {
+  if (!L || !out) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->state_set) return fail(AERO_ERR_STATE, "no state set");
+  CUDA_TRY(cudaSetDevice(L->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const dim3 grid = cell_grid(L);
+  if (is_f64(L)) {
+    const StepParams<double> p = make_params<double>(L, 1 - L->cur);
+    CUDA_TRY(get_ops<double>(L)->macro_out(p, out, -1, L->old_is_state, 0, grid, st));
+  } else {
+    const StepParams<float> p = make_params<float>(L, 1 - L->cur);
+    CUDA_TRY(get_ops<float>(L)->macro_out(p, out, -1, L->old_is_state, 0, grid, st));
+  }
+  return AERO_OK;
+}
+
 int aero_params_size(void) { return (int)sizeof(AeroParams); }
 
 int aero_enable_timing(AeroLattice *L, int32_t on) {

@@ -18,6 +18,9 @@ struct Ops {
   cudaError_t (*state_out)(const StepParams<Real> &, double *out, int step_delta, bool raw, int z0, dim3 grid,
                            cudaStream_t);
   cudaError_t (*load_state)(const StepParams<Real> &, const double *in, void *dst, dim3 grid, cudaStream_t);
+  // like state_out, but writes rho, ux, uy[, uz] (1 + dims planes) instead of f
+  cudaError_t (*macro_out)(const StepParams<Real> &, double *out, int step_delta, bool raw, int z0, dim3 grid,
+                           cudaStream_t);
   // row-tiled step (k_step_tiled): persistent grid of `blocks` blocks
   cudaError_t (*step_tiled)(const StepParams<Real> &, int blocks, cudaStream_t);
   // on the current device: raises the kernel's dynamic shared-memory limit and

@@ -54,6 +54,15 @@ struct Launch {
       k_state_out<L, S, false><<<grid, kStepBlock, 0, st>>>(p, out, delta, z0, plane);
     return cudaGetLastError();
   }
+  static cudaError_t macro_out(const StepParams<Real> &p, double *out, int delta, bool raw, int z0, dim3 grid,
+                               cudaStream_t st) {
+    const int64_t plane = (int64_t)grid.z * p.ny * p.nx;
+    if (raw)
+      k_macro_out<L, S, true><<<grid, kStepBlock, 0, st>>>(p, out, delta, z0, plane);
+    else
+      k_macro_out<L, S, false><<<grid, kStepBlock, 0, st>>>(p, out, delta, z0, plane);
+    return cudaGetLastError();
+  }
   static cudaError_t load_state(const StepParams<Real> &p, const double *in, void *dst, dim3 grid,
                                 cudaStream_t st) {
     k_load_state<L, S><<<grid, kStepBlock, 0, st>>>(p, in, static_cast<S *>(dst));
@@ -109,9 +118,9 @@ struct Launch {
       return cudaErrorNotSupported;
     }
   }
-  static constexpr Ops<Real> table = {&step,       &step_shaped, &moments,    &finalize,      &state_out,     &load_state,
-                                      &step_tiled, &tiled_setup, &step_batch, &moments_batch, &finalize_batch,
-                                      &recycle_mean, &step_pair, (int)sizeof(S)};
+  static constexpr Ops<Real> table = {&step,       &step_shaped, &moments,      &finalize,   &state_out,
+                                      &load_state, &macro_out,   &step_tiled,   &tiled_setup, &step_batch,
+                                      &moments_batch, &finalize_batch, &recycle_mean, &step_pair, (int)sizeof(S)};
 };
 
 template <class S>

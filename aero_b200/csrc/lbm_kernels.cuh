@@ -1552,6 +1552,47 @@ __global__ void __launch_bounds__(kStepBlock) k_state_out(const StepParams<typen
   });
 }
 
+// Density and velocity of the state (compute_macroscopic(_3d), d2q9.py:44-63,
+// d3q19.py:80-102) straight from the population buffers: out holds planes
+// rho, ux, uy[, uz] of out_plane cells each (z0 .. z0 + gridDim.z - 1), FP64,
+// with f_i = w_i + d_i summed in direction order and u = (sum e_i f_i) / rho
+// taken as (1 / rho) * sum, 0 where rho <= 0, as the reference writes it.
+template <class L, class S, bool RAW>
+__global__ void __launch_bounds__(kStepBlock) k_macro_out(const StepParams<typename StoreOps<S>::Real> p,
+                                                          double *out, int step_delta, int z0, int64_t out_plane) {
+  using Real = typename StoreOps<S>::Real;
+  using SO = StoreOps<S>;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y, z = blockIdx.z + z0;
+  if (x >= p.nx) return;
+  const uint32_t c = cell_index(p, x, y, z);
+  Real d[L::Q];
+  if constexpr (RAW) {
+    const S *P = static_cast<const S *>(p.P);
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      d[i] = SO::template load<i, L>(P, elem(p, i, c));
+    });
+  } else {
+    full_state<L, S, Real>(p, x, y, z, *p.step + step_delta, d, nullptr, nullptr);
+  }
+  double rho = 0.0, jx = 0.0, jy = 0.0, jz = 0.0;
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    const double f = Dir<L, i>::w + (double)d[i];
+    rho += f;
+    jx += (double)Dir<L, i>::x * f;
+    jy += (double)Dir<L, i>::y * f;
+    if constexpr (L::DIMS == 3) jz += (double)Dir<L, i>::z * f;
+  });
+  const double inv = rho > 0.0 ? 1.0 / rho : 0.0;
+  const int64_t oc = (int64_t)c - (int64_t)z0 * p.ny * p.nx;
+  out[oc] = rho;
+  out[out_plane + oc] = inv * jx;
+  out[2 * out_plane + oc] = inv * jy;
+  if constexpr (L::DIMS == 3) out[3 * out_plane + oc] = inv * jz;
+}
+
 // Converts absolute FP64 populations (Q, ncells) into the storage format.
 template <class L, class S>
 __global__ void __launch_bounds__(kStepBlock) k_load_state(const StepParams<typename StoreOps<S>::Real> p,

@@ -126,6 +126,14 @@ class Engine:
                 self.h, int(z0), int(nzs), out.data_ptr(), self.stream()))
         return out
 
+    def macroscopic_device(self):
+        """(1 + dims, *shape) float64 device tensor: rho, ux, uy (, uz) of the state."""
+        t = self.torch
+        out = t.empty((1 + self.dims,) + self.shape, dtype=t.float64, device=self.device)
+        with t.cuda.device(self.device):
+            check("aero_get_macroscopic", self.lib.aero_get_macroscopic(self.h, out.data_ptr(), self.stream()))
+        return out
+
     def set_inflow(self, fields: np.ndarray, first_step: int) -> None:
         """Uploads the transverse inlet velocities of steps first_step.. (n, dims-1, nz*ny)."""
         a = np.ascontiguousarray(fields, dtype=np.float64)

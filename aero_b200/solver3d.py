@@ -155,7 +155,7 @@ class Solver3D(LatticeSolverBase):
         )
 
     def _result(self, avg_window, stop_reason, last_conv, last_st) -> dict:
-        rho, ux, uy, uz = (a.cpu().numpy() for a in self._macroscopic_device())
+        rho, ux, uy, uz = self._macroscopic_host()
         tail = lambda h: np.array(h[-avg_window:]) if h else np.zeros(1)
         r = {}
         for k in ("Cd", "Cly", "Clz", "Cmx", "Cmy", "Cmz"):

@@ -293,6 +293,13 @@ AERO_API int aero_params_size(void);
  * the mid plane, solver3d.py:608-615). */
 AERO_API int aero_get_state_slab(AeroLattice *lat, int32_t z0, int32_t nzs, double *f, void *stream);
 
+/* Density and velocity of the current state, computed on the device without
+ * materialising f: out (caller DEVICE memory) receives 1 + dims planes of
+ * nz*ny*nx doubles, rho, ux, uy (, uz).  Replaces compute_macroscopic(_3d)
+ * (d2q9.py:44-63, d3q19.py:80-102) on self.f, as Solver.run's result uses it
+ * (solver.py:603-632, solver3d.py:654-723).  Asynchronous. */
+AERO_API int aero_get_macroscopic(AeroLattice *lat, double *out, void *stream);
+
 /* ---- Surface links built on the device --------------------------------
  * Replaces build_surface_links (boundary.py:232-280) and
  * build_surface_links_3d (boundary3d.py:279-329) for geometry that already
