@@ -36,9 +36,13 @@ struct Ops {
                                 cudaStream_t);
   // mean ux of the recycle plane (3D recycling inlet), before the step kernel
   cudaError_t (*recycle_mean)(const StepParams<Real> &, cudaStream_t);
-  // regular step, two cells per thread (k_step_pair; D3Q19 MRT, 4-byte
+  // regular step, two cells per thread (k_step_pair; D3Q19, 4-byte
   // arithmetic); cudaErrorNotSupported for other classes
   cudaError_t (*step_pair)(const StepParams<Real> &, cudaStream_t);
+  // batched step of a class in the pair layout (k_step_batch_pair; D3Q19,
+  // 4-byte arithmetic); blocks = the members' pair_batch_layout blocks
+  cudaError_t (*step_batch_pair)(const StepParams<Real> *params, const int64_t *first, int n, int64_t blocks,
+                                 cudaStream_t);
   int store_bytes;
 };
 

@@ -108,8 +108,22 @@ struct Launch {
     }
     return cudaErrorInvalidValue;  // recycling exists in 3D only
   }
+  static cudaError_t step_batch_pair(const StepParams<Real> *params, const int64_t *first, int n, int64_t blocks,
+                                     cudaStream_t st) {
+    if constexpr (std::is_same<Real, float>::value && L::DIMS == 3) {
+      k_step_batch_pair<L, S, COLL><<<(unsigned)blocks, kPairBlock, 0, st>>>(params, first, n);
+      return cudaGetLastError();
+    } else {
+      (void)params;
+      (void)first;
+      (void)n;
+      (void)blocks;
+      (void)st;
+      return cudaErrorNotSupported;
+    }
+  }
   static cudaError_t step_pair(const StepParams<Real> &p, cudaStream_t st) {
-    if constexpr (std::is_same<Real, float>::value && L::DIMS == 3 && COLL == COLL_MRT) {
+    if constexpr (std::is_same<Real, float>::value && L::DIMS == 3) {
       k_step_pair<L, S, COLL><<<pair_grid(p), kPairBlock, 0, st>>>(p);
       return cudaGetLastError();
     } else {
@@ -120,7 +134,8 @@ struct Launch {
   }
   static constexpr Ops<Real> table = {&step,       &step_shaped, &moments,      &finalize,   &state_out,
                                       &load_state, &macro_out,   &step_tiled,   &tiled_setup, &step_batch,
-                                      &moments_batch, &finalize_batch, &recycle_mean, &step_pair, (int)sizeof(S)};
+                                      &moments_batch, &finalize_batch, &recycle_mean, &step_pair,
+                                      &step_batch_pair, (int)sizeof(S)};
 };
 
 template <class S>

@@ -1,13 +1,13 @@
-// lbm_pair.cuh -- the D3Q19 MRT step with two cells per thread on the packed
-// FP32 instructions of sm_100 (FADD2 / FMUL2 / FFMA2).
+// lbm_pair.cuh -- the D3Q19 step with two cells per thread on the packed FP32
+// instructions of sm_100 (FADD2 / FMUL2 / FFMA2), single lattices and batches.
 //
 // The per-cell step kernel is issue-bound once populations are 16-bit: its
 // collision, conversions and addressing take more instruction slots than the
 // halved bytes take DRAM time.  Here a thread takes the cells (x, x+1) of one
 // row, x even, in the columns clear of the inlet and the outlet.  When both
 // are plain fluid cells -- no flag bit (solid, link), not a wall row -- the
-// pair runs through the same sponge and collision (mrt3_core) with every
-// value a float2, so each arithmetic step is one instruction for both cells;
+// pair runs through the same sponge and collision (mrt3_core for MRT,
+// collide_pair_bt for BGK / TRT) with every value a float2, so each arithmetic step is one instruction for both cells;
 // the loads of directions with e_x = 0 and every store move both cells'
 // values as one aligned 8-byte (FP32) or 4-byte (16-bit) access.  Other pairs
 // run the per-cell step for each cell, and the edge columns run it in blocks
@@ -17,6 +17,8 @@
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+
+#include <type_traits>
 
 #include "lbm_kernels.cuh"
 
@@ -167,6 +169,104 @@ __device__ __forceinline__ void pair_sponge(const StepParams<float> &p, int x, F
   });
 }
 
+// BGK / TRT collision of the pair, the operations of collide() (BGK:
+// kernels.py:42-92, TRT: kernels_trt.py:125-174) lane by lane: moments,
+// per-direction equilibrium, relaxation as a correction to d.  om is the
+// pair's relaxation rate (the base rate, or each cell's LES rate, in which
+// case TRT derives each cell's s- from it).  Plain fluid cells: no solid.
+template <class L, int COLL>
+__device__ __forceinline__ F2 collide_pair_bt(const StepParams<float> &p, F2 (&d)[L::Q], F2 om,
+                                              bool per_cell_omega) {
+  F2 drho(0.f), jx(0.f), jy(0.f), jz(0.f);
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    drho = drho + d[i];
+    if constexpr (Dir<L, i>::x > 0) jx = jx + d[i];
+    if constexpr (Dir<L, i>::x < 0) jx = jx - d[i];
+    if constexpr (Dir<L, i>::y > 0) jy = jy + d[i];
+    if constexpr (Dir<L, i>::y < 0) jy = jy - d[i];
+    if constexpr (Dir<L, i>::z > 0) jz = jz + d[i];
+    if constexpr (Dir<L, i>::z < 0) jz = jz - d[i];
+  });
+  const F2 rho = F2(1.f) + drho;
+  const F2 inv = pos_recip(rho);
+  const F2 ux = jx * inv, uy = jy * inv, uz = jz * inv;
+  const F2 usq = ux * ux + uy * uy + uz * uz;
+  // equilibrium deviation of direction i, evaluated where it is used (no
+  // array of 19 values stays live beside the populations)
+  auto deq = [&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    constexpr int ex = Dir<L, i>::x, ey = Dir<L, i>::y, ez = Dir<L, i>::z;
+    F2 eu(0.f);
+    if constexpr (ex > 0) eu = eu + ux;
+    if constexpr (ex < 0) eu = eu - ux;
+    if constexpr (ey > 0) eu = eu + uy;
+    if constexpr (ey < 0) eu = eu - uy;
+    if constexpr (ez > 0) eu = eu + uz;
+    if constexpr (ez < 0) eu = eu - uz;
+    const F2 poly = 3.f * eu + (4.5f * eu) * eu - 1.5f * usq;
+    return F2(float(Dir<L, i>::w) * (drho + rho * poly));
+  };
+  if constexpr (COLL == COLL_TRT) {
+    F2 sm(p.trt_sminus);
+    if (per_cell_omega) {
+      float smv[2];
+      const float omv[2] = {om.v.x, om.v.y};
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        const float tau = 1.f / omv[k], lam = p.trt_lambda;
+        const float tp = lam * tau + (1.f - lam);
+        const float tm = (tp * tau - 0.5f) / (tp - 0.5f);
+        smv[k] = 1.f / tm;
+      }
+      sm = F2(make_float2(smv[0], smv[1]));
+    }
+    d[0] = d[0] + om * (deq(std::integral_constant<int, 0>{}) - d[0]);
+    static_for<L::NP>([&](auto pc) {
+      constexpr int k = decltype(pc)::value;
+      constexpr int i = L::pair[k], o = L::opp[L::pair[k]];
+      const F2 qi = deq(std::integral_constant<int, i>{}), qo = deq(std::integral_constant<int, o>{});
+      const F2 fp = 0.5f * (d[i] + d[o]), fm = 0.5f * (d[i] - d[o]);
+      const F2 ep = 0.5f * (qi + qo), em = 0.5f * (qi - qo);
+      const F2 a = om * (ep - fp), b = sm * (em - fm);
+      d[i] = d[i] + (a + b);
+      d[o] = d[o] + (a - b);
+    });
+  } else {
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      d[i] = d[i] + om * (deq(ic) - d[i]);
+    });
+  }
+  return rho;
+}
+
+// The step of a plain pair (x, x+1), x even, c its first cell: gather,
+// sponge, collision (MRT in the adapted basis, or BGK / TRT with the LES
+// rate of each cell), divergence guard, store.
+template <class L, class S, int COLL>
+__device__ __forceinline__ void pair_step_plain(const StepParams<float> &p, int x, int y, int z, uint32_t c,
+                                                int64_t step_now) {
+  F2 d[L::Q];
+  pair_gather<L, S>(p, x, y, z, d);
+  pair_sponge<L>(p, x, d);
+  F2 rho;
+  if constexpr (COLL == COLL_MRT) {
+    rho = mrt3_core<float, F2>(p.mrt3, d, false);
+  } else {
+    const bool les = p.feat & FEAT_LES;
+    F2 om(p.omega);
+    if (les) om = F2(make_float2(les_omega<L>(p, x, y, z, c, false), les_omega<L>(p, x + 1, y, z, c + 1, false)));
+    rho = collide_pair_bt<L, COLL>(p, d, om, les);
+  }
+  guard_bad(p, !(rho.v.x > 0.f) || !isfinite(rho.v.x) || !(rho.v.y > 0.f) || !isfinite(rho.v.y), step_now);
+  S *Pn = static_cast<S *>(p.Pn);
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    PairOps<S>::template store<i, L>(Pn, elem(p, i, c), d[i]);
+  });
+}
+
 // Resident blocks of 128 threads per SM the pair kernel is built for (7: 72
 // registers a thread, the most blocks without spills).
 #ifndef AERO_PAIR_MINB
@@ -208,7 +308,7 @@ __host__ __device__ __forceinline__ PairSplit pair_split(const StepParams<Real> 
 // step_cell.
 template <class L, class S, int COLL>
 __global__ void __launch_bounds__(kPairBlock, kPairMinBlocks) k_step_pair(const StepParams<float> p) {
-  static_assert(L::DIMS == 3 && COLL == COLL_MRT, "the pair kernel covers the D3Q19 MRT step");
+  static_assert(L::DIMS == 3, "the pair kernel covers the D3Q19 step");
   const PairSplit sp = pair_split(p);
   const int64_t step_now = *p.step;
   if (blockIdx.y == kPairRows) {
@@ -229,21 +329,55 @@ __global__ void __launch_bounds__(kPairBlock, kPairMinBlocks) k_step_pair(const 
   bool plain = !(p.wall != WALL_NONE && (y == 0 || y == p.ny - 1));
   if (plain) plain = *reinterpret_cast<const uint16_t *>(p.flags + c) == 0;  // both flag bytes, c even
   if (plain) {
-    F2 d[L::Q];
-    pair_gather<L, S>(p, x, y, z, d);
-    pair_sponge<L>(p, x, d);
-    const F2 rho = mrt3_core<float, F2>(p.mrt3, d, false);
-    guard_bad(p, !(rho.v.x > 0.f) || !isfinite(rho.v.x) || !(rho.v.y > 0.f) || !isfinite(rho.v.y), step_now);
-    S *Pn = static_cast<S *>(p.Pn);
-    static_for<L::Q>([&](auto ic) {
-      constexpr int i = decltype(ic)::value;
-      PairOps<S>::template store<i, L>(Pn, elem(p, i, c), d[i]);
-    });
+    pair_step_plain<L, S, COLL>(p, x, y, z, c, step_now);
     return;
   }
   const GlobalGather<L, S, float> gather{p, y, z};
 #pragma unroll 1
   for (int k = 0; k < 2; k++) step_cell<L, S, COLL>(p, x + k, y, z, step_now, gather);
+}
+
+// The batched step (k_step_batch) of a lattice class whose members all take
+// the pair layout (pair_batch_layout): D3Q19, even nx >= 6, no body force or
+// scalar lattice.  The member's parameters are copied into shared memory as
+// in k_step_batch.
+template <class L, class S, int COLL>
+__global__ void __launch_bounds__(kPairBlock, kPairMinBlocks)
+    k_step_batch_pair(const StepParams<float> *__restrict__ params, const int64_t *__restrict__ first,
+                      int nmembers) {
+  static_assert(L::DIMS == 3, "the pair kernel covers the D3Q19 step");
+  __shared__ StepParams<float> sp;
+  const int m = find_member(first, nmembers, blockIdx.x);
+  params_to_smem(sp, params + m);
+  const int64_t b = (int64_t)blockIdx.x - __ldg(first + m);
+  const PairBatchLayout lay = pair_batch_layout(sp.nx, sp.ny, sp.nz);
+  const int64_t step_now = *sp.step;
+  if (b >= lay.pair_blocks) {
+    // edge block: cell k of row 32 * e + threadIdx.x / 4
+    const int k = threadIdx.x & 3;
+    const int64_t r = (b - lay.pair_blocks) * 32 + (threadIdx.x >> 2);
+    if (r >= lay.rows) return;
+    const int y = (int)(r % sp.ny), z = (int)(r / sp.ny);
+    step_cell<L, S, COLL>(sp, k < 2 ? k : sp.nx - 4 + k, y, z, step_now, GlobalGather<L, S, float>{sp, y, z});
+    return;
+  }
+  const int64_t g = b / lay.bpr;
+  const int t = (int)(b - g * lay.bpr) * kPairBlock + (int)threadIdx.x;
+  const int rl = lay.TP <= kPairBlock ? t / lay.TP : 0;
+  const int k = lay.TP <= kPairBlock ? t - rl * lay.TP : t;
+  const int64_t r = g * lay.RB + rl;
+  if (rl >= lay.RB || r >= lay.rows || k >= lay.P) return;
+  const int x = 2 + 2 * k, y = (int)(r % sp.ny), z = (int)(r / sp.ny);
+  const uint32_t c = cell_index(sp, x, y, z);
+  bool plain = !(sp.wall != WALL_NONE && (y == 0 || y == sp.ny - 1));
+  if (plain) plain = *reinterpret_cast<const uint16_t *>(sp.flags + c) == 0;  // both flag bytes, c even
+  if (plain) {
+    pair_step_plain<L, S, COLL>(sp, x, y, z, c, step_now);
+    return;
+  }
+  const GlobalGather<L, S, float> gather{sp, y, z};
+#pragma unroll 1
+  for (int kk = 0; kk < 2; kk++) step_cell<L, S, COLL>(sp, x + kk, y, z, step_now, gather);
 }
 
 template <class Real>

@@ -135,4 +135,29 @@ struct StepParams {
   Mrt3Adapted<Real> mrt3;   // D3Q19
 };
 
+// Block layout of one lattice in the two-cells-per-thread batch kernel
+// (128-thread blocks).  A row's P pairs (x, x+1), x = 2, 4, .., nx - 4, take
+// TP threads (P rounded up to whole warps); a block holds RB rows of them
+// (TP <= 128) or a row takes bpr blocks (TP > 128).  The four edge cells of
+// a row (x = 0, 1, nx - 2, nx - 1) follow, 32 rows per block.  nx even.
+struct PairBatchLayout {
+  int P, TP, RB, bpr;
+  int64_t rows, pair_blocks, edge_blocks;
+};
+
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline PairBatchLayout pair_batch_layout(int nx, int ny, int nz) {
+  PairBatchLayout l;
+  l.P = nx >= 6 ? (nx - 4) / 2 : 0;
+  l.TP = (l.P + 31) / 32 * 32;
+  l.RB = (l.TP > 0 && l.TP <= 128) ? 128 / l.TP : 1;
+  l.bpr = l.TP > 128 ? (l.TP + 127) / 128 : 1;
+  l.rows = (int64_t)ny * nz;
+  l.pair_blocks = l.P > 0 ? (l.rows + l.RB - 1) / l.RB * l.bpr : 0;
+  l.edge_blocks = (l.rows + 31) / 32;
+  return l;
+}
+
 }  // namespace aero

@@ -135,7 +135,7 @@ class Server:
 
     def __init__(self, hbm_cap: float = 150e9, max_members: int = 256, chunk: int = 200,
                  window: int = 2000, tol: float = 1e-3, device=None, hist_capacity: int = 4096,
-                 on_admit=None, admit_per_round: int = 8, on_round=None):
+                 on_admit=None, admit_per_round: int = 64, on_round=None, admit_idle: int = 8):
         if window > hist_capacity:
             raise ValueError("the convergence window must fit the force history ring")
         self.hbm_cap = float(hbm_cap)
@@ -150,9 +150,14 @@ class Server:
         # optional callback(case, solver) run before a new solver joins the
         # batch, e.g. to set a state of its own
         self.on_admit = on_admit
-        # requests set up per round: the rest wait for the next round, so a
-        # burst of arrivals does not hold the GPU idle behind serial set-up
+        # requests set up per round.  While a chunk runs, set-up continues as
+        # long as this round's set-up time stays below the previous chunk's
+        # GPU time (so it hides behind the chunk), up to admit_per_round;
+        # with nothing running, or before a chunk has been timed, at most
+        # admit_idle, so a burst of arrivals does not hold the GPU idle
+        # behind serial set-up
         self.admit_per_round = max(int(admit_per_round), 1)
+        self.admit_idle = max(int(admit_idle), 1)
         # optional callback(server, round) after each round, e.g. to cancel requests
         self.on_round = on_round
         self.cancelled = set()
@@ -183,8 +188,10 @@ class Server:
         wait_s = 0.0
         t0 = clock()
         rounds = 0
+        chunk_s = None  # launch-to-result time of the last chunk
         while pending or queue or active:
             stepped = bool(active)
+            t_launch = clock()
             if stepped:
                 self.batch.step(self.chunk)
                 cell_steps += self.chunk * sum(_cells(a[0]) for a in active)
@@ -198,8 +205,10 @@ class Server:
                                           _cells(c), 0))
             # admission, first come first served, by device footprint
             joining = []
-            while (queue and len(active) + len(joining) < self.max_members
-                   and len(joining) < self.admit_per_round):
+            budget = chunk_s if (stepped and chunk_s is not None) else None
+            cap = self.admit_per_round if budget is not None else self.admit_idle
+            while (queue and len(active) + len(joining) < self.max_members and len(joining) < cap
+                   and (budget is None or not joining or clock() - t_launch < budget)):
                 c = queue[0]
                 need = footprint(c, self.hist_capacity)
                 if need > self.hbm_cap:
@@ -224,6 +233,12 @@ class Server:
                 tw = clock()
                 table = self.batch.converge(self.window, self.tol)  # waits for the chunk
                 wait_s += clock() - tw
+                if clock() - tw > 1e-4:
+                    # the chunk outlasted this round's set-up, so the wait
+                    # ended with it: launch-to-result is its GPU time
+                    chunk_s = clock() - t_launch
+                elif chunk_s is not None:
+                    chunk_s *= 0.5  # set-up outlasted the chunk: the GPU idled, admit fewer
                 rounds += 1
                 t = clock() - t0
                 keep = []

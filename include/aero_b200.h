@@ -165,8 +165,8 @@ AERO_API int aero_step_plan(const AeroLattice *lat, int32_t *tiled, int32_t *til
  * 0, 1, 2 = the per-cell-gather kernel with blocks of 128x1, 256x1 or 32x4
  * cells (x by y); 3 = the row-tiled kernel (AERO_ERR_UNSUPPORTED where rows
  * do not fit it); 4 = two cells per thread on packed FP32 arithmetic (D3Q19
- * MRT, FP32/FP16/BF16 storage, even nx, no body force or scalar lattice;
- * else AERO_ERR_UNSUPPORTED).  Results are the same for every choice up to
+ * BGK/TRT/MRT, FP32/FP16/BF16 storage, even nx, no body force or scalar
+ * lattice; else AERO_ERR_UNSUPPORTED).  Results are the same for every choice up to
  * FP rounding of the compiled variant.  Takes effect at the next aero_step. */
 AERO_API int aero_set_step_kernel(AeroLattice *lat, int32_t kernel);
 AERO_API int aero_get_step_kernel(const AeroLattice *lat, int32_t *kernel);

@@ -33,7 +33,9 @@ def test_batch_create_checks_arguments():
 
 def _cases():
     """Solver constructors of mixed class: 2D/3D, BGK/TRT/MRT, LES (moments
-    pass), thermal scalar, fp32/fp64/fp16s/bf16s, Bouzidi, uneven sizes."""
+    pass), thermal scalar, fp32/fp64/fp16s/bf16s, Bouzidi, uneven sizes.  The
+    16-bit 3D members without body force or scalar and with even nx run in
+    the two-cells-per-thread batch kernel."""
     from aero_b200 import Box, Cylinder, Rectangle, Solver, Solver3D, Sphere
 
     def c2d(ny, nx, geo, **kw):
@@ -58,6 +60,9 @@ def _cases():
             precision="fp32"),
         c3d(12, 14, 30, Sphere(radius=3, cx_frac=0.3, cy_frac=0.5, cz_frac=0.5), omega=1 / 0.7, u0=0.05,
             collision="bgk", les=True, les_cs=0.1, wall_bc="noslip", precision="fp16s"),
+        c3d(14, 12, 36, Sphere(radius=3, cx_frac=0.3, cy_frac=0.5, cz_frac=0.5), omega=1 / 0.8, u0=0.05,
+            collision="trt", trt_lambda=0.25, les=True, les_cs=0.12, wall_bc="slip", sponge_thickness=5,
+            precision="fp16s"),
         c3d(12, 16, 24, Box(width=4, height=4, depth=12, cx_frac=0.3, cy_frac=0.25, cz_frac=0.5),
             omega=1 / 0.8, u0=0.05, collision="trt", trt_lambda=0.25, wall_bc="noslip", streamwise_bc="periodic",
             body_force_x=1e-6, thermal=True, alpha_T=0.02, buoyancy=True, g_gravity=1e-4, beta=1.0,

@@ -1,6 +1,6 @@
-"""The two-cells-per-thread D3Q19 MRT step kernel (step kernel 4, packed FP32
-arithmetic) against the per-cell kernel, the reference fixtures and the FP64
-oracle.
+"""The two-cells-per-thread D3Q19 step kernel (step kernel 4, packed FP32
+arithmetic; MRT, BGK and TRT) against the per-cell kernel, the reference
+fixtures and the FP64 oracle.
 
 Tolerances: each lane runs the per-cell step's operations in the same order;
 only the fusion of a product into a sum may differ, an FP32 rounding per
@@ -20,12 +20,20 @@ PAIR = 4
 TOL = {"fp32": 1e-6, "fp16s": 1e-4, "bf16s": 1e-3}
 
 
-def _sphere(precision, kernel, nz=20, ny=22, nx=64, steps=60):
+# TRT runs at tau 0.8: with the reference's lambda semantics (trt2d.py:8-18)
+# tau 0.6 gives s- = 10 and diverges.  BGK and TRT run with Smagorinsky LES,
+# so each cell of a pair relaxes at its own rate.
+COLL = {"mrt": dict(collision="mrt", omega=1 / 0.6),
+        "bgk": dict(collision="bgk", omega=1 / 0.6, les=True, les_cs=0.15),
+        "trt": dict(collision="trt", omega=1 / 0.8, les=True, les_cs=0.15, trt_lambda=0.25)}
+
+
+def _sphere(precision, kernel, nz=20, ny=22, nx=64, steps=60, collision="mrt"):
     from aero_b200 import Solver3D, Sphere
     sph = Sphere(radius=4, cx_frac=0.3, cy_frac=0.5, cz_frac=0.5)
     solid, phi = sph.mark_solid(nz, ny, nx), sph.sdf_field(nz, ny, nx)
-    kw = dict(omega=1 / 0.6, u0=0.05, D=sph.reference_length(), collision="mrt", bouzidi=True, phi=phi,
-              wall_bc="slip", outlet_bc="convective", sponge_thickness=6, inlet_perturbation=0.05)
+    kw = dict(u0=0.05, D=sph.reference_length(), bouzidi=True, phi=phi, wall_bc="slip",
+              outlet_bc="convective", sponge_thickness=6, inlet_perturbation=0.05, **COLL[collision])
     s = Solver3D(Nz=nz, Ny=ny, Nx=nx, solid=solid, precision=precision, **kw)
     s._engine.set_step_kernel(kernel)
     assert s._engine.get_step_kernel() == kernel
@@ -33,12 +41,13 @@ def _sphere(precision, kernel, nz=20, ny=22, nx=64, steps=60):
     return s.f, np.array(r["Cd_history"])
 
 
+@pytest.mark.parametrize("collision", ["mrt", "bgk", "trt"])
 @pytest.mark.parametrize("precision", ["fp32", "fp16s", "bf16s"])
-def test_pair_kernel_equals_per_cell_kernel(precision):
-    """3D MRT + Bouzidi sphere with slip walls (wall rows), sponge and
-    convective outlet (per-cell fallback columns), y and z wrap."""
-    fa, cda = _sphere(precision, PAIR)
-    fb, cdb = _sphere(precision, 0)
+def test_pair_kernel_equals_per_cell_kernel(precision, collision):
+    """3D Bouzidi sphere with slip walls (wall rows), sponge and convective
+    outlet (per-cell edge columns), y and z wrap; MRT, and BGK / TRT with LES."""
+    fa, cda = _sphere(precision, PAIR, collision=collision)
+    fb, cdb = _sphere(precision, 0, collision=collision)
     np.testing.assert_allclose(fa, fb, rtol=0, atol=TOL[precision] * np.abs(fb).max())
     np.testing.assert_allclose(cda, cdb, rtol=0, atol=10 * TOL[precision] * np.abs(cdb).max())
 
@@ -105,8 +114,7 @@ def test_pair_kernel_refused_outside_its_cover():
         args.update(kw)
         return Solver3D(Nz=12, Ny=12, Nx=nx, solid=solid, **args)
 
-    for s in (make(nx=33), make(collision="bgk"), make(precision="fp64"),
-              make(body_force_x=1e-6, streamwise_bc="periodic")):
+    for s in (make(nx=33), make(precision="fp64"), make(body_force_x=1e-6, streamwise_bc="periodic")):
         with pytest.raises(AeroError, match="AERO_ERR_UNSUPPORTED"):
             s._engine.set_step_kernel(PAIR)
         assert s._engine.get_step_kernel() == 0
