@@ -7,13 +7,14 @@
 // row, x even, in the columns clear of the inlet and the outlet.  When both
 // are plain fluid cells -- no flag bit (solid, link), not a wall row -- the
 // pair runs through the same sponge and collision (mrt3_core for MRT,
-// collide_pair_bt for BGK / TRT) with every value a float2, so each arithmetic step is one instruction for both cells;
-// the loads of directions with e_x = 0 and every store move both cells'
-// values as one aligned 8-byte (FP32) or 4-byte (16-bit) access.  Other pairs
-// run the per-cell step for each cell, and the edge columns run it in blocks
-// of their own.  Each lane does the per-cell step's operations in the same
-// order; only where the per-cell compile fuses a product into a sum
-// differently can the last bit differ.
+// collide_pair_bt for BGK / TRT) with every value a float2, so each
+// arithmetic step is one instruction for both cells; the loads of directions
+// with e_x = 0 and every store move both cells' values as one aligned 8-byte
+// (FP32) or 4-byte (16-bit) access.  Other pairs run the per-cell step for
+// each cell, and the edge columns run it in blocks of their own.  Each lane
+// does the per-cell step's operations in the same order; only where the
+// per-cell compile fuses a product into a sum differently can the last bit
+// differ.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
