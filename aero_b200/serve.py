@@ -151,8 +151,9 @@ class Server:
         # batch, e.g. to set a state of its own
         self.on_admit = on_admit
         # requests set up per round.  While a chunk runs, set-up continues as
-        # long as this round's set-up time stays below the previous chunk's
-        # GPU time (so it hides behind the chunk), up to admit_per_round;
+        # long as this round's set-up time plus one more set-up (at its
+        # running mean) stays within the previous chunk's GPU time (so it
+        # hides behind the chunk), up to admit_per_round;
         # with nothing running, or before a chunk has been timed, at most
         # admit_idle, so a burst of arrivals does not hold the GPU idle
         # behind serial set-up
@@ -189,6 +190,7 @@ class Server:
         t0 = clock()
         rounds = 0
         chunk_s = None  # launch-to-result time of the last chunk
+        setup_avg = None  # running mean of one request's set-up time
         while pending or queue or active:
             stepped = bool(active)
             t_launch = clock()
@@ -208,7 +210,7 @@ class Server:
             budget = chunk_s if (stepped and chunk_s is not None) else None
             cap = self.admit_per_round if budget is not None else self.admit_idle
             while (queue and len(active) + len(joining) < self.max_members and len(joining) < cap
-                   and (budget is None or not joining or clock() - t_launch < budget)):
+                   and (budget is None or not joining or clock() - t_launch + (setup_avg or 0.0) <= budget)):
                 c = queue[0]
                 need = footprint(c, self.hist_capacity)
                 if need > self.hbm_cap:
@@ -226,7 +228,9 @@ class Server:
                     if self.on_admit is not None:
                         self.on_admit(c, s)
                         s._flush_host_state()
-                setup_s += clock() - ts
+                dt = clock() - ts
+                setup_s += dt
+                setup_avg = dt if setup_avg is None else 0.8 * setup_avg + 0.2 * dt
                 used += need
                 joining.append((c, s, clock() - t0, need))
             if stepped:

@@ -215,3 +215,73 @@ def test_cancelled_requests_leave_and_others_finish():
     clean.close()
     for k in (0, 2, 3, 5):
         assert (res[k].status, res[k].steps, res[k].cd_mean) == (ref[k].status, ref[k].steps, ref[k].cd_mean)
+
+
+def test_admission_is_budgeted_by_the_chunk_time(monkeypatch):
+    """While a chunk runs, requests are set up until one more set-up would
+    outlast the previous chunk's GPU time: with a 50 ms chunk and 4 ms per
+    set-up, 12 a round once the chunk is timed; 8 (admit_idle) before that.
+    Simulated clock, fake batch and solvers: no GPU."""
+    import contextlib
+    import sys
+    import types
+
+    t = [0.0]
+    clock = lambda: t[0]
+
+    def sleep(dt):
+        t[0] += dt
+
+    class FakeBatch:
+        chunk_time = 0.05
+
+        def __init__(self, *a, **k):
+            self.device = None
+            self.members = []
+            self.steps = {}
+            self.joins = [0]       # joins after each round's admissions
+            self.launched = None
+
+        def step(self, n):
+            self.launched = t[0]
+            for s in self.members:
+                self.steps[id(s)] += n
+
+        def converge(self, window, tol):
+            t[0] = max(t[0], self.launched + self.chunk_time)  # waits for the chunk
+            self.joins.append(0)
+            rows = np.zeros((len(self.members), len(serve.CONVERGE_FIELDS)))
+            for k, s in enumerate(self.members):
+                rows[k, serve._F["steps"]] = self.steps[id(s)]
+                rows[k, serve._F["ratio"]] = math.inf
+            return rows
+
+        def add(self, s):
+            self.members.append(s)
+            self.steps[id(s)] = 0
+            self.joins[-1] += 1
+
+        def remove(self, s):
+            self.members.remove(s)
+
+        def close(self):
+            pass
+
+    def fake_solver(case, device=None, hist_capacity=4096):
+        t[0] += 0.004  # set-up time of one request
+        return types.SimpleNamespace(case=case)
+
+    monkeypatch.setattr(serve, "Batch", FakeBatch)
+    monkeypatch.setattr(serve, "make_solver", fake_solver)
+    fake_torch = types.SimpleNamespace(cuda=types.SimpleNamespace(
+        synchronize=lambda d=None: None, Stream=lambda d=None: None, stream=lambda s: contextlib.nullcontext()))
+    monkeypatch.setitem(sys.modules, "torch", fake_torch)
+    cases = [serve.Case(i, 2, 64, 32, max_steps=40) for i in range(60)]
+    srv = serve.Server(hbm_cap=1e12, max_members=256, chunk=10, window=10, tol=0.0)
+    res = srv.run(cases, clock=clock, sleep=sleep)
+    joins = srv.batch.joins
+    srv.close()
+    assert joins[:3] == [8, 8, 12]
+    assert all(j <= 12 for j in joins)
+    assert sorted(r.id for r in res) == list(range(60))
+    assert all(r.status == "max_steps" and r.steps == 40 for r in res)
