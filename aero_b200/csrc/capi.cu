@@ -1288,9 +1288,9 @@ int batch_build(AeroBatch *B, cudaStream_t st) {
     return at;
   };
   auto cell_blocks = [](const AeroLattice *L) {
-    const int64_t rows = (int64_t)L->prm.ny * L->prm.nz;
     const int64_t R = L->ncells < kBatchSmallCells ? 1 : kBatchRows;  // as make_params' batch_rows
-    return (int64_t)blocks_for(L->prm.nx, kStepBlock) * ((rows + R - 1) / R);
+    const int64_t per_block = R * kStepBlock;                          // consecutive cells of a block
+    return (L->ncells + per_block - 1) / per_block;
   };
   auto step_blocks = [&](const AeroLattice *L, bool pair) {
     if (!pair) return cell_blocks(L);

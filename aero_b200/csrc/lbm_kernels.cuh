@@ -1419,9 +1419,8 @@ __global__ void __launch_bounds__(kFinalizeBlock) k_finalize(const StepParams<Re
 // --------------------------------------------------------------------------
 // Batched stepping: many lattices of one class (lattice, storage format,
 // collision) advance in one launch.  Member m owns blocks [first[m],
-// first[m + 1]) of the grid, with the same cell mapping as the single-lattice
-// kernel (one block per kStepBlock-cell x segment of kBatchRows rows, or per
-// finalisation block); each block copies its member's parameters into shared
+// first[m + 1]) of the grid (blocks of consecutive cells, or finalisation
+// blocks); each block copies its member's parameters into shared
 // memory, then runs the same per-cell code.  The parameter arrays live in
 // device memory, so a captured launch stays valid while the members advance.
 // --------------------------------------------------------------------------
@@ -1465,11 +1464,13 @@ __device__ __forceinline__ void params_to_smem(StepParams<Real> &dst, const Step
   __syncthreads();
 }
 
-// A block of a batched cell kernel covers one kStepBlock-cell x segment of
-// batch_rows consecutive rows (y, then z) of its member: kBatchRows for
-// large members, so the member lookup and the parameter copy are paid once
-// per kBatchRows segments, and 1 for members below kBatchSmallCells, so a
-// few small members still spread over the whole GPU.
+// A block of a batched cell kernel covers batch_rows * kStepBlock
+// consecutive cells of its member in C order (batch_rows passes of one cell
+// per thread): kBatchRows for large members, so the member lookup and the
+// parameter copy are paid once per kBatchRows passes, and 1 for members below
+// kBatchSmallCells, so a few small members still spread over the whole GPU.
+// Cells rather than x segments: rows of 96 or 160 cells would leave a quarter
+// or more of a 128-thread block idle.
 constexpr int kBatchRows = 4;
 constexpr int64_t kBatchSmallCells = 1 << 16;
 
@@ -1481,16 +1482,17 @@ __global__ void __launch_bounds__(kStepBlock, sizeof(typename StoreOps<S>::Real)
   __shared__ StepParams<Real> sp;
   const int m = find_member(first, nmembers, blockIdx.x);
   params_to_smem(sp, params + m);
+  // block b takes cells [b, b + 1) * R * kStepBlock of the member in C order
+  // (R = batch_rows passes of kStepBlock consecutive cells), so rows shorter
+  // or longer than a block leave no thread idle but in the member's last block
   const int64_t b = (int64_t)blockIdx.x - __ldg(first + m);
-  const int nxb = (sp.nx + kStepBlock - 1) / kStepBlock;
-  const int64_t rg = b / nxb;
-  const int x = (int)(b - rg * nxb) * kStepBlock + threadIdx.x;
-  if (x >= sp.nx) return;
-  const int64_t nrows = (int64_t)sp.ny * sp.nz;
   const int64_t step_now = *sp.step;
   const int R = sp.batch_rows;
-  for (int64_t row = rg * R; row < nrows && row < (rg + 1) * R; ++row) {
-    const int y = (int)(row % sp.ny), z = (int)(row / sp.ny);
+  for (int k = 0; k < R; ++k) {
+    const int64_t c = (b * R + k) * kStepBlock + threadIdx.x;
+    if (c >= sp.ncells) return;
+    const int64_t row = c / sp.nx;
+    const int x = (int)(c - row * sp.nx), y = (int)(row % sp.ny), z = (int)(row / sp.ny);
     step_cell<L, S, COLL>(sp, x, y, z, step_now, GlobalGather<L, S, Real>{sp, y, z});
   }
 }
@@ -1502,15 +1504,15 @@ __global__ void __launch_bounds__(kStepBlock) k_moments_batch(const StepParams<t
   __shared__ StepParams<Real> sp;
   const int m = find_member(first, nmembers, blockIdx.x);
   params_to_smem(sp, params + m);
+  // the cell blocks of k_step_batch
   const int64_t b = (int64_t)blockIdx.x - __ldg(first + m);
-  const int nxb = (sp.nx + kStepBlock - 1) / kStepBlock;
-  const int64_t rg = b / nxb;
-  const int x = (int)(b - rg * nxb) * kStepBlock + threadIdx.x;
-  if (x >= sp.nx) return;
-  const int64_t nrows = (int64_t)sp.ny * sp.nz;
   const int R = sp.batch_rows;
-  for (int64_t row = rg * R; row < nrows && row < (rg + 1) * R; ++row)
-    moments_cell<L, S, false>(sp, x, (int)(row % sp.ny), (int)(row / sp.ny));
+  for (int k = 0; k < R; ++k) {
+    const int64_t c = (b * R + k) * kStepBlock + threadIdx.x;
+    if (c >= sp.ncells) return;
+    const int64_t row = c / sp.nx;
+    moments_cell<L, S, false>(sp, (int)(c - row * sp.nx), (int)(row % sp.ny), (int)(row / sp.ny));
+  }
 }
 
 template <class Real>
