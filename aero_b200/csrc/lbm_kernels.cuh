@@ -778,17 +778,15 @@ AERO_HD Real collide(const StepParams<Real> &p, Real (&d)[L::Q], bool solid, Rea
     (void)om;
     (void)per_cell_omega;
   } else {
-    // BGK / TRT.  The equilibrium is evaluated per direction exactly as the
-    // reference writes it, and the update is applied as a correction to d
-    // (d + omega (feq - d)); both choices keep the FP32 rounding smallest
-    // (measured against the FP64 oracle on the 400x200 channel).
+    // BGK / TRT.  The equilibrium of an opposite pair (i, o) splits into an
+    // even part w (drho + rho (4.5 (e.u)^2 - 1.5 u^2)), shared by both, and an
+    // odd part 3 w rho (e.u), taken with opposite signs (the reference's
+    // w rho (1 + 3 e.u + 4.5 (e.u)^2 - 1.5 u^2) in deviation form); each part
+    // is evaluated once per pair.  The update is applied as a correction to d
+    // (d + omega (feq - d)), which keeps the FP32 rounding small.
     const Real usq = ux * ux + uy * uy + uz * uz;
-    Real deq[L::Q];
-    static_for<L::Q>([&](auto ic) {
-      constexpr int i = decltype(ic)::value;
-      const Real eu = Dir<L, i>::x * ux + Dir<L, i>::y * uy + Dir<L, i>::z * uz;
-      deq[i] = Real(Dir<L, i>::w) * (drho + rho * (Real(3) * eu + Real(4.5) * eu * eu - Real(1.5) * usq));
-    });
+    const Real u15 = Real(1.5) * usq;
+    const Real deq0 = Real(Dir<L, 0>::w) * (drho - rho * u15);
     if constexpr (COLL == COLL_TRT) {
       Real sm = p.trt_sminus;
       if (per_cell_omega) {
@@ -797,20 +795,28 @@ AERO_HD Real collide(const StepParams<Real> &p, Real (&d)[L::Q], bool solid, Rea
         const Real tm = (tp * tau - Real(0.5)) / (tp - Real(0.5));
         sm = Real(1) / tm;
       }
-      d[0] = d[0] + om * (deq[0] - d[0]);  // the rest population is even
+      d[0] = d[0] + om * (deq0 - d[0]);  // the rest population is even
       static_for<L::NP>([&](auto pc) {
         constexpr int k = decltype(pc)::value;
         constexpr int i = L::pair[k], o = L::opp[L::pair[k]];
+        const Real eu = Dir<L, i>::x * ux + Dir<L, i>::y * uy + Dir<L, i>::z * uz;
+        const Real ep = Real(Dir<L, i>::w) * (drho + rho * (Real(4.5) * eu * eu - u15));
+        const Real em = Real(Dir<L, i>::w) * (Real(3) * rho * eu);
         const Real fp = Real(0.5) * (d[i] + d[o]), fm = Real(0.5) * (d[i] - d[o]);
-        const Real ep = Real(0.5) * (deq[i] + deq[o]), em = Real(0.5) * (deq[i] - deq[o]);
         const Real a = om * (ep - fp), b = sm * (em - fm);
         d[i] = d[i] + (a + b);
         d[o] = d[o] + (a - b);
       });
     } else {
-      static_for<L::Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        d[i] = d[i] + om * (deq[i] - d[i]);
+      d[0] = d[0] + om * (deq0 - d[0]);
+      static_for<L::NP>([&](auto pc) {
+        constexpr int k = decltype(pc)::value;
+        constexpr int i = L::pair[k], o = L::opp[L::pair[k]];
+        const Real eu = Dir<L, i>::x * ux + Dir<L, i>::y * uy + Dir<L, i>::z * uz;
+        const Real ep = Real(Dir<L, i>::w) * (drho + rho * (Real(4.5) * eu * eu - u15));
+        const Real em = Real(Dir<L, i>::w) * (Real(3) * rho * eu);
+        d[i] = d[i] + om * ((ep + em) - d[i]);
+        d[o] = d[o] + om * ((ep - em) - d[o]);
       });
     }
     (void)per_cell_omega;
