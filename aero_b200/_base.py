@@ -21,7 +21,7 @@ from typing import Optional
 import numpy as np
 
 from . import _lib
-from .diagnostics import check_stability, coefficient_spectrum, detect_statistical_stationarity
+from .diagnostics import FieldHealth, detect_statistical_stationarity
 from .engine import Engine
 from .lattice import feq, macroscopic, scalar_weights, tables
 from .links import build_surface_links
@@ -347,6 +347,22 @@ class LatticeSolverBase:
         """Device divergence flags (bit 0: non-finite or non-positive density seen)."""
         return self._engine.status()
 
+    def field_statistics(self) -> dict:
+        """FP64 statistics of the whole current state, reduced on the GPU
+        (no counterpart in the reference): the mass (sum of rho), mean
+        density, largest |(ux, uy)|, NaN populations, cells with rho <= 0 and,
+        with a scalar, its total and the Nusselt numbers at the two Dirichlet
+        rows (mean -dT/dy at the row times (Ny - 1) / (T_hot - T_cold))."""
+        self._flush_host_state()
+        h = FieldHealth.from_stats(self._engine.field_stats())
+        out = {"mass": h.mass, "mean_density": h.mean_density, "max_speed": h.max_speed,
+               "nan_populations": h.nan_populations, "nonpositive_cells": h.nonpositive_cells,
+               "cells": h.cells}
+        if self.thermal:
+            nu = h.nusselt(float(self.solid.shape[-2] - 1), self.T_hot - self.T_cold) or (None, None)
+            out.update(scalar_total=h.scalar_total, Nu_bottom=nu[0], Nu_top=nu[1])
+        return out
+
     # ------------------------------------------------------------------ checkpoints
     def save_checkpoint(self, path: str) -> None:
         params = self._checkpoint_params()
@@ -438,7 +454,7 @@ class LatticeSolverBase:
             if checkpoint_every and checkpoint_dir and step % checkpoint_every == 0:
                 self.save_checkpoint(str(pathlib.Path(checkpoint_dir) / self._checkpoint_name()))
             if step % check_every == 0:
-                macro = self._stability_check(step)
+                macro = self._stability_check(step, want_fields=callback is not None)
                 elapsed = time.perf_counter() - t0
                 if verbose:
                     self._print_progress(step, steps, check_every, step / max(elapsed, 1e-12))

@@ -14,6 +14,7 @@ from . import _build
 
 ABI_VERSION = 2
 FORCE_VALUES = 12
+FIELD_STATS = 10
 
 STORE = {"fp32": 0, "fp64": 1, "fp16s": 2, "bf16s": 3}
 COLLISION = {"bgk": 0, "trt": 1, "mrt": 2}
@@ -58,6 +59,7 @@ SIGNATURES = {
     "aero_get_state": ([_VP, _VP, _VP, _VP, _VP], ctypes.c_int),
     "aero_get_state_slab": ([_VP, _I32, _I32, _VP, _VP], ctypes.c_int),
     "aero_get_macroscopic": ([_VP, _VP, _VP], ctypes.c_int),
+    "aero_field_stats": ([_VP, _I32, _I32, _VP, _VP], ctypes.c_int),
     "aero_step": ([_VP, _I64, _VP], ctypes.c_int),
     "aero_read_forces": ([_VP, _VP, _I64, ctypes.POINTER(_I64), _VP], ctypes.c_int),
     "aero_read_profile": ([_VP, _VP, _VP], ctypes.c_int),

@@ -42,12 +42,14 @@ int fail(int code, const char *fmt, ...) {
     if (e_ != cudaSuccess) return fail(AERO_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
   } while (0)
 
+static_assert(kStatsValues == AERO_FIELD_STATS, "field statistics layout");
+
 constexpr uint64_t kAlign = 256;
 uint64_t align_up(uint64_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
 struct Layout {
   uint64_t P[2], flags, lbits, loff, lc_mask, lc_q, lc_cell, lc_contrib, fin_partial, prof_off, force_const, prof_const,
-      prev[2], g[2], U, cs_cell, inflow, recycle, hist, prof_out, counters, total;
+      prev[2], g[2], U, cs_cell, inflow, recycle, hist, prof_out, counters, stats, total;
 };
 
 struct WTab {
@@ -723,6 +725,8 @@ int aero_set_geometry(AeroLattice *L, const uint8_t *solid, const int32_t *links
   y.hist = take(8 * 12 * (uint64_t)L->hist_cap);
   y.prof_out = take(24 * (uint64_t)L->nprof);
   y.counters = take(64);
+  // k_field_stats: per-block partials, the combined values, the ticket
+  y.stats = take(8 * ((uint64_t)kStatsBlocks * kStatsValues + kStatsValues + 1));
   y.total = o;
   L->geometry = true;
   return AERO_OK;
@@ -836,6 +840,31 @@ int aero_get_macroscopic(AeroLattice *L, double *out, void *stream) {
     const StepParams<float> p = make_params<float>(L, 1 - L->cur);
     CUDA_TRY(get_ops<float>(L)->macro_out(p, out, -1, L->old_is_state, 0, grid, st));
   }
+  return AERO_OK;
+}
+
+int aero_field_stats(AeroLattice *L, int32_t z0, int32_t nzs, double *out, void *stream) {
+  if (!L || !out) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (!L->state_set) return fail(AERO_ERR_STATE, "no state set");
+  if (z0 < 0 || nzs < 1 || z0 + nzs > L->prm.nz) return fail(AERO_ERR_INVALID, "planes outside the grid");
+  CUDA_TRY(cudaSetDevice(L->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  double *partial = reinterpret_cast<double *>(L->ws + L->lay.stats);
+  double *dout = partial + (size_t)kStatsBlocks * kStatsValues;
+  uint32_t *ticket = reinterpret_cast<uint32_t *>(dout + kStatsValues);
+  // the state of the last step comes from the previous buffers (as in
+  // aero_get_macroscopic); the scalar of the last step is the current one
+  if (is_f64(L)) {
+    const StepParams<double> p = make_params<double>(L, 1 - L->cur);
+    const double *g = L->prm.thermal ? reinterpret_cast<const double *>(L->ws + L->lay.g[L->cur]) : nullptr;
+    CUDA_TRY(get_ops<double>(L)->field_stats(p, g, z0, nzs, -1, L->old_is_state, partial, ticket, dout, st));
+  } else {
+    const StepParams<float> p = make_params<float>(L, 1 - L->cur);
+    const float *g = L->prm.thermal ? reinterpret_cast<const float *>(L->ws + L->lay.g[L->cur]) : nullptr;
+    CUDA_TRY(get_ops<float>(L)->field_stats(p, g, z0, nzs, -1, L->old_is_state, partial, ticket, dout, st));
+  }
+  CUDA_TRY(cudaMemcpyAsync(out, dout, sizeof(double) * kStatsValues, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
   return AERO_OK;
 }
 

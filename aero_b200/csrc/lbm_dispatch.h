@@ -43,6 +43,12 @@ struct Ops {
   // 4-byte arithmetic); blocks = the members' pair_batch_layout blocks
   cudaError_t (*step_batch_pair)(const StepParams<Real> *params, const int64_t *first, int n, int64_t blocks,
                                  cudaStream_t);
+  // FP64 field statistics of the current state over planes z0 .. z0+nzs-1
+  // (k_field_stats): gcur is the current scalar buffer (NULL without a
+  // scalar); partial / ticket are workspace scratch; out (device) receives
+  // kStatsValues doubles
+  cudaError_t (*field_stats)(const StepParams<Real> &, const Real *gcur, int z0, int nzs, int step_delta, bool raw,
+                             double *partial, uint32_t *ticket, double *out, cudaStream_t);
   int store_bytes;
 };
 

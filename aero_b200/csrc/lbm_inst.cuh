@@ -132,10 +132,18 @@ struct Launch {
       return cudaErrorNotSupported;
     }
   }
+  static cudaError_t field_stats(const StepParams<Real> &p, const Real *gcur, int z0, int nzs, int delta, bool raw,
+                                 double *partial, uint32_t *ticket, double *out, cudaStream_t st) {
+    if (raw)
+      k_field_stats<L, S, true><<<kStatsBlocks, kStatsBlock, 0, st>>>(p, gcur, z0, nzs, delta, partial, ticket, out);
+    else
+      k_field_stats<L, S, false><<<kStatsBlocks, kStatsBlock, 0, st>>>(p, gcur, z0, nzs, delta, partial, ticket, out);
+    return cudaGetLastError();
+  }
   static constexpr Ops<Real> table = {&step,       &step_shaped, &moments,      &finalize,   &state_out,
                                       &load_state, &macro_out,   &step_tiled,   &tiled_setup, &step_batch,
                                       &moments_batch, &finalize_batch, &recycle_mean, &step_pair,
-                                      &step_batch_pair, (int)sizeof(S)};
+                                      &step_batch_pair, &field_stats, (int)sizeof(S)};
 };
 
 template <class S>

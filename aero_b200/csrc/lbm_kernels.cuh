@@ -1601,6 +1601,130 @@ __global__ void __launch_bounds__(kStepBlock) k_macro_out(const StepParams<typen
   if constexpr (L::DIMS == 3) out[3 * out_plane + oc] = inv * jz;
 }
 
+// --------------------------------------------------------------------------
+// Field statistics of the current state, summed in FP64 on the device: the
+// global mass and scalar totals, the quantities check_stability tests
+// (diagnostics.py:32-71: NaN populations, rho <= 0, max |(ux, uy)|, mean
+// rho) and the wall heat-flux sums of the Nusselt number, over the planes
+// z0 .. z0 + nzs - 1.  A fixed grid of kStatsBlocks blocks strides over the
+// cells; each block stores its partial values and the block that finishes
+// last combines the partials in block order, so every figure is the same
+// from run to run.
+//
+// Nusselt number (the reference computes none): at the Dirichlet rows y = 0
+// (T_hot) and y = ny-1 (T_cold), the wall-normal gradient of T = sum_i g_i
+// by the second-order one-sided difference, for every (x, z) column whose
+// two cells next to the wall are fluid; Nu = mean(-dT/dy) (ny - 1) /
+// (T_hot - T_cold), which is 1 for pure conduction between the rows.
+// --------------------------------------------------------------------------
+constexpr int kStatsBlocks = 296;
+constexpr int kStatsBlock = 256;
+constexpr int kStatsValues = 10;  // see aero_field_stats in aero_b200.h for the order
+
+template <class L, class S, bool RAW>
+__global__ void __launch_bounds__(kStatsBlock)
+    k_field_stats(const StepParams<typename StoreOps<S>::Real> p, const typename StoreOps<S>::Real *gcur, int z0,
+                  int nzs, int step_delta, double *partial, uint32_t *ticket, double *out) {
+  using Real = typename StoreOps<S>::Real;
+  using SO = StoreOps<S>;
+  __shared__ double red[kStatsValues][kStatsBlock / 32];
+  __shared__ bool last;
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  double a[kStatsValues];
+#pragma unroll
+  for (int k = 0; k < kStatsValues; k++) a[k] = 0.0;
+  const int64_t plane = (int64_t)p.nx * p.ny;
+  const int64_t n = plane * nzs;
+  const bool thermal = (p.feat & FEAT_THERMAL) && gcur != nullptr;
+  const int Qg = (p.feat & FEAT_SCALAR_REDUCED) ? ScalarReduced<L>::Lat::Q : L::Q;
+  auto Tcell = [&](int x, int y, int z) {
+    const uint32_t cc = cell_index(p, x, y, z);
+    double T = 0.0;
+    for (int i = 0; i < Qg; i++) T += (double)gcur[elem(p, i, cc)];
+    return T;
+  };
+  for (int64_t k = (int64_t)blockIdx.x * kStatsBlock + t; k < n; k += (int64_t)kStatsBlocks * kStatsBlock) {
+    const int z = z0 + (int)(k / plane);
+    const int64_t r = k - (int64_t)(z - z0) * plane;
+    const int y = (int)(r / p.nx), x = (int)(r - (int64_t)y * p.nx);
+    const uint32_t c = cell_index(p, x, y, z);
+    Real d[L::Q];
+    if constexpr (RAW) {
+      const S *P = static_cast<const S *>(p.P);
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        d[i] = SO::template load<i, L>(P, elem(p, i, c));
+      });
+    } else {
+      full_state<L, S, Real>(p, x, y, z, *p.step + step_delta, d, nullptr, nullptr);
+    }
+    double rho = 0.0, jx = 0.0, jy = 0.0;
+    int nan = 0;
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      nan += isnan(d[i]) ? 1 : 0;
+      const double f = Dir<L, i>::w + (double)d[i];
+      rho += f;
+      jx += (double)Dir<L, i>::x * f;
+      jy += (double)Dir<L, i>::y * f;
+    });
+    const double inv = rho > 0.0 ? 1.0 / rho : 0.0;
+    const double ux = inv * jx, uy = inv * jy;
+    a[0] += (double)nan;
+    a[1] += rho <= 0.0 ? 1.0 : 0.0;
+    a[2] = fmax(a[2], sqrt(ux * ux + uy * uy));
+    a[3] += rho;
+    a[4] += 1.0;
+    if (thermal) {
+      a[5] += Tcell(x, y, z);
+      if (p.ny >= 3 && (y == 0 || y == p.ny - 1)) {
+        const int s = y == 0 ? 1 : -1;  // into the fluid
+        const bool fluid = !(p.flags[cell_index(p, x, y + s, z)] & FLAG_SOLID) &&
+                           !(p.flags[cell_index(p, x, y + 2 * s, z)] & FLAG_SOLID);
+        if (fluid) {
+          const double T0 = Tcell(x, y, z), T1 = Tcell(x, y + s, z), T2 = Tcell(x, y + 2 * s, z);
+          // one-sided d T / d(distance into the fluid), then as -dT/dy
+          const double dn = 0.5 * (-3.0 * T0 + 4.0 * T1 - T2);
+          const double mdTdy = y == 0 ? -dn : dn;
+          a[y == 0 ? 6 : 8] += mdTdy;
+          a[y == 0 ? 7 : 9] += 1.0;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kStatsValues; k++) {
+    double v = a[k];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double o = __shfl_down_sync(0xffffffffu, v, off);
+      v = k == 2 ? fmax(v, o) : v + o;
+    }
+    if (lane == 0) red[k][wid] = v;
+  }
+  __syncthreads();
+  if (t < kStatsValues) {
+    double v = 0.0;
+    for (int w = 0; w < kStatsBlock / 32; w++) v = t == 2 ? fmax(v, red[t][w]) : v + red[t][w];
+    partial[blockIdx.x * kStatsValues + t] = v;
+    __threadfence();
+  }
+  __syncthreads();
+  if (t == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (t < kStatsValues) {
+    double v = 0.0;
+    for (int b = 0; b < (int)gridDim.x; b++) {
+      const double pb = __ldcg(partial + b * kStatsValues + t);
+      v = t == 2 ? fmax(v, pb) : v + pb;
+    }
+    out[t] = v;
+  }
+  if (t == 0) *ticket = 0u;
+}
+
 // Converts absolute FP64 populations (Q, ncells) into the storage format.
 template <class L, class S>
 __global__ void __launch_bounds__(kStepBlock) k_load_state(const StepParams<typename StoreOps<S>::Real> p,

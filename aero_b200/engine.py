@@ -134,6 +134,16 @@ class Engine:
             check("aero_get_macroscopic", self.lib.aero_get_macroscopic(self.h, out.data_ptr(), self.stream()))
         return out
 
+    def field_stats(self, z0: int = 0, nzs: Optional[int] = None) -> np.ndarray:
+        """FP64 statistics of the state over planes z0 .. z0+nzs-1 (all by
+        default), reduced on the device (aero_field_stats)."""
+        nzs = (self.params.nz - int(z0)) if nzs is None else int(nzs)
+        out = np.empty(_lib.FIELD_STATS, dtype=np.float64)
+        with self.torch.cuda.device(self.device):
+            check("aero_field_stats", self.lib.aero_field_stats(self.h, int(z0), nzs, out.ctypes.data,
+                                                                self.stream()))
+        return out
+
     def set_inflow(self, fields: np.ndarray, first_step: int) -> None:
         """Uploads the transverse inlet velocities of steps first_step.. (n, dims-1, nz*ny)."""
         a = np.ascontiguousarray(fields, dtype=np.float64)
@@ -179,6 +189,12 @@ class Engine:
         k = ctypes.c_int32()
         check("aero_get_step_kernel", self.lib.aero_get_step_kernel(self.h, ctypes.byref(k)))
         return int(k.value)
+
+    def les_fused(self) -> bool:
+        """Whether the step kernel computes the LES rate from a shared-memory
+        velocity stencil of its own (True) or reads the velocity side output
+        of a separate moments pass (False)."""
+        return False
 
     def step_plan(self) -> dict:
         """Step kernel in use: {"tiled": bool, "tile_rows": r, "blocks": b}."""

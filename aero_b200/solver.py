@@ -17,7 +17,7 @@ from typing import Optional
 import numpy as np
 
 from ._base import LatticeSolverBase, _check_layout
-from .diagnostics import check_stability, coefficient_spectrum
+from .diagnostics import FieldHealth, check_field_health, coefficient_spectrum
 
 
 class Solver(LatticeSolverBase):
@@ -106,11 +106,13 @@ class Solver(LatticeSolverBase):
         print(f"  step {step:6d}/{steps}  Cd={float(np.mean(self.Cd_history[-w:])):+.4f}  "
               f"Cl={float(np.mean(self.Cl_history[-w:])):+.4f}  [{sps:.0f} steps/s]", flush=True)
 
-    def _stability_check(self, step):
-        f = self.f
-        rho, ux, uy = _macro2(f)
-        check_stability(f, rho, ux, uy, step)
-        return rho, ux, uy
+    def _stability_check(self, step, want_fields=False):
+        # solver.py:522-531 checks the whole field; the device reduces it
+        check_field_health(FieldHealth.from_stats(self._engine.field_stats()), step)
+        if not want_fields:
+            return None
+        m = self._engine.macroscopic_device().cpu().numpy()
+        return m[0], m[1], m[2]
 
     def _callback(self, callback, step, macro):
         rho, ux, uy = macro

@@ -16,7 +16,7 @@ from typing import Optional
 import numpy as np
 
 from ._base import LatticeSolverBase, _check_layout
-from .diagnostics import check_stability, coefficient_spectrum
+from .diagnostics import FieldHealth, check_field_health, coefficient_spectrum
 
 
 class Solver3D(LatticeSolverBase):
@@ -118,15 +118,9 @@ class Solver3D(LatticeSolverBase):
         print(f"  step {step:6d}/{steps}  Cd={float(np.mean(self.Cd_history[-w:])):+.4f}  "
               f"Cl_y={float(np.mean(self.Cly_history[-w:])):+.4f}  [{sps:.0f} steps/s]", flush=True)
 
-    def _stability_check(self, step):
-        # solver3d.py:608-615: the mid z-plane only
-        f_mid = self._engine.get_slab_device(self.Nz // 2, 1)[:, 0].cpu().numpy()
-        rho = f_mid.sum(axis=0)
-        inv = np.where(rho > 0, 1.0 / np.where(rho > 0, rho, 1.0), 0.0)
-        from .lattice import E3
-        ux = inv * np.einsum("i,iyx->yx", E3[:, 0].astype(np.float64), f_mid)
-        uy = inv * np.einsum("i,iyx->yx", E3[:, 1].astype(np.float64), f_mid)
-        check_stability(f_mid, rho, ux, uy, step)
+    def _stability_check(self, step, want_fields=False):
+        # solver3d.py:608-615 checks the mid z-plane only; the device reduces it
+        check_field_health(FieldHealth.from_stats(self._engine.field_stats(self.Nz // 2, 1)), step)
         return None
 
     def _callback(self, callback, step, macro):

@@ -20,12 +20,21 @@ One JSON line on stdout (rank 0):
             and the read-back of forces, stability plane and final fields;
   roofline: the fused step kernel's algorithmic bytes per launch
             (2 Q bytes-per-population + 1 flag byte per cell, plus the scalar
-            lattice and the LES side pass where present) over its average
-            CUDA-event duration, measured in a separate phase of up to 200
-            steps with events around each kernel, against the measured HBM
-            copy rate;
+            lattice, and the 12-byte LES velocity side output where the LES
+            rate is read from one) over its average CUDA-event duration,
+            measured over a separate phase of 1000 steps (the sustained rate,
+            whatever K is) with events around each kernel, against the
+            measured HBM copy rate;
+  clocks  : NVML samples (every ~2 ms) inside the K timed steps and the
+            1000-step kernel phase;
+  precision_variants: the same workload, K and W in the other storage
+            formats (FP16 / BF16 deviations), with their kernel roofline;
   cpu_baseline: the FP64 oracle (C/OpenMP restatement of the reference step)
             on a bounded slab of the same workload, on this host's cores.
+
+``--workload box256`` adds ``scalar_check``: the thermal channel in every
+storage format against the FP64 engine at a stable relaxation time (Nusselt
+numbers, mass and scalar totals, velocity).
 
 ``--impl reference`` times that CPU path alone (rank 0; other ranks exit).
 Multi-GPU (torchrun): every rank advances its own replica (no exchange);
@@ -75,7 +84,7 @@ WORKLOADS = {
                     wall_bc="noslip", streamwise_bc="periodic", body_force_x=1e-6, thermal=True,
                     T_hot=1.0, T_cold=0.0, alpha_T=0.01, buoyancy=True, g_gravity=1e-5, beta=1.0,
                     T_ref=0.5, scalar_lattice="reduced"),
-        u0=0.05, nu=0.01, perturb=0.0,
+        u0=0.05, nu=0.01, perturb=0.0, T_noise=1e-3,
         desc="D3Q19 TRT+WALE thermal channel 256x128x128, D3Q7 scalar, box obstacle, body force"),
 }
 
@@ -123,58 +132,110 @@ def _geometry(w):
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples the SM clock, power draw and clock-event reasons of the bench
+    GPU through NVML (read-only queries) every ~2 ms from a helper thread.
+    Each sample carries its host time, so the summary can be restricted to
+    the windows the caller timed (the K timed steps, the event-timed kernel
+    phase); nvidia-smi polling is the fallback when NVML is unavailable."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASON_BITS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+                   "hw_power_brake_slowdown": 0x80, "sw_power_cap": 0x4}
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
-        self.lines = []
-        self.proc = None
+    def __init__(self, device, period_s: float = 0.002):
+        self.device = device
+        self.period = period_s
+        self.samples = []  # (host time, sm MHz, max sm MHz, watts, reason bits)
+        self._stop = threading.Event()
+        self._h = None
+        self._nvml = None
+        self.windows = []
+
+    def _handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        self._nvml = pynvml
+        uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+        for cand in (uuid, "GPU-" + uuid):
+            try:
+                return pynvml.nvmlDeviceGetHandleByUUID(cand)
+            except Exception:
+                pass
+        for k in range(pynvml.nvmlDeviceGetCount()):
+            h = pynvml.nvmlDeviceGetHandleByIndex(k)
+            u = pynvml.nvmlDeviceGetUUID(h)
+            u = u.decode() if isinstance(u, bytes) else u
+            if u.endswith(uuid):
+                return h
+        raise RuntimeError("GPU not found through NVML")
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100", "-i", str(self.gpu)], stdout=subprocess.PIPE,
-                stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            self._h = self._handle()
+            self._max = float(self._nvml.nvmlDeviceGetMaxClockInfo(self._h, self._nvml.NVML_CLOCK_SM))
+            self.t = threading.Thread(target=self._poll, daemon=True)
         except Exception:
-            self.proc = None
+            self._h = None
+            self.t = threading.Thread(target=self._poll_smi, daemon=True)
+        self.t.start()
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _poll(self):
+        nv, h = self._nvml, self._h
+        while not self._stop.is_set():
+            t = time.perf_counter()
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                w = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                bits = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                self.samples.append((t, mhz, self._max, w, bits))
+            except Exception:
+                pass
+            self._stop.wait(self.period)
+
+    def _poll_smi(self):
+        fields = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_power_cap")
+        try:
+            idx = self.device.index if hasattr(self.device, "index") else int(self.device)
+            proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={fields}", "--format=csv,noheader,nounits",
+                                     "-lms", "100", "-i", str(idx)], stdout=subprocess.PIPE,
+                                    stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            return
+        bits_of = [0x8, 0x20, 0x40, 0x4]
+        for line in proc.stdout:
+            if self._stop.is_set():
+                break
+            parts = [p.strip() for p in line.split(",")]
+            try:
+                bits = sum(b for b, v in zip(bits_of, parts[3:7]) if v.lower() in ("active", "1"))
+                self.samples.append((time.perf_counter(), float(parts[0]), float(parts[1]),
+                                     float(parts[2]), bits))
+            except (ValueError, IndexError):
+                continue
+        proc.terminate()
+
+    def window(self, t0: float, t1: float) -> None:
+        """Marks [t0, t1] (perf_counter seconds) as a region under load."""
+        self.windows.append((t0, t1))
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        self._stop.set()
+        self.t.join(timeout=5)
 
     def summary(self):
-        mhz, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                mhz.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() in ("active", "1"):
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(mhz)}
+        inside = [s for s in self.samples if any(a <= s[0] <= b for a, b in self.windows)] \
+            if self.windows else list(self.samples)
+        reasons = sorted(n for n, b in self.REASON_BITS.items() if any(s[4] & b for s in inside))
+        mhz = [s[1] for s in inside]
+        return {"sm_mhz": statistics.median(mhz) if mhz else None,
+                "sm_max_mhz": inside[0][2] if inside else None,
+                "reasons": reasons, "samples": len(inside),
+                "power_w_max": max(s[3] for s in inside) if inside else None,
+                "source": "nvml" if self._h is not None else "nvidia-smi",
+                "windows_s": [round(b - a, 4) for a, b in self.windows]}
 
 
 def cpu_oracle_sample(w, target_s=15.0, max_steps=None, nz_sample=32, threads=None):
@@ -428,6 +489,247 @@ def run_serve(args):
     return 0
 
 
+def scalar_precision_check(w, args, dev, tau=0.8, steps=2000, formats=("fp32", "bf16s", "fp16s")):
+    """The thermal channel (configuration 3) in each storage format against
+    the FP64 engine, at a relaxation time where the reference's TRT is stable
+    (its lambda semantics diverge at the configuration's tau 0.53): the
+    configuration's geometry, body force, scalar and buoyancy, the scalar
+    started at T_ref + seeded U(-1e-3, 1e-3), `steps` steps.  Reports per
+    format the Nusselt numbers of both Dirichlet rows, the mass and scalar
+    totals (FP64 sums on the device) and their relative differences to FP64,
+    and the relative L2 difference of u."""
+    import numpy as np
+    import torch
+    from aero_b200.lattice import scalar_weights
+    wk = dict(w, nu=(tau - 0.5) / 3.0)
+    shp = (wk["nz"], wk["ny"], wk["nx"])
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(4321)
+    T0 = wk["kwargs"]["T_ref"] + 1e-3 * (2.0 * torch.rand(shp, generator=gen, device=dev, dtype=torch.float64) - 1.0)
+    out = {"tau": tau, "steps": steps, "nu": wk["nu"],
+           "desc": "configuration 3 at tau %.2f (stable under the reference's TRT lambda semantics), scalar "
+                   "T_ref + U(-1e-3, 1e-3) seed 4321" % tau}
+    ref = None
+    for prec in ("fp64",) + tuple(formats):
+        s = _build_solver(wk, prec, dev, steps, 0)
+        f0, prev0, _ = s._uniform_state_device()
+        wg = torch.tensor(scalar_weights(3, s.scalar_lattice == "reduced"), dtype=torch.float64, device=dev)
+        g0 = (wg.reshape(-1, 1, 1, 1) * T0[None]).contiguous()
+        s._engine.set_state(f0, prev0, g0, 0)
+        st0 = s.field_statistics()
+        t0 = time.perf_counter()
+        s._advance(steps)
+        torch.cuda.synchronize(dev)
+        dt = time.perf_counter() - t0
+        st = s.field_statistics()
+        u = s._engine.macroscopic_device()[1:].cpu().numpy()
+        rec = {"Nu_bottom": st["Nu_bottom"], "Nu_top": st["Nu_top"], "mass": st["mass"],
+               "scalar_total": st["scalar_total"], "mass_drift": (st["mass"] - st0["mass"]) / st0["mass"],
+               "scalar_drift": (st["scalar_total"] - st0["scalar_total"]) / st0["scalar_total"],
+               "status": s.status(), "seconds": dt}
+        if ref is None:
+            ref = dict(rec, u=u)
+        else:
+            rec["mass_err_vs_fp64"] = abs(st["mass"] - ref["mass"]) / ref["mass"]
+            rec["scalar_err_vs_fp64"] = abs(st["scalar_total"] - ref["scalar_total"]) / ref["scalar_total"]
+            rec["Nu_bottom_err_vs_fp64"] = abs(st["Nu_bottom"] - ref["Nu_bottom"]) / abs(ref["Nu_bottom"])
+            rec["Nu_top_err_vs_fp64"] = abs(st["Nu_top"] - ref["Nu_top"]) / abs(ref["Nu_top"])
+            rec["u_rel_l2_vs_fp64"] = float(np.linalg.norm(u - ref["u"]) / np.linalg.norm(ref["u"]))
+        out[prec] = rec
+        del s, f0, prev0, g0
+        torch.cuda.empty_cache()
+    out["fp64"].pop("u", None)
+    return out
+
+
+ROOFLINE_STEPS = 1000  # event-timed steps of the kernel phase (about a second at sphere512)
+
+
+def _build_solver(w, precision, dev, steps, warmup):
+    from aero_b200 import Solver, Solver3D
+    g = _geometry(w)
+    dims = w["dims"]
+    nz, ny, nx = w["nz"], w["ny"], w["nx"]
+    shp = (ny, nx) if dims == 2 else (nz, ny, nx)
+    solid = g.mark_solid(*shp)
+    phi = g.sdf_field(*shp) if w["kwargs"].get("bouzidi") else None
+    cap = max(4096, steps + warmup + ROOFLINE_STEPS + 8)
+    common = dict(solid=solid, omega=1.0 / (3.0 * w["nu"] + 0.5), u0=w["u0"], D=g.reference_length(),
+                  phi=phi, precision=precision, device=dev, hist_capacity=cap, **w["kwargs"])
+    return Solver(Ny=ny, Nx=nx, **common) if dims == 2 else Solver3D(Nz=nz, Ny=ny, Nx=nx, **common)
+
+
+def _initial_fields(w, dev, rank):
+    """The seeded initial velocity of the workload: ux = u0 (1 + p U(-1, 1))
+    (p the workload's perturbation), uy = U(-a, a) where the workload sets a."""
+    import torch
+    shp = (w["ny"], w["nx"]) if w["dims"] == 2 else (w["nz"], w["ny"], w["nx"])
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234 + rank)
+    ux = w["u0"] * (1.0 + w["perturb"] * (2.0 * torch.rand(shp, generator=gen, device=dev,
+                                                           dtype=torch.float64) - 1.0))
+    uy = (w["perturb_uy"] * (2.0 * torch.rand(shp, generator=gen, device=dev, dtype=torch.float64) - 1.0)
+          if w.get("perturb_uy") else None)
+    return ux, uy
+
+
+def _bytes_per_cell(s, precision):
+    """Algorithmic bytes of one cell update of the fused step: read and write
+    Q populations (2 Q s) and the flag byte, the scalar populations where a
+    scalar runs (2 Qg x 4 or 8), and the LES velocity side output the step
+    reads back where the BGK/TRT LES rate is computed from it (3 values).
+    Returns (bytes, the parts, bytes of the moments pass that are not
+    algorithmic: its second read of the populations)."""
+    sb = {"fp32": 4, "fp64": 8, "fp16s": 2, "bf16s": 2}[precision]
+    rb = 8 if precision == "fp64" else 4
+    Q = 9 if s.dims == 2 else 19
+    parts = {"populations": 2 * Q * sb, "flags": 1}
+    extra = 0
+    if s.thermal:
+        qg = (5 if s.dims == 2 else 7) if s.scalar_lattice == "reduced" else Q
+        parts["scalar"] = 2 * qg * rb
+    if s.les and s.collision != "mrt" and not s._engine.les_fused():
+        parts["les_side_output"] = 3 * rb
+        extra = Q * sb + 3 * rb
+    return sum(parts.values()), parts, extra
+
+
+def measure_lattice(w, precision, args, dev, rank=0, world=1, dist=None, e2e=True, label="main"):
+    """One single-lattice measurement: set-up and autotune (untimed), W warm-up
+    steps, K steps timed with CUDA events as the engine runs them (graphs),
+    then ROOFLINE_STEPS steps with events around each kernel for the step
+    kernel's sustained duration, clocks sampled over both; optionally the
+    end-to-end run through the public API.  Returns a dict of results."""
+    import numpy as np
+    import torch
+    s = _build_solver(w, precision, dev, args.steps, args.warmup)
+    eng = s._engine
+    ncells = w["nx"] * w["ny"] * w["nz"]
+    ux0, uy0 = _initial_fields(w, dev, rank)
+    f0, prev0, g0 = s._uniform_state_device(ux=ux0, uy=uy0)
+    del ux0, uy0
+    if g0 is not None and w.get("T_noise"):
+        # the scalar starts at T_ref + U(-a, a), seeded
+        from aero_b200.lattice import scalar_weights
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(4321 + rank)
+        T0 = s.T_ref + w["T_noise"] * (2.0 * torch.rand(s.solid.shape, generator=gen, device=dev,
+                                                         dtype=torch.float64) - 1.0)
+        wg = torch.tensor(scalar_weights(s.dims, s.scalar_lattice == "reduced"), dtype=torch.float64, device=dev)
+        g0 = (wg.reshape((-1,) + (1,) * s.dims) * T0[None]).contiguous()
+        del T0
+    eng.set_state(f0, prev0, g0, 0)
+    stream = torch.cuda.current_stream(dev)
+    tune = None
+    if args.kernel == "auto":
+        tune = s.autotune(steps=10)
+    elif args.kernel == "pair":
+        eng.set_step_kernel(4)
+    eng.step(args.warmup)
+    eng.read_forces()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        t0 = time.perf_counter()
+        e0.record(stream)
+        eng.step(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        clk.window(t0, time.perf_counter())
+        if dist:
+            dist.barrier()
+        ms = e0.elapsed_time(e1)
+        raw = eng.read_forces()
+        # the step kernel's sustained duration: eager launches with events
+        # around each kernel, over ROOFLINE_STEPS steps
+        eng.enable_timing(True)
+        eng.kernel_times()  # reset
+        t1 = time.perf_counter()
+        eng.step(ROOFLINE_STEPS)
+        step_ms, force_ms, nt = eng.kernel_times()
+        clk.window(t1, time.perf_counter())
+        eng.enable_timing(False)
+    eng.read_forces()
+    s.step_count += args.warmup + args.steps + ROOFLINE_STEPS
+    status, first_bad = eng.status(), eng.first_bad_step()
+    ms = max_over_ranks(ms, dist, dev)
+    peak, peak_kind = _peak_hbm()
+    bpc, parts, extra = _bytes_per_cell(s, precision)
+    k_ms = step_ms / max(nt, 1)
+    achieved = bpc * ncells / (k_ms / 1e3) / 1e9
+    plan = eng.step_plan()
+    plan["kernel_id"] = eng.get_step_kernel()
+    plan["les_fused"] = eng.les_fused()
+    if tune is not None:
+        plan["autotune_ms_per_step"] = {str(k): v for k, v in tune["ms_per_step"].items()}
+    kname = "k_step_tiled" if plan["tiled"] else ("k_step_pair" if plan["kernel_id"] == 4 else "k_step")
+    # DRAM bytes per launch from the committed ncu summary of this kernel,
+    # workload and precision (a smaller case scaled by cells where the summary
+    # says so); None when no capture covers it
+    traffic = None
+    pat = re.compile(rf"^- {re.escape(args.workload)}: dram bytes per launch = (\d+)\s*$", re.M)
+    for md in sorted((ROOT / "profiles").glob(f"{kname}_*_{precision}.md")):
+        if kname == "k_step" and md.name.startswith(("k_step_tiled", "k_step_pair")):
+            continue
+        m = pat.search(md.read_text())
+        if m:
+            traffic = int(m.group(1))
+            break
+    res = {
+        "solver": s, "ms": ms, "value": whole_job_mlups(ncells, world, args.steps, ms / 1e3), "raw": raw,
+        "status": status, "first_bad": first_bad, "clocks": clk.summary(),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": traffic,
+                     "kernel": f"{kname} (fused stream/BC/collide" + (
+                         ", source rows staged in shared memory by bulk async copies)" if plan["tiled"]
+                         else ", two cells per thread on packed FP32 arithmetic)" if plan["kernel_id"] == 4
+                         else ", per-cell global gather, blocks " + ("128x1", "256x1", "32x4")[plan["kernel_id"]]
+                         + ")"),
+                     "step_plan": plan, "alg_bytes_per_launch": bpc * ncells, "bytes_per_cell": bpc,
+                     "bytes_per_cell_parts": parts, "non_algorithmic_bytes_per_cell": extra,
+                     "kernel_ms": k_ms, "kernel_steps_timed": int(nt), "finalize_ms": force_ms / max(nt, 1)},
+    }
+    res["launches_per_step"] = 2 + (1 if (s.les and s.collision != "mrt" and not eng.les_fused()) else 0)
+    if e2e:
+        res["e2e"] = _measure_e2e(s, w, args, dev, f0, prev0, g0, world, dist)
+    del f0, prev0, g0
+    return res
+
+
+def _measure_e2e(s, w, args, dev, f0, prev0, g0, world, dist):
+    """MLUPS of Solver.run(K) end to end: the initial state copied from
+    pinned host memory, K steps, the force history and the result's fields
+    read back, timed on the host."""
+    import torch
+    eng = s._engine
+    ncells = w["nx"] * w["ny"] * w["nz"]
+    Q = 9 if w["dims"] == 2 else 19
+    f0_host = f0.cpu().pin_memory()
+    prev_host = prev0.cpu().pin_memory()
+    g_host = None if g0 is None else g0.cpu().pin_memory()
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    eng.set_state(f0_host, prev_host, g_host, 0)
+    s.step_count = 0
+    s._init_histories()
+    # one stability check at the end would raise on a diverged state; the
+    # throughput measurement does not depend on it, so none is requested
+    r = s.run(args.steps, check_every=args.steps + 1, verbose=False)
+    torch.cuda.synchronize(dev)
+    dt = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    h2d = f0_host.numel() * 8 + prev_host.numel() * 8 + (0 if g_host is None else g_host.numel() * 8)
+    d2h = (args.steps * 12 * 8 + (w["nz"] if w["dims"] == 3 else w["ny"]) * 3 * 8
+           + (1 + w["dims"]) * ncells * 8 + (ncells * 8 if s.thermal else 0))
+    return {"value": whole_job_mlups(ncells, world, args.steps, dt), "unit": "MLUPS",
+            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+            "call": f"{type(s).__name__}.run(K) after uploading the initial state from pinned host memory",
+            "Cd_mean": r["Cd_mean"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -436,7 +738,11 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="sphere512", choices=sorted(WORKLOADS) + ["batch96", "serve"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16s", "bf16s", "fp64"])
+    ap.add_argument("--variants", default="fp16s,bf16s",
+                    help="storage formats timed after the main run on the same workload, steps and warm-up "
+                         "(comma-separated; 'none' to skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-scalar-check", action="store_true", help="box256: skip the storage-format check")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--collision", default=None, choices=["bgk", "trt", "mrt"],
                     help="override the workload's collision operator (profiling)")
@@ -480,138 +786,34 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
-
-    from aero_b200 import Solver, Solver3D
-    g = _geometry(w)
+    ncells = w["nx"] * w["ny"] * w["nz"]
     dims = w["dims"]
-    nz, ny, nx = w["nz"], w["ny"], w["nx"]
-    shp = (ny, nx) if dims == 2 else (nz, ny, nx)
-    solid = g.mark_solid(*shp)
-    phi = g.sdf_field(*shp) if w["kwargs"].get("bouzidi") else None
-    D = g.reference_length()
-    omega = 1.0 / (3.0 * w["nu"] + 0.5)
-    cap = max(4096, args.steps + args.warmup + 8)
-    common = dict(solid=solid, omega=omega, u0=w["u0"], D=D, phi=phi, precision=args.precision, device=dev,
-                  hist_capacity=cap, **w["kwargs"])
-    s = Solver(Ny=ny, Nx=nx, **common) if dims == 2 else Solver3D(Nz=nz, Ny=ny, Nx=nx, **common)
-    del phi
-    eng = s._engine
-    ncells = nx * ny * nz
-    # seeded +-1% uniform perturbation of the initial streamwise velocity
-    gen = torch.Generator(device=dev)
-    gen.manual_seed(1234 + rank)
-    ux0 = w["u0"] * (1.0 + w["perturb"] * (2.0 * torch.rand(shp, generator=gen, device=dev,
-                                                            dtype=torch.float64) - 1.0))
-    uy0 = (w["perturb_uy"] * (2.0 * torch.rand(shp, generator=gen, device=dev, dtype=torch.float64) - 1.0)
-           if w.get("perturb_uy") else None)
-    f0, prev0, g0 = s._uniform_state_device(ux=ux0, uy=uy0)
-    del ux0, uy0
-    eng.set_state(f0, prev0, g0, 0)
-    stream = torch.cuda.current_stream(dev)
-    tune = None
-    if args.kernel == "auto":
-        # set-up, outside the timed region: time each step kernel on this
-        # lattice, keep the fastest, restore the initial state
-        tune = s.autotune(steps=10)
-    elif args.kernel == "pair":
-        eng.set_step_kernel(4)
 
-    # ---------------- device-timed region --------------------------------
-    # steps run as the engine runs them (CUDA graphs); the split between the
-    # step kernel and the force kernel comes from a separate phase in which
-    # CUDA events bracket every kernel (which needs eager launches)
-    eng.step(args.warmup)
-    eng.read_forces()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(dev.index if world == 1 else local) as clk:
-        e0.record(stream)
-        eng.step(args.steps)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-    if dist:
-        dist.barrier()
-    ms = e0.elapsed_time(e1)
-    raw = eng.read_forces()
-    n_split = max(min(args.steps, 200), 20)
-    eng.enable_timing(True)
-    eng.kernel_times()  # reset
-    eng.step(n_split)
-    step_ms, force_ms, nt = eng.kernel_times()
-    eng.enable_timing(False)
-    eng.read_forces()
-    s.step_count += args.warmup + args.steps + n_split
-    status = eng.status()
-    first_bad = eng.first_bad_step()
-    ms = max_over_ranks(ms, dist, dev)
-    value = whole_job_mlups(ncells, world, args.steps, ms / 1e3)
-    launches_per_step = 2 + (1 if (s.les and s.collision != "mrt") else 0)
+    m = measure_lattice(w, args.precision, args, dev, rank, world, dist, e2e=not args.no_e2e)
+    s = m.pop("solver")
+    Cd_last = float(m["raw"][-1, 0] / s._drag_norm()) if len(m["raw"]) else 0.0
+    links = int(len(s.surface_links))
+    extra = {}
+    if args.workload == "box256" and not args.no_scalar_check:
+        extra["scalar_check"] = scalar_precision_check(w, args, dev)
+    del s
+    torch.cuda.empty_cache()
 
-    # roofline of the fused step kernel
-    peak, peak_kind = _peak_hbm()
-    sb = {"fp32": 4, "fp64": 8, "fp16s": 2, "bf16s": 2}[args.precision]
-    Q = 9 if dims == 2 else 19
-    bytes_per_cell = 2 * Q * sb + 1
-    rb = 8 if args.precision == "fp64" else 4
-    if s.thermal:
-        qg = (5 if dims == 2 else 7) if s.scalar_lattice == "reduced" else Q
-        bytes_per_cell += 2 * qg * rb
-    if s.les and s.collision != "mrt":
-        # the LES side pass reads the populations once more and writes the
-        # velocity buffer, which the step kernel reads back
-        bytes_per_cell += Q * sb + 2 * 3 * rb
-    alg_bytes = bytes_per_cell * ncells
-    k_ms = step_ms / max(nt, 1)
-    achieved = alg_bytes / (k_ms / 1e3) / 1e9
-    # DRAM bytes per launch from the committed ncu capture summary of this
-    # kernel and precision (a smaller case scaled by cells where the summary
-    # says so); None when no capture covers the workload
-    plan = eng.step_plan()
-    plan["kernel_id"] = eng.get_step_kernel()
-    if tune is not None:
-        plan["autotune_ms_per_step"] = {str(k): v for k, v in tune["ms_per_step"].items()}
-    kname = "k_step_tiled" if plan["tiled"] else ("k_step_pair" if plan["kernel_id"] == 4 else "k_step")
-    traffic = None
-    pat = re.compile(rf"^- {re.escape(args.workload)}: dram bytes per launch = (\d+)\s*$", re.M)
-    for md in sorted((ROOT / "profiles").glob(f"{kname}_*_{args.precision}.md")):
-        if kname == "k_step" and md.name.startswith(("k_step_tiled", "k_step_pair")):
-            continue
-        m = pat.search(md.read_text())
-        if m:
-            traffic = int(m.group(1))
-            break
-
-    # ---------------- end to end through the public API ------------------
-    e2e = None
-    if not args.no_e2e:
-        f0_host = f0.cpu().pin_memory()
-        prev_host = prev0.cpu().pin_memory()
-        g_host = None if g0 is None else g0.cpu().pin_memory()
-        del f0, prev0, g0
-        torch.cuda.synchronize(dev)
-        if dist:
-            dist.barrier()
-        t0 = time.perf_counter()
-        eng.set_state(f0_host, prev_host, g_host, 0)
-        s.step_count = 0
-        s._init_histories()
-        # one stability check at the end would raise on a diverged state; the
-        # throughput measurement does not depend on it, so none is requested
-        r = s.run(args.steps, check_every=args.steps + 1, verbose=False)
-        torch.cuda.synchronize(dev)
-        dt = time.perf_counter() - t0
-        dt = max_over_ranks(dt, dist, dev)
-        h2d = f0_host.numel() * 8 + prev_host.numel() * 8 + (0 if g_host is None else g_host.numel() * 8)
-        d2h = (args.steps * 12 * 8 + (nz if dims == 3 else ny) * 3 * 8 + Q * ny * nx * 8 + 4 * ncells * 8
-               + (ncells * 8 if s.thermal else 0))
-        e2e = {"value": whole_job_mlups(ncells, world, args.steps, dt), "unit": "MLUPS",
-               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "call": f"{type(s).__name__}.run(K) after uploading the initial state from pinned host memory",
-               "Cd_mean": r["Cd_mean"]}
-    else:
-        del f0, prev0, g0
+    # the same workload, steps and warm-up in the other storage formats
+    variants = {}
+    if args.variants and args.variants != "none":
+        for prec in [v for v in args.variants.split(",") if v and v != args.precision]:
+            v = measure_lattice(w, prec, args, dev, rank, world, dist, e2e=False, label=prec)
+            v.pop("solver")
+            variants[prec] = {"value": v["value"], "unit": "MLUPS", "ms_per_step": v["ms"] / args.steps,
+                              "speedup_vs_main": v["value"] / m["value"],
+                              "kernel_ms": v["roofline"]["kernel_ms"],
+                              "bytes_per_cell": v["roofline"]["bytes_per_cell"],
+                              "achieved_gbs": v["roofline"]["achieved"], "frac": v["roofline"]["frac"],
+                              "kernel": v["roofline"]["kernel"], "clocks": v["clocks"],
+                              "status": v["status"], "first_nonfinite_step": v["first_bad"]}
+            del v
+            torch.cuda.empty_cache()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -622,11 +824,10 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    cd = raw[:, 0] / s._drag_norm() if len(raw) else np.zeros(1)
     line = {
-        "metric": "D2Q9 MLUPS" if dims == 2 else "D3Q19 MLUPS", "value": value, "unit": "MLUPS",
+        "metric": "D2Q9 MLUPS" if dims == 2 else "D3Q19 MLUPS", "value": m["value"], "unit": "MLUPS",
         "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms"] / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": {"fp32": "f32", "fp64": "f64", "fp16s": "f16 storage / f32 compute",
                   "bf16s": "bf16 storage / f32 compute"}[args.precision],
@@ -634,28 +835,20 @@ def main():
         "config": {"workload": args.workload, "desc": w["desc"], "cells": ncells,
                    "precision": args.precision, "parallelism": f"replicas x{world}",
                    "l2": "state (2 x Q x cells) far larger than L2; no flush needed",
-                   "links": int(len(s.surface_links))},
-        # per step: k_step, k_finalize (+ the LES moments pass for BGK/TRT);
+                   "links": links},
+        # per step: k_step, k_finalize (+ the LES moments pass where it runs);
         # per aero_step call: one launch recording the step whose profile is summed
-        "gpu_launches": launches_per_step * args.steps + 1,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": traffic,
-                     "kernel": f"{kname} (fused stream/BC/collide" + (
-                         ", source rows staged in shared memory by bulk async copies)" if plan["tiled"]
-                         else ", two cells per thread on packed FP32 arithmetic)" if plan["kernel_id"] == 4
-                         else ", per-cell global gather, blocks "
-                         + ("128x1", "256x1", "32x4")[plan["kernel_id"]] + ")"),
-                     "step_plan": plan,
-                     "alg_bytes_per_launch": alg_bytes, "bytes_per_cell": bytes_per_cell,
-                     "kernel_ms": k_ms, "finalize_ms": force_ms / max(nt, 1)},
-        "clocks": clk.summary(),
-        "e2e": e2e,
+        "gpu_launches": m["launches_per_step"] * args.steps + 1,
+        "roofline": m["roofline"],
+        "clocks": m["clocks"],
+        "e2e": m.get("e2e"),
         "cpu_baseline": cpu,
-        "status": status,
-        "first_nonfinite_step": first_bad,
-        "Cd_last": float(cd[-1]),
+        "precision_variants": variants,
+        "status": m["status"],
+        "first_nonfinite_step": m["first_bad"],
+        "Cd_last": Cd_last,
     }
+    line.update(extra)
     print(json.dumps(line), flush=True)
     return 0
 

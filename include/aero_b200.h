@@ -300,6 +300,23 @@ AERO_API int aero_get_state_slab(AeroLattice *lat, int32_t z0, int32_t nzs, doub
  * (solver.py:603-632, solver3d.py:654-723).  Asynchronous. */
 AERO_API int aero_get_macroscopic(AeroLattice *lat, double *out, void *stream);
 
+/* FP64 statistics of the current state over the planes z0 .. z0+nzs-1 (2D:
+ * z0 = 0, nzs = 1), reduced on the device in a fixed order.  out (HOST)
+ * receives AERO_FIELD_STATS doubles:
+ *   0 NaN populations, 1 cells with rho <= 0, 2 max sqrt(ux^2 + uy^2),
+ *   3 sum of rho, 4 cells, 5 sum of the scalar T = sum_i g_i (0 without a
+ *   scalar), 6 sum of -dT/dy at the y = 0 row, 7 columns in that sum,
+ *   8 sum of -dT/dy at the y = ny-1 row, 9 columns in that sum.
+ * Values 0-4 are what check_stability (diagnostics.py:32-71) tests on the
+ * field (solver.py:522-531 on the whole 2D field, solver3d.py:608-615 on
+ * the mid plane); 3 and 5 are the global mass and scalar totals.  The wall
+ * gradients (the reference computes no Nusselt number) are second-order
+ * one-sided differences of T at the Dirichlet rows, over the (x, z) columns
+ * whose two cells next to the wall are fluid: the Nusselt number is
+ * (sum / columns) (ny - 1) / (T_hot - T_cold).  Synchronous. */
+#define AERO_FIELD_STATS 10
+AERO_API int aero_field_stats(AeroLattice *lat, int32_t z0, int32_t nzs, double *out, void *stream);
+
 /* ---- Surface links built on the device --------------------------------
  * Replaces build_surface_links (boundary.py:232-280) and
  * build_surface_links_3d (boundary3d.py:279-329) for geometry that already
