@@ -188,8 +188,8 @@ class LatticeSolverBase:
             P.inflow_ring = 64
         P.recycling = 1 if (self.dims == 3 and streamwise_bc == "recycling") else 0
         self._params = P
-        self._engine = Engine(P, self.solid, self.surface_links, self.q_vals,
-                              phi if (self.van_driest and phi is not None) else None, device)
+        self._engine_phi = phi if (self.van_driest and phi is not None) else None
+        self._engine = Engine(P, self.solid, self.surface_links, self.q_vals, self._engine_phi, device)
 
         # initial state: equilibrium at (rho0, u0, 0) everywhere, solids included
         # (solver.py:218-227, solver3d.py:239-247); built on the GPU
@@ -198,9 +198,7 @@ class LatticeSolverBase:
         self.step_count = 0
         self._f_host = self._prev_host = self._g_host = None
         self._pristine = {}
-        f0, prev0, g0 = self._uniform_state_device()
-        self._engine.set_state(f0, prev0, g0, 0)
-        del f0, prev0, g0
+        self._engine.set_equilibrium()
         self._init_histories()
 
     def _uniform_state_device(self, ux=None, uy=None):
@@ -230,6 +228,24 @@ class LatticeSolverBase:
         return f0, prev0, g0
 
     # ------------------------------------------------------------------ state
+    def set_equilibrium_state(self, rho=None, ux=None, uy=None, uz=None, T=None) -> None:
+        """Sets the state to the equilibrium of macroscopic fields -- what
+        ``s.f = compute_feq(rho, ux, uy[, uz])`` with the outlet state taken
+        from its last column and, with a scalar, ``s.g = w T`` would set --
+        built on the GPU from the fields (no counterpart in the reference).
+        One value per cell crosses to the device for each field given,
+        instead of Q populations.  Each field is an array of the lattice
+        shape (numpy or torch, host or device) or None for the uniform value
+        (rho0, u0, 0, 0, T_ref).  The step count is kept."""
+        if uz is not None and self.dims != 3:
+            raise ValueError("uz is a 3D field")
+        if T is not None and not self.thermal:
+            raise ValueError("T needs thermal=True")
+        self._handed = set()
+        self._f_host = self._prev_host = self._g_host = None
+        self._pristine = {}
+        self._engine.set_equilibrium(rho, ux, uy, uz, T, self.step_count)
+
     def _cache(self):
         if self._f_host is None:
             f, p, g = self._engine.get_state()
@@ -365,13 +381,22 @@ class LatticeSolverBase:
 
     # ------------------------------------------------------------------ checkpoints
     def save_checkpoint(self, path: str) -> None:
+        """Writes the reference's checkpoint (solver.py:638-686,
+        solver3d.py:727-780): the same keys and dtypes, params_json holding
+        exactly the reference constructor's keywords (so the reference's
+        from_checkpoint can rebuild the solver; backend "numpy" as the 3D
+        reference writes it), and one extra key the reference ignores,
+        b200_options, with the engine's own options (precision, scalar
+        lattice)."""
         params = self._checkpoint_params()
+        params["backend"] = "numpy"
         f = self.f
         kwargs = dict(
             f=f, f_outlet_prev=self._f_outlet_prev, solid=self.solid,
             surface_links=self.surface_links, q_vals=self.q_vals,
             step_count=np.array(self.step_count, dtype=np.int64),
             params_json=np.array(json.dumps(params)),
+            b200_options=np.array(json.dumps(self._b200_options())),
             **{k: np.array(getattr(self, k), dtype=np.float64) for k in self._history_keys()},
         )
         if self.phi is not None:
@@ -380,7 +405,15 @@ class LatticeSolverBase:
             kwargs["g"] = self.g
         np.savez_compressed(path, **kwargs)
 
+    def _b200_options(self) -> dict:
+        return {"precision": self.precision, "scalar_lattice": self.scalar_lattice}
+
     def load_checkpoint(self, path: str) -> None:
+        """Restores f, the outlet state, the scalar, the histories and the
+        step count, and adopts the checkpoint's surface links and q values
+        when it has them (solver.py:688-709, solver3d.py:782-811).  A link
+        table that differs from the one built from the solid mask is
+        uploaded to the engine (which checks it against the mask)."""
         data = _open_checkpoint(path)
         for key in ("f", "f_outlet_prev", "step_count"):
             if key not in data:
@@ -388,13 +421,17 @@ class LatticeSolverBase:
         if tuple(data["f"].shape) != (self.Q,) + tuple(self.solid.shape):
             raise ValueError(f"checkpoint {path}: f has shape {tuple(data['f'].shape)}, "
                              f"the solver needs {(self.Q,) + tuple(self.solid.shape)}")
+        links, q = data.get("surface_links"), data.get("q_vals")
+        if links is not None and q is not None and (
+                links.shape != self.surface_links.shape or not np.array_equal(links, self.surface_links)
+                or not np.array_equal(q, self.q_vals)):
+            if links.ndim != 2 or links.shape[1] != self.dims + 1 or len(q) != len(links):
+                raise ValueError(f"checkpoint {path}: surface_links / q_vals have shapes {links.shape} / {q.shape}")
+            self._adopt_links(np.ascontiguousarray(links, dtype=np.int32), np.ascontiguousarray(q, dtype=np.float32))
         for k in self._history_keys():
             if k in data:
                 setattr(self, k, list(data[k]))
         self.step_count = int(data["step_count"])
-        if "surface_links" in data and not np.array_equal(data["surface_links"], self.surface_links):
-            warnings.warn("checkpoint link table differs from the one built from its solid mask; "
-                          "the engine keeps the rebuilt one", RuntimeWarning)
         g = data["g"] if ("g" in data and self.thermal) else None
         if self.thermal and g is None:
             g = self.g
@@ -402,16 +439,31 @@ class LatticeSolverBase:
         self._f_host = None
         self._engine.set_state(data["f"], data["f_outlet_prev"], g, self.step_count)
 
+    def _adopt_links(self, links: np.ndarray, q: np.ndarray) -> None:
+        """A new engine for this lattice with the given link table (the step
+        kernel choice returns to the default)."""
+        P, dev = self._params, self._engine.device
+        old = self._engine
+        self._engine = Engine(P, self.solid, links, q, self._engine_phi, dev)
+        del old
+        self.surface_links, self.q_vals = links, q
+
     @classmethod
     def from_checkpoint(cls, path: str, backend: Optional[str] = None, **overrides):
+        """Rebuilds a solver from a checkpoint of this engine or of the
+        reference: the constructor keywords from params_json (the reference's
+        backend name replaced by "b200"), this engine's options from
+        b200_options when present, then `overrides`."""
         data = _open_checkpoint(path)
         for key in ("params_json", "solid"):
             if key not in data:
                 raise ValueError(f"checkpoint {path} has no '{key}' entry")
         try:
             params = json.loads(str(data["params_json"]))
+            extra = json.loads(str(data["b200_options"])) if "b200_options" in data else {}
         except json.JSONDecodeError as e:
             raise ValueError(f"checkpoint {path}: unreadable params_json ({e})") from e
+        params.update(extra)
         params["backend"] = "b200"
         params.update(overrides)
         solid = data["solid"]

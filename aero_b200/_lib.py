@@ -60,6 +60,7 @@ SIGNATURES = {
     "aero_get_state_slab": ([_VP, _I32, _I32, _VP, _VP], ctypes.c_int),
     "aero_get_macroscopic": ([_VP, _VP, _VP], ctypes.c_int),
     "aero_field_stats": ([_VP, _I32, _I32, _VP, _VP], ctypes.c_int),
+    "aero_set_equilibrium": ([_VP, _VP, _VP, _VP, _VP, _VP, _I64, _VP], ctypes.c_int),
     "aero_step": ([_VP, _I64, _VP], ctypes.c_int),
     "aero_read_forces": ([_VP, _VP, _I64, ctypes.POINTER(_I64), _VP], ctypes.c_int),
     "aero_read_profile": ([_VP, _VP, _VP], ctypes.c_int),

@@ -388,6 +388,9 @@ int do_steps(AeroLattice *L, int64_t n, cudaStream_t st) {
 }
 
 template <class Real>
+int finish_set_state(AeroLattice *L, int64_t steps, cudaStream_t st);
+
+template <class Real>
 int do_set_state(AeroLattice *L, const double *f, const double *prev, const double *g, int64_t steps,
                  cudaStream_t st) {
   const Ops<Real> *ops = get_ops<Real>(L);
@@ -408,10 +411,21 @@ int do_set_state(AeroLattice *L, const double *f, const double *prev, const doub
                                                      L->ncells, L->cs);
     CUDA_TRY(cudaGetLastError());
   }
+  return finish_set_state<Real>(L, steps, st);
+}
+
+// After a state has been written into the old population buffer (and the
+// outlet and scalar buffers): the step counter, then the collision of the
+// state into the current buffer.
+template <class Real>
+int finish_set_state(AeroLattice *L, int64_t steps, cudaStream_t st) {
+  const Ops<Real> *ops = get_ops<Real>(L);
+  const int old = 1 - L->cur;
+  const dim3 grid = cell_grid(L);
   int64_t *ctr = reinterpret_cast<int64_t *>(L->ws + L->lay.counters);
   k_set_i64<<<1, 1, 0, st>>>(ctr, steps);
   CUDA_TRY(cudaGetLastError());
-  StepParams<Real> q = p;
+  StepParams<Real> q = make_params<Real>(L, L->cur);
   q.P = L->ws + L->lay.P[old];
   q.Pn = L->ws + L->lay.P[L->cur];
   if (les_active(L)) CUDA_TRY(ops->moments(q, true, grid, st));
@@ -422,6 +436,17 @@ int do_set_state(AeroLattice *L, const double *f, const double *prev, const doub
   L->inflow_upto = steps;  // inflow fields are uploaded again from the new step count
   L->state_set = true;
   return AERO_OK;
+}
+
+template <class Real>
+int do_set_equilibrium(AeroLattice *L, const EqFields &e, int64_t steps, cudaStream_t st) {
+  const Ops<Real> *ops = get_ops<Real>(L);
+  const int old = 1 - L->cur;
+  const StepParams<Real> p = make_params<Real>(L, L->cur);
+  Real *prev = reinterpret_cast<Real *>(L->ws + L->lay.prev[L->cur]);
+  Real *g = L->prm.thermal ? reinterpret_cast<Real *>(L->ws + L->lay.g[L->cur]) : nullptr;
+  CUDA_TRY(ops->init_eq(p, e, L->ws + L->lay.P[old], prev, g, cell_grid(L), st));
+  return finish_set_state<Real>(L, steps, st);
 }
 
 template <class Real>
@@ -806,6 +831,20 @@ int aero_set_state(AeroLattice *L, const double *f, const double *prev, const do
   CUDA_TRY(cudaSetDevice(L->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   return is_f64(L) ? do_set_state<double>(L, f, prev, g, steps, st) : do_set_state<float>(L, f, prev, g, steps, st);
+}
+
+int aero_set_equilibrium(AeroLattice *L, const double *rho, const double *ux, const double *uy, const double *uz,
+                         const double *T, int64_t steps, void *stream) {
+  if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
+  if (L->batch) return fail(AERO_ERR_STATE, "the lattice is a batch member; remove it from the batch first");
+  if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
+  if (steps < 0) return fail(AERO_ERR_INVALID, "negative step count");
+  if (uz && L->prm.dims != 3) return fail(AERO_ERR_INVALID, "uz is a 3D field");
+  if (T && !L->prm.thermal) return fail(AERO_ERR_INVALID, "T needs a lattice with a scalar");
+  CUDA_TRY(cudaSetDevice(L->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const EqFields e{rho, ux, uy, uz, T, L->prm.rho0, L->prm.u0, L->prm.T_ref};
+  return is_f64(L) ? do_set_equilibrium<double>(L, e, steps, st) : do_set_equilibrium<float>(L, e, steps, st);
 }
 
 int aero_get_state(AeroLattice *L, double *f, double *prev, double *g, void *stream) {

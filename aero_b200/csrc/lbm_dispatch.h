@@ -49,6 +49,10 @@ struct Ops {
   // kStatsValues doubles
   cudaError_t (*field_stats)(const StepParams<Real> &, const Real *gcur, int z0, int nzs, int step_delta, bool raw,
                              double *partial, uint32_t *ticket, double *out, cudaStream_t);
+  // equilibrium state of the fields into dst (populations), prev (outlet
+  // state, may be NULL) and g (scalar, may be NULL); grid as for step
+  cudaError_t (*init_eq)(const StepParams<Real> &, const EqFields &, void *dst, Real *prev, Real *g, dim3 grid,
+                         cudaStream_t);
   int store_bytes;
 };
 

@@ -140,10 +140,15 @@ struct Launch {
       k_field_stats<L, S, false><<<kStatsBlocks, kStatsBlock, 0, st>>>(p, gcur, z0, nzs, delta, partial, ticket, out);
     return cudaGetLastError();
   }
+  static cudaError_t init_eq(const StepParams<Real> &p, const EqFields &e, void *dst, Real *prev, Real *g,
+                             dim3 grid, cudaStream_t st) {
+    k_init_equilibrium<L, S><<<grid, kStepBlock, 0, st>>>(p, e, static_cast<S *>(dst), prev, g);
+    return cudaGetLastError();
+  }
   static constexpr Ops<Real> table = {&step,       &step_shaped, &moments,      &finalize,   &state_out,
                                       &load_state, &macro_out,   &step_tiled,   &tiled_setup, &step_batch,
                                       &moments_batch, &finalize_batch, &recycle_mean, &step_pair,
-                                      &step_batch_pair, &field_stats, (int)sizeof(S)};
+                                      &step_batch_pair, &field_stats, &init_eq, (int)sizeof(S)};
 };
 
 template <class S>

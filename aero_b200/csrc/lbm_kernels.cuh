@@ -1725,6 +1725,68 @@ __global__ void __launch_bounds__(kStatsBlock)
   if (t == 0) *ticket = 0u;
 }
 
+// --------------------------------------------------------------------------
+// Equilibrium state from macroscopic fields, built on the device: the
+// reference's initial state f = feq(rho, u) at every cell, solids included
+// (solver.py:218-227, solver3d.py:239-247), with the convective outlet state
+// = the x = nx-1 column of f and the scalar g_i = w_i T.  Each field is an
+// FP64 array of ncells values or, when NULL, the uniform value (rho0, u0,
+// 0, 0, T_ref).  feq is evaluated in FP64 with the operations of
+// compute_feq(_3d) (d2q9.py:66-89, d3q19.py:105-129) in their order, each
+// rounded on its own (no fused multiply-adds), so a state built here equals
+// one built from the same fields on the host; the deviation f - w is rounded
+// once to the storage format.
+// --------------------------------------------------------------------------
+template <class L, int I>
+__device__ __forceinline__ double feq_exact(double rho, double ux, double uy, double uz, double usq) {
+  constexpr double ex = Dir<L, I>::x, ey = Dir<L, I>::y, ez = Dir<L, I>::z;
+  double eu = __dadd_rn(ex * ux, ey * uy);  // products with 0 / +-1 are exact
+  eu = __dadd_rn(eu, L::DIMS == 3 ? ez * uz : 0.0);
+  const double poly = __dsub_rn(__dadd_rn(__dadd_rn(1.0, __dmul_rn(3.0, eu)), __dmul_rn(__dmul_rn(4.5, eu), eu)),
+                                __dmul_rn(1.5, usq));
+  return __dmul_rn(__dmul_rn(Dir<L, I>::w, rho), poly);
+}
+
+template <class L, class S>
+__global__ void __launch_bounds__(kStepBlock) k_init_equilibrium(const StepParams<typename StoreOps<S>::Real> p,
+                                                                 EqFields e, S *dst,
+                                                                 typename StoreOps<S>::Real *prev_dst,
+                                                                 typename StoreOps<S>::Real *g_dst) {
+  using Real = typename StoreOps<S>::Real;
+  using SO = StoreOps<S>;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y, z = blockIdx.z;
+  if (x >= p.nx) return;
+  const uint32_t c = cell_index(p, x, y, z);
+  const double rho = e.rho ? e.rho[c] : e.rho0;
+  const double ux = e.ux ? e.ux[c] : e.u0;
+  const double uy = e.uy ? e.uy[c] : 0.0;
+  const double uz = (L::DIMS == 3 && e.uz) ? e.uz[c] : 0.0;
+  const double usq = __dadd_rn(__dadd_rn(__dmul_rn(ux, ux), __dmul_rn(uy, uy)), __dmul_rn(uz, uz));
+  const bool outlet = prev_dst && x == p.nx - 1;
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    const double dv = __dsub_rn(feq_exact<L, i>(rho, ux, uy, uz, usq), Dir<L, i>::w);
+    SO::template store<i, L>(dst, elem(p, i, c), (Real)dv);
+    if (outlet) prev_dst[((int64_t)z * p.ny + y) * L::QP + i] = (Real)dv;
+  });
+  if (g_dst) {
+    const double T = e.T ? e.T[c] : e.T0;
+    if (p.feat & FEAT_SCALAR_REDUCED) {
+      using G = typename ScalarReduced<L>::Lat;
+      static_for<G::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        g_dst[elem(p, i, c)] = (Real)__dmul_rn(Dir<G, i>::w, T);
+      });
+    } else {
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        g_dst[elem(p, i, c)] = (Real)__dmul_rn(Dir<L, i>::w, T);
+      });
+    }
+  }
+}
+
 // Converts absolute FP64 populations (Q, ncells) into the storage format.
 template <class L, class S>
 __global__ void __launch_bounds__(kStepBlock) k_load_state(const StepParams<typename StoreOps<S>::Real> p,

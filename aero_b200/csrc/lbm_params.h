@@ -135,6 +135,13 @@ struct StepParams {
   Mrt3Adapted<Real> mrt3;   // D3Q19
 };
 
+// Macroscopic fields of an equilibrium state (k_init_equilibrium): FP64
+// device arrays of ncells values, or NULL for the uniform value.
+struct EqFields {
+  const double *rho, *ux, *uy, *uz, *T;
+  double rho0, u0, T0;
+};
+
 // Block layout of one lattice in the two-cells-per-thread batch kernel
 // (128-thread blocks).  A row's P pairs (x, x+1), x = 2, 4, .., nx - 4, take
 // TP threads (P rounded up to whole warps); a block holds RB rows of them

@@ -14,9 +14,17 @@
 // them, so nothing needs clearing, but two calls that overlap on the GPU
 // (different streams, no ordering between them) race on it.
 //
-// The first call on a device looks the array's address up with
-// cudaGetSymbolAddress, with that device current, and caches it; make that
-// first call before any stream capture begins.
+// Every call made outside stream capture looks the array's address up with
+// cudaGetSymbolAddress, with the call's device current, and refreshes a
+// per-device cache (so a device reset, which reloads the module, cannot
+// leave a stale address behind).  A call made while its stream is being
+// captured uses the cached address, since the lookup may load the module;
+// the first call on a device must therefore come before any stream capture.
+//
+// Link rows with a direction outside 1..Q-1 or a cell outside the grid
+// (which the reference's fancy indexing rejects with IndexError,
+// forces.py:27-33) make the call write NaN to every output value, so a
+// malformed list cannot pass for a plausible force.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -71,8 +79,8 @@ __global__ void k_link_contrib(const double *__restrict__ f_pre, const double *_
   const int i = lk[0], z = g.dims == 3 ? lk[1] : 0, y = lk[lw - 2], x = lk[lw - 1];
   double *out = scratch + k * kSlot;
   if (i < 1 || i >= g.Q || x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) {
-    for (int j = 0; j < 12; j++) out[j] = 0.0;  // invalid rows contribute nothing
-    out[12] = -1.0;
+    for (int j = 0; j < 12; j++) out[j] = 0.0;
+    out[12] = -1.0;  // marks the row invalid: the reduction then writes NaN
     return;
   }
   const long long c = ((long long)z * g.ny + y) * g.nx + x;
@@ -126,13 +134,18 @@ __global__ void __launch_bounds__(kReduceBlock) k_link_reduce(const double *scra
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
     if (lane == 0) sm[j][wid] = v;
   }
-  __syncthreads();
+  // invalid rows (bin -1): counted, and the outputs become NaN
+  int bad = 0;
+  for (long long k = t; k < n_links; k += kReduceBlock) bad += scratch[k * kSlot + 12] < 0.0 ? 1 : 0;
+  bad = __syncthreads_or(bad);
   if (t < 12) {
     double v = 0.0;
     for (int w = 0; w < kReduceBlock / 32; w++) v += sm[t][w];
-    out12[t] = v;
+    out12[t] = bad ? __longlong_as_double(0x7ff8000000000000LL) : v;
   }
-  if (profile) {
+  if (profile && bad) {
+    for (int b = t; b < 3 * nprof; b += kReduceBlock) profile[b] = __longlong_as_double(0x7ff8000000000000LL);
+  } else if (profile) {
     for (int b = t; b < nprof; b += kReduceBlock) {
       double p0 = 0.0, p1 = 0.0, p2 = 0.0;
       for (long long k = 0; k < n_links; k++) {
@@ -151,20 +164,27 @@ __global__ void __launch_bounds__(kReduceBlock) k_link_reduce(const double *scra
 std::mutex g_mu;
 double *g_addr[kMaxDevices] = {nullptr};
 
-// Device address of g_link_scratch on the current device, looked up once per
-// device (with that device current) and cached.
-cudaError_t scratch_ptr(double **ptr, int *device) {
+// Device address of g_link_scratch on the current device.  Outside stream
+// capture it is looked up on every call (with that device current) and the
+// per-device cache refreshed; during capture the cached address is used,
+// and a device never looked up before capture is an error.
+cudaError_t scratch_ptr(cudaStream_t st, double **ptr, int *device) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
   *device = dev;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(st, &cap);
+  if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_addr[dev]) {
+  if (cap == cudaStreamCaptureStatusNone) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_link_scratch);
     if (e != cudaSuccess) return e;
     g_addr[dev] = static_cast<double *>(p);
+  } else if (!g_addr[dev]) {
+    return cudaErrorStreamCaptureUnsupported;
   }
   *ptr = g_addr[dev];
   return cudaSuccess;
@@ -187,13 +207,17 @@ int aero_link_forces_static(int32_t dims, int32_t nx, int32_t ny, int32_t nz, co
              (long long)n_links, kStaticMaxLinks);
     return aero::set_error(AERO_ERR_CAPACITY, msg);
   }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
   double *scratch = nullptr;
   int dev = -1;
-  cudaError_t e = scratch_ptr(&scratch, &dev);
+  cudaError_t e = scratch_ptr(st, &scratch, &dev);
+  if (e == cudaErrorStreamCaptureUnsupported) {
+    return aero::set_error(AERO_ERR_STATE,
+                           "aero_link_forces_static: the first call on a device must come before stream capture");
+  }
   if (e != cudaSuccess) {
     return aero::set_error(AERO_ERR_CUDA, cudaGetErrorString(e));
   }
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   Geometry g{dims, dims == 2 ? 9 : 19, nx, ny, nz, (long long)nx * ny * nz, center[0], center[1], center[2]};
   if (n_links > 0) {
     const int b = 128;

@@ -102,6 +102,16 @@ class Engine:
             # keep the staging tensors alive until the copies ran
             self.torch.cuda.current_stream(self.device).synchronize()
 
+    def set_equilibrium(self, rho=None, ux=None, uy=None, uz=None, T=None, step_count: int = 0) -> None:
+        """State = feq of the given fields (numpy or torch, host or device;
+        None = the uniform value), built on the device (aero_set_equilibrium).
+        Host fields are copied as FP64, one array per given field."""
+        fields = [None if a is None else self._dev(a, self.shape) for a in (rho, ux, uy, uz, T)]
+        with self.torch.cuda.device(self.device):
+            check("aero_set_equilibrium", self.lib.aero_set_equilibrium(
+                self.h, *[None if a is None else a.data_ptr() for a in fields], int(step_count), self.stream()))
+            self.torch.cuda.current_stream(self.device).synchronize()
+
     def get_state_device(self, want_prev=True, want_g=True):
         t = self.torch
         f = t.empty((self.Q,) + self.shape, dtype=t.float64, device=self.device)

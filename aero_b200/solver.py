@@ -135,7 +135,7 @@ class Solver(LatticeSolverBase):
             synthetic_inflow_intensity=self.synthetic_inflow_intensity, thermal=self.thermal,
             T_hot=self.T_hot, T_cold=self.T_cold, alpha_T=self.alpha_T, buoyancy=self.buoyancy,
             g_gravity=self.g_gravity, beta=self.beta, T_ref=self.T_ref, collision=self.collision,
-            backend=self.backend, precision=self.precision, scalar_lattice=self.scalar_lattice,
+            backend=self.backend,
         )
 
     def _result(self, avg_window, stop_reason, last_conv, last_st) -> dict:

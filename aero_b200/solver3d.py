@@ -45,6 +45,7 @@ class Solver3D(LatticeSolverBase):
                 f"Unknown streamwise_bc '{streamwise_bc}'. Choose 'open', 'periodic', or 'recycling'.")
         self.Nz, self.Ny, self.Nx = int(Nz), int(Ny), int(Nx)
         self.sem_inlet = bool(sem_inlet)
+        self.sem_Tu, self.sem_L_int, self.sem_N = float(sem_Tu), float(sem_L_int), int(sem_N)
         self._setup(
             shape=(self.Nz, self.Ny, self.Nx), solid=solid, omega=omega, u0=u0, D=D, rho0=rho0,
             wall_bc=wall_bc, inlet_bc=inlet_bc, outlet_bc=outlet_bc, streamwise_bc=streamwise_bc,
@@ -129,6 +130,12 @@ class Solver3D(LatticeSolverBase):
     def _checkpoint_name(self):
         return f"checkpoint3d_{self.step_count:08d}.npz"
 
+    def _b200_options(self) -> dict:
+        opts = super()._b200_options()
+        if self.sem_inlet:
+            opts.update(sem_inlet=True, sem_Tu=self.sem_Tu, sem_L_int=self.sem_L_int, sem_N=self.sem_N)
+        return opts
+
     def _checkpoint_params(self):
         return dict(
             Nz=self.Nz, Ny=self.Ny, Nx=self.Nx, omega=self.omega, u0=self.u0, D=self.D,
@@ -145,7 +152,6 @@ class Solver3D(LatticeSolverBase):
             synthetic_inflow_intensity=self.synthetic_inflow_intensity, thermal=self.thermal,
             T_hot=self.T_hot, T_cold=self.T_cold, alpha_T=self.alpha_T, buoyancy=self.buoyancy,
             g_gravity=self.g_gravity, beta=self.beta, T_ref=self.T_ref,
-            precision=self.precision, scalar_lattice=self.scalar_lattice,
         )
 
     def _result(self, avg_window, stop_reason, last_conv, last_st) -> dict:

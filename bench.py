@@ -500,7 +500,6 @@ def scalar_precision_check(w, args, dev, tau=0.8, steps=2000, formats=("fp32", "
     and the relative L2 difference of u."""
     import numpy as np
     import torch
-    from aero_b200.lattice import scalar_weights
     wk = dict(w, nu=(tau - 0.5) / 3.0)
     shp = (wk["nz"], wk["ny"], wk["nx"])
     gen = torch.Generator(device=dev)
@@ -512,10 +511,7 @@ def scalar_precision_check(w, args, dev, tau=0.8, steps=2000, formats=("fp32", "
     ref = None
     for prec in ("fp64",) + tuple(formats):
         s = _build_solver(wk, prec, dev, steps, 0)
-        f0, prev0, _ = s._uniform_state_device()
-        wg = torch.tensor(scalar_weights(3, s.scalar_lattice == "reduced"), dtype=torch.float64, device=dev)
-        g0 = (wg.reshape(-1, 1, 1, 1) * T0[None]).contiguous()
-        s._engine.set_state(f0, prev0, g0, 0)
+        s.set_equilibrium_state(T=T0)
         st0 = s.field_statistics()
         t0 = time.perf_counter()
         s._advance(steps)
@@ -536,7 +532,7 @@ def scalar_precision_check(w, args, dev, tau=0.8, steps=2000, formats=("fp32", "
             rec["Nu_top_err_vs_fp64"] = abs(st["Nu_top"] - ref["Nu_top"]) / abs(ref["Nu_top"])
             rec["u_rel_l2_vs_fp64"] = float(np.linalg.norm(u - ref["u"]) / np.linalg.norm(ref["u"]))
         out[prec] = rec
-        del s, f0, prev0, g0
+        del s
         torch.cuda.empty_cache()
     out["fp64"].pop("u", None)
     return out
@@ -559,9 +555,10 @@ def _build_solver(w, precision, dev, steps, warmup):
     return Solver(Ny=ny, Nx=nx, **common) if dims == 2 else Solver3D(Nz=nz, Ny=ny, Nx=nx, **common)
 
 
-def _initial_fields(w, dev, rank):
-    """The seeded initial velocity of the workload: ux = u0 (1 + p U(-1, 1))
-    (p the workload's perturbation), uy = U(-a, a) where the workload sets a."""
+def _initial_fields(w, dev, rank, s):
+    """The seeded initial fields of the workload (device FP64): ux = u0 (1 +
+    p U(-1, 1)) with p the workload's perturbation; uy = U(-a, a) where the
+    workload sets a; the scalar T = T_ref + U(-b, b) where it sets b."""
     import torch
     shp = (w["ny"], w["nx"]) if w["dims"] == 2 else (w["nz"], w["ny"], w["nx"])
     gen = torch.Generator(device=dev)
@@ -570,7 +567,11 @@ def _initial_fields(w, dev, rank):
                                                            dtype=torch.float64) - 1.0))
     uy = (w["perturb_uy"] * (2.0 * torch.rand(shp, generator=gen, device=dev, dtype=torch.float64) - 1.0)
           if w.get("perturb_uy") else None)
-    return ux, uy
+    T = None
+    if s.thermal and w.get("T_noise"):
+        gen.manual_seed(4321 + rank)
+        T = s.T_ref + w["T_noise"] * (2.0 * torch.rand(shp, generator=gen, device=dev, dtype=torch.float64) - 1.0)
+    return ux, uy, T
 
 
 def _bytes_per_cell(s, precision):
@@ -605,20 +606,8 @@ def measure_lattice(w, precision, args, dev, rank=0, world=1, dist=None, e2e=Tru
     s = _build_solver(w, precision, dev, args.steps, args.warmup)
     eng = s._engine
     ncells = w["nx"] * w["ny"] * w["nz"]
-    ux0, uy0 = _initial_fields(w, dev, rank)
-    f0, prev0, g0 = s._uniform_state_device(ux=ux0, uy=uy0)
-    del ux0, uy0
-    if g0 is not None and w.get("T_noise"):
-        # the scalar starts at T_ref + U(-a, a), seeded
-        from aero_b200.lattice import scalar_weights
-        gen = torch.Generator(device=dev)
-        gen.manual_seed(4321 + rank)
-        T0 = s.T_ref + w["T_noise"] * (2.0 * torch.rand(s.solid.shape, generator=gen, device=dev,
-                                                         dtype=torch.float64) - 1.0)
-        wg = torch.tensor(scalar_weights(s.dims, s.scalar_lattice == "reduced"), dtype=torch.float64, device=dev)
-        g0 = (wg.reshape((-1,) + (1,) * s.dims) * T0[None]).contiguous()
-        del T0
-    eng.set_state(f0, prev0, g0, 0)
+    ux0, uy0, T0 = _initial_fields(w, dev, rank, s)
+    eng.set_equilibrium(ux=ux0, uy=uy0, T=T0)
     stream = torch.cuda.current_stream(dev)
     tune = None
     if args.kernel == "auto":
@@ -693,40 +682,38 @@ def measure_lattice(w, precision, args, dev, rank=0, world=1, dist=None, e2e=Tru
     }
     res["launches_per_step"] = 2 + (1 if (s.les and s.collision != "mrt" and not eng.les_fused()) else 0)
     if e2e:
-        res["e2e"] = _measure_e2e(s, w, args, dev, f0, prev0, g0, world, dist)
-    del f0, prev0, g0
+        res["e2e"] = _measure_e2e(s, w, args, dev, (ux0, uy0, T0), world, dist)
+    del ux0, uy0, T0
     return res
 
 
-def _measure_e2e(s, w, args, dev, f0, prev0, g0, world, dist):
-    """MLUPS of Solver.run(K) end to end: the initial state copied from
-    pinned host memory, K steps, the force history and the result's fields
-    read back, timed on the host."""
+def _measure_e2e(s, w, args, dev, fields, world, dist):
+    """MLUPS of Solver.run(K) end to end: the initial fields (ux, and uy / T
+    where the workload seeds them) copied from pinned host memory and turned
+    into the equilibrium state on the device (set_equilibrium_state), K
+    steps, the force history and the result's fields read back, timed on the
+    host."""
     import torch
-    eng = s._engine
     ncells = w["nx"] * w["ny"] * w["nz"]
-    Q = 9 if w["dims"] == 2 else 19
-    f0_host = f0.cpu().pin_memory()
-    prev_host = prev0.cpu().pin_memory()
-    g_host = None if g0 is None else g0.cpu().pin_memory()
+    host = [None if a is None else a.cpu().pin_memory() for a in fields]
     torch.cuda.synchronize(dev)
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
-    eng.set_state(f0_host, prev_host, g_host, 0)
     s.step_count = 0
     s._init_histories()
+    s.set_equilibrium_state(ux=host[0], uy=host[1], T=host[2])
     # one stability check at the end would raise on a diverged state; the
     # throughput measurement does not depend on it, so none is requested
     r = s.run(args.steps, check_every=args.steps + 1, verbose=False)
     torch.cuda.synchronize(dev)
     dt = max_over_ranks(time.perf_counter() - t0, dist, dev)
-    h2d = f0_host.numel() * 8 + prev_host.numel() * 8 + (0 if g_host is None else g_host.numel() * 8)
+    h2d = sum(a.numel() * 8 for a in host if a is not None)
     d2h = (args.steps * 12 * 8 + (w["nz"] if w["dims"] == 3 else w["ny"]) * 3 * 8
            + (1 + w["dims"]) * ncells * 8 + (ncells * 8 if s.thermal else 0))
     return {"value": whole_job_mlups(ncells, world, args.steps, dt), "unit": "MLUPS",
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-            "call": f"{type(s).__name__}.run(K) after uploading the initial state from pinned host memory",
+            "call": f"{type(s).__name__}.set_equilibrium_state(fields from pinned host memory) + run(K)",
             "Cd_mean": r["Cd_mean"]}
 
 

@@ -122,6 +122,20 @@ AERO_API int aero_bind_workspace(AeroLattice *lat, void *device_ptr, uint64_t by
 AERO_API int aero_set_state(AeroLattice *lat, const double *f, const double *f_outlet_prev, const double *g,
                    int64_t step_count, void *stream);
 
+/* Sets the state to the equilibrium of macroscopic fields, built on the
+ * device: f = feq(rho, u) at every cell (solids included, as the
+ * reference's initial state, solver.py:218-227 / solver3d.py:239-247, and
+ * as a caller's `s.f = compute_feq(...)` assignment), the convective outlet
+ * state = the x = nx-1 column of that f, and the scalar g_i = w_i T.  rho,
+ * ux, uy, uz, T are caller DEVICE arrays of nz*ny*nx float64 values in the
+ * reference's (z, y, x) order, or NULL for the uniform value (rho0, u0, 0,
+ * 0, T_ref); uz only in 3D, T only with a scalar.  feq is evaluated in FP64
+ * with the operations of compute_feq(_3d) (d2q9.py:66-89,
+ * d3q19.py:105-129), so the state equals aero_set_state of the same f.
+ * Moves one field per cell where aero_set_state moves Q populations. */
+AERO_API int aero_set_equilibrium(AeroLattice *lat, const double *rho, const double *ux, const double *uy,
+                                  const double *uz, const double *T, int64_t step_count, void *stream);
+
 /* Writes the current state into caller DEVICE buffers (same layouts; any
  * pointer may be NULL).  The state is the reference's self.f after the last
  * step. */
@@ -234,9 +248,15 @@ AERO_API int aero_kernel_times(AeroLattice *lat, double *step_ms, double *forces
  * row/plane).  center is a HOST pointer to (x, y, z).  Its per-link scratch is
  * a fixed 4 MiB array in the library's device image, so n_links is limited to
  * 32768 (larger lists return AERO_ERR_CAPACITY).  Every call shares that
- * array: calls that overlap on the GPU race.  The first call on a device
- * looks the array's address up (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture. */
+ * array: calls that overlap on the GPU race.  Each call made outside stream
+ * capture looks the array's address up (cudaGetSymbolAddress) with its
+ * device current; a call on a capturing stream reuses the address found by
+ * an earlier call on that device, so make the first call on a device before
+ * any stream capture (otherwise AERO_ERR_STATE).  A row whose direction is
+ * outside 1..Q-1 or whose cell is outside the grid (the reference raises
+ * IndexError there) makes every output value NaN.  The profile is summed
+ * per row/plane in link order by one block (deterministic; its cost grows
+ * as rows x links, about 0.3 ms at the cap). */
 AERO_API int aero_link_forces_static(int32_t dims, int32_t nx, int32_t ny, int32_t nz, const double *f_pre,
                                      const double *f_post, const int32_t *links, int64_t n_links,
                                      const double *center, double *out, double *profile, void *stream);

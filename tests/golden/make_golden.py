@@ -4,7 +4,7 @@ Run in a container that has the Aero reference checked out (read-only is
 fine) and Numba installed:
 
     NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py \
-        --reference /root/reference
+        --reference <path to an Aero checkout>
 
 It imports the reference's own ``aero`` package and records, for a set of
 small seeded cases covering every hot-path feature, the initial state, the
@@ -322,6 +322,61 @@ def geometry_fixtures(out):
     np.savez_compressed(out / "geometry.npz", **rec)
 
 
+def checkpoint_fixtures(out):
+    """Checkpoints written by the reference's own save_checkpoint
+    (solver.py:638-686, solver3d.py:727-780), one 2D and one 3D thermal case,
+    each after `n1` steps from a seeded state, plus the state and histories
+    the reference reaches `n2` steps after it and the names of the
+    reference constructors' keyword arguments."""
+    import inspect
+
+    from aero.lbm.d2q9 import compute_feq
+    from aero.lbm.d3q19 import compute_feq_3d
+    from aero.lbm.solver import Solver
+    from aero.lbm.solver3d import Solver3D
+
+    specs = [
+        ("2d", Solver, ("cyl", 4.5, 0.3, 0.5), (24, 48),
+         dict(collision="bgk", wall_bc="noslip", outlet_bc="convective", bouzidi=True, thermal=True,
+              alpha_T=0.02, buoyancy=True, g_gravity=1e-3, beta=0.5, T_ref=0.5), 0.6, 10, 15),
+        ("3d", Solver3D, ("box", 4.0, 4.0, 100.0, 0.4, 2.0 / 10.0, 0.5), (8, 10, 18),
+         dict(collision="trt", trt_lambda=3.0 / 16.0, les=True, les_model="wale", les_cs=0.3,
+              streamwise_bc="periodic", body_force_x=1e-5, wall_bc="noslip", thermal=True, T_hot=1.0,
+              T_cold=0.0, alpha_T=0.01, buoyancy=True, g_gravity=1e-3, beta=1.0, T_ref=0.5), 0.75, 6, 8),
+    ]
+    for tag, cls, spec, shape, kw, tau, n1, n2 in specs:
+        rng = np.random.default_rng(zlib.crc32(f"ckpt_{tag}".encode()))
+        if tag == "2d":
+            geom, solid, phi = _geometry_2d(spec, *shape)
+            s = cls(Ny=shape[0], Nx=shape[1], solid=solid, omega=1.0 / tau, u0=0.05, D=geom.reference_length(),
+                    backend="numba", phi=phi, **kw)
+            rho = 1.0 + 1e-3 * rng.uniform(-1, 1, shape)
+            s.f = np.ascontiguousarray(compute_feq(rho, 0.05 + 2e-3 * rng.uniform(-1, 1, shape),
+                                                   2e-3 * rng.uniform(-1, 1, shape)))
+            w = s._w
+        else:
+            geom, solid, phi = _geometry_3d(spec, *shape)
+            s = cls(Nz=shape[0], Ny=shape[1], Nx=shape[2], solid=solid, omega=1.0 / tau, u0=0.05,
+                    D=geom.reference_length(), backend="numba", phi=phi, **kw)
+            rho = 1.0 + 1e-3 * rng.uniform(-1, 1, shape)
+            s.f = np.ascontiguousarray(compute_feq_3d(rho, 0.05 + 2e-3 * rng.uniform(-1, 1, shape),
+                                                      2e-3 * rng.uniform(-1, 1, shape),
+                                                      2e-3 * rng.uniform(-1, 1, shape)))
+            w = s._w_np
+        T0 = 0.5 + 0.05 * rng.uniform(-1, 1, shape)
+        s.g = np.ascontiguousarray(w.reshape((-1,) + (1,) * len(shape)) * T0[None])
+        s.run(n1, check_every=n1 + 1, verbose=False)
+        s.save_checkpoint(str(out / f"ckpt_ref_{tag}.npz"))
+        s.run(n2, check_every=n2 + 1, verbose=False)
+        hist = {k: np.array(getattr(s, k), dtype=np.float64) for k in
+                (("Cd_history", "Cl_history", "Cm_history") if tag == "2d" else
+                 ("Cd_history", "Cly_history", "Clz_history", "Cmx_history", "Cmy_history", "Cmz_history"))}
+        names = [n for n in inspect.signature(cls.__init__).parameters if n != "self"]
+        np.savez_compressed(out / f"ckpt_cont_{tag}.npz", f=s.f, f_outlet_prev=s._f_outlet_prev, g=s.g,
+                            step_count=np.array(s.step_count), n2=np.array(n2),
+                            ctor_params=np.array(json.dumps(names)), **hist)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="path of the Aero checkout")
@@ -343,6 +398,9 @@ def main():
     if not args.only:
         geometry_fixtures(out)
         print("wrote geometry", flush=True)
+    if not args.only or "ckpt" in args.only:
+        checkpoint_fixtures(out)
+        print("wrote checkpoints", flush=True)
 
 
 if __name__ == "__main__":
