@@ -18,6 +18,7 @@
 #include "../../include/aero_b200.h"
 #include "lbm_dispatch.h"
 #include "lbm_kernels.cuh"
+#include "lbm_quad.cuh"
 
 using namespace aero;
 
@@ -141,6 +142,7 @@ struct AeroLattice {
   int step_shape = 0;
   bool tiled = false;
   bool pair = false;
+  bool quad = false;
   int tile_blocks = 0, tile_rows = 0, tiles_per_plane = 0, ntiles = 0;
   uint32_t tile_extra_tx = 0;  // AERO_B200_TEST_STALL_TILES=1 at bind: stages never complete
   // optional per-kernel event timing (eager launches only)
@@ -159,6 +161,15 @@ bool is_f64(const AeroLattice *L) { return L->prm.storage == AERO_STORE_F64; }
 bool pair_capable(const AeroLattice *L, int min_nx) {
   return L->prm.dims == 3 && !is_f64(L) && L->prm.nx % 2 == 0 && L->prm.nx >= min_nx &&
          !(L->feat & (FEAT_BODY_FORCE | FEAT_THERMAL));
+}
+
+// Lattices the four-cells-per-thread kernel takes: D3Q19, 16-bit storage,
+// nx a multiple of 4 (>= 12 where open or recycling columns run per cell),
+// no body force or scalar lattice.
+bool quad_capable(const AeroLattice *L) {
+  const bool edges = L->prm.dims == 3 && (L->feat & (FEAT_OPEN | FEAT_RECYCLE));
+  return L->prm.dims == 3 && (L->prm.storage == AERO_STORE_F16 || L->prm.storage == AERO_STORE_BF16) &&
+         L->prm.nx % 4 == 0 && L->prm.nx >= (edges ? 12 : 8) && !(L->feat & (FEAT_BODY_FORCE | FEAT_THERMAL));
 }
 
 template <class Real>
@@ -332,6 +343,8 @@ int launch_step(AeroLattice *L, int cur, cudaStream_t st, bool timed = false) {
     CUDA_TRY(ops->step_tiled(p, L->tile_blocks, st));
   else if (L->pair)
     CUDA_TRY(ops->step_pair(p, st));
+  else if (L->quad)
+    CUDA_TRY(ops->step_quad(p, st));
   else if (L->step_shape != 0)
     CUDA_TRY(ops->step_shaped(p, L->step_shape, st));
   else
@@ -1048,7 +1061,7 @@ int aero_set_inflow(AeroLattice *L, const double *fields, int64_t first, int64_t
 int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
   if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
   if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
-  if (kernel < 0 || kernel > kStepPair) return fail(AERO_ERR_INVALID, "kernel must be 0..%d", kStepPair);
+  if (kernel < 0 || kernel > kStepQuad) return fail(AERO_ERR_INVALID, "kernel must be 0..%d", kStepQuad);
   CUDA_TRY(cudaSetDevice(L->device));
   if (kernel == kStepPair) {
     if (!pair_capable(L, 2))
@@ -1058,16 +1071,25 @@ int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
     if (((int64_t)L->prm.ny * L->prm.nz + 31) / 32 > 65535)
       return fail(AERO_ERR_UNSUPPORTED, "the two-cell kernel takes at most 65535 * 32 rows (ny * nz)");
   }
+  if (kernel == kStepQuad) {
+    if (!quad_capable(L))
+      return fail(AERO_ERR_UNSUPPORTED,
+                  "the four-cell kernel covers D3Q19 with 16-bit storage, nx a multiple of 4 (>= 12 with an open "
+                  "inlet), no body force or scalar lattice");
+    if (((int64_t)L->prm.ny * L->prm.nz + kQuadRows - 1) / kQuadRows > 65535)
+      return fail(AERO_ERR_UNSUPPORTED, "the four-cell kernel takes at most 65535 * 16 rows (ny * nz)");
+  }
   if (kernel == kStepShapes) {
     const int rc = is_f64(L) ? plan_tiles<double>(L, true) : plan_tiles<float>(L, true);
     if (rc != AERO_OK) return rc;
     if (!L->tiled) return fail(AERO_ERR_UNSUPPORTED, "rows of this lattice do not fit the row-tiled kernel");
-    L->pair = false;
+    L->pair = L->quad = false;
   } else {
     L->tiled = false;
     L->tile_blocks = L->tile_rows = L->tiles_per_plane = L->ntiles = 0;
     L->pair = kernel == kStepPair;
-    L->step_shape = L->pair ? 0 : kernel;
+    L->quad = kernel == kStepQuad;
+    L->step_shape = (L->pair || L->quad) ? 0 : kernel;
   }
   // captured step sequences launch the previous kernel
   for (auto &e : L->pair_exec)
@@ -1080,7 +1102,7 @@ int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
 
 int aero_get_step_kernel(const AeroLattice *L, int32_t *kernel) {
   if (!L || !kernel) return fail(AERO_ERR_INVALID, "NULL argument");
-  *kernel = L->tiled ? kStepShapes : (L->pair ? kStepPair : L->step_shape);
+  *kernel = L->tiled ? kStepShapes : (L->pair ? kStepPair : (L->quad ? kStepQuad : L->step_shape));
   return AERO_OK;
 }
 

@@ -53,6 +53,9 @@ struct Ops {
   // state, may be NULL) and g (scalar, may be NULL); grid as for step
   cudaError_t (*init_eq)(const StepParams<Real> &, const EqFields &, void *dst, Real *prev, Real *g, dim3 grid,
                          cudaStream_t);
+  // regular step, four cells per thread (k_step_quad; D3Q19, 16-bit
+  // storage); cudaErrorNotSupported for other classes
+  cudaError_t (*step_quad)(const StepParams<Real> &, cudaStream_t);
   int store_bytes;
 };
 
@@ -67,8 +70,10 @@ constexpr int kStepShapes = 3;
 constexpr int kStepShapeXY[kStepShapes][2] = {{128, 1}, {256, 1}, {32, 4}};
 
 // Step kernel ids beyond the shapes: kStepShapes = the row-tiled kernel,
-// kStepPair = the two-cells-per-thread kernel.
+// kStepPair = the two-cells-per-thread kernel, kStepQuad = the four-cells-
+// per-thread kernel for 16-bit storage.
 constexpr int kStepPair = kStepShapes + 1;
+constexpr int kStepQuad = kStepShapes + 2;
 
 inline dim3 step_grid(int shape, int nx, int ny, int nz) {
   const int bx = kStepShapeXY[shape][0], by = kStepShapeXY[shape][1];

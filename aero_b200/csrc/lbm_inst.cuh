@@ -6,6 +6,7 @@
 #include "lbm_dispatch.h"
 #include "lbm_kernels.cuh"
 #include "lbm_pair.cuh"
+#include "lbm_quad.cuh"
 
 namespace aero {
 namespace inst {
@@ -145,10 +146,20 @@ struct Launch {
     k_init_equilibrium<L, S><<<grid, kStepBlock, 0, st>>>(p, e, static_cast<S *>(dst), prev, g);
     return cudaGetLastError();
   }
+  static cudaError_t step_quad(const StepParams<Real> &p, cudaStream_t st) {
+    if constexpr (std::is_same<Real, float>::value && L::DIMS == 3 && sizeof(S) == 2) {
+      k_step_quad<L, S, COLL><<<quad_grid(p), kQuadBlock, 0, st>>>(p);
+      return cudaGetLastError();
+    } else {
+      (void)p;
+      (void)st;
+      return cudaErrorNotSupported;
+    }
+  }
   static constexpr Ops<Real> table = {&step,       &step_shaped, &moments,      &finalize,   &state_out,
                                       &load_state, &macro_out,   &step_tiled,   &tiled_setup, &step_batch,
                                       &moments_batch, &finalize_batch, &recycle_mean, &step_pair,
-                                      &step_batch_pair, &field_stats, &init_eq, (int)sizeof(S)};
+                                      &step_batch_pair, &field_stats, &init_eq, &step_quad, (int)sizeof(S)};
 };
 
 template <class S>

@@ -612,8 +612,8 @@ def measure_lattice(w, precision, args, dev, rank=0, world=1, dist=None, e2e=Tru
     tune = None
     if args.kernel == "auto":
         tune = s.autotune(steps=10)
-    elif args.kernel == "pair":
-        eng.set_step_kernel(4)
+    elif args.kernel in ("pair", "quad"):
+        eng.set_step_kernel(4 if args.kernel == "pair" else 5)
     eng.step(args.warmup)
     eng.read_forces()
     if dist:
@@ -653,14 +653,14 @@ def measure_lattice(w, precision, args, dev, rank=0, world=1, dist=None, e2e=Tru
     plan["les_fused"] = eng.les_fused()
     if tune is not None:
         plan["autotune_ms_per_step"] = {str(k): v for k, v in tune["ms_per_step"].items()}
-    kname = "k_step_tiled" if plan["tiled"] else ("k_step_pair" if plan["kernel_id"] == 4 else "k_step")
+    kname = "k_step_tiled" if plan["tiled"] else {4: "k_step_pair", 5: "k_step_quad"}.get(plan["kernel_id"], "k_step")
     # DRAM bytes per launch from the committed ncu summary of this kernel,
     # workload and precision (a smaller case scaled by cells where the summary
     # says so); None when no capture covers it
     traffic = None
     pat = re.compile(rf"^- {re.escape(args.workload)}: dram bytes per launch = (\d+)\s*$", re.M)
     for md in sorted((ROOT / "profiles").glob(f"{kname}_*_{precision}.md")):
-        if kname == "k_step" and md.name.startswith(("k_step_tiled", "k_step_pair")):
+        if kname == "k_step" and md.name.startswith(("k_step_tiled", "k_step_pair", "k_step_quad")):
             continue
         m = pat.search(md.read_text())
         if m:
@@ -674,6 +674,8 @@ def measure_lattice(w, precision, args, dev, rank=0, world=1, dist=None, e2e=Tru
                      "kernel": f"{kname} (fused stream/BC/collide" + (
                          ", source rows staged in shared memory by bulk async copies)" if plan["tiled"]
                          else ", two cells per thread on packed FP32 arithmetic)" if plan["kernel_id"] == 4
+                         else ", four cells per thread, 8-byte loads realigned by warp shuffles)"
+                         if plan["kernel_id"] == 5
                          else ", per-cell global gather, blocks " + ("128x1", "256x1", "32x4")[plan["kernel_id"]]
                          + ")"),
                      "step_plan": plan, "alg_bytes_per_launch": bpc * ncells, "bytes_per_cell": bpc,
@@ -733,10 +735,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--collision", default=None, choices=["bgk", "trt", "mrt"],
                     help="override the workload's collision operator (profiling)")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "rowgather", "tiled", "pair"],
+    ap.add_argument("--kernel", default="auto", choices=["auto", "rowgather", "tiled", "pair", "quad"],
                     help="step kernel: chosen by the autotuner (default), the per-cell global gather, "
-                         "rows staged in shared memory by bulk async copies, or two cells per thread "
-                         "on packed FP32 arithmetic")
+                         "rows staged in shared memory by bulk async copies, two cells per thread "
+                         "on packed FP32 arithmetic, or four cells per thread (16-bit storage)")
     ap.add_argument("--batch-every", type=int, default=1,
                     help="batch96: keep every k-th case (a smaller batch for profiling captures)")
     ap.add_argument("--serve-requests", type=int, default=128)

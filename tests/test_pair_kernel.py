@@ -118,3 +118,62 @@ def test_pair_kernel_refused_outside_its_cover():
         with pytest.raises(AeroError, match="AERO_ERR_UNSUPPORTED"):
             s._engine.set_step_kernel(PAIR)
         assert s._engine.get_step_kernel() == 0
+
+
+# ---------------------------------------------------------------------------
+# The four-cells-per-thread kernel (step kernel 5, 16-bit storage)
+# ---------------------------------------------------------------------------
+QUAD = 5
+
+
+@pytest.mark.parametrize("collision", ["mrt", "bgk", "trt"])
+@pytest.mark.parametrize("precision", ["fp16s", "bf16s"])
+def test_quad_kernel_equals_per_cell_and_pair_kernels(precision, collision):
+    """Open sphere lattice (inlet / outlet edge columns per cell, slip-wall
+    rows, Bouzidi link cells, sponge); nx = 64 leaves the row's last warp
+    partly idle (14 quads), so the shuffles' edge lanes are exercised."""
+    fq, cdq = _sphere(precision, QUAD, collision=collision)
+    fc, cdc = _sphere(precision, 0, collision=collision)
+    fp, _ = _sphere(precision, PAIR, collision=collision)
+    np.testing.assert_allclose(fq, fc, rtol=0, atol=TOL[precision] * np.abs(fc).max())
+    np.testing.assert_allclose(cdq, cdc, rtol=0, atol=10 * TOL[precision] * np.abs(cdc).max())
+    np.testing.assert_allclose(fq, fp, rtol=0, atol=TOL[precision] * np.abs(fp).max())
+
+
+@pytest.mark.parametrize("nx", [32, 136, 520])
+@pytest.mark.parametrize("precision", ["fp16s", "bf16s"])
+def test_quad_kernel_periodic_rows_wrap(precision, nx):
+    """Streamwise periodic lattice: the quads cover whole rows, the x wrap of
+    the first and last quad comes from the edge lanes' own loads; rows of 8,
+    34 and 130 quads (one partial warp, several warps, several blocks)."""
+    from aero_b200 import Solver3D, Sphere
+
+    def run(kernel):
+        nz, ny = 10, 12
+        sph = Sphere(radius=3, cx_frac=0.3, cy_frac=0.5, cz_frac=0.5)
+        solid, phi = sph.mark_solid(nz, ny, nx), sph.sdf_field(nz, ny, nx)
+        s = Solver3D(Nz=nz, Ny=ny, Nx=nx, solid=solid, omega=1 / 0.7, u0=0.05, D=6.0, collision="mrt",
+                     bouzidi=True, phi=phi, wall_bc="noslip", streamwise_bc="periodic", precision=precision)
+        rng = np.random.default_rng(3)
+        s.set_equilibrium_state(ux=0.05 + 0.01 * rng.uniform(-1, 1, solid.shape),
+                                uy=0.01 * rng.uniform(-1, 1, solid.shape), uz=0.01 * rng.uniform(-1, 1, solid.shape))
+        s._engine.set_step_kernel(kernel)
+        assert s._engine.get_step_kernel() == kernel
+        s.run(40, check_every=41, verbose=False)
+        return s.f
+
+    fq, fc = run(QUAD), run(0)
+    np.testing.assert_allclose(fq, fc, rtol=0, atol=TOL[precision] * np.abs(fc).max())
+
+
+def test_quad_kernel_refuses_other_lattices():
+    from aero_b200 import Solver3D
+    from aero_b200._lib import AeroError
+    solid = np.zeros((6, 6, 30), dtype=bool)
+    for kw in (dict(precision="fp32"), dict(precision="fp16s", body_force_x=1e-5, streamwise_bc="periodic")):
+        s = Solver3D(Nz=6, Ny=6, Nx=30, solid=solid, omega=1.5, u0=0.05, D=4.0, **kw)
+        with pytest.raises(AeroError):
+            s._engine.set_step_kernel(QUAD)
+    s = Solver3D(Nz=6, Ny=6, Nx=30, solid=solid, omega=1.5, u0=0.05, D=4.0, precision="fp16s")
+    with pytest.raises(AeroError):  # nx = 30 is not a multiple of 4
+        s._engine.set_step_kernel(QUAD)
