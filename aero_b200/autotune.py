@@ -6,7 +6,8 @@ row-tiled kernel that stages source rows in shared memory with bulk async
 copies (where a lattice's rows fit it), the D3Q19 kernel that takes two
 cells per thread on the packed FP32 instructions, and, for 16-bit storage,
 the D3Q19 kernel that takes four cells per thread with one 8-byte load per
-direction.  Which is fastest depends on the
+direction, and, for BGK / TRT with LES, the D3Q19 kernel that computes the
+LES rate from a shared-memory velocity stencil instead of a moments pass.  Which is fastest depends on the
 lattice's shape and storage format (short rows leave threads of wide blocks
 idle; the tiled kernel pays per-tile overhead).  ``autotune`` times each one
 on the lattice itself with CUDA events, keeps the fastest and puts the
@@ -26,7 +27,8 @@ from ._lib import AeroError
 KERNELS = {0: "per-cell gather, 128x1 blocks", 1: "per-cell gather, 256x1 blocks",
            2: "per-cell gather, 32x4 blocks", 3: "row-tiled, bulk async copies",
            4: "two cells per thread, packed FP32 arithmetic",
-           5: "four cells per thread, 8-byte loads realigned by warp shuffles (16-bit storage)"}
+           5: "four cells per thread, 8-byte loads realigned by warp shuffles (16-bit storage)",
+           6: "LES velocity stencil staged in shared memory, no moments pass (BGK/TRT + LES)"}
 
 
 def autotune(solver, steps: int = 20, warmup: int = 2) -> Dict:

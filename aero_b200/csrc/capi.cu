@@ -18,6 +18,7 @@
 #include "../../include/aero_b200.h"
 #include "lbm_dispatch.h"
 #include "lbm_kernels.cuh"
+#include "lbm_les.cuh"
 #include "lbm_quad.cuh"
 
 using namespace aero;
@@ -143,6 +144,8 @@ struct AeroLattice {
   bool tiled = false;
   bool pair = false;
   bool quad = false;
+  bool les_fused = false;  // k_step_les: LES velocity stencil in shared memory, no moments pass
+  int les_chunk = 0;       // planes per block of k_step_les
   int tile_blocks = 0, tile_rows = 0, tiles_per_plane = 0, ntiles = 0;
   uint32_t tile_extra_tx = 0;  // AERO_B200_TEST_STALL_TILES=1 at bind: stages never complete
   // optional per-kernel event timing (eager launches only)
@@ -209,6 +212,7 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   p.sponge_start = std::max(a.nx - a.sponge_thickness, 0);
   p.tile_rows = L->tile_rows;
   p.batch_rows = L->ncells < kBatchSmallCells ? 1 : kBatchRows;
+  p.les_chunk = L->les_chunk > 0 ? L->les_chunk : 1;
   p.tile_extra_tx = L->tile_extra_tx;
   p.tiles_per_plane = L->tiles_per_plane;
   p.ntiles = L->ntiles;
@@ -338,8 +342,10 @@ int launch_step(AeroLattice *L, int cur, cudaStream_t st, bool timed = false) {
     CUDA_TRY(cudaEventRecord(e[0], st));
   }
   if (L->feat & FEAT_RECYCLE) CUDA_TRY(ops->recycle_mean(p, st));
-  if (les_active(L)) CUDA_TRY(ops->moments(p, false, grid, st));
-  if (L->tiled)
+  if (les_active(L) && !L->les_fused) CUDA_TRY(ops->moments(p, false, grid, st));
+  if (L->les_fused)
+    CUDA_TRY(ops->step_les(p, st));
+  else if (L->tiled)
     CUDA_TRY(ops->step_tiled(p, L->tile_blocks, st));
   else if (L->pair)
     CUDA_TRY(ops->step_pair(p, st));
@@ -1061,7 +1067,7 @@ int aero_set_inflow(AeroLattice *L, const double *fields, int64_t first, int64_t
 int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
   if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
   if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
-  if (kernel < 0 || kernel > kStepQuad) return fail(AERO_ERR_INVALID, "kernel must be 0..%d", kStepQuad);
+  if (kernel < 0 || kernel > kStepLes) return fail(AERO_ERR_INVALID, "kernel must be 0..%d", kStepLes);
   CUDA_TRY(cudaSetDevice(L->device));
   if (kernel == kStepPair) {
     if (!pair_capable(L, 2))
@@ -1079,17 +1085,35 @@ int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
     if (((int64_t)L->prm.ny * L->prm.nz + kQuadRows - 1) / kQuadRows > 65535)
       return fail(AERO_ERR_UNSUPPORTED, "the four-cell kernel takes at most 65535 * 16 rows (ny * nz)");
   }
+  int les_chunk = 0;
+  if (kernel == kStepLes) {
+    if (!(L->prm.dims == 3 && L->prm.collision != AERO_MRT && les_active(L)))
+      return fail(AERO_ERR_UNSUPPORTED, "the fused LES kernel covers D3Q19 BGK / TRT lattices with LES");
+    const cudaError_t e =
+        is_f64(L) ? get_ops<double>(L)->les_setup() : get_ops<float>(L)->les_setup();
+    if (e != cudaSuccess) return fail(AERO_ERR_CUDA, "fused LES kernel set-up: %s", cudaGetErrorString(e));
+    // z chunks so that the grid holds about six blocks per SM; at least 8
+    // planes a chunk, since each chunk evaluates two planes beyond it
+    int sms = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, L->device));
+    const int64_t tiles = (int64_t)((L->prm.nx + kLesTileX - 1) / kLesTileX) * ((L->prm.ny + kLesRows - 1) / kLesRows);
+    const int64_t chunks = std::max<int64_t>(1, std::min<int64_t>(L->prm.nz, (6LL * sms + tiles - 1) / tiles));
+    les_chunk = (int)((L->prm.nz + chunks - 1) / chunks);
+    les_chunk = std::max(les_chunk, std::min(8, L->prm.nz));
+  }
   if (kernel == kStepShapes) {
     const int rc = is_f64(L) ? plan_tiles<double>(L, true) : plan_tiles<float>(L, true);
     if (rc != AERO_OK) return rc;
     if (!L->tiled) return fail(AERO_ERR_UNSUPPORTED, "rows of this lattice do not fit the row-tiled kernel");
-    L->pair = L->quad = false;
+    L->pair = L->quad = L->les_fused = false;
   } else {
     L->tiled = false;
     L->tile_blocks = L->tile_rows = L->tiles_per_plane = L->ntiles = 0;
     L->pair = kernel == kStepPair;
     L->quad = kernel == kStepQuad;
-    L->step_shape = (L->pair || L->quad) ? 0 : kernel;
+    L->les_fused = kernel == kStepLes;
+    L->les_chunk = les_chunk;
+    L->step_shape = (L->pair || L->quad || L->les_fused) ? 0 : kernel;
   }
   // captured step sequences launch the previous kernel
   for (auto &e : L->pair_exec)
@@ -1102,7 +1126,8 @@ int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
 
 int aero_get_step_kernel(const AeroLattice *L, int32_t *kernel) {
   if (!L || !kernel) return fail(AERO_ERR_INVALID, "NULL argument");
-  *kernel = L->tiled ? kStepShapes : (L->pair ? kStepPair : (L->quad ? kStepQuad : L->step_shape));
+  *kernel = L->tiled ? kStepShapes
+                    : (L->pair ? kStepPair : (L->quad ? kStepQuad : (L->les_fused ? kStepLes : L->step_shape)));
   return AERO_OK;
 }
 

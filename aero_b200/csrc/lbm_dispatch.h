@@ -56,6 +56,12 @@ struct Ops {
   // regular step, four cells per thread (k_step_quad; D3Q19, 16-bit
   // storage); cudaErrorNotSupported for other classes
   cudaError_t (*step_quad)(const StepParams<Real> &, cudaStream_t);
+  // regular step of a D3Q19 BGK / TRT + LES lattice with the LES rate from a
+  // shared-memory velocity stencil (k_step_les); cudaErrorNotSupported for
+  // other classes.  les_setup raises the kernel's shared-memory limit on the
+  // current device.
+  cudaError_t (*step_les)(const StepParams<Real> &, cudaStream_t);
+  cudaError_t (*les_setup)();
   int store_bytes;
 };
 
@@ -74,6 +80,9 @@ constexpr int kStepShapeXY[kStepShapes][2] = {{128, 1}, {256, 1}, {32, 4}};
 // per-thread kernel for 16-bit storage.
 constexpr int kStepPair = kStepShapes + 1;
 constexpr int kStepQuad = kStepShapes + 2;
+// kStepLes = the D3Q19 BGK / TRT step with the LES velocity stencil in
+// shared memory (no separate moments pass).
+constexpr int kStepLes = kStepShapes + 3;
 
 inline dim3 step_grid(int shape, int nx, int ny, int nz) {
   const int bx = kStepShapeXY[shape][0], by = kStepShapeXY[shape][1];

@@ -7,6 +7,7 @@
 #include "lbm_kernels.cuh"
 #include "lbm_pair.cuh"
 #include "lbm_quad.cuh"
+#include "lbm_les.cuh"
 
 namespace aero {
 namespace inst {
@@ -156,10 +157,31 @@ struct Launch {
       return cudaErrorNotSupported;
     }
   }
+  static constexpr bool kLesCapable = L::DIMS == 3 && COLL != COLL_MRT;
+  static cudaError_t step_les(const StepParams<Real> &p, cudaStream_t st) {
+    if constexpr (kLesCapable) {
+      const dim3 grid((unsigned)((p.nx + kLesTileX - 1) / kLesTileX), (unsigned)((p.ny + kLesRows - 1) / kLesRows),
+                      (unsigned)((p.nz + p.les_chunk - 1) / p.les_chunk));
+      k_step_les<L, S, COLL><<<grid, kLesThreads, les_smem_bytes<Real>(), st>>>(p);
+      return cudaGetLastError();
+    } else {
+      (void)p;
+      (void)st;
+      return cudaErrorNotSupported;
+    }
+  }
+  static cudaError_t les_setup() {
+    if constexpr (kLesCapable) {
+      return cudaFuncSetAttribute(k_step_les<L, S, COLL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)les_smem_bytes<Real>());
+    } else {
+      return cudaErrorNotSupported;
+    }
+  }
   static constexpr Ops<Real> table = {&step,       &step_shaped, &moments,      &finalize,   &state_out,
                                       &load_state, &macro_out,   &step_tiled,   &tiled_setup, &step_batch,
                                       &moments_batch, &finalize_batch, &recycle_mean, &step_pair,
-                                      &step_batch_pair, &field_stats, &init_eq, &step_quad, (int)sizeof(S)};
+                                      &step_batch_pair, &field_stats, &init_eq, &step_quad, &step_les, &les_setup, (int)sizeof(S)};
 };
 
 template <class S>

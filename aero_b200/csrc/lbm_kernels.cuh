@@ -525,80 +525,95 @@ __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int
 }
 
 // --------------------------------------------------------------------------
-// LES relaxation rate from the velocity side buffer (les.py:24-78,
-// :177-266, :273-344).  Edge planes and solid cells keep the base rate.
+// LES relaxation rate (les.py:24-78, :177-266, :273-344).
 // --------------------------------------------------------------------------
+// The eddy-viscosity model on the velocity gradient g[a][b] = d u_a / d x_b
+// (central differences, halved), then omega = 1 / (3 (nu0 + nu_t) + 1/2).
 template <class L, class Real>
-__device__ __forceinline__ Real les_omega(const StepParams<Real> &p, int x, int y, int z, uint32_t c, bool solid) {
-  Real nu_t = Real(0);
-  bool interior = x >= 1 && x <= p.nx - 2 && y >= 1 && y <= p.ny - 2;
-  if constexpr (L::DIMS == 3) interior = interior && z >= 1 && z <= p.nz - 2;
-  if (interior && !solid) {
-    const Real *UX = p.U, *UY = p.U + p.cs, *UZ = p.U + 2 * p.cs;
-    const uint32_t sx = 1, sy = p.nx;
-    Real g[3][3];
-    g[0][0] = Real(0.5) * (UX[c + sx] - UX[c - sx]);
-    g[0][1] = Real(0.5) * (UX[c + sy] - UX[c - sy]);
-    g[1][0] = Real(0.5) * (UY[c + sx] - UY[c - sx]);
-    g[1][1] = Real(0.5) * (UY[c + sy] - UY[c - sy]);
-    g[0][2] = g[1][2] = g[2][0] = g[2][1] = g[2][2] = Real(0);
-    if constexpr (L::DIMS == 3) {
-      const uint32_t sz = (uint32_t)p.nx * (uint32_t)p.ny;
-      g[0][2] = Real(0.5) * (UX[c + sz] - UX[c - sz]);
-      g[1][2] = Real(0.5) * (UY[c + sz] - UY[c - sz]);
-      g[2][0] = Real(0.5) * (UZ[c + sx] - UZ[c - sx]);
-      g[2][1] = Real(0.5) * (UZ[c + sy] - UZ[c - sy]);
-      g[2][2] = Real(0.5) * (UZ[c + sz] - UZ[c - sz]);
-    }
-    Real cs2 = p.les_cs2;
-    if (p.feat & FEAT_LES_CS_FIELD) {
-      const Real cc = p.cs_cell[c];
-      cs2 = cc * cc;
-    }
-    constexpr int D = L::DIMS;
-    if (p.feat & FEAT_LES_WALE) {
-      Real s_sq = 0, sd_sq = 0, gsq[3][3], tr = 0;
+__device__ __forceinline__ Real les_rate_from_gradient(const StepParams<Real> &p, const Real (&g)[3][3],
+                                                       uint32_t c) {
+  Real nu_t;
+  Real cs2 = p.les_cs2;
+  if (p.feat & FEAT_LES_CS_FIELD) {
+    const Real cc = p.cs_cell[c];
+    cs2 = cc * cc;
+  }
+  constexpr int D = L::DIMS;
+  if (p.feat & FEAT_LES_WALE) {
+    Real s_sq = 0, sd_sq = 0, gsq[3][3], tr = 0;
 #pragma unroll
-      for (int a = 0; a < D; a++)
+    for (int a = 0; a < D; a++)
 #pragma unroll
-        for (int b = 0; b < D; b++) {
-          const Real sab = Real(0.5) * (g[a][b] + g[b][a]);
-          s_sq += sab * sab;
-          Real acc = 0;
+      for (int b = 0; b < D; b++) {
+        const Real sab = Real(0.5) * (g[a][b] + g[b][a]);
+        s_sq += sab * sab;
+        Real acc = 0;
 #pragma unroll
-          for (int k = 0; k < D; k++) acc += g[a][k] * g[k][b];
-          gsq[a][b] = acc;
-        }
+        for (int k = 0; k < D; k++) acc += g[a][k] * g[k][b];
+        gsq[a][b] = acc;
+      }
 #pragma unroll
-      for (int a = 0; a < D; a++) tr += gsq[a][a];
-      tr = tr / Real(D);
+    for (int a = 0; a < D; a++) tr += gsq[a][a];
+    tr = tr / Real(D);
 #pragma unroll
-      for (int a = 0; a < D; a++)
+    for (int a = 0; a < D; a++)
 #pragma unroll
-        for (int b = 0; b < D; b++) {
-          const Real sd = Real(0.5) * (gsq[a][b] + gsq[b][a]) - (a == b ? tr : Real(0));
-          sd_sq += sd * sd;
-        }
-      // pow(sd, 1.5) / (pow(s, 2.5) + pow(sd, 1.25) + 1e-30) via square roots
-      const Real r_sd = sqrt_(sd_sq), r_s = sqrt_(s_sq);
-      const Real num = sd_sq * r_sd;
-      const Real den = s_sq * s_sq * r_s + sd_sq * sqrt_(r_sd) + Real(1e-30);
-      nu_t = cs2 * num / den;
-    } else {
-      const Real s11 = g[0][0], s22 = g[1][1], s33 = g[2][2];
-      const Real s12 = Real(0.5) * (g[0][1] + g[1][0]);
-      const Real s13 = Real(0.5) * (g[0][2] + g[2][0]);
-      const Real s23 = Real(0.5) * (g[1][2] + g[2][1]);
-      Real smag;
-      if constexpr (D == 2)
-        smag = sqrt_(Real(2) * (s11 * s11 + s22 * s22 + Real(2) * s12 * s12));
-      else
-        smag = sqrt_(Real(2) * (s11 * s11 + s22 * s22 + s33 * s33) +
-                      Real(4) * (s12 * s12 + s13 * s13 + s23 * s23));
-      nu_t = cs2 * smag;
-    }
+      for (int b = 0; b < D; b++) {
+        const Real sd = Real(0.5) * (gsq[a][b] + gsq[b][a]) - (a == b ? tr : Real(0));
+        sd_sq += sd * sd;
+      }
+    // pow(sd, 1.5) / (pow(s, 2.5) + pow(sd, 1.25) + 1e-30) via square roots
+    const Real r_sd = sqrt_(sd_sq), r_s = sqrt_(s_sq);
+    const Real num = sd_sq * r_sd;
+    const Real den = s_sq * s_sq * r_s + sd_sq * sqrt_(r_sd) + Real(1e-30);
+    nu_t = cs2 * num / den;
+  } else {
+    const Real s11 = g[0][0], s22 = g[1][1], s33 = g[2][2];
+    const Real s12 = Real(0.5) * (g[0][1] + g[1][0]);
+    const Real s13 = Real(0.5) * (g[0][2] + g[2][0]);
+    const Real s23 = Real(0.5) * (g[1][2] + g[2][1]);
+    Real smag;
+    if constexpr (D == 2)
+      smag = sqrt_(Real(2) * (s11 * s11 + s22 * s22 + Real(2) * s12 * s12));
+    else
+      smag = sqrt_(Real(2) * (s11 * s11 + s22 * s22 + s33 * s33) +
+                    Real(4) * (s12 * s12 + s13 * s13 + s23 * s23));
+    nu_t = cs2 * smag;
   }
   return Real(1) / (Real(3) * (p.base_nu + nu_t) + Real(0.5));
+}
+
+// Whether the LES rate applies at (x, y, z): interior cells (the edge planes
+// keep nu_t = 0, les.py:55-57, no periodic wrap) that are not solid.
+template <class L, class Real>
+__device__ __forceinline__ bool les_interior(const StepParams<Real> &p, int x, int y, int z) {
+  bool interior = x >= 1 && x <= p.nx - 2 && y >= 1 && y <= p.ny - 2;
+  if constexpr (L::DIMS == 3) interior = interior && z >= 1 && z <= p.nz - 2;
+  return interior;
+}
+
+// LES relaxation rate from the velocity side buffer (les.py:24-78,
+// :177-266, :273-344).  Edge planes and solid cells keep the base rate.
+template <class L, class Real>
+__device__ __forceinline__ Real les_omega(const StepParams<Real> &p, int x, int y, int z, uint32_t c, bool solid) {
+  if (!les_interior<L>(p, x, y, z) || solid) return Real(1) / (Real(3) * p.base_nu + Real(0.5));
+  const Real *UX = p.U, *UY = p.U + p.cs, *UZ = p.U + 2 * p.cs;
+  const uint32_t sx = 1, sy = p.nx;
+  Real g[3][3];
+  g[0][0] = Real(0.5) * (UX[c + sx] - UX[c - sx]);
+  g[0][1] = Real(0.5) * (UX[c + sy] - UX[c - sy]);
+  g[1][0] = Real(0.5) * (UY[c + sx] - UY[c - sx]);
+  g[1][1] = Real(0.5) * (UY[c + sy] - UY[c - sy]);
+  g[0][2] = g[1][2] = g[2][0] = g[2][1] = g[2][2] = Real(0);
+  if constexpr (L::DIMS == 3) {
+    const uint32_t sz = (uint32_t)p.nx * (uint32_t)p.ny;
+    g[0][2] = Real(0.5) * (UX[c + sz] - UX[c - sz]);
+    g[1][2] = Real(0.5) * (UY[c + sz] - UY[c - sz]);
+    g[2][0] = Real(0.5) * (UZ[c + sx] - UZ[c - sx]);
+    g[2][1] = Real(0.5) * (UZ[c + sy] - UZ[c - sy]);
+    g[2][2] = Real(0.5) * (UZ[c + sz] - UZ[c - sz]);
+  }
+  return les_rate_from_gradient<L>(p, g, c);
 }
 
 // --------------------------------------------------------------------------
@@ -941,19 +956,18 @@ __device__ __forceinline__ void guard_rho(const StepParams<Real> &p, Real rho, i
   guard_bad(p, !(rho > Real(0)) || !isfinite(rho), step_now);
 }
 
-// One regular step of cell (x, y, z): state of step n from P_n (gathered by
-// `gather`), link-cell forces, scalar step, collision, P_{n+1} stored.
-template <class L, class S, int COLL, class Gather>
-__device__ __forceinline__ void step_cell(const StepParams<typename StoreOps<S>::Real> &p, int x, int y, int z,
-                                          int64_t step_now, const Gather &gather) {
+// The part of a cell's step that follows its post-BC state d: link-cell
+// forces, scalar step, collision at rate om (per-cell rate when `les`),
+// divergence guard, P_{n+1} stored.
+template <class L, class S, int COLL>
+__device__ __forceinline__ void finish_cell(const StepParams<typename StoreOps<S>::Real> &p, int x, int y, int z,
+                                            uint32_t c, uint32_t fl, int64_t step_now,
+                                            typename StoreOps<S>::Real (&d)[L::Q],
+                                            const ScalarCtx<typename StoreOps<S>::Real> &sc,
+                                            typename StoreOps<S>::Real om, bool les) {
   using Real = typename StoreOps<S>::Real;
   using SO = StoreOps<S>;
-  const uint32_t c = cell_index(p, x, y, z);
-  const uint32_t fl = gather.flags(x);
   const bool solid = fl & FLAG_SOLID;
-  Real d[L::Q];
-  ScalarCtx<Real> sc;
-  full_state<L, S, Real>(p, x, y, z, step_now, d, p.prevn, &sc, gather);
   if ((p.feat & FEAT_OBSTACLE_BB) && (fl & FLAG_LINK)) {
     const int64_t slot = link_slot(p, x, y, z);
     if (slot >= 0) link_cell_forces<L, S, Real>(p, x, y, z, c, slot, d);
@@ -966,9 +980,6 @@ __device__ __forceinline__ void step_cell(const StepParams<typename StoreOps<S>:
       scalar_step<L, L>(p, x, y, z, c, solid, sc, Real(3));
     }
   }
-  Real om = p.omega;
-  const bool les = (COLL != COLL_MRT) && (p.feat & FEAT_LES);
-  if (les) om = les_omega<L>(p, x, y, z, c, solid);
   const Real rho = collide<L, Real, COLL>(p, d, solid, om, les);
   guard_rho(p, rho, step_now);
   S *Pn = static_cast<S *>(p.Pn);
@@ -976,6 +987,24 @@ __device__ __forceinline__ void step_cell(const StepParams<typename StoreOps<S>:
     constexpr int i = decltype(ic)::value;
     SO::template store<i, L>(Pn, elem(p, i, c), d[i]);
   });
+}
+
+// One regular step of cell (x, y, z): state of step n from P_n (gathered by
+// `gather`), link-cell forces, scalar step, collision, P_{n+1} stored.
+template <class L, class S, int COLL, class Gather>
+__device__ __forceinline__ void step_cell(const StepParams<typename StoreOps<S>::Real> &p, int x, int y, int z,
+                                          int64_t step_now, const Gather &gather) {
+  using Real = typename StoreOps<S>::Real;
+  const uint32_t c = cell_index(p, x, y, z);
+  const uint32_t fl = gather.flags(x);
+  const bool solid = fl & FLAG_SOLID;
+  Real d[L::Q];
+  ScalarCtx<Real> sc;
+  full_state<L, S, Real>(p, x, y, z, step_now, d, p.prevn, &sc, gather);
+  Real om = p.omega;
+  const bool les = (COLL != COLL_MRT) && (p.feat & FEAT_LES);
+  if (les) om = les_omega<L>(p, x, y, z, c, solid);
+  finish_cell<L, S, COLL>(p, x, y, z, c, fl, step_now, d, sc, om, les);
 }
 
 // One full step: state of step n from P_n, scalar step, collision -> P_{n+1}.

@@ -75,6 +75,7 @@ struct StepParams {
   // row tiles of the tiled step kernel: tile_rows y rows of one z plane
   int32_t tile_rows, tiles_per_plane, ntiles;
   int32_t batch_rows;   // rows per block in the batched cell kernels
+  int32_t les_chunk;    // planes per block of the fused LES step (k_step_les)
   uint32_t tile_extra_tx;  // bytes announced on a tile stage beyond its copies (0; > 0 only to test
                            // that the bounded stage waits give up)
 

@@ -202,9 +202,9 @@ class Engine:
 
     def les_fused(self) -> bool:
         """Whether the step kernel computes the LES rate from a shared-memory
-        velocity stencil of its own (True) or reads the velocity side output
-        of a separate moments pass (False)."""
-        return False
+        velocity stencil of its own (step kernel 6) rather than reading the
+        velocity side output of a separate moments pass."""
+        return self.get_step_kernel() == 6
 
     def step_plan(self) -> dict:
         """Step kernel in use: {"tiled": bool, "tile_rows": r, "blocks": b}."""

@@ -182,9 +182,11 @@ AERO_API int aero_step_plan(const AeroLattice *lat, int32_t *tiled, int32_t *til
  * BGK/TRT/MRT, FP32/FP16/BF16 storage, even nx, no body force or scalar
  * lattice; else AERO_ERR_UNSUPPORTED); 5 = four cells per thread with one
  * 8-byte load per direction (D3Q19 BGK/TRT/MRT, FP16/BF16 storage, nx a
- * multiple of 4, no body force or scalar lattice; else AERO_ERR_UNSUPPORTED).
- * Results are the same for every choice up to FP rounding of the compiled
- * variant.  Takes effect at the next aero_step. */
+ * multiple of 4, no body force or scalar lattice; else AERO_ERR_UNSUPPORTED);
+ * 6 = the D3Q19 BGK/TRT step with the LES velocity stencil staged in shared
+ * memory, no separate moments pass (lattices with LES; else
+ * AERO_ERR_UNSUPPORTED).  Results are the same for every choice up to FP
+ * rounding of the compiled variant.  Takes effect at the next aero_step. */
 AERO_API int aero_set_step_kernel(AeroLattice *lat, int32_t kernel);
 AERO_API int aero_get_step_kernel(const AeroLattice *lat, int32_t *kernel);
 
