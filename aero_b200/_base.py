@@ -544,11 +544,13 @@ class LatticeSolverBase:
         the population buffers (aero_get_macroscopic) and copied into the
         arrays run() prepared, or fresh ones."""
         import torch
+        t0 = time.perf_counter()
         dev = self._engine.macroscopic_device()
         buf = getattr(self, "_field_host", None)
         self._field_host = None
         host = buf.get() if buf is not None and buf.shape == tuple(dev.shape) else np.empty(tuple(dev.shape))
         torch.from_numpy(host).copy_(dev)
+        self._last_readback_s = time.perf_counter() - t0
         return tuple(host[k] for k in range(host.shape[0]))
 
 

@@ -1082,8 +1082,9 @@ int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
       return fail(AERO_ERR_UNSUPPORTED,
                   "the four-cell kernel covers D3Q19 with 16-bit storage, nx a multiple of 4 (>= 12 with an open "
                   "inlet), no body force or scalar lattice");
-    if (((int64_t)L->prm.ny * L->prm.nz + kQuadRows - 1) / kQuadRows > 65535)
-      return fail(AERO_ERR_UNSUPPORTED, "the four-cell kernel takes at most 65535 * 16 rows (ny * nz)");
+    if (((int64_t)L->prm.ny * L->prm.nz + kQuadRows - 1) / kQuadRows * ((L->prm.nx / 4 + 127) / 128 * 16 + 1) >=
+        ((int64_t)1 << 31))
+      return fail(AERO_ERR_UNSUPPORTED, "the four-cell kernel's grid exceeds 2^31 blocks");
   }
   int les_chunk = 0;
   if (kernel == kStepLes) {

@@ -12,10 +12,13 @@
 // through a warp shuffle (the first / last lane of a warp, or of a row,
 // loads it itself), and two funnel shifts realign the four values.  Every
 // load is issued before any arithmetic, so a thread has 152 bytes in flight
-// where the pair kernel has 76.  The quad then runs as two pairs through the
-// pair arithmetic of lbm_pair.cuh (sponge, MRT in the adapted basis or BGK /
-// TRT with each cell's LES rate, all on packed FP32 instructions), and each
-// pair's result is stored as one 4-byte half2 / bfloat162 per direction.
+// where the pair kernel has 76.  The realigned words are parked in shared
+// memory (each thread reads back only its own), so the two pair updates that
+// follow do not hold the raw data in registers: the quad runs as two pairs
+// through the pair arithmetic of lbm_pair.cuh (sponge, MRT in the adapted
+// basis or BGK / TRT with each cell's LES rate, all on packed FP32
+// instructions), and each pair's result is stored as one 4-byte half2 /
+// bfloat162 per direction.
 //
 // Work split: in lattices with an open inlet and outlet the columns 0 .. 3
 // and nx-4 .. nx-1 (inlet, outlet and the column the outlet copies) run the
@@ -75,15 +78,20 @@ __device__ __forceinline__ uint2 ld_quad(const void *p) {
 #endif
 }
 
-constexpr int kQuadBlock = 128;  // threads per block: 512 cells along x
-constexpr int kQuadRows = 16;    // rows per group; the group's edge block holds their 8 edge cells each
+constexpr int kQuadBlock = 128;  // threads per block
+constexpr int kQuadRows = 16;    // rows per group; a group's edge block holds their 8 edge cells each
 #ifndef AERO_QUAD_MINB
 #define AERO_QUAD_MINB 6
 #endif
 constexpr int kQuadMinBlocks = AERO_QUAD_MINB;
 
+// Work split.  A row's quads take TP threads (its quad count rounded up to
+// whole warps, so a warp never spans two rows and the shuffles stay within a
+// row); a block holds RB = 128 / TP rows when TP <= 128, else a row takes
+// bpr blocks.  Rows come in groups of kQuadRows: the group's quad blocks,
+// then (open lattices) its edge block.  One-dimensional grid.
 struct QuadSplit {
-  int x0, nquads, row_blocks, rows, groups;
+  int x0, nquads, TP, RB, bpr, rows, groups, gblocks;
   bool edges;  // open lattices: columns 0..3 and nx-4..nx-1 run per cell in edge blocks
 };
 
@@ -93,34 +101,38 @@ __host__ __device__ __forceinline__ QuadSplit quad_split(const StepParams<Real> 
   q.edges = (p.feat & (FEAT_OPEN | FEAT_RECYCLE)) != 0;  // inlet / outlet / recycling columns
   q.x0 = q.edges ? 4 : 0;
   q.nquads = q.edges ? (p.nx - 8) / 4 : p.nx / 4;
-  q.row_blocks = (q.nquads + kQuadBlock - 1) / kQuadBlock;
+  q.TP = (q.nquads + 31) / 32 * 32;
+  q.RB = q.TP <= kQuadBlock ? kQuadBlock / q.TP : 1;  // 4, 2 or 1: divides kQuadRows
+  q.bpr = q.TP <= kQuadBlock ? 1 : (q.TP + kQuadBlock - 1) / kQuadBlock;
   q.rows = p.ny * p.nz;
   q.groups = (q.rows + kQuadRows - 1) / kQuadRows;
+  q.gblocks = (kQuadRows / q.RB) * q.bpr + (q.edges ? 1 : 0);
   return q;
 }
 
 template <class Real>
 inline dim3 quad_grid(const StepParams<Real> &p) {
   const QuadSplit q = quad_split(p);
-  return dim3((unsigned)(q.row_blocks > 0 ? q.row_blocks : 1), (unsigned)(kQuadRows + (q.edges ? 1 : 0)),
-              (unsigned)q.groups);
+  return dim3((unsigned)((int64_t)q.groups * q.gblocks), 1, 1);
 }
 
-// The plain-quad step: per direction, the four source values assembled from
-// the lane's 8-byte load and a neighbour's, then the two pairs.
+// The plain-quad step: the two pairs of the quad, their 16-bit values read
+// back from the block's shared-memory parking area (sq: direction i, half h
+// at sq[(i * 2 + h) * kQuadBlock + tid]).
 template <class L, class S, int COLL>
 __device__ __forceinline__ void quad_step_plain(const StepParams<float> &p, int x, int y, int z, uint32_t c,
-                                                int64_t step_now, const uint2 (&raw)[L::Q]) {
+                                                int64_t step_now, const uint32_t *sq) {
   using QO = QuadOps<S>;
   S *Pn = static_cast<S *>(p.Pn);
   const bool les = (COLL != COLL_MRT) && (p.feat & FEAT_LES);
+  const int tid = threadIdx.x;
 #pragma unroll 1
   for (int h = 0; h < 2; h++) {
     const int xp = x + 2 * h;
     F2 d[L::Q];
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      d[i] = QO::template unpack<i, L>(h == 0 ? raw[i].x : raw[i].y);
+      d[i] = QO::template unpack<i, L>(sq[(i * 2 + h) * kQuadBlock + tid]);
     });
     pair_sponge<L>(p, xp, d);
     F2 rho;
@@ -143,27 +155,29 @@ __device__ __forceinline__ void quad_step_plain(const StepParams<float> &p, int 
 
 // One regular step of a D3Q19 lattice with 16-bit storage, four cells per
 // thread.  The host offers it for nx a multiple of 4 (>= 12 with an open
-// inlet), without body force or scalar lattice.  Grid: x = quad block of a
-// row, y = row of a group of kQuadRows rows (y = kQuadRows: the group's edge
-// block, x = 0 only), z = group.
+// inlet), without body force or scalar lattice.
 template <class L, class S, int COLL>
 __global__ void __launch_bounds__(kQuadBlock, kQuadMinBlocks) k_step_quad(const StepParams<float> p) {
   static_assert(L::DIMS == 3 && sizeof(S) == 2, "the quad kernel covers D3Q19 with 16-bit storage");
+  __shared__ uint32_t sq[L::Q * 2 * kQuadBlock];  // the realigned words of each thread's quad
   const QuadSplit qs = quad_split(p);
   const int64_t step_now = *p.step;
-  if (blockIdx.y == kQuadRows) {
-    // edge block: cell k (0..7) of row blockIdx.z * kQuadRows + threadIdx.x / 8
-    if (blockIdx.x != 0) return;
-    const int k = threadIdx.x & 7;
-    const int r = (int)(blockIdx.z * kQuadRows + (threadIdx.x >> 3));
+  const int g = (int)(blockIdx.x / (unsigned)qs.gblocks);
+  const int k = (int)(blockIdx.x - (unsigned)g * (unsigned)qs.gblocks);
+  if (qs.edges && k == qs.gblocks - 1) {
+    // edge block: cell e (0..7) of row g * kQuadRows + threadIdx.x / 8
+    const int e = threadIdx.x & 7;
+    const int r = g * kQuadRows + (int)(threadIdx.x >> 3);
     if (r >= qs.rows) return;
     const int y = r % p.ny, z = r / p.ny;
-    step_cell<L, S, COLL>(p, k < 4 ? k : p.nx - 8 + k, y, z, step_now, GlobalGather<L, S, float>{p, y, z});
+    step_cell<L, S, COLL>(p, e < 4 ? e : p.nx - 8 + e, y, z, step_now, GlobalGather<L, S, float>{p, y, z});
     return;
   }
-  const int r = (int)(blockIdx.z * kQuadRows + blockIdx.y);
-  if (r >= qs.rows) return;  // whole warps leave together (r is uniform in the block)
-  const int t = (int)(blockIdx.x * kQuadBlock + threadIdx.x);
+  const int slot = k / qs.bpr, part = k - slot * qs.bpr;  // RB-row slot of the group, block of the row
+  const int rl = qs.TP <= kQuadBlock ? (int)threadIdx.x / qs.TP : 0;
+  const int t = qs.TP <= kQuadBlock ? (int)threadIdx.x - rl * qs.TP : part * kQuadBlock + (int)threadIdx.x;
+  const int r = g * kQuadRows + slot * qs.RB + rl;
+  if (rl >= qs.RB || r >= qs.rows) return;  // whole warps (TP is a multiple of 32)
   const bool active = t < qs.nquads;
   // inactive lanes at the end of a row take part in the shuffles with the
   // row's last quad as their (unused) data
@@ -200,36 +214,39 @@ __global__ void __launch_bounds__(kQuadBlock, kQuadMinBlocks) k_step_quad(const 
       if (own_right) side[i] = ld_pop32(P + elem(p, i, row + xr));
     }
   });
+  // realign the shifted directions and park every word in shared memory
+  const int tid = threadIdx.x;
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     constexpr int ex = Dir<L, i>::x;
+    uint32_t lo = raw[i].x, hi = raw[i].y;
     if constexpr (ex > 0) {
       // cells x-1 .. x+2: the high half of the word left of x, then x .. x+2
       const uint32_t nb = __shfl_up_sync(0xffffffffu, raw[i].y, 1);
       const uint32_t left = own_left ? side[i] : nb;
-      const uint32_t lo = __funnelshift_r(left, raw[i].x, 16);
-      const uint32_t hi = __funnelshift_r(raw[i].x, raw[i].y, 16);
-      raw[i] = make_uint2(lo, hi);
+      lo = __funnelshift_r(left, raw[i].x, 16);
+      hi = __funnelshift_r(raw[i].x, raw[i].y, 16);
     } else if constexpr (ex < 0) {
       // cells x+1 .. x+4: x+1 .. x+3, then the low half of the word right of x+3
       const uint32_t nb = __shfl_down_sync(0xffffffffu, raw[i].x, 1);
       const uint32_t right = own_right ? side[i] : nb;
-      const uint32_t lo = __funnelshift_r(raw[i].x, raw[i].y, 16);
-      const uint32_t hi = __funnelshift_r(raw[i].y, right, 16);
-      raw[i] = make_uint2(lo, hi);
+      lo = __funnelshift_r(raw[i].x, raw[i].y, 16);
+      hi = __funnelshift_r(raw[i].y, right, 16);
     }
+    sq[(i * 2 + 0) * kQuadBlock + tid] = lo;
+    sq[(i * 2 + 1) * kQuadBlock + tid] = hi;
   });
   if (!active) return;
   const uint32_t c = cell_index(p, x, y, z);
   bool plain = !(p.wall != WALL_NONE && (y == 0 || y == p.ny - 1));
   if (plain) plain = *reinterpret_cast<const uint32_t *>(p.flags + c) == 0u;  // the four flag bytes, c % 4 == 0
   if (plain) {
-    quad_step_plain<L, S, COLL>(p, x, y, z, c, step_now, raw);
+    quad_step_plain<L, S, COLL>(p, x, y, z, c, step_now, sq);
     return;
   }
   const GlobalGather<L, S, float> gather{p, y, z};
 #pragma unroll 1
-  for (int k = 0; k < 4; k++) step_cell<L, S, COLL>(p, x + k, y, z, step_now, gather);
+  for (int e = 0; e < 4; e++) step_cell<L, S, COLL>(p, x + e, y, z, step_now, gather);
 }
 
 }  // namespace aero

@@ -705,17 +705,21 @@ def _measure_e2e(s, w, args, dev, fields, world, dist):
     s.step_count = 0
     s._init_histories()
     s.set_equilibrium_state(ux=host[0], uy=host[1], T=host[2])
+    t1 = time.perf_counter()
     # one stability check at the end would raise on a diverged state; the
     # throughput measurement does not depend on it, so none is requested
     r = s.run(args.steps, check_every=args.steps + 1, verbose=False)
     torch.cuda.synchronize(dev)
-    dt = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    t2 = time.perf_counter()
+    dt = max_over_ranks(t2 - t0, dist, dev)
     h2d = sum(a.numel() * 8 for a in host if a is not None)
     d2h = (args.steps * 12 * 8 + (w["nz"] if w["dims"] == 3 else w["ny"]) * 3 * 8
            + (1 + w["dims"]) * ncells * 8 + (ncells * 8 if s.thermal else 0))
     return {"value": whole_job_mlups(ncells, world, args.steps, dt), "unit": "MLUPS",
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
             "call": f"{type(s).__name__}.set_equilibrium_state(fields from pinned host memory) + run(K)",
+            "phases_s": {"initial_state": t1 - t0, "run_with_readback": t2 - t1,
+                         "readback": getattr(s, "_last_readback_s", None)},
             "Cd_mean": r["Cd_mean"]}
 
 
