@@ -31,16 +31,15 @@ PRECISIONS = tuple(_lib.STORE)
 _PRISTINE_LIMIT = 1 << 28  # elements; above this a handed-out array is always re-uploaded
 
 
+LAYOUTS = {"ab": 0, "aa": 1}
+
+
 def _check_layout(layout: str) -> None:
-    """Population layout: "ab" (two buffers, the engine's) is the only one
-    built.  The in-place "aa" pattern is not: several boundary conditions of
-    the fused step read other cells' values of the same step (the outlet and
-    recycling planes, Bouzidi neighbours, link-cell forces), which an in-place
-    update would overwrite."""
-    if layout == "aa":
-        raise NotImplementedError("layout='aa' (in-place AA pattern) is not part of the b200 engine")
-    if layout != "ab":
-        raise ValueError(f"Unknown layout '{layout}'. Choose 'ab'.")
+    """Population layout: "ab" (two buffers; every step kernel) or "aa" (one
+    buffer updated in place, the AA pattern: half the population memory; the
+    per-cell step kernel only; not in batches)."""
+    if layout not in LAYOUTS:
+        raise ValueError(f"Unknown layout '{layout}'. Choose 'ab' or 'aa'.")
 
 
 def _open_checkpoint(path: str):
@@ -65,7 +64,8 @@ class LatticeSolverBase:
                bouzidi, van_driest, van_driest_A, body_force, wall_velocity_top,
                wall_velocity_bottom, synthetic_inflow, synthetic_inflow_intensity,
                synthetic_inflow_seed, thermal, T_hot, T_cold, alpha_T, buoyancy, g_gravity, beta,
-               T_ref, precision, scalar_lattice, device, hist_capacity, rho_in=1.0, rho_out=1.0, sem=None):
+               T_ref, precision, scalar_lattice, device, hist_capacity, rho_in=1.0, rho_out=1.0, sem=None,
+               layout="ab"):
         if backend not in BACKENDS:
             raise ValueError(f"Unknown backend '{backend}'. Choose 'b200' or 'auto'.")
         if collision not in ("bgk", "mrt", "trt"):
@@ -187,6 +187,8 @@ class LatticeSolverBase:
             P.inflow_field = 1
             P.inflow_ring = 64
         P.recycling = 1 if (self.dims == 3 and streamwise_bc == "recycling") else 0
+        P.layout = LAYOUTS[layout]
+        self.layout = layout
         self._params = P
         self._engine_phi = phi if (self.van_driest and phi is not None) else None
         self._engine = Engine(P, self.solid, self.surface_links, self.q_vals, self._engine_phi, device)
@@ -406,7 +408,7 @@ class LatticeSolverBase:
         np.savez_compressed(path, **kwargs)
 
     def _b200_options(self) -> dict:
-        return {"precision": self.precision, "scalar_lattice": self.scalar_lattice}
+        return {"precision": self.precision, "scalar_lattice": self.scalar_lattice, "layout": self.layout}
 
     def load_checkpoint(self, path: str) -> None:
         """Restores f, the outlet state, the scalar, the histories and the

@@ -12,7 +12,7 @@ import pathlib
 
 from . import _build
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 FORCE_VALUES = 12
 FIELD_STATS = 10
 
@@ -43,7 +43,7 @@ class AeroParams(ctypes.Structure):
         ("body_force", _D * 3)] + [
         (n, _D) for n in ("alpha_T", "T_hot", "T_cold", "g_gravity", "beta", "T_ref")] + [
         ("center", _D * 3)] + [
-        (n, _I32) for n in ("recycling", "inflow_field", "inflow_ring")]
+        (n, _I32) for n in ("recycling", "inflow_field", "inflow_ring", "layout")]
 
 
 SIGNATURES = {

@@ -51,7 +51,7 @@ uint64_t align_up(uint64_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
 struct Layout {
   uint64_t P[2], flags, lbits, loff, lc_mask, lc_q, lc_cell, lc_contrib, fin_partial, prof_off, force_const, prof_const,
-      prev[2], g[2], U, cs_cell, inflow, recycle, hist, prof_out, counters, stats, total;
+      prev[2], g[2], U, cs_cell, inflow, recycle, hist, prof_out, counters, stats, stage_link, stage_nb, stage_out, total;
 };
 
 struct WTab {
@@ -145,7 +145,14 @@ struct AeroLattice {
   bool pair = false;
   bool quad = false;
   bool les_fused = false;  // k_step_les: LES velocity stencil in shared memory, no moments pass
+  // AA layout: one population buffer updated in place.  Between aero_step
+  // calls it holds the post-boundary state (aa_holds_state) in layout cur;
+  // a call first collides it in place, then runs its steps, the last of
+  // which stores its state instead of colliding it.
+  bool aa = false;
+  bool aa_holds_state = false;
   int les_chunk = 0;       // planes per block of k_step_les
+  int prefetch_rows = 0;   // AERO_B200_PREFETCH_ROWS at bind: L2 prefetch distance of the step kernels
   int tile_blocks = 0, tile_rows = 0, tiles_per_plane = 0, ntiles = 0;
   uint32_t tile_extra_tx = 0;  // AERO_B200_TEST_STALL_TILES=1 at bind: stages never complete
   // optional per-kernel event timing (eager launches only)
@@ -157,6 +164,15 @@ struct AeroLattice {
 namespace {
 
 bool is_f64(const AeroLattice *L) { return L->prm.storage == AERO_STORE_F64; }
+
+// Whether a step re-evaluates plane x = nx-2 at other cells (a convective or
+// zero-gradient outlet, or the recycling inlet): in the AA layout its pulled
+// populations are staged before each step.
+bool aa_stages_outlet(const AeroLattice *L) {
+  const bool open = L->feat & FEAT_OPEN;
+  return (open && (L->prm.outlet_bc == AERO_OUTLET_CONVECTIVE || L->prm.outlet_bc == AERO_OUTLET_ZEROGRADIENT)) ||
+         (L->feat & FEAT_RECYCLE);
+}
 
 // Lattices the two-cells-per-thread kernels take: D3Q19, 4- or 2-byte
 // storage, even nx (>= 6 in a batch, so that the four edge columns are
@@ -213,11 +229,18 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   p.tile_rows = L->tile_rows;
   p.batch_rows = L->ncells < kBatchSmallCells ? 1 : kBatchRows;
   p.les_chunk = L->les_chunk > 0 ? L->les_chunk : 1;
+  p.prefetch_rows = L->prefetch_rows;
   p.tile_extra_tx = L->tile_extra_tx;
   p.tiles_per_plane = L->tiles_per_plane;
   p.ntiles = L->ntiles;
-  p.P = ws + L->lay.P[cur];
-  p.Pn = ws + L->lay.P[nxt];
+  p.P = ws + L->lay.P[L->aa ? 0 : cur];
+  p.Pn = ws + L->lay.P[L->aa ? 0 : nxt];
+  p.aa = L->aa ? 1 : 0;
+  p.aa_layout = cur;
+  p.aa_store_state = 0;
+  p.stage_link = L->aa ? ws + L->lay.stage_link : nullptr;
+  p.stage_nb = L->aa ? ws + L->lay.stage_nb : nullptr;
+  p.stage_out = (L->aa && aa_stages_outlet(L)) ? ws + L->lay.stage_out : nullptr;
   p.flags = reinterpret_cast<const uint8_t *>(ws + L->lay.flags);
   p.lbits = reinterpret_cast<const uint32_t *>(ws + L->lay.lbits);
   p.loff = reinterpret_cast<const int32_t *>(ws + L->lay.loff);
@@ -326,9 +349,10 @@ int inflow_components(const AeroLattice *L) { return (L->feat & FEAT_INFLOW_SEM)
 // events bracket the fused step (moments pass + step kernel, which also
 // computes the link-cell force contributions) and the force finalisation.
 template <class Real>
-int launch_step(AeroLattice *L, int cur, cudaStream_t st, bool timed = false) {
+int launch_step(AeroLattice *L, int cur, cudaStream_t st, bool timed = false, bool store_state = false) {
   const Ops<Real> *ops = get_ops<Real>(L);
-  const StepParams<Real> p = make_params<Real>(L, cur);
+  StepParams<Real> p = make_params<Real>(L, cur);
+  p.aa_store_state = store_state ? 1 : 0;
   const dim3 grid = cell_grid(L);
   cudaEvent_t *e = nullptr;
   if (timed) {
@@ -341,26 +365,47 @@ int launch_step(AeroLattice *L, int cur, cudaStream_t st, bool timed = false) {
     e = &L->ev[3 * (size_t)L->timed_steps];
     CUDA_TRY(cudaEventRecord(e[0], st));
   }
-  if (L->feat & FEAT_RECYCLE) CUDA_TRY(ops->recycle_mean(p, st));
-  if (les_active(L) && !L->les_fused) CUDA_TRY(ops->moments(p, false, grid, st));
-  if (L->les_fused)
-    CUDA_TRY(ops->step_les(p, st));
-  else if (L->tiled)
-    CUDA_TRY(ops->step_tiled(p, L->tile_blocks, st));
-  else if (L->pair)
-    CUDA_TRY(ops->step_pair(p, st));
-  else if (L->quad)
-    CUDA_TRY(ops->step_quad(p, st));
-  else if (L->step_shape != 0)
-    CUDA_TRY(ops->step_shaped(p, L->step_shape, st));
-  else
-    CUDA_TRY(ops->step(p, false, grid, st));
+  if (L->aa) {
+    const int64_t n = (int64_t)L->lc_cell.size() + (aa_stages_outlet(L) ? L->prev_plane : 0);
+    if (n > 0) CUDA_TRY(ops->aa_stage(p, blocks_for(n, kStageBlock), st));
+    if (L->feat & FEAT_RECYCLE) CUDA_TRY(ops->aa_recycle_mean(p, st));
+    if (les_active(L)) CUDA_TRY(ops->aa_moments(p, grid, st));
+    CUDA_TRY(ops->aa_step(p, grid, st));
+  } else {
+    if (L->feat & FEAT_RECYCLE) CUDA_TRY(ops->recycle_mean(p, st));
+    if (les_active(L) && !L->les_fused) CUDA_TRY(ops->moments(p, false, grid, st));
+    if (L->les_fused)
+      CUDA_TRY(ops->step_les(p, st));
+    else if (L->tiled)
+      CUDA_TRY(ops->step_tiled(p, L->tile_blocks, st));
+    else if (L->pair)
+      CUDA_TRY(ops->step_pair(p, st));
+    else if (L->quad)
+      CUDA_TRY(ops->step_quad(p, st));
+    else if (L->step_shape != 0)
+      CUDA_TRY(ops->step_shaped(p, L->step_shape, st));
+    else
+      CUDA_TRY(ops->step(p, false, grid, st));
+  }
   if (timed) CUDA_TRY(cudaEventRecord(e[1], st));
   CUDA_TRY(ops->finalize(p, st));
   if (timed) {
     CUDA_TRY(cudaEventRecord(e[2], st));
     L->timed_steps++;
   }
+  return AERO_OK;
+}
+
+// AA layout: the in-place collision of the state the buffer holds (set by
+// the host or stored by the previous call's last step), before the steps.
+template <class Real>
+int aa_collide_state(AeroLattice *L, cudaStream_t st) {
+  const Ops<Real> *ops = get_ops<Real>(L);
+  const StepParams<Real> p = make_params<Real>(L, L->cur);
+  const dim3 grid = cell_grid(L);
+  if (les_active(L)) CUDA_TRY(ops->moments(p, true, grid, st));
+  CUDA_TRY(ops->step(p, true, grid, st));
+  L->aa_holds_state = false;
   return AERO_OK;
 }
 
@@ -385,8 +430,14 @@ int build_pair_graph(AeroLattice *L, int cur) {
 
 template <class Real>
 int do_steps(AeroLattice *L, int64_t n, cudaStream_t st) {
+  if (L->aa && n > 0 && L->aa_holds_state) {
+    const int rc = aa_collide_state<Real>(L, st);
+    if (rc != AERO_OK) return rc;
+  }
   while (n > 0) {
-    if (n >= 2 && L->use_graphs && !L->timing) {
+    // in the AA layout the call's last step stores its state (eager launch)
+    const int64_t full = L->aa ? n - 1 : n;
+    if (full >= 2 && L->use_graphs && !L->timing) {
       if (!L->pair_exec[L->cur]) {
         const int rc = build_pair_graph<Real>(L, L->cur);
         if (rc != AERO_OK) return rc;
@@ -395,7 +446,7 @@ int do_steps(AeroLattice *L, int64_t n, cudaStream_t st) {
       n -= 2;
       L->step_count += 2;
     } else {
-      const int rc = launch_step<Real>(L, L->cur, st, L->timing);
+      const int rc = launch_step<Real>(L, L->cur, st, L->timing, L->aa && n == 1);
       if (rc != AERO_OK) return rc;
       L->cur ^= 1;
       n -= 1;
@@ -403,6 +454,7 @@ int do_steps(AeroLattice *L, int64_t n, cudaStream_t st) {
     }
     L->old_is_state = false;
   }
+  if (L->aa) L->aa_holds_state = true;
   return AERO_OK;
 }
 
@@ -416,8 +468,10 @@ int do_set_state(AeroLattice *L, const double *f, const double *prev, const doub
   const int old = 1 - L->cur;
   const dim3 grid = cell_grid(L);
   StepParams<Real> p = make_params<Real>(L, L->cur);
-  // raw state into the old buffer, then collide it into the current one
-  CUDA_TRY(ops->load_state(p, f, L->ws + L->lay.P[old], grid, st));
+  // raw state into the old buffer, then collide it into the current one (A/B
+  // layout); in the AA layout the state goes into the single buffer in
+  // layout cur and is collided by the next aero_step
+  CUDA_TRY(ops->load_state(p, f, L->ws + L->lay.P[L->aa ? 0 : old], grid, st));
   if (prev) {
     const int64_t n = (int64_t)L->Q * L->prev_plane;
     k_prev_in<Real><<<blocks_for(n, 256), 256, 0, st>>>(reinterpret_cast<Real *>(L->ws + L->lay.prev[L->cur]),
@@ -444,11 +498,15 @@ int finish_set_state(AeroLattice *L, int64_t steps, cudaStream_t st) {
   int64_t *ctr = reinterpret_cast<int64_t *>(L->ws + L->lay.counters);
   k_set_i64<<<1, 1, 0, st>>>(ctr, steps);
   CUDA_TRY(cudaGetLastError());
-  StepParams<Real> q = make_params<Real>(L, L->cur);
-  q.P = L->ws + L->lay.P[old];
-  q.Pn = L->ws + L->lay.P[L->cur];
-  if (les_active(L)) CUDA_TRY(ops->moments(q, true, grid, st));
-  CUDA_TRY(ops->step(q, true, grid, st));
+  if (L->aa) {
+    L->aa_holds_state = true;
+  } else {
+    StepParams<Real> q = make_params<Real>(L, L->cur);
+    q.P = L->ws + L->lay.P[old];
+    q.Pn = L->ws + L->lay.P[L->cur];
+    if (les_active(L)) CUDA_TRY(ops->moments(q, true, grid, st));
+    CUDA_TRY(ops->step(q, true, grid, st));
+  }
   L->old_is_state = true;
   L->step_count = steps;
   L->read_upto = steps;
@@ -464,20 +522,29 @@ int do_set_equilibrium(AeroLattice *L, const EqFields &e, int64_t steps, cudaStr
   const StepParams<Real> p = make_params<Real>(L, L->cur);
   Real *prev = reinterpret_cast<Real *>(L->ws + L->lay.prev[L->cur]);
   Real *g = L->prm.thermal ? reinterpret_cast<Real *>(L->ws + L->lay.g[L->cur]) : nullptr;
-  CUDA_TRY(ops->init_eq(p, e, L->ws + L->lay.P[old], prev, g, cell_grid(L), st));
+  CUDA_TRY(ops->init_eq(p, e, L->ws + L->lay.P[L->aa ? 0 : old], prev, g, cell_grid(L), st));
   return finish_set_state<Real>(L, steps, st);
+}
+
+// Parameters and mode of the kernels that read the current state: with two
+// buffers the state of the last step is evaluated from the previous buffer
+// (or read as is after a set state); in the AA layout the buffer holds the
+// state itself between calls, in layout cur.
+template <class Real>
+StepParams<Real> reader_params(const AeroLattice *L, bool *raw) {
+  *raw = L->aa ? true : L->old_is_state;
+  return make_params<Real>(L, L->aa ? L->cur : 1 - L->cur);
 }
 
 template <class Real>
 int do_get_state(AeroLattice *L, double *f, double *prev, double *g, int z0, int nzs, cudaStream_t st) {
   const Ops<Real> *ops = get_ops<Real>(L);
-  const int old = 1 - L->cur;
   if (f) {
-    // the state of the last step is evaluated from the previous buffers
-    StepParams<Real> p = make_params<Real>(L, old);
+    bool raw = false;
+    StepParams<Real> p = reader_params<Real>(L, &raw);
     dim3 grid = cell_grid(L);
     grid.z = (unsigned)nzs;
-    CUDA_TRY(ops->state_out(p, f, -1, L->old_is_state, z0, grid, st));
+    CUDA_TRY(ops->state_out(p, f, -1, raw, z0, grid, st));
   }
   if (prev) {
     const int64_t n = (int64_t)L->Q * L->prev_plane;
@@ -552,6 +619,8 @@ int check_params(const AeroParams *a) {
     return fail(AERO_ERR_INVALID, "inflow_field is 0, 1 (synthetic inflow) or 2 (SEM, 3D)");
   if (a->inflow_ring < 0 || a->inflow_ring > 65536) return fail(AERO_ERR_INVALID, "inflow_ring must be in 0..65536");
   if (a->hist_capacity < 0) return fail(AERO_ERR_INVALID, "hist_capacity < 0");
+  if (a->layout != AERO_LAYOUT_AB && a->layout != AERO_LAYOUT_AA)
+    return fail(AERO_ERR_INVALID, "layout must be AERO_LAYOUT_AB or AERO_LAYOUT_AA");
   return AERO_OK;
 }
 
@@ -616,6 +685,7 @@ int aero_create(const AeroParams *params, AeroLattice **out) {
     if (a.scalar_reduced) f |= FEAT_SCALAR_REDUCED;
   }
   L->feat = f;
+  L->aa = a.layout == AERO_LAYOUT_AA;
   if (a.collision == AERO_MRT && !build_mrt(a.dims, a.omega, L->mrt, nullptr, nullptr)) {
     delete L;
     return fail(AERO_ERR_INVALID, "MRT operator is not block diagonal in the pair basis");
@@ -745,7 +815,7 @@ int aero_set_geometry(AeroLattice *L, const uint8_t *solid, const int32_t *links
     return at;
   };
   y.P[0] = take(sb * L->Q * L->cs);
-  y.P[1] = take(sb * L->Q * L->cs);
+  y.P[1] = take(L->aa ? 0 : sb * L->Q * L->cs);  // the AA layout has one buffer
   y.flags = take(L->cs + 32);  // slack for 16-byte-widened tile copies
   y.lbits = take(4 * L->nwords);
   y.loff = take(4 * L->nwords);
@@ -771,6 +841,10 @@ int aero_set_geometry(AeroLattice *L, const uint8_t *solid, const int32_t *links
   y.counters = take(64);
   // k_field_stats: per-block partials, the combined values, the ticket
   y.stats = take(8 * ((uint64_t)kStatsBlocks * kStatsValues + kStatsValues + 1));
+  // AA layout: the staged cross-cell reads of a step
+  y.stage_link = take(L->aa ? rb * L->Q * nlc : 0);
+  y.stage_nb = take((L->aa && (L->feat & FEAT_BOUZIDI)) ? rb * L->Q * nlc : 0);
+  y.stage_out = take((L->aa && aa_stages_outlet(L)) ? rb * L->Q * (uint64_t)L->prev_plane : 0);
   y.total = o;
   L->geometry = true;
   return AERO_OK;
@@ -832,6 +906,10 @@ int aero_bind_workspace(AeroLattice *L, void *dptr, uint64_t bytes, void *stream
   // Test of the bounded waits of the row-tiled kernel: every stage announces
   // 16 bytes more than its copies deliver, so no stage completes; the waits
   // give up after their limit, raise status bit 1 and the kernel returns.
+  // Row-ahead L2 prefetch distance of the per-cell and pair step kernels
+  // (rows in grid order; 0 or unset: off)
+  const char *pf = std::getenv("AERO_B200_PREFETCH_ROWS");
+  L->prefetch_rows = pf ? std::max(0, std::atoi(pf)) : 0;
   const char *stall = std::getenv("AERO_B200_TEST_STALL_TILES");
   L->tile_extra_tx = (stall && stall[0] == '1') ? 16u : 0u;
   L->bound = true;
@@ -891,12 +969,13 @@ int aero_get_macroscopic(AeroLattice *L, double *out, void *stream) {
   CUDA_TRY(cudaSetDevice(L->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const dim3 grid = cell_grid(L);
+  bool raw = false;
   if (is_f64(L)) {
-    const StepParams<double> p = make_params<double>(L, 1 - L->cur);
-    CUDA_TRY(get_ops<double>(L)->macro_out(p, out, -1, L->old_is_state, 0, grid, st));
+    const StepParams<double> p = reader_params<double>(L, &raw);
+    CUDA_TRY(get_ops<double>(L)->macro_out(p, out, -1, raw, 0, grid, st));
   } else {
-    const StepParams<float> p = make_params<float>(L, 1 - L->cur);
-    CUDA_TRY(get_ops<float>(L)->macro_out(p, out, -1, L->old_is_state, 0, grid, st));
+    const StepParams<float> p = reader_params<float>(L, &raw);
+    CUDA_TRY(get_ops<float>(L)->macro_out(p, out, -1, raw, 0, grid, st));
   }
   return AERO_OK;
 }
@@ -912,14 +991,15 @@ int aero_field_stats(AeroLattice *L, int32_t z0, int32_t nzs, double *out, void 
   uint32_t *ticket = reinterpret_cast<uint32_t *>(dout + kStatsValues);
   // the state of the last step comes from the previous buffers (as in
   // aero_get_macroscopic); the scalar of the last step is the current one
+  bool raw = false;
   if (is_f64(L)) {
-    const StepParams<double> p = make_params<double>(L, 1 - L->cur);
+    const StepParams<double> p = reader_params<double>(L, &raw);
     const double *g = L->prm.thermal ? reinterpret_cast<const double *>(L->ws + L->lay.g[L->cur]) : nullptr;
-    CUDA_TRY(get_ops<double>(L)->field_stats(p, g, z0, nzs, -1, L->old_is_state, partial, ticket, dout, st));
+    CUDA_TRY(get_ops<double>(L)->field_stats(p, g, z0, nzs, -1, raw, partial, ticket, dout, st));
   } else {
-    const StepParams<float> p = make_params<float>(L, 1 - L->cur);
+    const StepParams<float> p = reader_params<float>(L, &raw);
     const float *g = L->prm.thermal ? reinterpret_cast<const float *>(L->ws + L->lay.g[L->cur]) : nullptr;
-    CUDA_TRY(get_ops<float>(L)->field_stats(p, g, z0, nzs, -1, L->old_is_state, partial, ticket, dout, st));
+    CUDA_TRY(get_ops<float>(L)->field_stats(p, g, z0, nzs, -1, raw, partial, ticket, dout, st));
   }
   CUDA_TRY(cudaMemcpyAsync(out, dout, sizeof(double) * kStatsValues, cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
@@ -1068,6 +1148,8 @@ int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
   if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
   if (!L->bound) return fail(AERO_ERR_STATE, "workspace not bound");
   if (kernel < 0 || kernel > kStepLes) return fail(AERO_ERR_INVALID, "kernel must be 0..%d", kStepLes);
+  if (L->aa && kernel != 0)
+    return fail(AERO_ERR_UNSUPPORTED, "the AA layout runs the per-cell step kernel (0) only");
   CUDA_TRY(cudaSetDevice(L->device));
   if (kernel == kStepPair) {
     if (!pair_capable(L, 2))
@@ -1631,6 +1713,7 @@ int aero_batch_add(AeroBatch *B, AeroLattice *L, double cd_norm) {
   if (!(cd_norm > 0.0) || !std::isfinite(cd_norm)) return fail(AERO_ERR_INVALID, "cd_norm must be > 0");
   if (L->feat & (FEAT_INFLOW_FIELD | FEAT_RECYCLE))
     return fail(AERO_ERR_UNSUPPORTED, "lattices with synthetic inflow or a recycling inlet step only on their own");
+  if (L->aa) return fail(AERO_ERR_UNSUPPORTED, "lattices in the AA layout step only on their own");
   L->batch = B;
   L->cd_norm = cd_norm;
   B->members.push_back(L);

@@ -178,10 +178,30 @@ struct Launch {
       return cudaErrorNotSupported;
     }
   }
+  static cudaError_t aa_stage(const StepParams<Real> &p, unsigned blocks, cudaStream_t st) {
+    k_aa_stage<L, S><<<blocks, kStageBlock, 0, st>>>(p);
+    return cudaGetLastError();
+  }
+  static cudaError_t aa_recycle_mean(const StepParams<Real> &p, cudaStream_t st) {
+    if constexpr (L::DIMS == 3) {
+      k_recycle_mean<L, S, true><<<p.recycle_blocks, kRecycleBlock, 0, st>>>(p);
+      return cudaGetLastError();
+    }
+    return cudaErrorInvalidValue;  // recycling exists in 3D only
+  }
+  static cudaError_t aa_moments(const StepParams<Real> &p, dim3 grid, cudaStream_t st) {
+    k_moments<L, S, false, true><<<grid, kStepBlock, 0, st>>>(p);
+    return cudaGetLastError();
+  }
+  static cudaError_t aa_step(const StepParams<Real> &p, dim3 grid, cudaStream_t st) {
+    k_step<L, S, COLL, false, kStepBlock, 1, true><<<grid, kStepBlock, 0, st>>>(p);
+    return cudaGetLastError();
+  }
   static constexpr Ops<Real> table = {&step,       &step_shaped, &moments,      &finalize,   &state_out,
                                       &load_state, &macro_out,   &step_tiled,   &tiled_setup, &step_batch,
                                       &moments_batch, &finalize_batch, &recycle_mean, &step_pair,
-                                      &step_batch_pair, &field_stats, &init_eq, &step_quad, &step_les, &les_setup, (int)sizeof(S)};
+                                      &step_batch_pair, &field_stats, &init_eq, &step_quad, &step_les, &les_setup, &aa_stage,
+                                      &aa_recycle_mean, &aa_moments, &aa_step, (int)sizeof(S)};
 };
 
 template <class S>

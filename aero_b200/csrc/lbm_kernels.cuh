@@ -292,7 +292,164 @@ struct GlobalGather {
   __device__ __forceinline__ uint32_t flags(int x) const { return p.flags[cell_index(p, x, y, z)]; }
   // convective outlet state of the row, direction i
   __device__ __forceinline__ Real prev(int i) const { return p.prev[((int64_t)z * p.ny + y) * L::QP + i]; }
+  // pre-stream population I of cell c (link cell slot `slot`)
+  template <int I>
+  __device__ __forceinline__ Real pre(uint32_t c, int64_t slot) const {
+    (void)slot;
+    return StoreOps<S>::template load<I, L>(static_cast<const S *>(p.P), elem(p, I, c));
+  }
+  // pre-stream population I of cell (xn, yn, zn) (the clipped neighbour of a
+  // Bouzidi link with q >= 1/2)
+  template <int I>
+  __device__ __forceinline__ Real nbr(int xn, int yn, int zn, int64_t slot) const {
+    (void)slot;
+    return StoreOps<S>::template load<I, L>(static_cast<const S *>(p.P), elem(p, I, cell_index(p, xn, yn, zn)));
+  }
+  // stores the post-collision population I of cell x (index c) of the row
+  template <int I>
+  __device__ __forceinline__ void put(int x, uint32_t c, Real v) const {
+    (void)x;
+    StoreOps<S>::template store<I, L>(static_cast<S *>(p.Pn), elem(p, I, c), v);
+  }
+  static constexpr bool kAA = false;
 };
+
+// Element offset of the value V_I of cell (x, y, z) (index c) in the AA
+// layout `layout`: plane opp(I) at c (layout 0), or plane I at the periodic
+// neighbour x + e_I (layout 1).
+template <class L, int I, class Real>
+__device__ __forceinline__ uint32_t aa_own(const StepParams<Real> &p, int layout, int x, int y, int z, uint32_t c) {
+  constexpr int o = L::opp[I];
+  if (layout == 0) return elem(p, o, c);
+  constexpr int ex = Dir<L, I>::x, ey = Dir<L, I>::y, ez = Dir<L, I>::z;
+  const int xn = ex ? wrap_n(x + ex, p.nx) : x;
+  const int yn = ey ? wrap_n(y + ey, p.ny) : y;
+  const int zn = (L::DIMS == 3 && ez) ? wrap_n(z + ez, p.nz) : z;
+  return elem(p, I, cell_index(p, xn, yn, zn));
+}
+
+// Population access of a step in the AA layout (one buffer, p.P == p.Pn).
+// A step reading layout 0 gathers V_i(x - e_i) from plane opp(i) at the
+// source cell and writes its result V'_i(x) to plane i at x + e_i (layout
+// 1); a step reading layout 1 gathers from plane i at x itself and writes to
+// plane opp(i) at x (layout 0).  Either way a cell writes exactly the slots
+// it read, so the update is race-free in place.  The reads that cross cells
+// within a step -- the pre-stream values of link cells (bounce-back and
+// forces) and the pulled populations of plane nx-2 (which the outlet and
+// recycling cells re-evaluate) -- come from the staging area k_aa_stage
+// fills before the step.
+template <class L, class S, class Real>
+struct AAGather {
+  const StepParams<Real> &p;
+  int y, z;
+  __device__ __forceinline__ void operator()(int x, Real (&d)[L::Q]) const {
+    if (x == p.nx - 2 && p.stage_out) {
+      const Real *so = static_cast<const Real *>(p.stage_out) + ((int64_t)z * p.ny + y) * L::Q;
+      static_for<L::Q>([&](auto ic) { d[decltype(ic)::value] = so[decltype(ic)::value]; });
+      return;
+    }
+    raw(x, d);
+  }
+  // the pulled populations of cell x straight from the buffer
+  __device__ __forceinline__ void raw(int x, Real (&d)[L::Q]) const {
+    using SO = StoreOps<S>;
+    const S *A = static_cast<const S *>(p.P);
+    if (p.aa_layout == 1) {
+      const uint32_t c = cell_index(p, x, y, z);
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        d[i] = SO::template load<i, L>(A, elem(p, i, c));
+      });
+      return;
+    }
+    const uint32_t nx = p.nx, nxy = (uint32_t)p.nx * (uint32_t)p.ny;
+    const uint32_t xs_p = x == 0 ? nx - 1 : x - 1;
+    const uint32_t xs_m = x == p.nx - 1 ? 0 : x + 1;
+    const uint32_t ry_0 = (uint32_t)y * nx;
+    const uint32_t ry_p = (y == 0 ? p.ny - 1 : y - 1) * nx;
+    const uint32_t ry_m = (y == p.ny - 1 ? 0 : y + 1) * nx;
+    uint32_t pz_0 = 0, pz_p = 0, pz_m = 0;
+    if constexpr (L::DIMS == 3) {
+      pz_0 = (uint32_t)z * nxy;
+      pz_p = (z == 0 ? p.nz - 1 : z - 1) * nxy;
+      pz_m = (z == p.nz - 1 ? 0 : z + 1) * nxy;
+    }
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      constexpr int ex = Dir<L, i>::x, ey = Dir<L, i>::y, ez = Dir<L, i>::z;
+      const uint32_t src = (ex > 0 ? xs_p : (ex < 0 ? xs_m : (uint32_t)x)) +
+                           (ey > 0 ? ry_p : (ey < 0 ? ry_m : ry_0)) +
+                           (ez > 0 ? pz_p : (ez < 0 ? pz_m : pz_0));
+      constexpr int o = L::opp[i];
+      d[i] = SO::template load<i, L>(A, elem(p, o, src));
+    });
+  }
+  __device__ __forceinline__ uint32_t flags(int x) const { return p.flags[cell_index(p, x, y, z)]; }
+  __device__ __forceinline__ Real prev(int i) const { return p.prev[((int64_t)z * p.ny + y) * L::QP + i]; }
+  template <int I>
+  __device__ __forceinline__ Real pre(uint32_t c, int64_t slot) const {
+    (void)c;
+    return static_cast<const Real *>(p.stage_link)[slot * L::Q + I];
+  }
+  template <int I>
+  __device__ __forceinline__ Real nbr(int xn, int yn, int zn, int64_t slot) const {
+    (void)xn;
+    (void)yn;
+    (void)zn;
+    return static_cast<const Real *>(p.stage_nb)[slot * L::Q + I];
+  }
+  template <int I>
+  __device__ __forceinline__ void put(int x, uint32_t c, Real v) const {
+    // layout 0 read -> write layout 1 (plane I at x + e_I); 1 -> 0 (plane opp(I) at x)
+    StoreOps<S>::template store<I, L>(static_cast<S *>(p.Pn), aa_own<L, I>(p, 1 - p.aa_layout, x, y, z, c), v);
+  }
+  static constexpr bool kAA = true;
+};
+
+// Value V_I of cell (x, y, z) (index c) of a buffer that holds a state or
+// a post-collision set stored per cell: plane I at c with two buffers, its
+// AA slot in layout p.aa_layout in the AA layout.  Used where a kernel reads
+// or writes a cell's own values only (the collision of a set state, the
+// readers of the state, the initial state, the AA staging).
+template <class L, int I, class Real>
+__device__ __forceinline__ uint32_t own_elem(const StepParams<Real> &p, int x, int y, int z, uint32_t c) {
+  return p.aa ? aa_own<L, I>(p, p.aa_layout, x, y, z, c) : elem(p, I, c);
+}
+template <class L, class S, int I, class Real>
+__device__ __forceinline__ Real own_value(const StepParams<Real> &p, int x, int y, int z, uint32_t c) {
+  return StoreOps<S>::template load<I, L>(static_cast<const S *>(p.P), own_elem<L, I>(p, x, y, z, c));
+}
+
+// L2 prefetch ahead of the grid: the lanes `lane` of a warp name, for each
+// direction, the source line of its first cell in the row p.prefetch_rows
+// rows later in the grid's order (a row a block about one wave later will
+// gather), so that block's gather finds its lines in L2.  No registers stay
+// live and no data returns; a few instructions per warp.
+template <class L, class S, class Real>
+__device__ __forceinline__ void prefetch_rows_ahead(const StepParams<Real> &p, int x, int y, int z) {
+  const int rows = p.ny * p.nz;
+  int r = z * p.ny + y + p.prefetch_rows;
+  if (r >= rows) r -= rows;
+  if (r < 0 || r >= rows) return;
+  const int y2 = r % p.ny, z2 = r / p.ny;
+  const uint32_t nx = p.nx, nxy = (uint32_t)p.nx * (uint32_t)p.ny;
+  const uint32_t ry_0 = (uint32_t)y2 * nx;
+  const uint32_t ry_p = (y2 == 0 ? p.ny - 1 : y2 - 1) * nx;
+  const uint32_t ry_m = (y2 == p.ny - 1 ? 0 : y2 + 1) * nx;
+  uint32_t pz_0 = 0, pz_p = 0, pz_m = 0;
+  if constexpr (L::DIMS == 3) {
+    pz_0 = (uint32_t)z2 * nxy;
+    pz_p = (z2 == 0 ? p.nz - 1 : z2 - 1) * nxy;
+    pz_m = (z2 == p.nz - 1 ? 0 : z2 + 1) * nxy;
+  }
+  const S *P = static_cast<const S *>(p.P);
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    constexpr int ey = Dir<L, i>::y, ez = Dir<L, i>::z;
+    const uint32_t src = (uint32_t)x + (ey > 0 ? ry_p : (ey < 0 ? ry_m : ry_0)) + (ez > 0 ? pz_p : (ez < 0 ? pz_m : pz_0));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(P + elem(p, i, src)));
+  });
+}
 
 // Pull gather from a shared-memory tile: slab i (CAP elements) holds, for
 // every row of the tile, the whole source row of direction i, i.e. row
@@ -308,8 +465,25 @@ struct SmemGather {
   int nx;
   const uint8_t *fl;
   const Real *pv;
+  const StepParams<Real> *pp;
   __device__ __forceinline__ uint32_t flags(int x) const { return fl[x]; }
   __device__ __forceinline__ Real prev(int i) const { return pv[i]; }
+  template <int I>
+  __device__ __forceinline__ Real pre(uint32_t c, int64_t slot) const {
+    (void)slot;
+    return StoreOps<S>::template load<I, L>(static_cast<const S *>(pp->P), elem(*pp, I, c));
+  }
+  template <int I>
+  __device__ __forceinline__ Real nbr(int xn, int yn, int zn, int64_t slot) const {
+    (void)slot;
+    return StoreOps<S>::template load<I, L>(static_cast<const S *>(pp->P), elem(*pp, I, cell_index(*pp, xn, yn, zn)));
+  }
+  template <int I>
+  __device__ __forceinline__ void put(int x, uint32_t c, Real v) const {
+    (void)x;
+    StoreOps<S>::template store<I, L>(static_cast<S *>(pp->Pn), elem(*pp, I, c), v);
+  }
+  static constexpr bool kAA = false;
   __device__ __forceinline__ void operator()(int x, Real (&d)[L::Q]) const {
     using SO = StoreOps<S>;
     const uint32_t o_0 = row + (uint32_t)x;
@@ -329,8 +503,6 @@ struct SmemGather {
 template <class L, class S, class Real, class Gather>
 __device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, int y, int z, int64_t step_now,
                                               Real (&d)[L::Q], const Gather &gather) {
-  using SO = StoreOps<S>;
-  const S *P = static_cast<const S *>(p.P);
   gather(x, d);
   const uint32_t c = cell_index(p, x, y, z);
   if constexpr (L::DIMS == 3) {
@@ -369,19 +541,19 @@ __device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, 
         if constexpr (i > 0) {
           if ((mask >> i) & 1u) {
             constexpr int o = L::opp[i];
-            const Real fi = SO::template load<i, L>(P, elem(p, i, c));
+            const Real fi = gather.template pre<i>(c, slot);
             if (!bouzidi) {
               d[o] = fi;
             } else {
               const Real q = (Real)__ldg(p.lc_q + slot * L::Q + i);
               if (q < Real(0.5)) {
-                const Real fo = SO::template load<o, L>(P, elem(p, o, c));
+                const Real fo = gather.template pre<o>(c, slot);
                 d[o] = Real(2) * q * fi + (Real(1) - Real(2) * q) * fo;
               } else {
                 const int xn = clamp_n(x + Dir<L, o>::x, p.nx);
                 const int yn = clamp_n(y + Dir<L, o>::y, p.ny);
                 const int zn = L::DIMS == 3 ? clamp_n(z + Dir<L, o>::z, p.nz) : 0;
-                const Real fn = SO::template load<i, L>(P, elem(p, i, cell_index(p, xn, yn, zn)));
+                const Real fn = gather.template nbr<i>(xn, yn, zn, slot);
                 const Real inv2q = Real(1) / (Real(2) * q);
                 d[o] = inv2q * fi + (Real(1) - inv2q) * fn;
               }
@@ -882,15 +1054,13 @@ __device__ __forceinline__ void scalar_step(const StepParams<Real> &p, int x, in
 // post-BC state d; the split uses feq of the f_pre moments at the cell.  The
 // rest-weight part of every term (2 w_i e_i, and r x 2 w_i e_i) is constant
 // and added once per step by k_finalize, so only deviations are summed here.
-template <class L, class S, class Real>
+template <class L, class S, class Real, class Gather>
 __device__ __forceinline__ void link_cell_forces(const StepParams<Real> &p, int x, int y, int z, uint32_t c,
-                                                 int64_t slot, const Real (&d)[L::Q]) {
-  using SO = StoreOps<S>;
-  const S *P = static_cast<const S *>(p.P);
+                                                 int64_t slot, const Real (&d)[L::Q], const Gather &gather) {
   Real drho = 0, jx = 0, jy = 0, jz = 0;
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    const Real v = SO::template load<i, L>(P, elem(p, i, c));
+    const Real v = gather.template pre<i>(c, slot);
     drho += v;
     if (Dir<L, i>::x) jx += Dir<L, i>::x * v;
     if (Dir<L, i>::y) jy += Dir<L, i>::y * v;
@@ -910,7 +1080,7 @@ __device__ __forceinline__ void link_cell_forces(const StepParams<Real> &p, int 
       if ((mask >> i) & 1u) {
         constexpr int o = L::opp[i];
         constexpr Real ex = Dir<L, i>::x, ey = Dir<L, i>::y, ez = Dir<L, i>::z;
-        const Real fi = SO::template load<i, L>(P, elem(p, i, c));
+        const Real fi = gather.template pre<i>(c, slot);
         const Real eui = ex * ux + ey * uy + ez * uz;
         const Real quad = Real(4.5) * eui * eui - Real(1.5) * usq;
         const Real deq_i = Real(Dir<L, i>::w) * (drho + rho * (Real(3) * eui + quad));
@@ -958,19 +1128,19 @@ __device__ __forceinline__ void guard_rho(const StepParams<Real> &p, Real rho, i
 
 // The part of a cell's step that follows its post-BC state d: link-cell
 // forces, scalar step, collision at rate om (per-cell rate when `les`),
-// divergence guard, P_{n+1} stored.
-template <class L, class S, int COLL>
+// divergence guard, P_{n+1} stored through the access functor.  In the AA
+// layout's state-storing step the state itself is stored, uncollided.
+template <class L, class S, int COLL, class Gather>
 __device__ __forceinline__ void finish_cell(const StepParams<typename StoreOps<S>::Real> &p, int x, int y, int z,
                                             uint32_t c, uint32_t fl, int64_t step_now,
                                             typename StoreOps<S>::Real (&d)[L::Q],
                                             const ScalarCtx<typename StoreOps<S>::Real> &sc,
-                                            typename StoreOps<S>::Real om, bool les) {
+                                            typename StoreOps<S>::Real om, bool les, const Gather &gather) {
   using Real = typename StoreOps<S>::Real;
-  using SO = StoreOps<S>;
   const bool solid = fl & FLAG_SOLID;
   if ((p.feat & FEAT_OBSTACLE_BB) && (fl & FLAG_LINK)) {
     const int64_t slot = link_slot(p, x, y, z);
-    if (slot >= 0) link_cell_forces<L, S, Real>(p, x, y, z, c, slot, d);
+    if (slot >= 0) link_cell_forces<L, S, Real>(p, x, y, z, c, slot, d, gather);
   }
   if (p.feat & FEAT_THERMAL) {
     if (p.feat & FEAT_SCALAR_REDUCED) {
@@ -980,12 +1150,21 @@ __device__ __forceinline__ void finish_cell(const StepParams<typename StoreOps<S
       scalar_step<L, L>(p, x, y, z, c, solid, sc, Real(3));
     }
   }
+  if constexpr (Gather::kAA) {
+    if (p.aa_store_state) {
+      guard_rho(p, Real(1) + sum_dev<L>(d), step_now);
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        gather.template put<i>(x, c, d[i]);
+      });
+      return;
+    }
+  }
   const Real rho = collide<L, Real, COLL>(p, d, solid, om, les);
   guard_rho(p, rho, step_now);
-  S *Pn = static_cast<S *>(p.Pn);
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    SO::template store<i, L>(Pn, elem(p, i, c), d[i]);
+    gather.template put<i>(x, c, d[i]);
   });
 }
 
@@ -1004,7 +1183,7 @@ __device__ __forceinline__ void step_cell(const StepParams<typename StoreOps<S>:
   Real om = p.omega;
   const bool les = (COLL != COLL_MRT) && (p.feat & FEAT_LES);
   if (les) om = les_omega<L>(p, x, y, z, c, solid);
-  finish_cell<L, S, COLL>(p, x, y, z, c, fl, step_now, d, sc, om, les);
+  finish_cell<L, S, COLL>(p, x, y, z, c, fl, step_now, d, sc, om, les, gather);
 }
 
 // One full step: state of step n from P_n, scalar step, collision -> P_{n+1}.
@@ -1019,7 +1198,7 @@ struct StepShape {
   static constexpr int min_blocks4 = kStepMinBlocks * 128 / (BX * BY);
 };
 
-template <class L, class S, int COLL, bool FROM_STATE, int BX = kStepBlock, int BY = 1>
+template <class L, class S, int COLL, bool FROM_STATE, int BX = kStepBlock, int BY = 1, bool AA = false>
 __global__ void __launch_bounds__(BX *BY, sizeof(typename StoreOps<S>::Real) == 4 ? StepShape<BX, BY>::min_blocks4
                                                                                   : StepShape<BX, BY>::min_blocks4 / 2)
     k_step(const StepParams<typename StoreOps<S>::Real> p) {
@@ -1029,13 +1208,14 @@ __global__ void __launch_bounds__(BX *BY, sizeof(typename StoreOps<S>::Real) == 
   const int y = BY == 1 ? (int)blockIdx.y : (int)(blockIdx.y * BY + threadIdx.y), z = blockIdx.z;
   if (x >= p.nx || y >= p.ny) return;
   if constexpr (FROM_STATE) {
+    // the collision of a state the host set: each cell reads and writes its
+    // own values only (in place in the AA layout)
     const uint32_t c = cell_index(p, x, y, z);
     const bool solid = p.flags[c] & FLAG_SOLID;
     Real d[L::Q];
-    const S *P = static_cast<const S *>(p.P);
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      d[i] = SO::template load<i, L>(P, elem(p, i, c));
+      d[i] = own_value<L, S, i>(p, x, y, z, c);
     });
     Real om = p.omega;
     const bool les = (COLL != COLL_MRT) && (p.feat & FEAT_LES);
@@ -1044,9 +1224,12 @@ __global__ void __launch_bounds__(BX *BY, sizeof(typename StoreOps<S>::Real) == 
     S *Pn = static_cast<S *>(p.Pn);
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      SO::template store<i, L>(Pn, elem(p, i, c), d[i]);
+      SO::template store<i, L>(Pn, own_elem<L, i>(p, x, y, z, c), d[i]);
     });
+  } else if constexpr (AA) {
+    step_cell<L, S, COLL>(p, x, y, z, *p.step, AAGather<L, S, Real>{p, y, z});
   } else {
+    if (p.prefetch_rows > 0 && (threadIdx.x & 31) == 0) prefetch_rows_ahead<L, S>(p, x, y, z);
     step_cell<L, S, COLL>(p, x, y, z, *p.step, GlobalGather<L, S, Real>{p, y, z});
   }
 }
@@ -1271,7 +1454,7 @@ __global__ void __launch_bounds__(TileCfg<L, S>::threads, TileCfg<L, S>::min_blo
     for (int k = tid; k < ncell; k += Cfg::threads) {
       const uint32_t row = (uint32_t)(r * p.nx);
       step_cell<L, S, COLL>(p, x, t.y0 + r, t.z, step_now,
-                            SmemGather<L, S, Real, Cfg::cap>{st, row, p.nx, fl + row, pv + r * L::QP});
+                            SmemGather<L, S, Real, Cfg::cap>{st, row, p.nx, fl + row, pv + r * L::QP, &p});
       x += Cfg::threads;
       while (x >= p.nx) { x -= p.nx; ++r; }
     }
@@ -1291,18 +1474,18 @@ __global__ void __launch_bounds__(TileCfg<L, S>::threads, TileCfg<L, S>::min_blo
 
 // LES side pass: velocity of the current state (les.py:288 / :325 use
 // compute_macroscopic of the pre-collision state, solids not zeroed).
-template <class L, class S, bool FROM_STATE>
+template <class L, class S, bool FROM_STATE, bool AA = false>
 __device__ __forceinline__ void moments_cell(const StepParams<typename StoreOps<S>::Real> &p, int x, int y, int z) {
   using Real = typename StoreOps<S>::Real;
-  using SO = StoreOps<S>;
   const uint32_t c = cell_index(p, x, y, z);
   Real d[L::Q];
   if constexpr (FROM_STATE) {
-    const S *P = static_cast<const S *>(p.P);
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      d[i] = SO::template load<i, L>(P, elem(p, i, c));
+      d[i] = own_value<L, S, i>(p, x, y, z, c);
     });
+  } else if constexpr (AA) {
+    full_state<L, S, Real>(p, x, y, z, *p.step, d, nullptr, nullptr, AAGather<L, S, Real>{p, y, z});
   } else {
     full_state<L, S, Real>(p, x, y, z, *p.step, d, nullptr, nullptr);
   }
@@ -1321,11 +1504,60 @@ __device__ __forceinline__ void moments_cell(const StepParams<typename StoreOps<
   p.Uw[2 * p.cs + c] = jz * inv;
 }
 
-template <class L, class S, bool FROM_STATE>
+template <class L, class S, bool FROM_STATE, bool AA = false>
 __global__ void __launch_bounds__(kStepBlock) k_moments(const StepParams<typename StoreOps<S>::Real> p) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= p.nx) return;
-  moments_cell<L, S, FROM_STATE>(p, x, (int)blockIdx.y, (int)blockIdx.z);
+  moments_cell<L, S, FROM_STATE, AA>(p, x, (int)blockIdx.y, (int)blockIdx.z);
+}
+
+// AA layout, before each step: the pre-stream populations of every link
+// cell, the clipped-neighbour values of its Bouzidi links with q >= 1/2, and
+// the pulled populations of plane x = nx-2 (where an outlet or the
+// recycling inlet re-evaluates it), copied out of the buffer the step is
+// about to update in place.  Threads [0, n_lc) take link cells, the rest
+// the (y, z) rows of plane nx-2.
+constexpr int kStageBlock = 256;
+
+template <class L, class S>
+__global__ void __launch_bounds__(kStageBlock) k_aa_stage(const StepParams<typename StoreOps<S>::Real> p) {
+  using Real = typename StoreOps<S>::Real;
+  const int64_t k = (int64_t)blockIdx.x * kStageBlock + threadIdx.x;
+  if (k < p.n_lc) {
+    const int64_t c = p.lc_cell[k];
+    const int x = (int)(c % p.nx);
+    const int64_t row = c / p.nx;
+    const int y = (int)(row % p.ny), z = (int)(row / p.ny);
+    Real *sl = static_cast<Real *>(p.stage_link) + k * L::Q;
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      sl[i] = own_value<L, S, i>(p, x, y, z, (uint32_t)c);
+    });
+    if (p.feat & FEAT_BOUZIDI) {
+      const uint32_t mask = __ldg(p.lc_mask + k);
+      Real *sn = static_cast<Real *>(p.stage_nb) + k * L::Q;
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        if constexpr (i > 0) {
+          if (((mask >> i) & 1u) && __ldg(p.lc_q + k * L::Q + i) >= 0.5f) {
+            constexpr int o = L::opp[i];
+            const int xn = clamp_n(x + Dir<L, o>::x, p.nx);
+            const int yn = clamp_n(y + Dir<L, o>::y, p.ny);
+            const int zn = L::DIMS == 3 ? clamp_n(z + Dir<L, o>::z, p.nz) : 0;
+            sn[i] = own_value<L, S, i>(p, xn, yn, zn, cell_index(p, xn, yn, zn));
+          }
+        }
+      });
+    }
+    return;
+  }
+  const int64_t r = k - p.n_lc;
+  if (!p.stage_out || r >= (int64_t)p.ny * p.nz) return;
+  const int y = (int)(r % p.ny), z = (int)(r / p.ny);
+  Real d[L::Q];
+  AAGather<L, S, Real>{p, y, z}.raw(p.nx - 2, d);
+  Real *so = static_cast<Real *>(p.stage_out) + r * L::Q;
+  static_for<L::Q>([&](auto ic) { so[decltype(ic)::value] = d[decltype(ic)::value]; });
 }
 
 // Mean ux of the recycle plane x = nx-2 of the current step's post-bounce-
@@ -1334,7 +1566,7 @@ __global__ void __launch_bounds__(kStepBlock) k_moments(const StepParams<typenam
 // sum in a fixed order, the last block adds the block sums in block order.
 constexpr int kRecycleBlock = 256;
 
-template <class L, class S>
+template <class L, class S, bool AA = false>
 __global__ void __launch_bounds__(kRecycleBlock) k_recycle_mean(const StepParams<typename StoreOps<S>::Real> p) {
   using Real = typename StoreOps<S>::Real;
   __shared__ double red[kRecycleBlock / 32];
@@ -1346,7 +1578,10 @@ __global__ void __launch_bounds__(kRecycleBlock) k_recycle_mean(const StepParams
   if (k < plane) {
     const int y = (int)(k % p.ny), z = (int)(k / p.ny);
     Real d[L::Q];
-    partial_state<L, S, Real>(p, p.nx - 2, y, z, *p.step, d, GlobalGather<L, S, Real>{p, y, z});
+    if constexpr (AA)
+      partial_state<L, S, Real>(p, p.nx - 2, y, z, *p.step, d, AAGather<L, S, Real>{p, y, z});
+    else
+      partial_state<L, S, Real>(p, p.nx - 2, y, z, *p.step, d, GlobalGather<L, S, Real>{p, y, z});
     Real drho = 0, jx = 0;
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
@@ -1574,10 +1809,9 @@ __global__ void __launch_bounds__(kStepBlock) k_state_out(const StepParams<typen
   const uint32_t c = cell_index(p, x, y, z);
   Real d[L::Q];
   if constexpr (RAW) {
-    const S *P = static_cast<const S *>(p.P);
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      d[i] = SO::template load<i, L>(P, elem(p, i, c));
+      d[i] = own_value<L, S, i>(p, x, y, z, c);
     });
   } else {
     full_state<L, S, Real>(p, x, y, z, *p.step + step_delta, d, nullptr, nullptr);
@@ -1605,10 +1839,9 @@ __global__ void __launch_bounds__(kStepBlock) k_macro_out(const StepParams<typen
   const uint32_t c = cell_index(p, x, y, z);
   Real d[L::Q];
   if constexpr (RAW) {
-    const S *P = static_cast<const S *>(p.P);
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      d[i] = SO::template load<i, L>(P, elem(p, i, c));
+      d[i] = own_value<L, S, i>(p, x, y, z, c);
     });
   } else {
     full_state<L, S, Real>(p, x, y, z, *p.step + step_delta, d, nullptr, nullptr);
@@ -1679,10 +1912,9 @@ __global__ void __launch_bounds__(kStatsBlock)
     const uint32_t c = cell_index(p, x, y, z);
     Real d[L::Q];
     if constexpr (RAW) {
-      const S *P = static_cast<const S *>(p.P);
       static_for<L::Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
-        d[i] = SO::template load<i, L>(P, elem(p, i, c));
+        d[i] = own_value<L, S, i>(p, x, y, z, c);
       });
     } else {
       full_state<L, S, Real>(p, x, y, z, *p.step + step_delta, d, nullptr, nullptr);
@@ -1796,7 +2028,7 @@ __global__ void __launch_bounds__(kStepBlock) k_init_equilibrium(const StepParam
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
     const double dv = __dsub_rn(feq_exact<L, i>(rho, ux, uy, uz, usq), Dir<L, i>::w);
-    SO::template store<i, L>(dst, elem(p, i, c), (Real)dv);
+    SO::template store<i, L>(dst, own_elem<L, i>(p, x, y, z, c), (Real)dv);
     if (outlet) prev_dst[((int64_t)z * p.ny + y) * L::QP + i] = (Real)dv;
   });
   if (g_dst) {
@@ -1828,7 +2060,7 @@ __global__ void __launch_bounds__(kStepBlock) k_load_state(const StepParams<type
   const uint32_t c = cell_index(p, x, y, z);
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    SO::template store<i, L>(dst, elem(p, i, c), (Real)(in[(int64_t)i * p.ncells + c] - Dir<L, i>::w));
+    SO::template store<i, L>(dst, own_elem<L, i>(p, x, y, z, c), (Real)(in[(int64_t)i * p.ncells + c] - Dir<L, i>::w));
   });
 }
 

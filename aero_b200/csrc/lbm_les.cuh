@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(kLesThreads, sizeof(typename StoreOps<S>::Real
         }
         om = les_rate_from_gradient<L>(p, g, c);
       }
-      finish_cell<L, S, COLL>(p, x, y, zb, c, flc, step_now, d, sc, om, true);
+      finish_cell<L, S, COLL>(p, x, y, zb, c, flc, step_now, d, sc, om, true, GlobalGather<L, S, Real>{p, y, zb});
     }
   }
 }

@@ -76,12 +76,24 @@ struct StepParams {
   int32_t tile_rows, tiles_per_plane, ntiles;
   int32_t batch_rows;   // rows per block in the batched cell kernels
   int32_t les_chunk;    // planes per block of the fused LES step (k_step_les)
+  int32_t prefetch_rows;  // > 0: the step kernels ask L2 for the source lines of the row this many
+                          // rows ahead in grid order (0: off)
   uint32_t tile_extra_tx;  // bytes announced on a tile stage beyond its copies (0; > 0 only to test
                            // that the bounded stage waits give up)
 
   // populations (deviation from the rest weights, see Store<>)
   const void *P;        // current post-collision populations (read)
-  void *Pn;             // next post-collision populations (written)
+  void *Pn;             // next post-collision populations (written); = P in the AA layout
+  // AA layout (one buffer updated in place).  aa_layout 0: value V_i of cell
+  // x at plane opp(i), cell x; 1: at plane i, cell x + e_i (x-, y-, z-periodic).
+  int32_t aa;             // 1 in the AA layout
+  int32_t aa_layout;      // layout of the buffer's contents before this launch
+  int32_t aa_store_state; // the step stores its post-boundary state instead of colliding it
+  void *stage_link;       // per link cell: its Q pre-stream populations (Real)
+  void *stage_nb;         // per link cell: the clipped neighbour's pre-stream value of each Bouzidi
+                          // link with q >= 1/2 (Real, Q per link cell)
+  void *stage_out;        // the pulled populations of plane x = nx-2, (nz, ny, Q) Real; NULL
+                          // without an outlet that re-evaluates that plane
   const uint8_t *flags; // (cells) CellFlag bits; the buffer has 32 bytes of slack past cs
   const uint32_t *lbits;  // per 32-cell word: bit k set when cell k of the word has links
   const int32_t *loff;    // per 32-cell word: index of its first link cell

@@ -53,7 +53,7 @@ class Solver(LatticeSolverBase):
             synthetic_inflow_seed=synthetic_inflow_seed, thermal=thermal, T_hot=T_hot,
             T_cold=T_cold, alpha_T=alpha_T, buoyancy=buoyancy, g_gravity=g_gravity, beta=beta,
             T_ref=T_ref, precision=precision, scalar_lattice=scalar_lattice, device=device,
-            hist_capacity=hist_capacity, rho_in=rho_in, rho_out=rho_out)
+            hist_capacity=hist_capacity, rho_in=rho_in, rho_out=rho_out, layout=layout)
         self._ref_center_x, self._ref_center_y = self._ref_center[0], self._ref_center[1]
         self.rho = self.ux = self.uy = None
 

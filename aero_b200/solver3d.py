@@ -60,7 +60,7 @@ class Solver3D(LatticeSolverBase):
             if sem_inlet else None, thermal=thermal, T_hot=T_hot,
             T_cold=T_cold, alpha_T=alpha_T, buoyancy=buoyancy, g_gravity=g_gravity, beta=beta,
             T_ref=T_ref, precision=precision, scalar_lattice=scalar_lattice, device=device,
-            hist_capacity=hist_capacity)
+            hist_capacity=hist_capacity, layout=layout)
         self.body_force_x, self.body_force_y, self.body_force_z = self._body_force
         self._ref_center_x, self._ref_center_y, self._ref_center_z = self._ref_center
 

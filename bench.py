@@ -541,7 +541,7 @@ def scalar_precision_check(w, args, dev, tau=0.8, steps=2000, formats=("fp32", "
 ROOFLINE_STEPS = 1000  # event-timed steps of the kernel phase (about a second at sphere512)
 
 
-def _build_solver(w, precision, dev, steps, warmup):
+def _build_solver(w, precision, dev, steps, warmup, layout="ab"):
     from aero_b200 import Solver, Solver3D
     g = _geometry(w)
     dims = w["dims"]
@@ -551,7 +551,7 @@ def _build_solver(w, precision, dev, steps, warmup):
     phi = g.sdf_field(*shp) if w["kwargs"].get("bouzidi") else None
     cap = max(4096, steps + warmup + ROOFLINE_STEPS + 8)
     common = dict(solid=solid, omega=1.0 / (3.0 * w["nu"] + 0.5), u0=w["u0"], D=g.reference_length(),
-                  phi=phi, precision=precision, device=dev, hist_capacity=cap, **w["kwargs"])
+                  phi=phi, precision=precision, device=dev, hist_capacity=cap, layout=layout, **w["kwargs"])
     return Solver(Ny=ny, Nx=nx, **common) if dims == 2 else Solver3D(Nz=nz, Ny=ny, Nx=nx, **common)
 
 
@@ -603,7 +603,7 @@ def measure_lattice(w, precision, args, dev, rank=0, world=1, dist=None, e2e=Tru
     end-to-end run through the public API.  Returns a dict of results."""
     import numpy as np
     import torch
-    s = _build_solver(w, precision, dev, args.steps, args.warmup)
+    s = _build_solver(w, precision, dev, args.steps, args.warmup, layout=args.layout)
     eng = s._engine
     ncells = w["nx"] * w["ny"] * w["nz"]
     ux0, uy0, T0 = _initial_fields(w, dev, rank, s)
@@ -734,6 +734,8 @@ def main():
     ap.add_argument("--variants", default="fp16s,bf16s",
                     help="storage formats timed after the main run on the same workload, steps and warm-up "
                          "(comma-separated; 'none' to skip)")
+    ap.add_argument("--layout", default="ab", choices=["ab", "aa"],
+                    help="population layout: two buffers (ab) or one buffer updated in place (aa)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-scalar-check", action="store_true", help="box256: skip the storage-format check")
     ap.add_argument("--no-e2e", action="store_true")
@@ -826,7 +828,7 @@ def main():
                   "bf16s": "bf16 storage / f32 compute"}[args.precision],
         "data": "synthetic",
         "config": {"workload": args.workload, "desc": w["desc"], "cells": ncells,
-                   "precision": args.precision, "parallelism": f"replicas x{world}",
+                   "precision": args.precision, "layout": args.layout, "parallelism": f"replicas x{world}",
                    "l2": "state (2 x Q x cells) far larger than L2; no flush needed",
                    "links": links},
         # per step: k_step, k_finalize (+ the LES moments pass where it runs);

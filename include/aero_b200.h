@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define AERO_ABI_VERSION 2
+#define AERO_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define AERO_API __attribute__((visibility("default")))
@@ -84,7 +84,11 @@ typedef struct AeroParams {
                                aero_set_inflow: 1 = synthetic inflow (transverse velocities),
                                2 = SEM fluctuations (u', v', w'; 3D) */
   int32_t inflow_ring;      /* steps of inflow fields held on the device (0 = 64) */
+  int32_t layout;           /* AERO_LAYOUT_AB: two population buffers; AERO_LAYOUT_AA: one buffer
+                               updated in place (AA pattern; half the population memory) */
 } AeroParams;
+
+enum { AERO_LAYOUT_AB = 0, AERO_LAYOUT_AA = 1 };
 
 typedef struct AeroLattice AeroLattice;
 

@@ -199,13 +199,16 @@ def test_corrupt_checkpoint_is_rejected_before_gpu_work(tmp_path):
 
 
 def test_layout_option():
-    """layout='ab' is the engine's; 'aa' is refused before any device work."""
+    """layout is 'ab' (two buffers) or 'aa' (one buffer in place); anything
+    else is refused before any device work, and the C ABI takes the layout
+    field of AeroParams."""
+    from aero_b200 import _lib
+    from aero_b200._base import LAYOUTS, _check_layout
     from aero_b200.solver import Solver
-    from aero_b200.solver3d import Solver3D
     solid = np.zeros((8, 16), bool)
-    with pytest.raises(NotImplementedError, match="AA pattern"):
-        Solver(Ny=8, Nx=16, solid=solid, omega=1.0, u0=0.05, D=4.0, layout="aa")
-    with pytest.raises(NotImplementedError, match="AA pattern"):
-        Solver3D(Nz=4, Ny=8, Nx=16, solid=np.zeros((4, 8, 16), bool), omega=1.0, u0=0.05, D=4.0, layout="aa")
+    for name in ("ab", "aa"):
+        _check_layout(name)
+    assert LAYOUTS == {"ab": 0, "aa": 1}
     with pytest.raises(ValueError, match="Unknown layout"):
         Solver(Ny=8, Nx=16, solid=solid, omega=1.0, u0=0.05, D=4.0, layout="soa")
+    assert "layout" in dict(_lib.AeroParams._fields_)
