@@ -152,7 +152,6 @@ struct AeroLattice {
   bool aa = false;
   bool aa_holds_state = false;
   int les_chunk = 0;       // planes per block of k_step_les
-  int prefetch_rows = 0;   // AERO_B200_PREFETCH_ROWS at bind: L2 prefetch distance of the step kernels
   int tile_blocks = 0, tile_rows = 0, tiles_per_plane = 0, ntiles = 0;
   uint32_t tile_extra_tx = 0;  // AERO_B200_TEST_STALL_TILES=1 at bind: stages never complete
   // optional per-kernel event timing (eager launches only)
@@ -229,7 +228,6 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   p.tile_rows = L->tile_rows;
   p.batch_rows = L->ncells < kBatchSmallCells ? 1 : kBatchRows;
   p.les_chunk = L->les_chunk > 0 ? L->les_chunk : 1;
-  p.prefetch_rows = L->prefetch_rows;
   p.tile_extra_tx = L->tile_extra_tx;
   p.tiles_per_plane = L->tiles_per_plane;
   p.ntiles = L->ntiles;
@@ -906,10 +904,6 @@ int aero_bind_workspace(AeroLattice *L, void *dptr, uint64_t bytes, void *stream
   // Test of the bounded waits of the row-tiled kernel: every stage announces
   // 16 bytes more than its copies deliver, so no stage completes; the waits
   // give up after their limit, raise status bit 1 and the kernel returns.
-  // Row-ahead L2 prefetch distance of the per-cell and pair step kernels
-  // (rows in grid order; 0 or unset: off)
-  const char *pf = std::getenv("AERO_B200_PREFETCH_ROWS");
-  L->prefetch_rows = pf ? std::max(0, std::atoi(pf)) : 0;
   const char *stall = std::getenv("AERO_B200_TEST_STALL_TILES");
   L->tile_extra_tx = (stall && stall[0] == '1') ? 16u : 0u;
   L->bound = true;

@@ -420,37 +420,6 @@ __device__ __forceinline__ Real own_value(const StepParams<Real> &p, int x, int 
   return StoreOps<S>::template load<I, L>(static_cast<const S *>(p.P), own_elem<L, I>(p, x, y, z, c));
 }
 
-// L2 prefetch ahead of the grid: the lanes `lane` of a warp name, for each
-// direction, the source line of its first cell in the row p.prefetch_rows
-// rows later in the grid's order (a row a block about one wave later will
-// gather), so that block's gather finds its lines in L2.  No registers stay
-// live and no data returns; a few instructions per warp.
-template <class L, class S, class Real>
-__device__ __forceinline__ void prefetch_rows_ahead(const StepParams<Real> &p, int x, int y, int z) {
-  const int rows = p.ny * p.nz;
-  int r = z * p.ny + y + p.prefetch_rows;
-  if (r >= rows) r -= rows;
-  if (r < 0 || r >= rows) return;
-  const int y2 = r % p.ny, z2 = r / p.ny;
-  const uint32_t nx = p.nx, nxy = (uint32_t)p.nx * (uint32_t)p.ny;
-  const uint32_t ry_0 = (uint32_t)y2 * nx;
-  const uint32_t ry_p = (y2 == 0 ? p.ny - 1 : y2 - 1) * nx;
-  const uint32_t ry_m = (y2 == p.ny - 1 ? 0 : y2 + 1) * nx;
-  uint32_t pz_0 = 0, pz_p = 0, pz_m = 0;
-  if constexpr (L::DIMS == 3) {
-    pz_0 = (uint32_t)z2 * nxy;
-    pz_p = (z2 == 0 ? p.nz - 1 : z2 - 1) * nxy;
-    pz_m = (z2 == p.nz - 1 ? 0 : z2 + 1) * nxy;
-  }
-  const S *P = static_cast<const S *>(p.P);
-  static_for<L::Q>([&](auto ic) {
-    constexpr int i = decltype(ic)::value;
-    constexpr int ey = Dir<L, i>::y, ez = Dir<L, i>::z;
-    const uint32_t src = (uint32_t)x + (ey > 0 ? ry_p : (ey < 0 ? ry_m : ry_0)) + (ez > 0 ? pz_p : (ez < 0 ? pz_m : pz_0));
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(P + elem(p, i, src)));
-  });
-}
-
 // Pull gather from a shared-memory tile: slab i (CAP elements) holds, for
 // every row of the tile, the whole source row of direction i, i.e. row
 // (y - ey, z - ez) with the y/z wrap already resolved when the tile was
@@ -1229,7 +1198,6 @@ __global__ void __launch_bounds__(BX *BY, sizeof(typename StoreOps<S>::Real) == 
   } else if constexpr (AA) {
     step_cell<L, S, COLL>(p, x, y, z, *p.step, AAGather<L, S, Real>{p, y, z});
   } else {
-    if (p.prefetch_rows > 0 && (threadIdx.x & 31) == 0) prefetch_rows_ahead<L, S>(p, x, y, z);
     step_cell<L, S, COLL>(p, x, y, z, *p.step, GlobalGather<L, S, Real>{p, y, z});
   }
 }

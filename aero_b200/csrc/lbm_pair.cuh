@@ -326,8 +326,6 @@ __global__ void __launch_bounds__(kPairBlock, kPairMinBlocks) k_step_pair(const 
   const int t = (int)(blockIdx.x * kPairBlock + threadIdx.x);
   if (r >= sp.rows || t >= sp.npairs) return;
   const int x = 2 + 2 * t, y = r % p.ny, z = r / p.ny;
-  // lanes 0 and 16 each name a line (64 cells of 16-bit data, or 32 of FP32)
-  if (p.prefetch_rows > 0 && (threadIdx.x & 15) == 0) prefetch_rows_ahead<L, S>(p, x, y, z);
   const uint32_t c = cell_index(p, x, y, z);
   bool plain = !(p.wall != WALL_NONE && (y == 0 || y == p.ny - 1));
   if (plain) plain = *reinterpret_cast<const uint16_t *>(p.flags + c) == 0;  // both flag bytes, c even

@@ -76,8 +76,6 @@ struct StepParams {
   int32_t tile_rows, tiles_per_plane, ntiles;
   int32_t batch_rows;   // rows per block in the batched cell kernels
   int32_t les_chunk;    // planes per block of the fused LES step (k_step_les)
-  int32_t prefetch_rows;  // > 0: the step kernels ask L2 for the source lines of the row this many
-                          // rows ahead in grid order (0: off)
   uint32_t tile_extra_tx;  // bytes announced on a tile stage beyond its copies (0; > 0 only to test
                            // that the bounded stage waits give up)
 

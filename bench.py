@@ -430,7 +430,9 @@ def run_serve(args):
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     kw = dict(chunk=args.serve_chunk, window=args.serve_window, tol=args.serve_tol)
-    mk = dict(n=args.serve_requests, seed=5, nx2=(256, 512), nx3=(96, 160), max_steps=args.steps,
+    nx2 = tuple(int(v) for v in args.serve_nx2.split(","))
+    nx3 = tuple(int(v) for v in args.serve_nx3.split(","))
+    mk = dict(n=args.serve_requests, seed=5, nx2=nx2, nx3=nx3, max_steps=args.steps,
               precision=args.precision, tau_min=args.serve_tau_min)
     # capacity: the whole trace queued at once
     cal = serve.trace(rate=0.0, **mk)
@@ -467,11 +469,12 @@ def run_serve(args):
         {"fp32": "f32", "fp64": "f64", "fp16s": "f16 storage / f32 compute",
          "bf16s": "bf16 storage / f32 compute"}[args.precision],
         {"workload": "serve", "requests": len(cases), "arrivals": "Poisson at 0.8 x measured capacity",
+         "nx2": list(nx2), "nx3": list(nx3),
          "capacity_solves_per_s": cap, "chunk": args.serve_chunk, "window": args.serve_window,
          "tol": args.serve_tol, "max_steps": args.steps, "hbm_cap_gb": args.serve_hbm_gb,
          "tau_min": args.serve_tau_min,
-         "desc": "70% D2Q9 (nx 256..512) / 30% D3Q19 (nx 96..160), cylinder/rectangle/sphere/box, "
-                 "Re log-uniform 50..500, BGK/TRT/MRT, Smagorinsky above Re 200"},
+         "desc": f"70% D2Q9 (nx {nx2[0]}..{nx2[1]}) / 30% D3Q19 (nx {nx3[0]}..{nx3[1]}), "
+                 "cylinder/rectangle/sphere/box, Re log-uniform 50..500, BGK/TRT/MRT, Smagorinsky above Re 200"},
         latency={"p50_s": summ["p50_latency_s"], "p99_s": summ["p99_latency_s"]},
         status=summ["status"], aggregate_mlups=stats["cell_steps"] / span / 1e6,
         served_time={"setup_s": stats["setup_s"], "gpu_wait_s": stats["gpu_wait_s"], "rounds": stats["rounds"]},
@@ -752,6 +755,10 @@ def main():
     ap.add_argument("--serve-window", type=int, default=1000)
     ap.add_argument("--serve-tol", type=float, default=1e-3)
     ap.add_argument("--serve-hbm-gb", type=float, default=150.0)
+    ap.add_argument("--serve-nx2", default="256,512",
+                    help="nx range of the 2D requests (the configuration's trace: 256,1024)")
+    ap.add_argument("--serve-nx3", default="96,160",
+                    help="nx range of the 3D requests (the configuration's trace: 96,320)")
     ap.add_argument("--serve-tau-min", type=float, default=0.51,
                     help="smallest relaxation time of a request (u0 raised, then Re lowered, to reach it)")
     args = ap.parse_args()
