@@ -1385,6 +1385,15 @@ struct FinPlan {
   uint64_t params[2] = {0, 0}, first = 0;
 };
 
+// Members at least this large fill the GPU on their own: they step through
+// their single-lattice kernels (the step kernel their autotuning chose, their
+// own force finalisation) as branches of the batch graph, which is faster per
+// cell than the class kernels' member lookup and parameter copy.  Smaller
+// members share the class kernels.
+constexpr int64_t kBatchSoloCells = (int64_t)1 << 20;
+
+bool batch_solo(const AeroLattice *L) { return L->ncells >= kBatchSoloCells; }
+
 // In a batch the two-cell kernel runs for 16-bit storage only: measured on
 // the 96-case sweep it is 5% faster there and 9% slower with FP32 storage,
 // where the per-cell kernel's traffic, not its instructions, sets the pace.
@@ -1406,6 +1415,8 @@ struct AeroBatch {
   // plan (device offsets into ws)
   std::vector<ClassPlan> classes;
   FinPlan fin[2];  // [0] float members, [1] double members
+  std::vector<AeroLattice *> solo;  // members stepped by their own kernels
+  std::vector<int> solo_cur;        // their buffer parity when the plan was built
   uint64_t ctr_ptrs = 0, conv_items = 0, conv_out = 0;
   std::vector<char> host_plan;
   cudaStream_t cap_stream = nullptr;
@@ -1457,7 +1468,14 @@ int batch_build(AeroBatch *B, cudaStream_t st) {
   B->classes.clear();
   B->fin[0] = FinPlan{};
   B->fin[1] = FinPlan{};
+  B->solo.clear();
+  B->solo_cur.clear();
   for (AeroLattice *L : B->members) {
+    if (batch_solo(L)) {
+      B->solo.push_back(L);
+      B->solo_cur.push_back(L->cur);
+      continue;
+    }
     const ClassKey k = class_of(L);
     auto it = std::find_if(B->classes.begin(), B->classes.end(), [&](const ClassPlan &c) { return c.key == k; });
     if (it == B->classes.end()) {
@@ -1500,7 +1518,7 @@ int batch_build(AeroBatch *B, cudaStream_t st) {
     int k = 0, kl = 0;
     int64_t blocks = 0, blocks_les = 0;
     for (AeroLattice *L : B->members) {
-      if (!(class_of(L) == c.key)) continue;
+      if (batch_solo(L) || !(class_of(L) == c.key)) continue;
       for (int j = 0; j < 2; j++) {
         const int par = (L->cur + j) & 1;  // parity at steps with (phase + j') % 2 == j, phase = 0 after a build
         if (c.f64) put_params<double>(h, c.params[j] + sp * k, L, par);
@@ -1532,7 +1550,7 @@ int batch_build(AeroBatch *B, cudaStream_t st) {
     int k = 0;
     int64_t blocks = 0;
     for (AeroLattice *L : B->members) {
-      if ((is_f64(L) ? 1 : 0) != r) continue;
+      if (batch_solo(L) || (is_f64(L) ? 1 : 0) != r) continue;
       for (int j = 0; j < 2; j++) {
         const int par = (L->cur + j) & 1;
         if (r) put_params<double>(h, f.params[j] + sp * k, L, par);
@@ -1579,8 +1597,9 @@ int batch_build(AeroBatch *B, cudaStream_t st) {
 // classes parallel branches of the graph: they touch disjoint lattices).
 int batch_launch_step(AeroBatch *B, int j, cudaStream_t st, bool branches = false) {
   char *ws = B->ws;
+  const size_t nbranch = B->classes.size() + B->solo.size();
   if (branches) {
-    while (B->branch.size() < B->classes.size()) {
+    while (B->branch.size() < nbranch) {
       cudaStream_t bs;
       cudaEvent_t ev;
       CUDA_TRY(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
@@ -1623,6 +1642,23 @@ int batch_launch_step(AeroBatch *B, int j, cudaStream_t st, bool branches = fals
       CUDA_TRY(cudaStreamWaitEvent(st, B->branch_done[ci], 0));
     }
   }
+  // large members: their own step and finalisation, at their parity for this step
+  for (size_t k = 0; k < B->solo.size(); k++) {
+    AeroLattice *L = B->solo[k];
+    const size_t bi = B->classes.size() + k;
+    cudaStream_t cs = st;
+    if (branches) {
+      cs = B->branch[bi];
+      CUDA_TRY(cudaStreamWaitEvent(cs, B->fork, 0));
+    }
+    const int par = (B->solo_cur[k] + j) & 1;
+    const int rc = is_f64(L) ? launch_step<double>(L, par, cs) : launch_step<float>(L, par, cs);
+    if (rc != AERO_OK) return rc;
+    if (branches) {
+      CUDA_TRY(cudaEventRecord(B->branch_done[bi], cs));
+      CUDA_TRY(cudaStreamWaitEvent(st, B->branch_done[bi], 0));
+    }
+  }
   // the finalisation kernels do not depend on the lattice class, so any
   // table of the right arithmetic type launches them
   if (B->fin[0].n)
@@ -1643,7 +1679,7 @@ int batch_graph(AeroBatch *B, int steps, int phase, cudaGraphExec_t *out) {
     if (!B->cap_stream) CUDA_TRY(cudaStreamCreateWithFlags(&B->cap_stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaStreamBeginCapture(B->cap_stream, cudaStreamCaptureModeThreadLocal));
     int rc = AERO_OK;
-    const bool branches = B->classes.size() > 1;
+    const bool branches = B->classes.size() + B->solo.size() > 1;
     for (int j = 0; j < steps && rc == AERO_OK; j++)
       rc = batch_launch_step(B, (phase + j) & 1, B->cap_stream, branches);
     cudaGraph_t graph = nullptr;

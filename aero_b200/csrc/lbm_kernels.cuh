@@ -400,8 +400,26 @@ struct AAGather {
   }
   template <int I>
   __device__ __forceinline__ void put(int x, uint32_t c, Real v) const {
-    // layout 0 read -> write layout 1 (plane I at x + e_I); 1 -> 0 (plane opp(I) at x)
-    StoreOps<S>::template store<I, L>(static_cast<S *>(p.Pn), aa_own<L, I>(p, 1 - p.aa_layout, x, y, z, c), v);
+    // layout 0 read -> write layout 1 (plane I at x + e_I); 1 -> 0 (plane opp(I) at x).
+    // Away from the domain faces x + e_I is c plus a constant offset per
+    // direction (ex + ey nx + ez nx ny); only face cells need the wrap.
+    S *A = static_cast<S *>(p.Pn);
+    if (p.aa_layout == 1) {
+      constexpr int o = L::opp[I];
+      StoreOps<S>::template store<I, L>(A, elem(p, o, c), v);
+      return;
+    }
+    constexpr int ex = Dir<L, I>::x, ey = Dir<L, I>::y, ez = Dir<L, I>::z;
+    const bool inner = x >= 1 && x <= p.nx - 2 && y >= 1 && y <= p.ny - 2 &&
+                       (L::DIMS == 2 || (z >= 1 && z <= p.nz - 2));
+    if (inner) {
+      const uint32_t sy = (uint32_t)p.nx, sz = (uint32_t)p.nx * (uint32_t)p.ny;
+      const uint32_t dst = c + (uint32_t)ex + (ey > 0 ? sy : (ey < 0 ? 0u - sy : 0u)) +
+                           (ez > 0 ? sz : (ez < 0 ? 0u - sz : 0u));
+      StoreOps<S>::template store<I, L>(A, elem(p, I, dst), v);
+    } else {
+      StoreOps<S>::template store<I, L>(A, aa_own<L, I>(p, 1, x, y, z, c), v);
+    }
   }
   static constexpr bool kAA = true;
 };

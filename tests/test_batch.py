@@ -209,3 +209,40 @@ def test_device_convergence_matches_analyze_convergence():
         assert row[4] == 100 and row[5] == 0
         np.testing.assert_allclose(row[6], np.mean(cd[-W:]), rtol=1e-12)
     b.close()
+
+
+@pytest.mark.gpu
+def test_large_members_step_on_their_own_kernels():
+    """A member of at least 2^20 cells steps in the batch through its own
+    single-lattice kernels (its autotuned step kernel and its finalisation),
+    as a branch beside the class kernels of the small members: its populations
+    and forces equal those of the same lattice stepped alone through
+    Solver3D.run, bit for bit, over calls of even and odd lengths."""
+    from aero_b200 import Batch, Solver3D, Sphere
+    makes = _cases()[:4]
+
+    def big(precision):
+        nz, ny, nx = 96, 96, 128  # 1,179,648 cells
+        sph = Sphere(radius=8, cx_frac=0.3, cy_frac=0.5, cz_frac=0.5)
+        solid, phi = sph.mark_solid(nz, ny, nx), sph.sdf_field(nz, ny, nx)
+        return Solver3D(Nz=nz, Ny=ny, Nx=nx, solid=solid, omega=1 / 0.6, u0=0.05, D=16.0, collision="mrt",
+                        bouzidi=True, phi=phi, wall_bc="slip", outlet_bc="convective", sponge_thickness=8,
+                        precision=precision)
+
+    for precision, kernel in (("fp32", 0), ("fp16s", 4)):
+        alone = big(precision)
+        alone._engine.set_step_kernel(kernel)
+        r = alone.run(25, check_every=26, verbose=False)
+        b = Batch(max_members=8)
+        mix = [m() for m in makes]
+        s = big(precision)
+        s._engine.set_step_kernel(kernel)
+        for x in mix[:2] + [s] + mix[2:]:
+            b.add(x)
+        b.step(10)
+        b.step(15)
+        cd = s._coefficients(s._engine.read_forces())["Cd"]
+        np.testing.assert_array_equal(cd, np.array(r["Cd_history"]))
+        b.remove(s)
+        np.testing.assert_array_equal(s.f, alone.f)
+        b.close()
