@@ -35,11 +35,13 @@ LAYOUTS = {"ab": 0, "aa": 1}
 
 
 def _check_layout(layout: str) -> None:
-    """Population layout: "ab" (two buffers; every step kernel) or "aa" (one
+    """Population layout: "ab" (two buffers; every step kernel), "aa" (one
     buffer updated in place, the AA pattern: half the population memory; the
-    per-cell step kernel only; not in batches)."""
-    if layout not in LAYOUTS:
-        raise ValueError(f"Unknown layout '{layout}'. Choose 'ab' or 'aa'.")
+    per-cell step kernel only; not in batches) or "auto" (the faster "ab"
+    when its workspace fits the device's free memory with headroom, else
+    "aa"; the choice is in the solver's `layout` attribute)."""
+    if layout not in LAYOUTS and layout != "auto":
+        raise ValueError(f"Unknown layout '{layout}'. Choose 'ab', 'aa' or 'auto'.")
 
 
 def _open_checkpoint(path: str):
@@ -187,11 +189,12 @@ class LatticeSolverBase:
             P.inflow_field = 1
             P.inflow_ring = 64
         P.recycling = 1 if (self.dims == 3 and streamwise_bc == "recycling") else 0
-        P.layout = LAYOUTS[layout]
-        self.layout = layout
+        P.layout = LAYOUTS["ab" if layout == "auto" else layout]
         self._params = P
         self._engine_phi = phi if (self.van_driest and phi is not None) else None
-        self._engine = Engine(P, self.solid, self.surface_links, self.q_vals, self._engine_phi, device)
+        self._engine = Engine(P, self.solid, self.surface_links, self.q_vals, self._engine_phi, device,
+                              layout_auto=layout == "auto")
+        self.layout = "aa" if P.layout == LAYOUTS["aa"] else "ab"
 
         # initial state: equilibrium at (rho0, u0, 0) everywhere, solids included
         # (solver.py:218-227, solver3d.py:239-247); built on the GPU

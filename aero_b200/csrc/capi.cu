@@ -164,13 +164,24 @@ namespace {
 
 bool is_f64(const AeroLattice *L) { return L->prm.storage == AERO_STORE_F64; }
 
-// Whether a step re-evaluates plane x = nx-2 at other cells (a convective or
-// zero-gradient outlet, or the recycling inlet): in the AA layout its pulled
-// populations are staged before each step.
+// A convective or zero-gradient outlet re-evaluates plane x = nx-2 at the
+// outlet cells x = nx-1.  In the AA layout, when nx-2 and nx-1 sit in one warp
+// of the step kernel (128-wide blocks along x, so unless nx-1 is a multiple of
+// 32) and nothing else reads that plane, the outlet thread takes the post-
+// boundary state of nx-2 from its neighbour lane by warp shuffles.
+bool aa_outlet_shuffle(const AeroLattice *L) {
+  const bool open = L->feat & FEAT_OPEN;
+  const bool copy = open && (L->prm.outlet_bc == AERO_OUTLET_CONVECTIVE || L->prm.outlet_bc == AERO_OUTLET_ZEROGRADIENT);
+  return copy && !(L->feat & FEAT_RECYCLE) && (L->prm.nx - 1) % 32 != 0;
+}
+
+// Whether a step re-evaluates plane x = nx-2 at cells of other warps (the
+// outlet when the shuffle does not apply, or the recycling inlet at x = 0):
+// in the AA layout its pulled populations are staged before each step.
 bool aa_stages_outlet(const AeroLattice *L) {
   const bool open = L->feat & FEAT_OPEN;
-  return (open && (L->prm.outlet_bc == AERO_OUTLET_CONVECTIVE || L->prm.outlet_bc == AERO_OUTLET_ZEROGRADIENT)) ||
-         (L->feat & FEAT_RECYCLE);
+  const bool copy = open && (L->prm.outlet_bc == AERO_OUTLET_CONVECTIVE || L->prm.outlet_bc == AERO_OUTLET_ZEROGRADIENT);
+  return (copy && !aa_outlet_shuffle(L)) || (L->feat & FEAT_RECYCLE);
 }
 
 // Lattices the two-cells-per-thread kernels take: D3Q19, 4- or 2-byte
@@ -236,6 +247,7 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   p.aa = L->aa ? 1 : 0;
   p.aa_layout = cur;
   p.aa_store_state = 0;
+  p.aa_shfl_out = (L->aa && aa_outlet_shuffle(L)) ? 1 : 0;
   p.stage_link = L->aa ? ws + L->lay.stage_link : nullptr;
   p.stage_nb = L->aa ? ws + L->lay.stage_nb : nullptr;
   p.stage_out = (L->aa && aa_stages_outlet(L)) ? ws + L->lay.stage_out : nullptr;

@@ -63,7 +63,7 @@ struct Ops {
   cudaError_t (*step_les)(const StepParams<Real> &, cudaStream_t);
   cudaError_t (*les_setup)();
   // AA layout (one buffer updated in place): the staging of the step's
-  // cross-cell reads (k_aa_stage, `blocks` blocks), then the recycle mean,
+  // cross-cell reads (k_aa_stage, `blocks` x Q blocks), then the recycle mean,
   // moments pass and step kernel reading through the AA access functor
   cudaError_t (*aa_stage)(const StepParams<Real> &, unsigned blocks, cudaStream_t);
   cudaError_t (*aa_recycle_mean)(const StepParams<Real> &, cudaStream_t);

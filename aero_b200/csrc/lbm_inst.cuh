@@ -179,7 +179,7 @@ struct Launch {
     }
   }
   static cudaError_t aa_stage(const StepParams<Real> &p, unsigned blocks, cudaStream_t st) {
-    k_aa_stage<L, S><<<blocks, kStageBlock, 0, st>>>(p);
+    k_aa_stage<L, S><<<dim3(blocks, L::Q), kStageBlock, 0, st>>>(p);
     return cudaGetLastError();
   }
   static cudaError_t aa_recycle_mean(const StepParams<Real> &p, cudaStream_t st) {
@@ -194,7 +194,12 @@ struct Launch {
     return cudaGetLastError();
   }
   static cudaError_t aa_step(const StepParams<Real> &p, dim3 grid, cudaStream_t st) {
-    k_step<L, S, COLL, false, kStepBlock, 1, true><<<grid, kStepBlock, 0, st>>>(p);
+    // one instantiation per read layout: the shifted and the own-cell
+    // addressing each compile without the other's branches
+    if (p.aa_layout == 0)
+      k_step<L, S, COLL, false, kStepBlock, 1, true, 0><<<grid, kStepBlock, 0, st>>>(p);
+    else
+      k_step<L, S, COLL, false, kStepBlock, 1, true, 1><<<grid, kStepBlock, 0, st>>>(p);
     return cudaGetLastError();
   }
   static constexpr Ops<Real> table = {&step,       &step_shaped, &moments,      &finalize,   &state_out,

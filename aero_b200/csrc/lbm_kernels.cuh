@@ -337,24 +337,43 @@ __device__ __forceinline__ uint32_t aa_own(const StepParams<Real> &p, int layout
 // within a step -- the pre-stream values of link cells (bounce-back and
 // forces) and the pulled populations of plane nx-2 (which the outlet and
 // recycling cells re-evaluate) -- come from the staging area k_aa_stage
-// fills before the step.
-template <class L, class S, class Real>
+// fills before the step.  RL is the layout the step reads when the kernel is
+// compiled for one (0 or 1), or -1 for p.aa_layout at run time.
+template <class L, class S, class Real, int RL = -1>
 struct AAGather {
   const StepParams<Real> &p;
   int y, z;
+  // the step kernel (one read layout compiled in): its outlet column may take
+  // the state of x = nx-2 by warp shuffles (p.aa_shfl_out)
+  static constexpr bool kStep = RL >= 0;
+  __device__ __forceinline__ int layout() const { return RL >= 0 ? RL : p.aa_layout; }
   __device__ __forceinline__ void operator()(int x, Real (&d)[L::Q]) const {
     if (x == p.nx - 2 && p.stage_out) {
-      const Real *so = static_cast<const Real *>(p.stage_out) + ((int64_t)z * p.ny + y) * L::Q;
-      static_for<L::Q>([&](auto ic) { d[decltype(ic)::value] = so[decltype(ic)::value]; });
+      const int64_t plane = (int64_t)p.ny * p.nz;
+      const Real *so = static_cast<const Real *>(p.stage_out) + (int64_t)z * p.ny + y;
+      static_for<L::Q>([&](auto ic) { d[decltype(ic)::value] = so[decltype(ic)::value * plane]; });
       return;
     }
     raw(x, d);
+  }
+  // the pulled population I of cell x straight from the buffer
+  template <int I>
+  __device__ __forceinline__ Real raw_one(int x) const {
+    using SO = StoreOps<S>;
+    const S *A = static_cast<const S *>(p.P);
+    if (layout() == 1) return SO::template load<I, L>(A, elem(p, I, cell_index(p, x, y, z)));
+    constexpr int ex = Dir<L, I>::x, ey = Dir<L, I>::y, ez = Dir<L, I>::z;
+    constexpr int o = L::opp[I];
+    const int xs = ex ? wrap_n(x - ex, p.nx) : x;
+    const int ys = ey ? wrap_n(y - ey, p.ny) : y;
+    const int zs = (L::DIMS == 3 && ez) ? wrap_n(z - ez, p.nz) : z;
+    return SO::template load<I, L>(A, elem(p, o, cell_index(p, xs, ys, zs)));
   }
   // the pulled populations of cell x straight from the buffer
   __device__ __forceinline__ void raw(int x, Real (&d)[L::Q]) const {
     using SO = StoreOps<S>;
     const S *A = static_cast<const S *>(p.P);
-    if (p.aa_layout == 1) {
+    if (layout() == 1) {
       const uint32_t c = cell_index(p, x, y, z);
       static_for<L::Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
@@ -400,26 +419,8 @@ struct AAGather {
   }
   template <int I>
   __device__ __forceinline__ void put(int x, uint32_t c, Real v) const {
-    // layout 0 read -> write layout 1 (plane I at x + e_I); 1 -> 0 (plane opp(I) at x).
-    // Away from the domain faces x + e_I is c plus a constant offset per
-    // direction (ex + ey nx + ez nx ny); only face cells need the wrap.
-    S *A = static_cast<S *>(p.Pn);
-    if (p.aa_layout == 1) {
-      constexpr int o = L::opp[I];
-      StoreOps<S>::template store<I, L>(A, elem(p, o, c), v);
-      return;
-    }
-    constexpr int ex = Dir<L, I>::x, ey = Dir<L, I>::y, ez = Dir<L, I>::z;
-    const bool inner = x >= 1 && x <= p.nx - 2 && y >= 1 && y <= p.ny - 2 &&
-                       (L::DIMS == 2 || (z >= 1 && z <= p.nz - 2));
-    if (inner) {
-      const uint32_t sy = (uint32_t)p.nx, sz = (uint32_t)p.nx * (uint32_t)p.ny;
-      const uint32_t dst = c + (uint32_t)ex + (ey > 0 ? sy : (ey < 0 ? 0u - sy : 0u)) +
-                           (ez > 0 ? sz : (ez < 0 ? 0u - sz : 0u));
-      StoreOps<S>::template store<I, L>(A, elem(p, I, dst), v);
-    } else {
-      StoreOps<S>::template store<I, L>(A, aa_own<L, I>(p, 1, x, y, z, c), v);
-    }
+    // layout 0 read -> write layout 1 (plane I at x + e_I); 1 -> 0 (plane opp(I) at x)
+    StoreOps<S>::template store<I, L>(static_cast<S *>(p.Pn), aa_own<L, I>(p, 1 - layout(), x, y, z, c), v);
   }
   static constexpr bool kAA = true;
 };
@@ -578,7 +579,25 @@ __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int
   const bool open = p.feat & FEAT_OPEN;
   const bool copy_out =
       open && x == p.nx - 1 && (p.outlet == OUTLET_CONVECTIVE || p.outlet == OUTLET_ZEROGRAD);
-  partial_state<L, S, Real>(p, copy_out ? p.nx - 2 : x, y, z, step_now, d, gather);
+  bool shfl = false;
+  if constexpr (Gather::kAA) shfl = Gather::kStep && p.aa_shfl_out;
+  partial_state<L, S, Real>(p, copy_out && !shfl ? p.nx - 2 : x, y, z, step_now, d, gather);
+  if constexpr (Gather::kAA) {
+    // In place, the x = nx-2 thread overwrites the slots it read, so the
+    // outlet thread takes that cell's post-boundary state from its lane
+    // instead of re-reading them.  Warp-uniform: the warp holding x = nx-1,
+    // whose lanes 0 .. (nx-1) mod 32 have cells (warps cover 32 consecutive
+    // x of one row).
+    if (shfl && (x | 31) >= p.nx - 1) {
+      const int last = (p.nx - 1) & 31;
+      const unsigned lanes = last == 31 ? 0xffffffffu : (2u << last) - 1u;
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        const Real v = __shfl_up_sync(lanes, d[i], 1);
+        if (copy_out) d[i] = v;
+      });
+    }
+  }
   if (copy_out) {
     if (p.outlet == OUTLET_CONVECTIVE) {
       // boundary.py:78-113, boundary3d.py:149-164
@@ -1137,17 +1156,9 @@ __device__ __forceinline__ void finish_cell(const StepParams<typename StoreOps<S
       scalar_step<L, L>(p, x, y, z, c, solid, sc, Real(3));
     }
   }
-  if constexpr (Gather::kAA) {
-    if (p.aa_store_state) {
-      guard_rho(p, Real(1) + sum_dev<L>(d), step_now);
-      static_for<L::Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        gather.template put<i>(x, c, d[i]);
-      });
-      return;
-    }
-  }
-  const Real rho = collide<L, Real, COLL>(p, d, solid, om, les);
+  // the last step of an AA call stores the state itself (uncollided)
+  const Real rho = Gather::kAA && p.aa_store_state ? Real(1) + sum_dev<L>(d)
+                                                   : collide<L, Real, COLL>(p, d, solid, om, les);
   guard_rho(p, rho, step_now);
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
@@ -1185,14 +1196,22 @@ struct StepShape {
   static constexpr int min_blocks4 = kStepMinBlocks * 128 / (BX * BY);
 };
 
-template <class L, class S, int COLL, bool FROM_STATE, int BX = kStepBlock, int BY = 1, bool AA = false>
-__global__ void __launch_bounds__(BX *BY, sizeof(typename StoreOps<S>::Real) == 4 ? StepShape<BX, BY>::min_blocks4
-                                                                                  : StepShape<BX, BY>::min_blocks4 / 2)
+// The AA variant keeps one block per SM less (72 registers instead of 64 for
+// 4-byte arithmetic): its address arithmetic for the shifted stores would
+// otherwise spill.
+constexpr int kStepAAMinBlocks = 7;
+template <class L, class S, int COLL, bool FROM_STATE, int BX = kStepBlock, int BY = 1, bool AA = false, int RL = -1>
+__global__ void __launch_bounds__(BX *BY, AA ? (sizeof(typename StoreOps<S>::Real) == 4 ? kStepAAMinBlocks
+                                                                                        : kStepAAMinBlocks / 2)
+                                             : (sizeof(typename StoreOps<S>::Real) == 4 ? StepShape<BX, BY>::min_blocks4
+                                                                                        : StepShape<BX, BY>::min_blocks4 / 2))
     k_step(const StepParams<typename StoreOps<S>::Real> p) {
   using Real = typename StoreOps<S>::Real;
   using SO = StoreOps<S>;
   const int x = blockIdx.x * BX + threadIdx.x;
   const int y = BY == 1 ? (int)blockIdx.y : (int)(blockIdx.y * BY + threadIdx.y), z = blockIdx.z;
+  // the AA outlet shuffle needs warps of 32 consecutive x of one row
+  static_assert(!AA || (BY == 1 && BX % 32 == 0), "the AA step kernel runs full-warp row segments");
   if (x >= p.nx || y >= p.ny) return;
   if constexpr (FROM_STATE) {
     // the collision of a state the host set: each cell reads and writes its
@@ -1214,7 +1233,7 @@ __global__ void __launch_bounds__(BX *BY, sizeof(typename StoreOps<S>::Real) == 
       SO::template store<i, L>(Pn, own_elem<L, i>(p, x, y, z, c), d[i]);
     });
   } else if constexpr (AA) {
-    step_cell<L, S, COLL>(p, x, y, z, *p.step, AAGather<L, S, Real>{p, y, z});
+    step_cell<L, S, COLL>(p, x, y, z, *p.step, AAGather<L, S, Real, RL>{p, y, z});
   } else {
     step_cell<L, S, COLL>(p, x, y, z, *p.step, GlobalGather<L, S, Real>{p, y, z});
   }
@@ -1501,49 +1520,53 @@ __global__ void __launch_bounds__(kStepBlock) k_moments(const StepParams<typenam
 // cell, the clipped-neighbour values of its Bouzidi links with q >= 1/2, and
 // the pulled populations of plane x = nx-2 (where an outlet or the
 // recycling inlet re-evaluates it), copied out of the buffer the step is
-// about to update in place.  Threads [0, n_lc) take link cells, the rest
-// the (y, z) rows of plane nx-2.
+// about to update in place.  Block row blockIdx.y is the direction; along x,
+// threads [0, n_lc) take link cells and the rest the (y, z) rows of plane
+// nx-2.  One load and one store per thread, the direction uniform in a block,
+// so the few link cells still spread over the whole GPU and no warp runs the
+// directions one after another.
 constexpr int kStageBlock = 256;
 
 template <class L, class S>
 __global__ void __launch_bounds__(kStageBlock) k_aa_stage(const StepParams<typename StoreOps<S>::Real> p) {
   using Real = typename StoreOps<S>::Real;
+  const int dir = blockIdx.y;
   const int64_t k = (int64_t)blockIdx.x * kStageBlock + threadIdx.x;
   if (k < p.n_lc) {
-    const int64_t c = p.lc_cell[k];
-    const int x = (int)(c % p.nx);
-    const int64_t row = c / p.nx;
-    const int y = (int)(row % p.ny), z = (int)(row / p.ny);
-    Real *sl = static_cast<Real *>(p.stage_link) + k * L::Q;
+    // cell indices are below 2^31
+    const uint32_t c = (uint32_t)p.lc_cell[k];
+    const uint32_t row = c / (uint32_t)p.nx;
+    const int x = (int)(c - row * (uint32_t)p.nx);
+    const int z = (int)(row / (uint32_t)p.ny), y = (int)(row - (uint32_t)z * (uint32_t)p.ny);
+    const int64_t t = k * L::Q + dir;
+    const bool bouzidi = p.feat & FEAT_BOUZIDI;
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      sl[i] = own_value<L, S, i>(p, x, y, z, (uint32_t)c);
-    });
-    if (p.feat & FEAT_BOUZIDI) {
-      const uint32_t mask = __ldg(p.lc_mask + k);
-      Real *sn = static_cast<Real *>(p.stage_nb) + k * L::Q;
-      static_for<L::Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        if constexpr (i > 0) {
-          if (((mask >> i) & 1u) && __ldg(p.lc_q + k * L::Q + i) >= 0.5f) {
-            constexpr int o = L::opp[i];
-            const int xn = clamp_n(x + Dir<L, o>::x, p.nx);
-            const int yn = clamp_n(y + Dir<L, o>::y, p.ny);
-            const int zn = L::DIMS == 3 ? clamp_n(z + Dir<L, o>::z, p.nz) : 0;
-            sn[i] = own_value<L, S, i>(p, xn, yn, zn, cell_index(p, xn, yn, zn));
-          }
+      if (dir != i) return;
+      static_cast<Real *>(p.stage_link)[t] = own_value<L, S, i>(p, x, y, z, c);
+      if constexpr (i > 0) {
+        if (bouzidi && ((__ldg(p.lc_mask + k) >> i) & 1u) && __ldg(p.lc_q + t) >= 0.5f) {
+          constexpr int o = L::opp[i];
+          const int xn = clamp_n(x + Dir<L, o>::x, p.nx);
+          const int yn = clamp_n(y + Dir<L, o>::y, p.ny);
+          const int zn = L::DIMS == 3 ? clamp_n(z + Dir<L, o>::z, p.nz) : 0;
+          static_cast<Real *>(p.stage_nb)[t] = own_value<L, S, i>(p, xn, yn, zn, cell_index(p, xn, yn, zn));
         }
-      });
-    }
+      }
+    });
     return;
   }
+  // plane x = nx-2, direction-major: a warp's stores are contiguous
+  const int64_t plane = (int64_t)p.ny * p.nz;
   const int64_t r = k - p.n_lc;
-  if (!p.stage_out || r >= (int64_t)p.ny * p.nz) return;
+  if (!p.stage_out || r >= plane) return;
   const int y = (int)(r % p.ny), z = (int)(r / p.ny);
-  Real d[L::Q];
-  AAGather<L, S, Real>{p, y, z}.raw(p.nx - 2, d);
-  Real *so = static_cast<Real *>(p.stage_out) + r * L::Q;
-  static_for<L::Q>([&](auto ic) { so[decltype(ic)::value] = d[decltype(ic)::value]; });
+  Real *so = static_cast<Real *>(p.stage_out) + r;
+  const AAGather<L, S, Real> g{p, y, z};
+  static_for<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    if (dir == i) so[i * plane] = g.template raw_one<i>(p.nx - 2);
+  });
 }
 
 // Mean ux of the recycle plane x = nx-2 of the current step's post-bounce-

@@ -87,10 +87,11 @@ struct StepParams {
   int32_t aa;             // 1 in the AA layout
   int32_t aa_layout;      // layout of the buffer's contents before this launch
   int32_t aa_store_state; // the step stores its post-boundary state instead of colliding it
+  int32_t aa_shfl_out;    // the outlet cells take the state of x = nx-2 from the neighbour lane
   void *stage_link;       // per link cell: its Q pre-stream populations (Real)
   void *stage_nb;         // per link cell: the clipped neighbour's pre-stream value of each Bouzidi
                           // link with q >= 1/2 (Real, Q per link cell)
-  void *stage_out;        // the pulled populations of plane x = nx-2, (nz, ny, Q) Real; NULL
+  void *stage_out;        // the pulled populations of plane x = nx-2, (Q, nz, ny) Real; NULL
                           // without an outlet that re-evaluates that plane
   const uint8_t *flags; // (cells) CellFlag bits; the buffer has 32 bytes of slack past cs
   const uint32_t *lbits;  // per 32-cell word: bit k set when cell k of the word has links

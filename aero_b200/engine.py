@@ -33,8 +33,12 @@ def _require_cuda(device):
 class Engine:
     """Owns an AeroLattice handle and the device workspace bound to it."""
 
+    # layout_auto: the share of the device's free memory the two-buffer
+    # workspace may take before the lattice switches to the AA layout
+    AUTO_LAYOUT_FREE_SHARE = 0.8
+
     def __init__(self, params: AeroParams, solid: np.ndarray, links: np.ndarray, q: np.ndarray,
-                 phi: Optional[np.ndarray] = None, device=None):
+                 phi: Optional[np.ndarray] = None, device=None, layout_auto: bool = False):
         import torch
         self.torch = torch
         self.lib = _lib.load()
@@ -47,25 +51,39 @@ class Engine:
         qg = ctypes.c_int32()
         check("aero_lattice_q", self.lib.aero_lattice_q(ctypes.byref(params), ctypes.byref(q_), ctypes.byref(qg)))
         self.Q, self.Qg = q_.value, qg.value
-        h = ctypes.c_void_p()
-        check("aero_create", self.lib.aero_create(ctypes.byref(params), ctypes.byref(h)))
-        self.h = h
         solid_u8 = np.ascontiguousarray(solid, dtype=np.uint8)
         links = np.ascontiguousarray(links, dtype=np.int32)
         q = np.ascontiguousarray(q, dtype=np.float32)
         phi_c = None if phi is None else np.ascontiguousarray(phi, dtype=np.float64)
-        check("aero_set_geometry", self.lib.aero_set_geometry(
-            h, solid_u8.ctypes.data, links.ctypes.data if len(links) else None,
-            q.ctypes.data if len(q) else None, len(links), None if phi_c is None else phi_c.ctypes.data))
-        nbytes = ctypes.c_uint64()
-        check("aero_workspace_size", self.lib.aero_workspace_size(h, ctypes.byref(nbytes)))
-        self.workspace_bytes = int(nbytes.value)
+        self._create(solid_u8, links, q, phi_c)
+        if layout_auto and params.layout == 0:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            if self.workspace_bytes > self.AUTO_LAYOUT_FREE_SHARE * free:
+                # two population buffers do not fit: one buffer updated in place
+                self.lib.aero_destroy(self.h)
+                self.h = None
+                params.layout = 1
+                self._create(solid_u8, links, q, phi_c)
+        h = self.h
         with torch.cuda.device(self.device):
             self.workspace = torch.empty(self.workspace_bytes, dtype=torch.uint8, device=self.device)
             check("aero_bind_workspace", self.lib.aero_bind_workspace(
                 h, self.workspace.data_ptr(), self.workspace_bytes, self.stream()))
         self.hist_capacity = params.hist_capacity or 4096
         self.nprof = params.nz if params.dims == 3 else params.ny
+
+    def _create(self, solid_u8, links, q, phi_c):
+        """aero_create + aero_set_geometry for self.params; sets self.h and
+        self.workspace_bytes (nothing allocated on the device yet)."""
+        h = ctypes.c_void_p()
+        check("aero_create", self.lib.aero_create(ctypes.byref(self.params), ctypes.byref(h)))
+        self.h = h
+        check("aero_set_geometry", self.lib.aero_set_geometry(
+            h, solid_u8.ctypes.data, links.ctypes.data if len(links) else None,
+            q.ctypes.data if len(q) else None, len(links), None if phi_c is None else phi_c.ctypes.data))
+        nbytes = ctypes.c_uint64()
+        check("aero_workspace_size", self.lib.aero_workspace_size(h, ctypes.byref(nbytes)))
+        self.workspace_bytes = int(nbytes.value)
 
     # ------------------------------------------------------------------
     def stream(self):

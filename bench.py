@@ -737,8 +737,9 @@ def main():
     ap.add_argument("--variants", default="fp16s,bf16s",
                     help="storage formats timed after the main run on the same workload, steps and warm-up "
                          "(comma-separated; 'none' to skip)")
-    ap.add_argument("--layout", default="ab", choices=["ab", "aa"],
-                    help="population layout: two buffers (ab) or one buffer updated in place (aa)")
+    ap.add_argument("--layout", default="ab", choices=["ab", "aa", "auto"],
+                    help="population layout: two buffers (ab), one buffer updated in place (aa), or auto "
+                         "(ab when it fits the free device memory, else aa)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-scalar-check", action="store_true", help="box256: skip the storage-format check")
     ap.add_argument("--no-e2e", action="store_true")
@@ -793,6 +794,7 @@ def main():
 
     m = measure_lattice(w, args.precision, args, dev, rank, world, dist, e2e=not args.no_e2e)
     s = m.pop("solver")
+    layout = s.layout
     Cd_last = float(m["raw"][-1, 0] / s._drag_norm()) if len(m["raw"]) else 0.0
     links = int(len(s.surface_links))
     extra = {}
@@ -835,7 +837,7 @@ def main():
                   "bf16s": "bf16 storage / f32 compute"}[args.precision],
         "data": "synthetic",
         "config": {"workload": args.workload, "desc": w["desc"], "cells": ncells,
-                   "precision": args.precision, "layout": args.layout, "parallelism": f"replicas x{world}",
+                   "precision": args.precision, "layout": layout, "parallelism": f"replicas x{world}",
                    "l2": "state (2 x Q x cells) far larger than L2; no flush needed",
                    "links": links},
         # per step: k_step, k_finalize (+ the LES moments pass where it runs);

@@ -4,7 +4,9 @@ A step reads each cell's pulled populations from the slots it then
 overwrites (alternating between two slot layouts), so no second buffer is
 needed; the reads that cross cells inside a step (the pre-stream values of
 link cells, the pulled populations of the plane x = nx-2 that the outlet and
-recycling cells re-evaluate) are staged before the step.  Between aero_step
+recycling cells re-evaluate) are staged before the step, except that an
+outlet cell whose x = nx-2 neighbour runs in its own warp takes that state by
+warp shuffles (nx-1 not a multiple of 32; both forms are covered below).  Between aero_step
 calls the buffer holds the post-boundary state itself (the call's last step
 stores it; the next call collides it in place), so the state read back is
 the reference's self.f as with two buffers.
@@ -44,9 +46,9 @@ def test_aa_fp64_matches_reference_golden(name):
     np.testing.assert_allclose(cd, ref, rtol=0, atol=1e-8 * max(np.abs(ref).max(), 1e-3))
 
 
-def _sphere(precision, layout, **extra):
+def _sphere(precision, layout, nx=48, **extra):
     from aero_b200 import Solver3D, Sphere
-    nz, ny, nx = 18, 20, 48
+    nz, ny = 18, 20
     sph = Sphere(radius=4, cx_frac=0.3, cy_frac=0.5, cz_frac=0.5)
     solid, phi = sph.mark_solid(nz, ny, nx), sph.sdf_field(nz, ny, nx)
     kw = dict(omega=1 / 0.7, u0=0.05, D=sph.reference_length(), collision="mrt", bouzidi=True, phi=phi,
@@ -79,6 +81,9 @@ def _cylinder(precision, layout):
 
 MAKERS = {
     "sphere_mrt_bouzidi_convective": lambda prec, lay: _sphere(prec, lay),
+    # nx - 1 = 64: the x = nx-2 and nx-1 cells run in different warps, so the
+    # outlet reads the staged plane instead of shuffling
+    "sphere_mrt_bouzidi_convective_staged_outlet": lambda prec, lay: _sphere(prec, lay, nx=65),
     "sphere_bgk_les_recycling": lambda prec, lay: _sphere(prec, lay, collision="bgk", les=True,
                                                            streamwise_bc="recycling", outlet_bc="zerogradient",
                                                            body_force_x=1e-5),
@@ -111,6 +116,21 @@ def test_aa_equals_ab_over_multistep_calls(case, precision):
     np.testing.assert_allclose(cda, cdb, rtol=0, atol=10 * tol * max(np.abs(cdb).max(), 1e-3))
     fa, fb = a.field_statistics(), b.field_statistics()
     assert abs(fa["mass"] - fb["mass"]) <= 10 * tol * fb["mass"]
+
+
+def test_auto_layout_takes_ab_when_it_fits_else_aa(monkeypatch):
+    """layout="auto" keeps the faster two-buffer layout when its workspace
+    fits the device's free memory with headroom, and otherwise builds the
+    lattice in the AA layout, which then steps exactly as layout="aa"."""
+    from aero_b200.engine import Engine
+    s = _sphere("fp32", "auto")
+    assert s.layout == "ab" and s._b200_options()["layout"] == "ab"
+    monkeypatch.setattr(Engine, "AUTO_LAYOUT_FREE_SHARE", 0.0)
+    a, b = _sphere("fp32", "auto"), _sphere("fp32", "aa")
+    assert a.layout == "aa" and a._engine.workspace_bytes == b._engine.workspace_bytes
+    ra, rb = a.run(12, check_every=13, verbose=False), b.run(12, check_every=13, verbose=False)
+    np.testing.assert_array_equal(a.f, b.f)
+    np.testing.assert_array_equal(ra["Cd_history"], rb["Cd_history"])
 
 
 def test_aa_halves_population_memory():

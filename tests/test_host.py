@@ -199,14 +199,14 @@ def test_corrupt_checkpoint_is_rejected_before_gpu_work(tmp_path):
 
 
 def test_layout_option():
-    """layout is 'ab' (two buffers) or 'aa' (one buffer in place); anything
-    else is refused before any device work, and the C ABI takes the layout
-    field of AeroParams."""
+    """layout is 'ab' (two buffers), 'aa' (one buffer in place) or 'auto'
+    (chosen by the memory the lattice needs); anything else is refused before
+    any device work, and the C ABI takes the layout field of AeroParams."""
     from aero_b200 import _lib
     from aero_b200._base import LAYOUTS, _check_layout
     from aero_b200.solver import Solver
     solid = np.zeros((8, 16), bool)
-    for name in ("ab", "aa"):
+    for name in ("ab", "aa", "auto"):
         _check_layout(name)
     assert LAYOUTS == {"ab": 0, "aa": 1}
     with pytest.raises(ValueError, match="Unknown layout"):
