@@ -17,6 +17,61 @@ from ._lib import AeroParams, check
 
 FORCE_VALUES = _lib.FORCE_VALUES
 
+# Device-to-host copies of large results (run()'s rho / u fields, the state)
+# go through two pinned bounce buffers of this many bytes: the copy engine
+# fills one at PCIe / C2C rate while the host threads copy the other into the
+# caller's array, instead of the driver's staged copy into pageable memory.
+READBACK_CHUNK = 32 << 20
+_bounce = []
+
+
+def _bounce_buffers():
+    """The process's two pinned bounce buffers, allocated on first use (a
+    lattice whose results need them allocates them at set-up)."""
+    import torch
+    if not _bounce:
+        _bounce.extend(torch.empty(READBACK_CHUNK, dtype=torch.uint8, pin_memory=True) for _ in range(2))
+    return _bounce
+
+
+def copy_to_host(src, out: Optional[np.ndarray] = None) -> np.ndarray:
+    """Contiguous CUDA tensor -> host numpy array of the same dtype and shape
+    (`out`, C-contiguous, or a new one).  Results above one bounce buffer are
+    copied chunk by chunk on the tensor's current stream, the device-to-host
+    copy of one chunk overlapping the host copy of the previous one."""
+    import torch
+    src = src.contiguous()
+    if out is None:
+        out = np.empty(tuple(src.shape), dtype=torch.empty((), dtype=src.dtype).numpy().dtype)
+    dst = torch.from_numpy(out).reshape(-1).view(torch.uint8)
+    flat = src.reshape(-1).view(torch.uint8)
+    n = flat.numel()
+    if n != dst.numel():
+        raise ValueError("copy_to_host: size mismatch")
+    if n <= READBACK_CHUNK:
+        dst.copy_(flat)
+        return out
+    ring = _bounce_buffers()
+    stream = torch.cuda.current_stream(src.device)
+    done = [torch.cuda.Event(), torch.cuda.Event()]
+    pending = None
+    with torch.cuda.device(src.device):
+        for k, off in enumerate(range(0, n, READBACK_CHUNK)):
+            m = min(READBACK_CHUNK, n - off)
+            # ring[k & 1] was last read by the host copy of chunk k - 2,
+            # which finished in the previous iteration
+            ring[k & 1][:m].copy_(flat[off:off + m], non_blocking=True)
+            done[k & 1].record(stream)
+            if pending is not None:
+                pk, poff, pm = pending
+                done[pk & 1].synchronize()
+                dst[poff:poff + pm].copy_(ring[pk & 1][:pm])
+            pending = (k, off, m)
+        pk, poff, pm = pending
+        done[pk & 1].synchronize()
+        dst[poff:poff + pm].copy_(ring[pk & 1][:pm])
+    return out
+
 
 def _require_cuda(device):
     import torch
@@ -71,6 +126,8 @@ class Engine:
                 h, self.workspace.data_ptr(), self.workspace_bytes, self.stream()))
         self.hist_capacity = params.hist_capacity or 4096
         self.nprof = params.nz if params.dims == 3 else params.ny
+        if (1 + self.dims) * self.ncells * 8 > READBACK_CHUNK:
+            _bounce_buffers()  # set-up cost, not a per-run one
 
     def _create(self, solid_u8, links, q, phi_c):
         """aero_create + aero_set_geometry for self.params; sets self.h and
@@ -144,7 +201,7 @@ class Engine:
 
     def get_state(self):
         f, p, g = self.get_state_device()
-        return (f.cpu().numpy(), p.cpu().numpy(), None if g is None else g.cpu().numpy())
+        return (copy_to_host(f), copy_to_host(p), None if g is None else copy_to_host(g))
 
     def get_slab_device(self, z0: int, nzs: int):
         t = self.torch

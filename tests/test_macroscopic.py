@@ -49,3 +49,23 @@ def test_run_result_fields_are_the_moments_of_the_state():
     # a second run hands out new arrays, not the first run's
     r2 = s.run(3, check_every=10, verbose=False)
     assert not np.shares_memory(r["rho"], r2["rho"])
+
+
+@pytest.mark.parametrize("n", [1000, (32 << 20) // 8, (32 << 20) // 8 + 1, 9_000_001])
+def test_copy_to_host_through_bounce_buffers(n):
+    """Results larger than one pinned bounce buffer (32 MiB) reach the host
+    chunk by chunk; the bytes equal those of a plain copy, whether the size
+    is below, at, just above or several buffers and a remainder above it,
+    into a fresh array or a given one, FP64 or FP32."""
+    import torch
+    from aero_b200.engine import copy_to_host
+    g = torch.Generator(device="cuda").manual_seed(n)
+    for dt in (torch.float64, torch.float32):
+        src = torch.rand((n,), generator=g, device="cuda", dtype=torch.float64).to(dt)
+        ref = src.cpu().numpy()
+        got = copy_to_host(src)
+        assert got.dtype == ref.dtype and got.shape == ref.shape
+        np.testing.assert_array_equal(got, ref)
+        out = np.full(ref.shape, -1.0, dtype=ref.dtype)
+        assert copy_to_host(src.reshape(1, -1), out.reshape(1, -1)) is not None
+        np.testing.assert_array_equal(out, ref)

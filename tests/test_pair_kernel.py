@@ -52,6 +52,44 @@ def test_pair_kernel_equals_per_cell_kernel(precision, collision):
     np.testing.assert_allclose(cda, cdb, rtol=0, atol=10 * TOL[precision] * np.abs(cdb).max())
 
 
+@pytest.mark.parametrize("nx", [64, 200, 520])
+@pytest.mark.parametrize("precision", ["fp16s", "bf16s"])
+def test_pair_kernel_equals_batched_pair_kernel(precision, nx):
+    """A 16-bit lattice alone in a batch runs the batched pair kernel (its
+    parameters in shared memory, blocks found on the batch's work-list); the
+    same lattice alone runs the single-lattice pair kernel.  Both do the same
+    operations, so populations and drag agree bit for bit.  Rows of 30, 98
+    and 258 pairs: one partial warp, several warps, and three blocks of which
+    the last holds two pairs."""
+    from aero_b200 import Batch, Solver3D, Sphere
+
+    def make():
+        nz, ny = 10, 12
+        sph = Sphere(radius=3, cx_frac=0.3, cy_frac=0.5, cz_frac=0.5)
+        solid, phi = sph.mark_solid(nz, ny, nx), sph.sdf_field(nz, ny, nx)
+        s = Solver3D(Nz=nz, Ny=ny, Nx=nx, solid=solid, omega=1 / 0.7, u0=0.05, D=6.0, collision="mrt",
+                     bouzidi=True, phi=phi, wall_bc="slip", outlet_bc="convective", sponge_thickness=6,
+                     precision=precision)
+        rng = np.random.default_rng(5)
+        s.set_equilibrium_state(ux=0.05 + 0.01 * rng.uniform(-1, 1, solid.shape),
+                                uy=0.01 * rng.uniform(-1, 1, solid.shape), uz=0.01 * rng.uniform(-1, 1, solid.shape))
+        return s
+
+    a = make()
+    a._engine.set_step_kernel(PAIR)
+    assert a._engine.get_step_kernel() == PAIR
+    r = a.run(30, check_every=31, verbose=False)
+    b = make()
+    bat = Batch(max_members=1)
+    bat.add(b)
+    bat.step(30)
+    np.testing.assert_array_equal(a._engine.get_state()[0], b._engine.get_state()[0])
+    cd = b._coefficients(b._engine.read_forces())["Cd"]
+    np.testing.assert_array_equal(cd, np.array(r["Cd_history"]))
+    bat.remove(b)
+    bat.close()
+
+
 def test_pair_kernel_sphere_matches_oracle_300_steps():
     """The acceptance bound of the plain FP32 form through the pair kernel:
     rel-L2(rho, u) <= 1e-5 after 300 steps against the FP64 oracle."""
