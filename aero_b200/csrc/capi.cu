@@ -1607,7 +1607,9 @@ int batch_build(AeroBatch *B, cudaStream_t st) {
 // With `branches`, every lattice class runs on its own stream forked from st
 // and joined back before the finalisation (during capture this makes the
 // classes parallel branches of the graph: they touch disjoint lattices).
-int batch_launch_step(AeroBatch *B, int j, cudaStream_t st, bool branches = false) {
+// `aa_store`: the call's last step, where members in the AA layout store
+// their post-boundary state instead of colliding it.
+int batch_launch_step(AeroBatch *B, int j, cudaStream_t st, bool branches = false, bool aa_store = false) {
   char *ws = B->ws;
   const size_t nbranch = B->classes.size() + B->solo.size();
   if (branches) {
@@ -1664,7 +1666,9 @@ int batch_launch_step(AeroBatch *B, int j, cudaStream_t st, bool branches = fals
       CUDA_TRY(cudaStreamWaitEvent(cs, B->fork, 0));
     }
     const int par = (B->solo_cur[k] + j) & 1;
-    const int rc = is_f64(L) ? launch_step<double>(L, par, cs) : launch_step<float>(L, par, cs);
+    const bool store = L->aa && aa_store;
+    const int rc = is_f64(L) ? launch_step<double>(L, par, cs, false, store)
+                             : launch_step<float>(L, par, cs, false, store);
     if (rc != AERO_OK) return rc;
     if (branches) {
       CUDA_TRY(cudaEventRecord(B->branch_done[bi], cs));
@@ -1755,7 +1759,10 @@ int aero_batch_add(AeroBatch *B, AeroLattice *L, double cd_norm) {
   if (!(cd_norm > 0.0) || !std::isfinite(cd_norm)) return fail(AERO_ERR_INVALID, "cd_norm must be > 0");
   if (L->feat & (FEAT_INFLOW_FIELD | FEAT_RECYCLE))
     return fail(AERO_ERR_UNSUPPORTED, "lattices with synthetic inflow or a recycling inlet step only on their own");
-  if (L->aa) return fail(AERO_ERR_UNSUPPORTED, "lattices in the AA layout step only on their own");
+  if (L->aa && !batch_solo(L))
+    return fail(AERO_ERR_UNSUPPORTED,
+                "a lattice in the AA layout joins a batch only with at least %lld cells (then it steps on its "
+                "own kernels)", (long long)kBatchSoloCells);
   L->batch = B;
   L->cd_norm = cd_norm;
   B->members.push_back(L);
@@ -1795,7 +1802,19 @@ int aero_batch_step(AeroBatch *B, int64_t n, void *stream) {
   k_set_profile_steps<<<blocks_for(nm, 128), 128, 0, st>>>(reinterpret_cast<int64_t *const *>(B->ws + B->ctr_ptrs),
                                                           nm, n);
   CUDA_TRY(cudaGetLastError());
-  int64_t left = n;
+  // members in the AA layout (all large, so stepped by their own kernels)
+  // first collide the state their last call stored, and the call's last
+  // step stores theirs: that step runs outside the graphs
+  bool any_aa = false;
+  for (AeroLattice *L : B->members) {
+    if (!L->aa) continue;
+    any_aa = true;
+    if (L->aa_holds_state) {
+      const int rc = is_f64(L) ? aa_collide_state<double>(L, st) : aa_collide_state<float>(L, st);
+      if (rc != AERO_OK) return rc;
+    }
+  }
+  int64_t left = any_aa ? n - 1 : n;
   while (left > 0) {
     const int steps = left >= 2 ? 2 : 1;
     cudaGraphExec_t g = nullptr;
@@ -1805,7 +1824,13 @@ int aero_batch_step(AeroBatch *B, int64_t n, void *stream) {
     B->phase = (B->phase + steps) & 1;
     left -= steps;
   }
+  if (any_aa) {
+    const int rc = batch_launch_step(B, B->phase, st, false, true);
+    if (rc != AERO_OK) return rc;
+    B->phase ^= 1;
+  }
   for (AeroLattice *L : B->members) {
+    if (L->aa) L->aa_holds_state = true;
     L->cur ^= (int)(n & 1);
     L->step_count += n;
     L->old_is_state = false;

@@ -94,15 +94,16 @@ def omega_of(case: Case, D: float) -> float:
     return 1.0 / (3.0 * nu + 0.5)
 
 
-def make_solver(case: Case, device=None, hist_capacity: int = 4096):
-    """The solver of a case, with the reference CLI's boundary conditions."""
+def make_solver(case: Case, device=None, hist_capacity: int = 4096, layout: str = "ab"):
+    """The solver of a case, with the reference CLI's boundary conditions, in
+    population layout `layout` ("ab" or "aa")."""
     from .solver import Solver
     from .solver3d import Solver3D
     geo = geometry(case)
     D = geo.reference_length()
     kw = dict(omega=omega_of(case, D), u0=case.u0, D=D, wall_bc="slip", inlet_bc="velocity",
               outlet_bc="convective", collision=case.collision, les=case.les, les_cs=0.16,
-              precision=case.precision, device=device, hist_capacity=hist_capacity)
+              precision=case.precision, device=device, hist_capacity=hist_capacity, layout=layout)
     if case.dims == 2:
         solid = geo.mark_solid(case.ny, case.nx)
         return Solver(Ny=case.ny, Nx=case.nx, solid=solid, **kw)
@@ -110,16 +111,24 @@ def make_solver(case: Case, device=None, hist_capacity: int = 4096):
     return Solver3D(Nz=case.nz, Ny=case.ny, Nx=case.nx, solid=solid, **kw)
 
 
-def footprint(case: Case, hist_capacity: int = 4096) -> int:
+def footprint(case: Case, hist_capacity: int = 4096, layout: str = "ab") -> int:
     """Upper bound of the device bytes a case holds while admitted: the
-    population buffers, flags, LES velocities and outlet state of its
-    workspace, the force ring, plus the FP64 initial state built during set-up."""
+    population buffers (two, or one in the AA layout plus its staging of
+    link cells and the outlet plane), flags, LES velocities and outlet state
+    of its workspace, the force ring, plus the FP64 initial state built
+    during set-up."""
     Q = 9 if case.dims == 2 else 19
     cells = case.nx * case.ny * case.nz
     cs = (cells + 63) // 64 * 64
     sb = {"fp32": 4, "fp64": 8, "fp16s": 2, "bf16s": 2}[case.precision]
     rb = 8 if case.precision == "fp64" else 4
-    ws = 2 * Q * cs * sb + cs + 32 + 8 * (cs // 32 + 64)
+    nbuf = 1 if layout == "aa" else 2
+    ws = nbuf * Q * cs * sb + cs + 32 + 8 * (cs // 32 + 64)
+    if layout == "aa":
+        # link-cell staging (an upper bound: every cell of the obstacle's
+        # bounding box a link cell) and the outlet plane
+        box = int(2 * case.size + 4) ** case.dims
+        ws += 2 * Q * rb * min(box, cells) + Q * rb * case.ny * case.nz
     ws += (3 * cs * rb if case.les and case.collision != "mrt" else 0)
     ws += 2 * 20 * case.ny * case.nz * rb + 96 * hist_capacity + (1 << 20)
     staging = Q * cells * 8 * 2
@@ -130,14 +139,29 @@ def _cells(case: Case) -> int:
     return case.nx * case.ny * case.nz
 
 
+# Requests of at least this many cells step in the batch on their own
+# kernels, which is what lets them take the AA layout there.
+AA_MIN_CELLS = 1 << 20
+
+
 class Server:
     """Continuous batching of wind-tunnel cases on one device."""
 
     def __init__(self, hbm_cap: float = 150e9, max_members: int = 256, chunk: int = 200,
                  window: int = 2000, tol: float = 1e-3, device=None, hist_capacity: int = 4096,
-                 on_admit=None, admit_per_round: int = 64, on_round=None, admit_idle: int = 8):
+                 on_admit=None, admit_per_round: int = 64, on_round=None, admit_idle: int = 8,
+                 layout: str = "auto"):
         if window > hist_capacity:
             raise ValueError("the convergence window must fit the force history ring")
+        if layout not in ("ab", "aa", "auto"):
+            raise ValueError(f"Unknown layout '{layout}'. Choose 'ab', 'aa' or 'auto'.")
+        # population layout of the requests large enough to step on their own
+        # kernels in the batch (AA_MIN_CELLS; smaller ones always take two
+        # buffers): "ab", "aa" (one buffer updated in place, half the
+        # population memory, 0.9x the rate), or "auto": "aa" only for a
+        # request whose two-buffer footprint does not fit beside the running
+        # ones while its one-buffer footprint does
+        self.layout = layout
         self.hbm_cap = float(hbm_cap)
         self.max_members = int(max_members)
         self.chunk = int(chunk)
@@ -184,6 +208,7 @@ class Server:
         active: List[tuple] = []     # (case, solver, admitted, bytes), join order = batch order
         results: List[Result] = []
         used = 0
+        aa_admitted = 0
         cell_steps = 0
         setup_s = 0.0
         wait_s = 0.0
@@ -212,7 +237,13 @@ class Server:
             while (queue and len(active) + len(joining) < self.max_members and len(joining) < cap
                    and (budget is None or not joining or clock() - t_launch + (setup_avg or 0.0) <= budget)):
                 c = queue[0]
+                layout = "ab"
                 need = footprint(c, self.hist_capacity)
+                if _cells(c) >= AA_MIN_CELLS and self.layout != "ab":
+                    need_aa = footprint(c, self.hist_capacity, "aa")
+                    if self.layout == "aa" or (used + need > self.hbm_cap and used + need_aa <= self.hbm_cap) \
+                            or need > self.hbm_cap >= need_aa:
+                        layout, need = "aa", need_aa
                 if need > self.hbm_cap:
                     queue.pop(0)
                     t = clock() - t0
@@ -224,10 +255,11 @@ class Server:
                 queue.pop(0)
                 ts = clock()
                 with torch.cuda.stream(side):
-                    s = make_solver(c, self.device, self.hist_capacity)
+                    s = make_solver(c, self.device, self.hist_capacity, layout)
                     if self.on_admit is not None:
                         self.on_admit(c, s)
                         s._flush_host_state()
+                aa_admitted += layout == "aa"
                 dt = clock() - ts
                 setup_s += dt
                 setup_avg = dt if setup_avg is None else 0.8 * setup_avg + 0.2 * dt
@@ -277,7 +309,7 @@ class Server:
         wall = clock() - t0
         self.stats = {"wall_s": wall, "rounds": rounds, "cell_steps": float(cell_steps),
                       "mlups": cell_steps / wall / 1e6 if wall > 0 else 0.0,
-                      "setup_s": setup_s, "gpu_wait_s": wait_s}
+                      "setup_s": setup_s, "gpu_wait_s": wait_s, "aa_admitted": aa_admitted}
         return results
 
     def close(self):

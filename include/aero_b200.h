@@ -293,7 +293,11 @@ AERO_API int aero_batch_bind_workspace(AeroBatch *batch, void *device_ptr, uint6
 /* Adds a bound lattice whose state is set.  cd_norm is the drag
  * normalisation used by aero_batch_converge: Cd = Fx / cd_norm (the
  * reference's 0.5 rho0 u0^2 D in 2D, forces.py:78-103, and 0.5 rho0 u0^2 D^2
- * in 3D, forces3d.py:70-101). */
+ * in 3D, forces3d.py:70-101).  A lattice of at least 2^20 cells steps on
+ * its own kernels as a branch of the batch step; only such a lattice may be
+ * in the AA layout (AERO_ERR_UNSUPPORTED otherwise): each aero_batch_step
+ * then collides the state it stored and ends on a state-storing step, as
+ * aero_step does. */
 AERO_API int aero_batch_add(AeroBatch *batch, AeroLattice *lat, double cd_norm);
 /* Removes a member; it can then be stepped, read or destroyed on its own. */
 AERO_API int aero_batch_remove(AeroBatch *batch, AeroLattice *lat);

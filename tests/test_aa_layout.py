@@ -139,7 +139,9 @@ def test_aa_halves_population_memory():
     assert b._engine.workspace_bytes - a._engine.workspace_bytes >= 0.9 * one_buffer
 
 
-def test_aa_refuses_other_kernels_and_batches():
+def test_aa_refuses_other_kernels_and_small_batch_members():
+    """The AA layout takes the per-cell step kernel only, and joins a batch
+    only with at least 2^20 cells (tests/test_batch.py covers that case)."""
     from aero_b200 import Batch
     from aero_b200._lib import AeroError
     s = _sphere("fp16s", "aa")

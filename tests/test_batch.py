@@ -246,3 +246,48 @@ def test_large_members_step_on_their_own_kernels():
         b.remove(s)
         np.testing.assert_array_equal(s.f, alone.f)
         b.close()
+
+
+@pytest.mark.gpu
+def test_large_aa_member_steps_in_the_batch_as_alone():
+    """A lattice in the AA layout joins a batch when it has at least 2^20
+    cells, and then steps on its own kernels as a branch of the batch step.
+    Each batch call first collides the state the member's previous call
+    stored and ends on a state-storing step, as a call of its own does, so
+    populations and drag equal those of the same lattice stepped alone in
+    the AA layout with calls of the same lengths (10, 15 and 1 steps), bit
+    for bit.  A smaller AA lattice is refused."""
+    from aero_b200 import Batch, Solver3D, Sphere
+    from aero_b200._lib import AeroError
+    makes = _cases()[:3]
+
+    def big():
+        nz, ny, nx = 96, 96, 128  # 1,179,648 cells
+        sph = Sphere(radius=8, cx_frac=0.3, cy_frac=0.5, cz_frac=0.5)
+        solid, phi = sph.mark_solid(nz, ny, nx), sph.sdf_field(nz, ny, nx)
+        return Solver3D(Nz=nz, Ny=ny, Nx=nx, solid=solid, omega=1 / 0.6, u0=0.05, D=16.0, collision="mrt",
+                        bouzidi=True, phi=phi, wall_bc="slip", outlet_bc="convective", sponge_thickness=8,
+                        precision="fp32", layout="aa")
+
+    calls = (10, 15, 1)
+    alone = big()
+    for n in calls:
+        r = alone.run(n, check_every=n + 1, verbose=False)
+    b = Batch(max_members=8)
+    mix = [m() for m in makes]
+    s = big()
+    for x in mix[:1] + [s] + mix[1:]:
+        b.add(x)
+    for n in calls:
+        b.step(n)
+    cd = s._coefficients(s._engine.read_forces())["Cd"]
+    np.testing.assert_array_equal(cd, np.array(r["Cd_history"]))
+    b.remove(s)
+    np.testing.assert_array_equal(s.f, alone.f)
+    b.close()
+    small = Solver3D(Nz=16, Ny=18, Nx=40, solid=np.zeros((16, 18, 40), bool), omega=1 / 0.6, u0=0.05, D=4.0,
+                     layout="aa")
+    b = Batch(max_members=2)
+    with pytest.raises(AeroError):
+        b.add(small)
+    b.close()

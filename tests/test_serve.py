@@ -70,6 +70,16 @@ def test_footprint_bounds_the_workspace():
         assert lib.aero_workspace_size(h, ctypes.byref(nb)) == 0
         assert serve.footprint(c) >= nb.value
         lib.aero_destroy(h)
+        # the same lattice in the AA layout: one population buffer plus staging
+        P.layout = 1
+        assert lib.aero_create(ctypes.byref(P), ctypes.byref(h)) == 0
+        assert lib.aero_set_geometry(h, s8.ctypes.data, links.ctypes.data if len(links) else None,
+                                     q.ctypes.data if len(q) else None, len(links), None) == 0
+        na = ctypes.c_uint64()
+        assert lib.aero_workspace_size(h, ctypes.byref(na)) == 0
+        assert na.value < nb.value
+        assert serve.footprint(c) > serve.footprint(c, layout="aa") >= na.value
+        lib.aero_destroy(h)
 
 
 def _small_cases():
@@ -164,6 +174,90 @@ def test_oversized_request_is_rejected_without_gpu_work(monkeypatch):
     srv = serve.Server(hbm_cap=1e6, max_members=4, chunk=10, window=10)
     (r,) = srv.run([serve.Case(0, 3, 128, 64, 64)])
     assert r.status == "rejected" and r.steps == 0
+
+
+def test_admission_takes_the_aa_layout_when_two_buffers_do_not_fit(monkeypatch):
+    """layout="auto": a request of at least 2^20 cells whose two-buffer
+    footprint does not fit beside the running requests, while its one-buffer
+    footprint does, is built in the AA layout; smaller requests and requests
+    that fit keep two buffers; layout="aa" builds every large request in it.
+    Checked with a fake batch and fake solvers, no GPU."""
+    import sys
+    import types
+    built = []
+
+    class FakeBatch:
+        def __init__(self, *a, **k):
+            self.device = None
+            self.members = []
+
+        def add(self, s):
+            self.members.append(s)
+
+        def remove(self, s):
+            self.members.remove(s)
+
+        def step(self, n):
+            pass
+
+        def converge(self, window, tol):
+            rows = np.zeros((len(self.members), len(serve.CONVERGE_FIELDS)))
+            rows[:, serve._F["converged"]] = 1.0
+            return rows
+
+        def close(self):
+            pass
+
+    monkeypatch.setattr(serve, "Batch", FakeBatch)
+    monkeypatch.setattr(serve, "make_solver", lambda c, dev, hist, layout="ab": built.append((c.id, layout)) or object())
+    fake_torch = types.SimpleNamespace(cuda=types.SimpleNamespace(
+        synchronize=lambda d=None: None, Stream=lambda d=None: None, stream=lambda st: _Null()))
+    monkeypatch.setitem(sys.modules, "torch", fake_torch)
+    big = serve.Case(0, 3, 128, 96, 96, shape="sphere", size=8)      # 1,179,648 cells
+    small = serve.Case(1, 3, 64, 32, 32, shape="sphere", size=4)     # 65,536 cells
+    ab, aa = serve.footprint(big), serve.footprint(big, layout="aa")
+    assert aa < ab
+    for layout, cap, want in (("auto", 10 * ab, "ab"), ("auto", (ab + aa) / 2, "aa"), ("aa", 10 * ab, "aa"),
+                              ("ab", (ab + aa) / 2, None)):
+        built.clear()
+        srv = serve.Server(hbm_cap=cap, max_members=4, chunk=10, window=10, layout=layout)
+        res = {r.id: r for r in srv.run([big, small])}
+        assert dict(built).get(1) == "ab"
+        if want is None:
+            assert res[0].status == "rejected" and 0 not in dict(built)
+        else:
+            assert dict(built)[0] == want and res[0].status == "converged"
+            assert srv.stats["aa_admitted"] == (want == "aa")
+    with pytest.raises(ValueError):
+        serve.Server(layout="ba")
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+@pytest.mark.gpu
+def test_aa_requests_serve_like_two_buffer_ones():
+    """A large request served in the AA layout (in the batch beside small
+    two-buffer requests) reaches the verdict and step count of the same
+    request served with two buffers, drag within FP32 rounding."""
+    cases = lambda: [serve.Case(0, 3, 128, 96, 96, shape="sphere", size=8, Re=40, collision="mrt", max_steps=150),
+                     serve.Case(1, 2, 96, 48, shape="cylinder", size=5, Re=30, collision="bgk", max_steps=150)]
+    out = {}
+    for layout in ("ab", "aa"):
+        srv = serve.Server(hbm_cap=8e9, max_members=4, chunk=50, window=100, tol=2e-3, layout=layout)
+        out[layout] = {r.id: r for r in srv.run(cases())}
+        assert srv.stats["aa_admitted"] == (layout == "aa")
+        srv.close()
+    for k, a in out["ab"].items():
+        b = out["aa"][k]
+        assert (a.status, a.steps) == (b.status, b.steps)
+        if math.isfinite(a.cd_mean) and a.cd_mean != 0.0:
+            assert abs(a.cd_mean - b.cd_mean) <= 1e-5 * abs(a.cd_mean)
 
 
 @pytest.mark.gpu
@@ -267,7 +361,7 @@ def test_admission_is_budgeted_by_the_chunk_time(monkeypatch):
         def close(self):
             pass
 
-    def fake_solver(case, device=None, hist_capacity=4096):
+    def fake_solver(case, device=None, hist_capacity=4096, layout="ab"):
         t[0] += 0.004  # set-up time of one request
         return types.SimpleNamespace(case=case)
 
