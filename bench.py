@@ -656,15 +656,19 @@ def measure_lattice(w, precision, args, dev, rank=0, world=1, dist=None, e2e=Tru
     plan["les_fused"] = eng.les_fused()
     if tune is not None:
         plan["autotune_ms_per_step"] = {str(k): v for k, v in tune["ms_per_step"].items()}
-    kname = "k_step_tiled" if plan["tiled"] else {4: "k_step_pair", 5: "k_step_quad"}.get(plan["kernel_id"], "k_step")
+    kname = "k_step_tiled" if plan["tiled"] else {4: "k_step_pair", 5: "k_step_quad",
+                                                  6: "k_step_les"}.get(plan["kernel_id"], "k_step")
+    if kname == "k_step" and s.layout == "aa":
+        kname = "k_step_aa"
     # DRAM bytes per launch from the committed ncu summary of this kernel,
     # workload and precision (a smaller case scaled by cells where the summary
     # says so); None when no capture covers it
     traffic = None
     pat = re.compile(rf"^- {re.escape(args.workload)}: dram bytes per launch = (\d+)\s*$", re.M)
+    others = ("k_step_tiled", "k_step_pair", "k_step_quad", "k_step_les", "k_step_aa", "k_step_batch")
     for md in sorted((ROOT / "profiles").glob(f"{kname}_*_{precision}.md")):
-        if kname == "k_step" and md.name.startswith(("k_step_tiled", "k_step_pair", "k_step_quad")):
-            continue
+        if any(md.name.startswith(o + "_") for o in others if o != kname and o.startswith(kname)):
+            continue  # a summary of another kernel whose name extends this one
         m = pat.search(md.read_text())
         if m:
             traffic = int(m.group(1))
@@ -679,6 +683,7 @@ def measure_lattice(w, precision, args, dev, rank=0, world=1, dist=None, e2e=Tru
                          else ", two cells per thread on packed FP32 arithmetic)" if plan["kernel_id"] == 4
                          else ", four cells per thread, 8-byte loads realigned by warp shuffles)"
                          if plan["kernel_id"] == 5
+                         else ", BGK/TRT with the LES velocity stencil in shared memory)" if plan["kernel_id"] == 6
                          else ", per-cell global gather, blocks " + ("128x1", "256x1", "32x4")[plan["kernel_id"]]
                          + ")"),
                      "step_plan": plan, "alg_bytes_per_launch": bpc * ncells, "bytes_per_cell": bpc,
