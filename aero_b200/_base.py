@@ -12,6 +12,7 @@ per-step forces kept in a device ring and read back in chunks.
 from __future__ import annotations
 
 import json
+import os
 import pathlib
 import threading
 import time
@@ -559,13 +560,12 @@ class LatticeSolverBase:
 
 
 class _HostBuffer:
-    """A float64 host array for run()'s result fields whose pages a daemon
-    thread touches in the background while the GPU steps, 16 MiB at a time.
-    get() stops the thread after its current chunk and hands the array over
-    however far it got: the read-back faults in the rest from several host
-    threads, faster than one thread would (a 1 GB result: about 115 ms for
-    one thread to touch, 30 ms to copy into touched pages, 50 ms into fresh
-    ones)."""
+    """A float64 host array for run()'s result fields whose pages helper
+    threads touch in the background while the GPU steps, 16 MiB chunks dealt
+    round-robin to up to 8 threads (the page faults of a fresh array are the
+    cost: one thread needs about 115 ms per GB).  get() stops the helpers
+    after their current chunks and hands the array over however far they
+    got; the read-back faults in the rest from torch's threads."""
 
     _CHUNK = 1 << 21  # float64 values (16 MiB)
 
@@ -573,17 +573,20 @@ class _HostBuffer:
         self.shape = tuple(shape)
         self._a = np.empty(self.shape)
         self._stop = threading.Event()
-        self._t = threading.Thread(target=self._fill, daemon=True)
-        self._t.start()
+        n = max(1, min(8, (os.cpu_count() or 1) // 2))
+        self._t = [threading.Thread(target=self._fill, args=(k, n), daemon=True) for k in range(n)]
+        for t in self._t:
+            t.start()
 
-    def _fill(self):
+    def _fill(self, k, n):
         flat = self._a.reshape(-1)
-        for off in range(0, flat.size, self._CHUNK):
+        for off in range(k * self._CHUNK, flat.size, n * self._CHUNK):
             if self._stop.is_set():
                 return
             flat[off:off + self._CHUNK:512] = 0.0  # one write per 4 KiB page
 
     def get(self):
         self._stop.set()
-        self._t.join()
+        for t in self._t:
+            t.join()
         return self._a
