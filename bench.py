@@ -541,6 +541,60 @@ def scalar_precision_check(w, args, dev, tau=0.8, steps=2000, formats=("fp32", "
     return out
 
 
+def sphere_precision_check(w, args, dev, tau=0.8, bouzidi=True, steps=6000, window=2000,
+                           formats=("fp32", "fp16s", "bf16s")):
+    """The sphere configuration in each storage format against the FP64
+    engine where the flow is stable.  The configuration's tau 0.5048
+    diverges, and so does every tau up to 0.6 with the reference's Bouzidi
+    rule (half-way bounce-back is stable at 0.56): the configuration's
+    geometry, MRT + Smagorinsky, Bouzidi or half-way bounce-back, slip walls,
+    sponge and seeded +-1% inflow perturbation (seed 1234), `steps` steps.
+    Reports per format the
+    mean Cd and the mean lift coefficients over the last `window` steps and
+    their differences to FP64, the centreline wake profile ux(x, ny/2, nz/2)
+    behind the sphere (relative L2 to FP64), and the mass (FP64 sum on the
+    device) relative to FP64."""
+    import numpy as np
+    import torch
+    wk = dict(w, nu=(tau - 0.5) / 3.0, kwargs=dict(w["kwargs"], bouzidi=bouzidi))
+    g = _geometry(wk)
+    D = g.reference_length()
+    x0 = int(wk["shape"][2] * wk["nx"] + wk["shape"][1]) + 2  # first plane behind the sphere
+    out = {"tau": tau, "bouzidi": bouzidi, "steps": steps, "window": window, "nu": wk["nu"],
+           "Re": wk["u0"] * D / wk["nu"],
+           "desc": "configuration 2 at tau %.2f with %s, seeded +-1%% inflow perturbation"
+                   % (tau, "Bouzidi" if bouzidi else "half-way bounce-back")}
+    ref = None
+    for prec in ("fp64",) + tuple(formats):
+        s = _build_solver(wk, prec, dev, steps, 0)
+        ux0, uy0, T0 = _initial_fields(wk, dev, 0, s)
+        s.set_equilibrium_state(ux=ux0, uy=uy0, T=T0)
+        t0 = time.perf_counter()
+        c = s._coefficients(s._advance(steps))
+        torch.cuda.synchronize(dev)
+        dt = time.perf_counter() - t0
+        m = s._engine.macroscopic_device()
+        wake = m[1, wk["nz"] // 2, wk["ny"] // 2, x0:].cpu().numpy()
+        mass = s.field_statistics()["mass"]
+        rec = {"Cd_mean": float(np.mean(c["Cd"][-window:])), "Cly_mean": float(np.mean(c["Cly"][-window:])),
+               "Clz_mean": float(np.mean(c["Clz"][-window:])), "mass": mass, "status": s.status(),
+               "seconds": dt}
+        if ref is None:
+            ref = dict(rec, wake=wake, Cd=c["Cd"][-window:], Cly=c["Cly"][-window:])
+        else:
+            rec["Cd_rel_err_vs_fp64"] = abs(rec["Cd_mean"] - ref["Cd_mean"]) / abs(ref["Cd_mean"])
+            rec["Cly_mean_abs_err_vs_fp64"] = abs(rec["Cly_mean"] - ref["Cly_mean"])
+            rec["Clz_mean_abs_err_vs_fp64"] = abs(rec["Clz_mean"] - ref["Clz_mean"])
+            rec["Cd_history_max_rel_err_vs_fp64"] = float(np.max(np.abs(c["Cd"][-window:] - ref["Cd"]))
+                                                          / abs(ref["Cd_mean"]))
+            rec["wake_rel_l2_vs_fp64"] = float(np.linalg.norm(wake - ref["wake"]) / np.linalg.norm(ref["wake"]))
+            rec["mass_err_vs_fp64"] = abs(mass - ref["mass"]) / ref["mass"]
+        out[prec] = rec
+        del s, m
+        torch.cuda.empty_cache()
+    return out
+
+
 ROOFLINE_STEPS = 1000  # event-timed steps of the kernel phase (about a second at sphere512)
 
 
@@ -747,6 +801,9 @@ def main():
                          "(ab when it fits the free device memory, else aa)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-scalar-check", action="store_true", help="box256: skip the storage-format check")
+    ap.add_argument("--sphere-check", action="store_true",
+                    help="sphere workloads: add the storage formats' Cd / lift / wake / mass against FP64 at a "
+                         "stable relaxation time (about a minute at sphere512)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--collision", default=None, choices=["bgk", "trt", "mrt"],
                     help="override the workload's collision operator (profiling)")
@@ -805,6 +862,9 @@ def main():
     extra = {}
     if args.workload == "box256" and not args.no_scalar_check:
         extra["scalar_check"] = scalar_precision_check(w, args, dev)
+    if args.sphere_check and args.workload in ("sphere512", "sphere256"):
+        extra["sphere_check"] = [sphere_precision_check(w, args, dev, tau=0.8, bouzidi=True),
+                                 sphere_precision_check(w, args, dev, tau=0.56, bouzidi=False)]
     del s
     torch.cuda.empty_cache()
 
