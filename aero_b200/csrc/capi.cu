@@ -51,7 +51,8 @@ uint64_t align_up(uint64_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
 struct Layout {
   uint64_t P[2], flags, lbits, loff, lc_mask, lc_q, lc_cell, lc_contrib, fin_partial, prof_off, force_const, prof_const,
-      prev[2], g[2], U, cs_cell, inflow, recycle, hist, prof_out, counters, stats, stage_link, stage_nb, stage_out, total;
+      prev[2], g[2], U, cs_cell, inflow, recycle, hist, prof_out, counters, stats, stage_link, stage_nb, stage_out,
+      lc_contrib2, run_params, total;
 };
 
 struct WTab {
@@ -154,6 +155,10 @@ struct AeroLattice {
   int les_chunk = 0;       // planes per block of k_step_les
   int tile_blocks = 0, tile_rows = 0, tiles_per_plane = 0, ntiles = 0;
   uint32_t tile_extra_tx = 0;  // AERO_B200_TEST_STALL_TILES=1 at bind: stages never complete
+  // persistent runs (k_run_small) for small lattices; run_stall_block >= 0
+  // only under AERO_B200_TEST_STALL_RUN=1 at bind (that block leaves early)
+  bool persistent = true;
+  int run_stall_block = -1;
   // optional per-kernel event timing (eager launches only)
   bool timing = false;
   std::vector<cudaEvent_t> ev;  // 4 events per timed step
@@ -419,6 +424,31 @@ int aa_collide_state(AeroLattice *L, cudaStream_t st) {
   return AERO_OK;
 }
 
+// Lattices stepped by the persistent runner: small (its point is the launch
+// and drain per step that dominate such a lattice), two buffers, the
+// per-cell step kernel, and no pass before the step (the LES moments pass of
+// BGK / TRT, the recycling mean).
+constexpr int64_t kRunSmallCells = (int64_t)1 << 19;
+bool run_small_ok(const AeroLattice *L) {
+  return L->persistent && !L->aa && !L->batch && !L->timing && !L->tiled && !L->pair && !L->quad &&
+         !L->les_fused && L->ncells <= kRunSmallCells && !(les_active(L) && L->prm.collision != AERO_MRT) &&
+         !(L->feat & FEAT_RECYCLE);
+}
+
+template <class Real>
+int launch_run_small(AeroLattice *L, int64_t n, cudaStream_t st) {
+  StepParams<Real> pp[2] = {make_params<Real>(L, L->cur), make_params<Real>(L, 1 - L->cur)};
+  pp[1].lc_contrib = reinterpret_cast<double *>(L->ws + L->lay.lc_contrib2);
+  auto *dpp = reinterpret_cast<StepParams<Real> *>(L->ws + L->lay.run_params);
+  // from pageable memory: the copy is staged before the call returns
+  CUDA_TRY(cudaMemcpyAsync(dpp, pp, sizeof(pp), cudaMemcpyHostToDevice, st));
+  int64_t *ctr = reinterpret_cast<int64_t *>(L->ws + L->lay.counters);
+  CUDA_TRY(cudaMemsetAsync(ctr + 6, 0, 4, st));  // barrier arrivals
+  const cudaError_t e = get_ops<Real>(L)->run_small(dpp, L->ncells, n, L->run_stall_block, st);
+  if (e != cudaSuccess) return fail(AERO_ERR_CUDA, "persistent run: %s", cudaGetErrorString(e));
+  return AERO_OK;
+}
+
 template <class Real>
 int build_pair_graph(AeroLattice *L, int cur) {
   if (!L->cap_stream) CUDA_TRY(cudaStreamCreateWithFlags(&L->cap_stream, cudaStreamNonBlocking));
@@ -440,6 +470,18 @@ int build_pair_graph(AeroLattice *L, int cur) {
 
 template <class Real>
 int do_steps(AeroLattice *L, int64_t n, cudaStream_t st) {
+  if (n >= 2 && run_small_ok(L)) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CUDA_TRY(cudaStreamIsCapturing(st, &cap));
+    if (cap == cudaStreamCaptureStatusNone) {
+      const int rc = launch_run_small<Real>(L, n, st);
+      if (rc != AERO_OK) return rc;
+      L->cur ^= (int)(n & 1);
+      L->step_count += n;
+      L->old_is_state = false;
+      return AERO_OK;
+    }
+  }
   if (L->aa && n > 0 && L->aa_holds_state) {
     const int rc = aa_collide_state<Real>(L, st);
     if (rc != AERO_OK) return rc;
@@ -855,6 +897,9 @@ int aero_set_geometry(AeroLattice *L, const uint8_t *solid, const int32_t *links
   y.stage_link = take(L->aa ? rb * L->Q * nlc : 0);
   y.stage_nb = take((L->aa && (L->feat & FEAT_BOUZIDI)) ? rb * L->Q * nlc : 0);
   y.stage_out = take((L->aa && aa_stages_outlet(L)) ? rb * L->Q * (uint64_t)L->prev_plane : 0);
+  // persistent runs: the odd steps' force terms and the two parameter sets
+  y.lc_contrib2 = take(96 * nlc);
+  y.run_params = take(2 * (is_f64(L) ? sizeof(StepParams<double>) : sizeof(StepParams<float>)));
   y.total = o;
   L->geometry = true;
   return AERO_OK;
@@ -918,6 +963,10 @@ int aero_bind_workspace(AeroLattice *L, void *dptr, uint64_t bytes, void *stream
   // give up after their limit, raise status bit 1 and the kernel returns.
   const char *stall = std::getenv("AERO_B200_TEST_STALL_TILES");
   L->tile_extra_tx = (stall && stall[0] == '1') ? 16u : 0u;
+  // Test of the bounded barrier of persistent runs: cell block 1 leaves
+  // before its first barrier, so the others' waits give up after their limit.
+  const char *rstall = std::getenv("AERO_B200_TEST_STALL_RUN");
+  L->run_stall_block = (rstall && rstall[0] == '1') ? 1 : -1;
   L->bound = true;
   return AERO_OK;
 }
@@ -1210,6 +1259,12 @@ int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
       cudaGraphExecDestroy(e);
       e = nullptr;
     }
+  return AERO_OK;
+}
+
+int aero_set_persistent(AeroLattice *L, int32_t enable) {
+  if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
+  L->persistent = enable != 0;
   return AERO_OK;
 }
 

@@ -69,6 +69,12 @@ struct Ops {
   cudaError_t (*aa_recycle_mean)(const StepParams<Real> &, cudaStream_t);
   cudaError_t (*aa_moments)(const StepParams<Real> &, dim3 grid, cudaStream_t);
   cudaError_t (*aa_step)(const StepParams<Real> &, dim3 grid, cudaStream_t);
+  // nsteps steps of a small lattice in one cooperative launch (k_run_small):
+  // pp (device) = the parameters of the call's even and odd steps; the grid
+  // is one finalisation block plus as many cell blocks as ncells needs and
+  // the device holds at once; stall_block is -1 (tests: a block that leaves)
+  cudaError_t (*run_small)(const StepParams<Real> *pp, int64_t ncells, int64_t nsteps, int stall_block,
+                           cudaStream_t);
   int store_bytes;
 };
 

@@ -1,6 +1,7 @@
 // lbm_inst.cuh -- explicit instantiation of the kernels for one storage type.
 // Included by lbm_inst_<storage>.cu with AERO_STORE / AERO_OPS_FN defined.
 #pragma once
+#include <algorithm>
 #include <type_traits>
 
 #include "lbm_dispatch.h"
@@ -202,11 +203,36 @@ struct Launch {
       k_step<L, S, COLL, false, kStepBlock, 1, true, 1><<<grid, kStepBlock, 0, st>>>(p);
     return cudaGetLastError();
   }
+  static cudaError_t run_small(const StepParams<Real> *pp, int64_t ncells, int64_t nsteps, int stall_block,
+                               cudaStream_t st) {
+    // resident blocks of this instantiation on the current device (every
+    // block of a cooperative launch must be resident at once)
+    static int per_sm = -1, sms = 0;
+    if (per_sm < 0) {
+      int dev = 0;
+      cudaError_t e = cudaGetDevice(&dev);
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_run_small<L, S, COLL>, kRunBlock, 0);
+      if (e != cudaSuccess) {
+        per_sm = -1;
+        return e;
+      }
+    }
+    const int64_t capacity = (int64_t)per_sm * sms;
+    if (capacity < 2) return cudaErrorCooperativeLaunchTooLarge;
+    // cell blocks: enough for one cell per thread, at most AERO_RUN_BLOCKS_PER_SM
+    // per SM (fewer arrivals at each grid barrier) and what stays resident
+    const int64_t cap = std::min<int64_t>(capacity - 1, (int64_t)AERO_RUN_BLOCKS_PER_SM * sms);
+    const int64_t cells = std::min<int64_t>((ncells + kRunBlock - 1) / kRunBlock, cap);
+    const dim3 grid((unsigned)(1 + cells));
+    void *args[] = {(void *)&pp, (void *)&nsteps, (void *)&stall_block};
+    return cudaLaunchCooperativeKernel((const void *)k_run_small<L, S, COLL>, grid, dim3(kRunBlock), args, 0, st);
+  }
   static constexpr Ops<Real> table = {&step,       &step_shaped, &moments,      &finalize,   &state_out,
                                       &load_state, &macro_out,   &step_tiled,   &tiled_setup, &step_batch,
                                       &moments_batch, &finalize_batch, &recycle_mean, &step_pair,
                                       &step_batch_pair, &field_stats, &init_eq, &step_quad, &step_les, &les_setup, &aa_stage,
-                                      &aa_recycle_mean, &aa_moments, &aa_step, (int)sizeof(S)};
+                                      &aa_recycle_mean, &aa_moments, &aa_step, &run_small, (int)sizeof(S)};
 };
 
 template <class S>

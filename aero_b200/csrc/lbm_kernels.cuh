@@ -1628,10 +1628,12 @@ __global__ void __launch_bounds__(kRecycleBlock) k_recycle_mean(const StepParams
 // order and stores 12 partial sums; the block that finishes last adds the
 // partials in block order, so the result does not depend on block timing.
 // Block `bid` of `nblocks` finalisation blocks of one lattice.
+// Finalisation block `bid`: the fixed-order FP64 sums of its chunk of the
+// link cells' force terms into fin_partial[bid].  Ends on a block barrier,
+// so a block may call it for several chunks in turn.
 template <class Real>
-__device__ __forceinline__ void finalize_block(const StepParams<Real> &p, int bid, int nblocks) {
+__device__ __forceinline__ void finalize_partial(const StepParams<Real> &p, int bid) {
   __shared__ double sm[12][kFinalizeBlock / 32];
-  __shared__ bool last;
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   const int64_t n = p.n_lc;
   const int64_t k0 = (int64_t)bid * p.fin_chunk;
@@ -1659,10 +1661,15 @@ __device__ __forceinline__ void finalize_block(const StepParams<Real> &p, int bi
     __threadfence();
   }
   __syncthreads();
-  if (t == 0) last = atomicAdd(p.fin_ticket, 1u) == (unsigned)nblocks - 1;
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
+}
+
+// The step's totals from the nblocks partials (in block order) plus the
+// rest-weight part, into the history ring; the force profile on the step the
+// call asked for; then the device step counter advances.
+template <class Real>
+__device__ __forceinline__ void finalize_total(const StepParams<Real> &p, int nblocks) {
+  const int t = threadIdx.x;
+  const int64_t n = p.n_lc;
   const int64_t step = *p.step;
   const int64_t slot = (step - *p.hist_base) % p.hist_cap;
   if (t < 12) {
@@ -1688,6 +1695,17 @@ __device__ __forceinline__ void finalize_block(const StepParams<Real> &p, int bi
     *p.fin_ticket = 0u;
     *p.step = step + 1;
   }
+}
+
+template <class Real>
+__device__ __forceinline__ void finalize_block(const StepParams<Real> &p, int bid, int nblocks) {
+  __shared__ bool last;
+  finalize_partial(p, bid);
+  if (threadIdx.x == 0) last = atomicAdd(p.fin_ticket, 1u) == (unsigned)nblocks - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  finalize_total(p, nblocks);
 }
 
 template <class Real>
@@ -2071,6 +2089,104 @@ __global__ void __launch_bounds__(kStepBlock) k_load_state(const StepParams<type
     constexpr int i = decltype(ic)::value;
     SO::template store<i, L>(dst, own_elem<L, i>(p, x, y, z, c), (Real)(in[(int64_t)i * p.ncells + c] - Dir<L, i>::w));
   });
+}
+
+// --------------------------------------------------------------------------
+// Persistent run of a small lattice: one cooperative launch takes all steps
+// of an aero_step call, so a lattice whose step is a few microseconds of work
+// stops paying a kernel launch and a grid drain per step and per force
+// finalisation.  Blocks 1.. take the cells (grid-stride over the cells in C
+// order, the per-cell step of k_step), block 0 finalises: after the barrier
+// that ends step s it sums step s's link-cell force terms (the chunks and
+// order of k_finalize, so the history is the same bit for bit) while the
+// other blocks compute step s + 1.  Consecutive steps write their force terms
+// to alternate buffers (the parameter sets of the two steps of a pair carry
+// the two pointers), and block 0 reaches the barrier of step s + 1 only after
+// that finalisation, so step s + 2 cannot overwrite terms still being read.
+// The grid barrier is bounded: a block that waits more than kWaitNs sets
+// STATUS_WAIT_TIMEOUT and returns, and so do the others at their next wait.
+// --------------------------------------------------------------------------
+constexpr int kRunBlock = kFinalizeBlock;  // block 0 runs the finalisation code, built for this width
+#ifndef AERO_RUN_BLOCKS_PER_SM
+#define AERO_RUN_BLOCKS_PER_SM 3
+#endif
+constexpr int kRunMinBlocks = 3;  // 85 registers (FP64 arithmetic: 2 blocks, 128)
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *q) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(q) : "memory");
+  return v;
+}
+
+// bar[0]: arrivals at the current barrier (zeroed by the host before the
+// launch), bar[1]: the barrier generation.  gen holds, in thread 0, the
+// generation this block last saw complete.
+__device__ __forceinline__ bool run_barrier(uint32_t *bar, uint32_t nblocks, uint32_t &gen, uint32_t *status) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    const uint32_t g = gen;
+    if (atomicAdd(bar, 1u) == nblocks - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicExch(bar + 1, g + 1u);
+    } else {
+      const uint64_t t0 = global_ns();
+      while (ld_acquire_u32(bar + 1) == g) {
+        __nanosleep(32);
+        if (global_ns() - t0 > kWaitNs) {
+          ok = 0;
+          atomicOr(status, (uint32_t)STATUS_WAIT_TIMEOUT);
+          break;
+        }
+      }
+    }
+    __threadfence();
+    gen = g + 1u;
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+// pp[0], pp[1]: the parameters of even and odd steps of the call (buffer
+// parities cur and 1 - cur, force terms in alternate buffers).  stall_block
+// (tests only, else -1): that block leaves before its first barrier, so the
+// others' bounded wait runs out.
+template <class L, class S, int COLL>
+__global__ void __launch_bounds__(kRunBlock, sizeof(typename StoreOps<S>::Real) == 4 ? kRunMinBlocks : 2)
+    k_run_small(const StepParams<typename StoreOps<S>::Real> *__restrict__ pp, int64_t nsteps, int stall_block) {
+  using Real = typename StoreOps<S>::Real;
+  __shared__ StepParams<Real> sp2[2];  // both parameter sets, loaded once
+  uint32_t *bar = reinterpret_cast<uint32_t *>(pp[0].step + 6);
+  const uint32_t nb = gridDim.x;
+  uint32_t gen = 0;
+  if (threadIdx.x == 0) gen = ld_acquire_u32(bar + 1);
+  // the call's first step; block 0 advances the counter only after the
+  // first barrier, which every block reaches after this read
+  const int64_t step0 = *pp[0].step;
+  const int64_t cstride = (int64_t)(nb - 1) * kRunBlock;
+  params_to_smem(sp2[0], pp);
+  params_to_smem(sp2[1], pp + 1);
+  for (int64_t s = 0; s < nsteps; ++s) {
+    const StepParams<Real> &sp = sp2[s & 1];
+    if (blockIdx.x != 0) {
+      if ((int)blockIdx.x == stall_block) return;
+      const int64_t step_now = step0 + s;
+      for (int64_t c = (int64_t)(blockIdx.x - 1) * kRunBlock + threadIdx.x; c < sp.ncells; c += cstride) {
+        const int64_t row = c / sp.nx;
+        const int x = (int)(c - row * sp.nx), y = (int)(row % sp.ny), z = (int)(row / sp.ny);
+        step_cell<L, S, COLL>(sp, x, y, z, step_now, GlobalGather<L, S, Real>{sp, y, z});
+      }
+    }
+    if (!run_barrier(bar, nb, gen, sp.status)) return;
+    if (blockIdx.x == 0) {
+      for (int b = 0; b < sp.fin_blocks; ++b) finalize_partial(sp, b);
+      finalize_total(sp, sp.fin_blocks);
+    }
+  }
 }
 
 }  // namespace aero

@@ -270,6 +270,11 @@ class Engine:
     def set_step_kernel(self, kernel: int) -> None:
         check("aero_set_step_kernel", self.lib.aero_set_step_kernel(self.h, int(kernel)))
 
+    def set_persistent(self, enable: bool) -> None:
+        """Persistent runs of small lattices (one cooperative launch per call;
+        on by default where the lattice qualifies, aero_set_persistent)."""
+        check("aero_set_persistent", self.lib.aero_set_persistent(self.h, 1 if enable else 0))
+
     def get_step_kernel(self) -> int:
         k = ctypes.c_int32()
         check("aero_get_step_kernel", self.lib.aero_get_step_kernel(self.h, ctypes.byref(k)))

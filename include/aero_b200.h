@@ -194,6 +194,16 @@ AERO_API int aero_step_plan(const AeroLattice *lat, int32_t *tiled, int32_t *til
 AERO_API int aero_set_step_kernel(AeroLattice *lat, int32_t kernel);
 AERO_API int aero_get_step_kernel(const AeroLattice *lat, int32_t *kernel);
 
+/* Persistent runs (no counterpart in the reference; on by default): a
+ * lattice of at most 2^19 cells in the two-buffer layout, stepped by the
+ * per-cell kernel with no pass before the step (no BGK/TRT LES, no recycling
+ * inlet), takes all steps of an aero_step call of two or more steps in one
+ * cooperative launch, its force finalisation overlapping the next step.  The
+ * results equal those of per-step launches bit for bit.  A bounded device
+ * barrier that gives up sets status bit 1 (aero_status).  enable = 0 keeps
+ * per-step launches (graphs).  Not used while the stream is capturing. */
+AERO_API int aero_set_persistent(AeroLattice *lat, int32_t enable);
+
 /* Inlet fields of steps first_step .. first_step+n_steps-1 for a lattice
  * with inflow_field set: `fields` (host) holds n_steps blocks of planes of
  * nz*ny doubles, (z, y) order.  Synthetic inflow: uy in 2D, uy then uz in

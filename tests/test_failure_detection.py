@@ -44,3 +44,29 @@ def test_tiled_stage_wait_gives_up_and_reports(monkeypatch):
     u = _sphere_solver()
     u.run(20, check_every=21, verbose=False)
     np.testing.assert_allclose(t.f, u.f, rtol=0, atol=1e-6 * np.abs(u.f).max())
+
+
+def test_persistent_barrier_wait_gives_up_and_reports(monkeypatch):
+    """AERO_B200_TEST_STALL_RUN=1 makes one cell block of the persistent
+    runner leave before its first grid barrier, so that barrier never
+    completes.  The other blocks' bounded waits give up after about a
+    second, the call returns with status bit 1, and a lattice built
+    afterwards steps normally on the same context."""
+    monkeypatch.setenv("AERO_B200_TEST_STALL_RUN", "1")
+    s = _sphere_solver()
+    t0 = time.perf_counter()
+    s._engine.step(4)
+    status = s._engine.status()  # synchronises the stream
+    dt = time.perf_counter() - t0
+    assert status & 2, status
+    assert dt < 30.0, dt
+    monkeypatch.delenv("AERO_B200_TEST_STALL_RUN")
+    t = _sphere_solver()
+    r = t.run(20, check_every=21, verbose=False)
+    assert t.status() == 0
+    assert np.isfinite(t.f).all() and np.isfinite(r["Cd_history"]).all()
+    u = _sphere_solver()
+    u._engine.set_persistent(False)
+    u.run(20, check_every=21, verbose=False)
+    # MRT: the two kernels round their FMAs differently
+    np.testing.assert_allclose(t.f, u.f, rtol=0, atol=1e-6 * np.abs(u.f).max())
