@@ -38,9 +38,10 @@ LAYOUTS = {"ab": 0, "aa": 1}
 def _check_layout(layout: str) -> None:
     """Population layout: "ab" (two buffers; every step kernel), "aa" (one
     buffer updated in place, the AA pattern: half the population memory; the
-    per-cell step kernel only; not in batches) or "auto" (the faster "ab"
-    when its workspace fits the device's free memory with headroom, else
-    "aa"; the choice is in the solver's `layout` attribute)."""
+    per-cell step kernel only; in batches with at least 2^20 cells) or
+    "auto" (the faster "ab" when its workspace fits the device's free memory
+    with headroom, else "aa"; the choice is in the solver's `layout`
+    attribute)."""
     if layout not in LAYOUTS and layout != "auto":
         raise ValueError(f"Unknown layout '{layout}'. Choose 'ab', 'aa' or 'auto'.")
 
