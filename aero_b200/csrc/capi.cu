@@ -443,9 +443,18 @@ int launch_run_small(AeroLattice *L, int64_t n, cudaStream_t st) {
   // from pageable memory: the copy is staged before the call returns
   CUDA_TRY(cudaMemcpyAsync(dpp, pp, sizeof(pp), cudaMemcpyHostToDevice, st));
   int64_t *ctr = reinterpret_cast<int64_t *>(L->ws + L->lay.counters);
-  CUDA_TRY(cudaMemsetAsync(ctr + 6, 0, 4, st));  // barrier arrivals
-  const cudaError_t e = get_ops<Real>(L)->run_small(dpp, L->ncells, n, L->run_stall_block, st);
-  if (e != cudaSuccess) return fail(AERO_ERR_CUDA, "persistent run: %s", cudaGetErrorString(e));
+  for (int64_t done = 0; done < n;) {
+    const int64_t k = std::min(n - done, kRunMaxSteps);
+    if (done > 0) {
+      // the next launch starts on the other parameter set when k was odd
+      if (k & 1) std::swap(pp[0], pp[1]);
+      CUDA_TRY(cudaMemcpyAsync(dpp, pp, sizeof(pp), cudaMemcpyHostToDevice, st));
+    }
+    CUDA_TRY(cudaMemsetAsync(ctr + 6, 0, 4, st));  // barrier arrivals
+    const cudaError_t e = get_ops<Real>(L)->run_small(dpp, L->ncells, k, L->run_stall_block, st);
+    if (e != cudaSuccess) return fail(AERO_ERR_CUDA, "persistent run: %s", cudaGetErrorString(e));
+    done += k;
+  }
   return AERO_OK;
 }
 
@@ -1265,6 +1274,12 @@ int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
 int aero_set_persistent(AeroLattice *L, int32_t enable) {
   if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
   L->persistent = enable != 0;
+  return AERO_OK;
+}
+
+int aero_get_persistent(const AeroLattice *L, int32_t *active) {
+  if (!L || !active) return fail(AERO_ERR_INVALID, "NULL argument");
+  *active = run_small_ok(L) ? 1 : 0;
   return AERO_OK;
 }
 

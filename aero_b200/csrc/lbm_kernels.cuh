@@ -2105,11 +2105,14 @@ __global__ void __launch_bounds__(kStepBlock) k_load_state(const StepParams<type
 // that finalisation, so step s + 2 cannot overwrite terms still being read.
 // The grid barrier is bounded: a block that waits more than kWaitNs sets
 // STATUS_WAIT_TIMEOUT and returns, and so do the others at their next wait.
+// A launch takes at most kRunMaxSteps steps (the arrival count stays below
+// 2^32); the host splits longer calls.
 // --------------------------------------------------------------------------
 constexpr int kRunBlock = kFinalizeBlock;  // block 0 runs the finalisation code, built for this width
 #ifndef AERO_RUN_BLOCKS_PER_SM
 #define AERO_RUN_BLOCKS_PER_SM 3
 #endif
+constexpr int64_t kRunMaxSteps = (int64_t)1 << 20;
 constexpr int kRunMinBlocks = 3;  // 85 registers (FP64 arithmetic: 2 blocks, 128)
 
 __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *q) {
@@ -2118,23 +2121,21 @@ __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *q) {
   return v;
 }
 
-// bar[0]: arrivals at the current barrier (zeroed by the host before the
-// launch), bar[1]: the barrier generation.  gen holds, in thread 0, the
-// generation this block last saw complete.
-__device__ __forceinline__ bool run_barrier(uint32_t *bar, uint32_t nblocks, uint32_t &gen, uint32_t *status) {
+// Barrier k of a launch completes when the arrival counter (zeroed by the
+// host before the launch) reaches (k + 1) * nblocks: each block adds one
+// after a fence over its writes, and waits, reading the counter with acquire
+// semantics, until it gets there; the last arrival releases the others with
+// its own increment.
+__device__ __forceinline__ bool run_barrier(uint32_t *count, uint32_t nblocks, uint32_t k, uint32_t *status) {
   __shared__ int ok_s;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
+    const uint32_t target = (k + 1u) * nblocks;
     __threadfence();
-    const uint32_t g = gen;
-    if (atomicAdd(bar, 1u) == nblocks - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicExch(bar + 1, g + 1u);
-    } else {
+    if (atomicAdd(count, 1u) + 1u < target) {
       const uint64_t t0 = global_ns();
-      while (ld_acquire_u32(bar + 1) == g) {
+      while (ld_acquire_u32(count) < target) {
         __nanosleep(32);
         if (global_ns() - t0 > kWaitNs) {
           ok = 0;
@@ -2144,7 +2145,6 @@ __device__ __forceinline__ bool run_barrier(uint32_t *bar, uint32_t nblocks, uin
       }
     }
     __threadfence();
-    gen = g + 1u;
     ok_s = ok;
   }
   __syncthreads();
@@ -2160,10 +2160,8 @@ __global__ void __launch_bounds__(kRunBlock, sizeof(typename StoreOps<S>::Real) 
     k_run_small(const StepParams<typename StoreOps<S>::Real> *__restrict__ pp, int64_t nsteps, int stall_block) {
   using Real = typename StoreOps<S>::Real;
   __shared__ StepParams<Real> sp2[2];  // both parameter sets, loaded once
-  uint32_t *bar = reinterpret_cast<uint32_t *>(pp[0].step + 6);
+  uint32_t *count = reinterpret_cast<uint32_t *>(pp[0].step + 6);
   const uint32_t nb = gridDim.x;
-  uint32_t gen = 0;
-  if (threadIdx.x == 0) gen = ld_acquire_u32(bar + 1);
   // the call's first step; block 0 advances the counter only after the
   // first barrier, which every block reaches after this read
   const int64_t step0 = *pp[0].step;
@@ -2181,7 +2179,7 @@ __global__ void __launch_bounds__(kRunBlock, sizeof(typename StoreOps<S>::Real) 
         step_cell<L, S, COLL>(sp, x, y, z, step_now, GlobalGather<L, S, Real>{sp, y, z});
       }
     }
-    if (!run_barrier(bar, nb, gen, sp.status)) return;
+    if (!run_barrier(count, nb, (uint32_t)s, sp.status)) return;
     if (blockIdx.x == 0) {
       for (int b = 0; b < sp.fin_blocks; ++b) finalize_partial(sp, b);
       finalize_total(sp, sp.fin_blocks);

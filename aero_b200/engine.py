@@ -275,6 +275,12 @@ class Engine:
         on by default where the lattice qualifies, aero_set_persistent)."""
         check("aero_set_persistent", self.lib.aero_set_persistent(self.h, 1 if enable else 0))
 
+    def persistent(self) -> bool:
+        """Whether calls of two or more steps run persistently."""
+        k = ctypes.c_int32()
+        check("aero_get_persistent", self.lib.aero_get_persistent(self.h, ctypes.byref(k)))
+        return bool(k.value)
+
     def get_step_kernel(self) -> int:
         k = ctypes.c_int32()
         check("aero_get_step_kernel", self.lib.aero_get_step_kernel(self.h, ctypes.byref(k)))

@@ -203,6 +203,9 @@ AERO_API int aero_get_step_kernel(const AeroLattice *lat, int32_t *kernel);
  * barrier that gives up sets status bit 1 (aero_status).  enable = 0 keeps
  * per-step launches (graphs).  Not used while the stream is capturing. */
 AERO_API int aero_set_persistent(AeroLattice *lat, int32_t enable);
+/* 1 when the lattice's next aero_step call of two or more steps runs
+ * persistently (enabled and the lattice qualifies), else 0. */
+AERO_API int aero_get_persistent(const AeroLattice *lat, int32_t *active);
 
 /* Inlet fields of steps first_step .. first_step+n_steps-1 for a lattice
  * with inflow_field set: `fields` (host) holds n_steps blocks of planes of
