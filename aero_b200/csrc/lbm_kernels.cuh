@@ -63,6 +63,17 @@ __device__ __forceinline__ uint32_t elem(const StepParams<Real> &p, int i, uint3
   return (uint32_t)i * (uint32_t)p.cs + c;
 }
 
+// (x, y, z) of cell index c in C order, in 32-bit arithmetic (a lattice has
+// fewer than 2^31 cells; 64-bit division costs several times as many
+// instructions).
+__device__ __forceinline__ void cell_xyz(uint32_t c, uint32_t nx, uint32_t ny, int &x, int &y, int &z) {
+  const uint32_t row = c / nx;
+  const uint32_t zz = row / ny;
+  x = (int)(c - row * nx);
+  y = (int)(row - zz * ny);
+  z = (int)zz;
+}
+
 // Link-cell slot of cell (x, y, z), or -1 when the cell has no link.
 template <class Real>
 __device__ __forceinline__ int64_t link_slot(const StepParams<Real> &p, int x, int y, int z) {
@@ -1788,8 +1799,8 @@ __global__ void __launch_bounds__(kStepBlock, sizeof(typename StoreOps<S>::Real)
   for (int k = 0; k < R; ++k) {
     const int64_t c = (b * R + k) * kStepBlock + threadIdx.x;
     if (c >= sp.ncells) return;
-    const int64_t row = c / sp.nx;
-    const int x = (int)(c - row * sp.nx), y = (int)(row % sp.ny), z = (int)(row / sp.ny);
+    int x, y, z;
+    cell_xyz((uint32_t)c, (uint32_t)sp.nx, (uint32_t)sp.ny, x, y, z);
     step_cell<L, S, COLL>(sp, x, y, z, step_now, GlobalGather<L, S, Real>{sp, y, z});
   }
 }
@@ -1807,8 +1818,9 @@ __global__ void __launch_bounds__(kStepBlock) k_moments_batch(const StepParams<t
   for (int k = 0; k < R; ++k) {
     const int64_t c = (b * R + k) * kStepBlock + threadIdx.x;
     if (c >= sp.ncells) return;
-    const int64_t row = c / sp.nx;
-    moments_cell<L, S, false>(sp, (int)(c - row * sp.nx), (int)(row % sp.ny), (int)(row / sp.ny));
+    int x, y, z;
+    cell_xyz((uint32_t)c, (uint32_t)sp.nx, (uint32_t)sp.ny, x, y, z);
+    moments_cell<L, S, false>(sp, x, y, z);
   }
 }
 
@@ -2174,8 +2186,8 @@ __global__ void __launch_bounds__(kRunBlock, sizeof(typename StoreOps<S>::Real) 
       if ((int)blockIdx.x == stall_block) return;
       const int64_t step_now = step0 + s;
       for (int64_t c = (int64_t)(blockIdx.x - 1) * kRunBlock + threadIdx.x; c < sp.ncells; c += cstride) {
-        const int64_t row = c / sp.nx;
-        const int x = (int)(c - row * sp.nx), y = (int)(row % sp.ny), z = (int)(row / sp.ny);
+        int x, y, z;
+        cell_xyz((uint32_t)c, (uint32_t)sp.nx, (uint32_t)sp.ny, x, y, z);
         step_cell<L, S, COLL>(sp, x, y, z, step_now, GlobalGather<L, S, Real>{sp, y, z});
       }
     }

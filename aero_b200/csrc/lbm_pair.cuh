@@ -358,7 +358,8 @@ __global__ void __launch_bounds__(kPairBlock, kPairMinBlocks)
     const int k = threadIdx.x & 3;
     const int64_t r = (b - lay.pair_blocks) * 32 + (threadIdx.x >> 2);
     if (r >= lay.rows) return;
-    const int y = (int)(r % sp.ny), z = (int)(r / sp.ny);
+    const uint32_t zz = (uint32_t)r / (uint32_t)sp.ny;  // rows < 2^31
+    const int y = (int)((uint32_t)r - zz * (uint32_t)sp.ny), z = (int)zz;
     step_cell<L, S, COLL>(sp, k < 2 ? k : sp.nx - 4 + k, y, z, step_now, GlobalGather<L, S, float>{sp, y, z});
     return;
   }
@@ -368,7 +369,8 @@ __global__ void __launch_bounds__(kPairBlock, kPairMinBlocks)
   const int k = lay.TP <= kPairBlock ? t - rl * lay.TP : t;
   const int64_t r = g * lay.RB + rl;
   if (rl >= lay.RB || r >= lay.rows || k >= lay.P) return;
-  const int x = 2 + 2 * k, y = (int)(r % sp.ny), z = (int)(r / sp.ny);
+  const uint32_t zz = (uint32_t)r / (uint32_t)sp.ny;  // rows < 2^31
+  const int x = 2 + 2 * k, y = (int)((uint32_t)r - zz * (uint32_t)sp.ny), z = (int)zz;
   const uint32_t c = cell_index(sp, x, y, z);
   bool plain = !(sp.wall != WALL_NONE && (y == 0 || y == sp.ny - 1));
   if (plain) plain = *reinterpret_cast<const uint16_t *>(sp.flags + c) == 0;  // both flag bytes, c even
