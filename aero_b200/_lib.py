@@ -72,6 +72,7 @@ SIGNATURES = {
     "aero_get_step_kernel": ([_VP, ctypes.POINTER(_I32)], ctypes.c_int),
     "aero_set_persistent": ([_VP, _I32], ctypes.c_int),
     "aero_get_persistent": ([_VP, ctypes.POINTER(_I32)], ctypes.c_int),
+    "aero_kernel_variant": ([_VP, ctypes.POINTER(_I32)], ctypes.c_int),
     "aero_first_bad_step": ([_VP, ctypes.POINTER(_I64), _VP], ctypes.c_int),
     "aero_destroy": ([_VP], ctypes.c_int),
     "aero_mrt_operator": ([_I32, _D, _VP, _VP], ctypes.c_int),

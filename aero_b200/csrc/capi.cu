@@ -159,6 +159,8 @@ struct AeroLattice {
   // only under AERO_B200_TEST_STALL_RUN=1 at bind (that block leaves early)
   bool persistent = true;
   int run_stall_block = -1;
+  // AERO_B200_GENERIC_KERNELS=1 at bind: no feature-specialised kernels
+  bool generic_kernels = false;
   // optional per-kernel event timing (eager launches only)
   bool timing = false;
   std::vector<cudaEvent_t> ev;  // 4 events per timed step
@@ -212,8 +214,17 @@ template <>
 const Ops<double> *get_ops<double>(const AeroLattice *L) {
   return ops_f64(L->prm.dims, L->prm.collision);
 }
+// Kernels compiled for this lattice's exact feature word, where there are
+// (0: the generic kernels; 1: the thermal channel's).
+int kernel_variant(const AeroLattice *L) {
+  if (!L->generic_kernels && L->prm.dims == 3 && L->prm.collision == AERO_TRT && L->feat == feat_fx_thermal() &&
+      ops_fx_thermal(L->prm.storage))
+    return 1;
+  return 0;
+}
 template <>
 const Ops<float> *get_ops<float>(const AeroLattice *L) {
+  if (kernel_variant(L) == 1) return ops_fx_thermal(L->prm.storage);
   switch (L->prm.storage) {
     case AERO_STORE_F32: return ops_f32(L->prm.dims, L->prm.collision);
     case AERO_STORE_F16: return ops_f16(L->prm.dims, L->prm.collision);
@@ -976,6 +987,8 @@ int aero_bind_workspace(AeroLattice *L, void *dptr, uint64_t bytes, void *stream
   // before its first barrier, so the others' waits give up after their limit.
   const char *rstall = std::getenv("AERO_B200_TEST_STALL_RUN");
   L->run_stall_block = (rstall && rstall[0] == '1') ? 1 : -1;
+  const char *gen = std::getenv("AERO_B200_GENERIC_KERNELS");
+  L->generic_kernels = gen && gen[0] == '1';
   L->bound = true;
   return AERO_OK;
 }
@@ -1274,6 +1287,12 @@ int aero_set_step_kernel(AeroLattice *L, int32_t kernel) {
 int aero_set_persistent(AeroLattice *L, int32_t enable) {
   if (!L) return fail(AERO_ERR_INVALID, "NULL argument");
   L->persistent = enable != 0;
+  return AERO_OK;
+}
+
+int aero_kernel_variant(const AeroLattice *L, int32_t *variant) {
+  if (!L || !variant) return fail(AERO_ERR_INVALID, "NULL argument");
+  *variant = kernel_variant(L);
   return AERO_OK;
 }
 

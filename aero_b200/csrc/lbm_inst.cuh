@@ -11,6 +11,7 @@
 #include "lbm_les.cuh"
 
 namespace aero {
+inline namespace AERO_KNS {
 namespace inst {
 
 template <class L, class S, int COLL>
@@ -254,4 +255,5 @@ const Ops<typename StoreOps<S>::Real> *lookup(int dims, int coll) {
 }
 
 }  // namespace inst
+}  // namespace AERO_KNS
 }  // namespace aero

@@ -32,7 +32,22 @@
 #include "lbm_params.h"
 #include "lbm_store.cuh"
 
+// Kernel variants.  Every translation unit that includes the kernels compiles
+// them into the inline namespace AERO_KNS (aero::gen by default), so a unit
+// that fixes the feature word at compile time (AERO_FIXED_FEAT: the features
+// of one lattice configuration, branches of the others removed) produces
+// kernels of its own names beside the generic ones.
+#ifndef AERO_KNS
+#define AERO_KNS gen
+#endif
+#ifdef AERO_FIXED_FEAT
+#define FEAT_OF(p) ((uint32_t)(AERO_FIXED_FEAT))
+#else
+#define FEAT_OF(p) ((p).feat)
+#endif
+
 namespace aero {
+inline namespace AERO_KNS {
 
 #ifndef AERO_STEP_BLOCK
 #define AERO_STEP_BLOCK 128
@@ -148,7 +163,7 @@ __device__ __forceinline__ void inlet_velocity_field(const StepParams<Real> &p, 
                                                      int64_t step_now) {
   const int64_t plane = (int64_t)p.nz * p.ny;
   if constexpr (L::DIMS == 3) {
-    if (p.feat & FEAT_INFLOW_SEM) {
+    if (FEAT_OF(p) & FEAT_INFLOW_SEM) {
       const Real *slot = p.inflow + (step_now % p.inflow_ring) * 3 * plane;
       const int64_t r = (int64_t)z * p.ny + y;
       const Real ux = p.u0 + slot[r];
@@ -506,7 +521,7 @@ __device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, 
   const uint32_t c = cell_index(p, x, y, z);
   if constexpr (L::DIMS == 3) {
     // Guo-style uniform body force on fluid cells (ibm_guo.py:263-301)
-    if ((p.feat & FEAT_BODY_FORCE) && !(gather.flags(x) & FLAG_SOLID)) {
+    if ((FEAT_OF(p) & FEAT_BODY_FORCE) && !(gather.flags(x) & FLAG_SOLID)) {
       Real drho = 0, jx = 0, jy = 0, jz = 0;
       static_for<L::Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
@@ -530,11 +545,11 @@ __device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, 
     }
   }
   // obstacle bounce-back (boundary.py:283-352, boundary3d.py:333-393)
-  if ((p.feat & FEAT_OBSTACLE_BB) && (gather.flags(x) & FLAG_LINK)) {
+  if ((FEAT_OF(p) & FEAT_OBSTACLE_BB) && (gather.flags(x) & FLAG_LINK)) {
     const int64_t slot = link_slot(p, x, y, z);
     if (slot >= 0) {
       const uint32_t mask = __ldg(p.lc_mask + slot);
-      const bool bouzidi = p.feat & FEAT_BOUZIDI;
+      const bool bouzidi = FEAT_OF(p) & FEAT_BOUZIDI;
       static_for<L::Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
         if constexpr (i > 0) {
@@ -562,9 +577,9 @@ __device__ __forceinline__ void partial_state(const StepParams<Real> &p, int x, 
       });
     }
   }
-  if ((p.feat & FEAT_OPEN) && x == 0) {
+  if ((FEAT_OF(p) & FEAT_OPEN) && x == 0) {
     if (p.inlet == INLET_VELOCITY) {
-      if (p.feat & FEAT_INFLOW_FIELD)
+      if (FEAT_OF(p) & FEAT_INFLOW_FIELD)
         inlet_velocity_field<L>(p, d, y, z, step_now);
       else
         inlet_velocity<L>(p, d, y, z, step_now);
@@ -587,7 +602,7 @@ template <class L, class S, class Real, class Gather>
 __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int y, int z, int64_t step_now,
                                            Real (&d)[L::Q], Real *prev_out, ScalarCtx<Real> *sc,
                                            const Gather &gather) {
-  const bool open = p.feat & FEAT_OPEN;
+  const bool open = FEAT_OF(p) & FEAT_OPEN;
   const bool copy_out =
       open && x == p.nx - 1 && (p.outlet == OUTLET_CONVECTIVE || p.outlet == OUTLET_ZEROGRAD);
   bool shfl = false;
@@ -627,7 +642,7 @@ __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int
     // solver3d.py:460-461): the inlet plane takes the equilibrium of the
     // x = nx-2 cell's post-bounce-back state with its velocity scaled so that
     // the plane's mean ux becomes u0
-    if ((p.feat & FEAT_RECYCLE) && x == 0) {
+    if ((FEAT_OF(p) & FEAT_RECYCLE) && x == 0) {
       Real r[L::Q];
       partial_state<L, S, Real>(p, p.nx - 2, y, z, step_now, r, gather);
       Real drho = 0, jx = 0, jy = 0, jz = 0;
@@ -652,7 +667,7 @@ __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int
     }
   }
   // sponge (sponge.py:8-70)
-  if ((p.feat & FEAT_SPONGE) && x >= p.sponge_start) {
+  if ((FEAT_OF(p) & FEAT_SPONGE) && x >= p.sponge_start) {
     const double frac = (double)(x - p.sponge_start + 1) / (double)(p.sponge_thickness > 1 ? p.sponge_thickness : 1);
     const Real sg = (Real)((double)p.sponge_sigma_max * frac * frac);
     if (sg > Real(0)) {
@@ -671,11 +686,11 @@ __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int
     if (y == 0) walls<L>(p, d, true);
     if (y == p.ny - 1) walls<L>(p, d, false);
   }
-  if (p.feat & FEAT_THERMAL) {
+  if (FEAT_OF(p) & FEAT_THERMAL) {
     // thermal.py:103-124 / :206-222 with the order of solver.py:432-439
     const uint32_t c = cell_index(p, x, y, z);
     Real T = 0;
-    if (p.feat & FEAT_SCALAR_REDUCED) {
+    if (FEAT_OF(p) & FEAT_SCALAR_REDUCED) {
       using G = typename ScalarReduced<L>::Lat;
       static_for<G::Q>([&](auto ic) { T += p.g[elem(p, decltype(ic)::value, c)]; });
     } else {
@@ -697,7 +712,7 @@ __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int
       sc->u[1] = jy * inv;
       sc->u[2] = jz * inv;
     }
-    if (p.feat & FEAT_BUOYANCY) {
+    if (FEAT_OF(p) & FEAT_BUOYANCY) {
       const Real buoy = p.gbeta * (T - p.T_ref);
       static_for<L::Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
@@ -723,12 +738,12 @@ __device__ __forceinline__ Real les_rate_from_gradient(const StepParams<Real> &p
                                                        uint32_t c) {
   Real nu_t;
   Real cs2 = p.les_cs2;
-  if (p.feat & FEAT_LES_CS_FIELD) {
+  if (FEAT_OF(p) & FEAT_LES_CS_FIELD) {
     const Real cc = p.cs_cell[c];
     cs2 = cc * cc;
   }
   constexpr int D = L::DIMS;
-  if (p.feat & FEAT_LES_WALE) {
+  if (FEAT_OF(p) & FEAT_LES_WALE) {
     Real s_sq = 0, sd_sq = 0, gsq[3][3], tr = 0;
 #pragma unroll
     for (int a = 0; a < D; a++)
@@ -1155,12 +1170,12 @@ __device__ __forceinline__ void finish_cell(const StepParams<typename StoreOps<S
                                             typename StoreOps<S>::Real om, bool les, const Gather &gather) {
   using Real = typename StoreOps<S>::Real;
   const bool solid = fl & FLAG_SOLID;
-  if ((p.feat & FEAT_OBSTACLE_BB) && (fl & FLAG_LINK)) {
+  if ((FEAT_OF(p) & FEAT_OBSTACLE_BB) && (fl & FLAG_LINK)) {
     const int64_t slot = link_slot(p, x, y, z);
     if (slot >= 0) link_cell_forces<L, S, Real>(p, x, y, z, c, slot, d, gather);
   }
-  if (p.feat & FEAT_THERMAL) {
-    if (p.feat & FEAT_SCALAR_REDUCED) {
+  if (FEAT_OF(p) & FEAT_THERMAL) {
+    if (FEAT_OF(p) & FEAT_SCALAR_REDUCED) {
       using G = typename ScalarReduced<L>::Lat;
       scalar_step<L, G>(p, x, y, z, c, solid, sc, Real(G::cs2inv));
     } else {
@@ -1190,7 +1205,7 @@ __device__ __forceinline__ void step_cell(const StepParams<typename StoreOps<S>:
   ScalarCtx<Real> sc;
   full_state<L, S, Real>(p, x, y, z, step_now, d, p.prevn, &sc, gather);
   Real om = p.omega;
-  const bool les = (COLL != COLL_MRT) && (p.feat & FEAT_LES);
+  const bool les = (COLL != COLL_MRT) && (FEAT_OF(p) & FEAT_LES);
   if (les) om = les_omega<L>(p, x, y, z, c, solid);
   finish_cell<L, S, COLL>(p, x, y, z, c, fl, step_now, d, sc, om, les, gather);
 }
@@ -1235,7 +1250,7 @@ __global__ void __launch_bounds__(BX *BY, AA ? (sizeof(typename StoreOps<S>::Rea
       d[i] = own_value<L, S, i>(p, x, y, z, c);
     });
     Real om = p.omega;
-    const bool les = (COLL != COLL_MRT) && (p.feat & FEAT_LES);
+    const bool les = (COLL != COLL_MRT) && (FEAT_OF(p) & FEAT_LES);
     if (les) om = les_omega<L>(p, x, y, z, c, solid);
     collide<L, Real, COLL>(p, d, solid, om, les);
     S *Pn = static_cast<S *>(p.Pn);
@@ -1384,7 +1399,7 @@ __device__ __forceinline__ void issue_tile(const StepParams<Real> &p, int tile, 
   const int64_t c0 = ((int64_t)t.z * p.ny + t.y0) * p.nx;  // first cell of the tile
   const int64_t fa = c0 & ~(int64_t)15;
   const uint32_t fbytes = (uint32_t)(((c0 + (int64_t)t.rows * p.nx + 15) & ~(int64_t)15) - fa);
-  const bool conv = (p.feat & FEAT_OPEN) && p.outlet == OUTLET_CONVECTIVE;
+  const bool conv = (FEAT_OF(p) & FEAT_OPEN) && p.outlet == OUTLET_CONVECTIVE;
   const uint32_t pbytes = conv ? (uint32_t)t.rows * (uint32_t)(L::QP * sizeof(Real)) : 0u;
   mbar_arrive_expect_tx(bar, (uint32_t)L::Q * (uint32_t)t.rows * row_bytes + fbytes + pbytes + p.tile_extra_tx);
   const char *P = static_cast<const char *>(p.P);
@@ -1550,7 +1565,7 @@ __global__ void __launch_bounds__(kStageBlock) k_aa_stage(const StepParams<typen
     const int x = (int)(c - row * (uint32_t)p.nx);
     const int z = (int)(row / (uint32_t)p.ny), y = (int)(row - (uint32_t)z * (uint32_t)p.ny);
     const int64_t t = k * L::Q + dir;
-    const bool bouzidi = p.feat & FEAT_BOUZIDI;
+    const bool bouzidi = FEAT_OF(p) & FEAT_BOUZIDI;
     static_for<L::Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
       if (dir != i) return;
@@ -1936,8 +1951,8 @@ __global__ void __launch_bounds__(kStatsBlock)
   for (int k = 0; k < kStatsValues; k++) a[k] = 0.0;
   const int64_t plane = (int64_t)p.nx * p.ny;
   const int64_t n = plane * nzs;
-  const bool thermal = (p.feat & FEAT_THERMAL) && gcur != nullptr;
-  const int Qg = (p.feat & FEAT_SCALAR_REDUCED) ? ScalarReduced<L>::Lat::Q : L::Q;
+  const bool thermal = (FEAT_OF(p) & FEAT_THERMAL) && gcur != nullptr;
+  const int Qg = (FEAT_OF(p) & FEAT_SCALAR_REDUCED) ? ScalarReduced<L>::Lat::Q : L::Q;
   auto Tcell = [&](int x, int y, int z) {
     const uint32_t cc = cell_index(p, x, y, z);
     double T = 0.0;
@@ -2072,7 +2087,7 @@ __global__ void __launch_bounds__(kStepBlock) k_init_equilibrium(const StepParam
   });
   if (g_dst) {
     const double T = e.T ? e.T[c] : e.T0;
-    if (p.feat & FEAT_SCALAR_REDUCED) {
+    if (FEAT_OF(p) & FEAT_SCALAR_REDUCED) {
       using G = typename ScalarReduced<L>::Lat;
       static_for<G::Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
@@ -2199,4 +2214,5 @@ __global__ void __launch_bounds__(kRunBlock, sizeof(typename StoreOps<S>::Real) 
   }
 }
 
+}  // namespace AERO_KNS
 }  // namespace aero

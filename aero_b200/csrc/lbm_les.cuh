@@ -36,6 +36,7 @@
 #include "lbm_kernels.cuh"
 
 namespace aero {
+inline namespace AERO_KNS {
 
 constexpr int kLesTileX = 32;                      // one warp per tile row
 constexpr int kLesRows = 8;                        // tile rows (y)
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(kLesThreads, sizeof(typename StoreOps<S>::Real
           constexpr int i = decltype(ic)::value;
           sm.s[k][i][it] = d[i];
         });
-        if (p.feat & FEAT_THERMAL) {
+        if (FEAT_OF(p) & FEAT_THERMAL) {
           sm.sc[k][0][it] = sc.T;
           sm.sc[k][1][it] = sc.u[0];
           sm.sc[k][2][it] = sc.u[1];
@@ -157,7 +158,7 @@ __global__ void __launch_bounds__(kLesThreads, sizeof(typename StoreOps<S>::Real
         d[i] = sm.s[k][i][it];
       });
       ScalarCtx<Real> sc{};
-      if (p.feat & FEAT_THERMAL) {
+      if (FEAT_OF(p) & FEAT_THERMAL) {
         sc.T = sm.sc[k][0][it];
         sc.u[0] = sm.sc[k][1][it];
         sc.u[1] = sm.sc[k][2][it];
@@ -187,4 +188,5 @@ __global__ void __launch_bounds__(kLesThreads, sizeof(typename StoreOps<S>::Real
   }
 }
 
+}  // namespace AERO_KNS
 }  // namespace aero

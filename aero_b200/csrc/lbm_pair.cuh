@@ -24,6 +24,7 @@
 #include "lbm_kernels.cuh"
 
 namespace aero {
+inline namespace AERO_KNS {
 
 struct P2;
 
@@ -148,7 +149,7 @@ __device__ __forceinline__ void pair_gather(const StepParams<float> &p, int x, i
 // the cell's depth into the sponge; lanes outside the sponge keep d.
 template <class L>
 __device__ __forceinline__ void pair_sponge(const StepParams<float> &p, int x, F2 (&d)[L::Q]) {
-  if (!(p.feat & FEAT_SPONGE) || x + 1 < p.sponge_start) return;
+  if (!(FEAT_OF(p) & FEAT_SPONGE) || x + 1 < p.sponge_start) return;
   float sgv[2];
 #pragma unroll
   for (int k = 0; k < 2; k++) {
@@ -255,7 +256,7 @@ __device__ __forceinline__ void pair_step_plain(const StepParams<float> &p, int 
   if constexpr (COLL == COLL_MRT) {
     rho = mrt3_core<float, F2>(p.mrt3, d, false);
   } else {
-    const bool les = p.feat & FEAT_LES;
+    const bool les = FEAT_OF(p) & FEAT_LES;
     F2 om(p.omega);
     if (les) om = F2(make_float2(les_omega<L>(p, x, y, z, c, false), les_omega<L>(p, x + 1, y, z, c + 1, false)));
     rho = collide_pair_bt<L, COLL>(p, d, om, les);
@@ -389,4 +390,5 @@ inline dim3 pair_grid(const StepParams<Real> &p) {
   return dim3((unsigned)(sp.row_blocks > 0 ? sp.row_blocks : 1), (unsigned)(kPairRows + 1), (unsigned)sp.groups);
 }
 
+}  // namespace AERO_KNS
 }  // namespace aero

@@ -36,6 +36,7 @@
 #include "lbm_pair.cuh"
 
 namespace aero {
+inline namespace AERO_KNS {
 
 // Two cells packed in 32 bits <-> their deviations as F2, with the scales
 // and conversions of PairOps (bit-identical values).
@@ -98,7 +99,7 @@ struct QuadSplit {
 template <class Real>
 __host__ __device__ __forceinline__ QuadSplit quad_split(const StepParams<Real> &p) {
   QuadSplit q;
-  q.edges = (p.feat & (FEAT_OPEN | FEAT_RECYCLE)) != 0;  // inlet / outlet / recycling columns
+  q.edges = (FEAT_OF(p) & (FEAT_OPEN | FEAT_RECYCLE)) != 0;  // inlet / outlet / recycling columns
   q.x0 = q.edges ? 4 : 0;
   q.nquads = q.edges ? (p.nx - 8) / 4 : p.nx / 4;
   q.TP = (q.nquads + 31) / 32 * 32;
@@ -124,7 +125,7 @@ __device__ __forceinline__ void quad_step_plain(const StepParams<float> &p, int 
                                                 int64_t step_now, const uint32_t *sq) {
   using QO = QuadOps<S>;
   S *Pn = static_cast<S *>(p.Pn);
-  const bool les = (COLL != COLL_MRT) && (p.feat & FEAT_LES);
+  const bool les = (COLL != COLL_MRT) && (FEAT_OF(p) & FEAT_LES);
   const int tid = threadIdx.x;
 #pragma unroll 1
   for (int h = 0; h < 2; h++) {
@@ -249,4 +250,5 @@ __global__ void __launch_bounds__(kQuadBlock, kQuadMinBlocks) k_step_quad(const 
   for (int e = 0; e < 4; e++) step_cell<L, S, COLL>(p, x + e, y, z, step_now, gather);
 }
 
+}  // namespace AERO_KNS
 }  // namespace aero

@@ -275,6 +275,13 @@ class Engine:
         on by default where the lattice qualifies, aero_set_persistent)."""
         check("aero_set_persistent", self.lib.aero_set_persistent(self.h, 1 if enable else 0))
 
+    def kernel_variant(self) -> int:
+        """0: the generic kernels; 1: the kernels compiled for the thermal
+        channel's feature word (aero_kernel_variant)."""
+        k = ctypes.c_int32()
+        check("aero_kernel_variant", self.lib.aero_kernel_variant(self.h, ctypes.byref(k)))
+        return int(k.value)
+
     def persistent(self) -> bool:
         """Whether calls of two or more steps run persistently."""
         k = ctypes.c_int32()

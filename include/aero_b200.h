@@ -207,6 +207,16 @@ AERO_API int aero_set_persistent(AeroLattice *lat, int32_t enable);
  * persistently (enabled and the lattice qualifies), else 0. */
 AERO_API int aero_get_persistent(const AeroLattice *lat, int32_t *active);
 
+/* Which compiled kernel set the lattice steps with (no counterpart in the
+ * reference): 0 = the generic kernels, which read the feature word at run
+ * time; 1 = kernels compiled for the feature word of the thermal channel
+ * (D3Q19 TRT + WALE, body force, D3Q7 scalar with buoyancy, obstacle,
+ * streamwise periodic; FP32 / FP16 / BF16 storage), whose other features'
+ * branches are removed.  Results agree with the generic kernels' up to FP
+ * rounding of the compiled variant.  AERO_B200_GENERIC_KERNELS=1 in the
+ * environment at aero_bind_workspace keeps the generic set. */
+AERO_API int aero_kernel_variant(const AeroLattice *lat, int32_t *variant);
+
 /* Inlet fields of steps first_step .. first_step+n_steps-1 for a lattice
  * with inflow_field set: `fields` (host) holds n_steps blocks of planes of
  * nz*ny doubles, (z, y) order.  Synthetic inflow: uy in 2D, uy then uz in
