@@ -218,7 +218,7 @@ const Ops<double> *get_ops<double>(const AeroLattice *L) {
 // (0: the generic kernels; 1: the thermal channel's).
 int kernel_variant(const AeroLattice *L) {
   if (!L->generic_kernels && L->prm.dims == 3 && L->prm.collision == AERO_TRT && L->feat == feat_fx_thermal() &&
-      ops_fx_thermal(L->prm.storage))
+      L->prm.wall_bc == wall_fx_thermal() && ops_fx_thermal(L->prm.storage))
     return 1;
   return 0;
 }

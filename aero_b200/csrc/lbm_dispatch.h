@@ -82,9 +82,11 @@ const Ops<float> *ops_f32(int dims, int coll);
 const Ops<double> *ops_f64(int dims, int coll);
 const Ops<float> *ops_f16(int dims, int coll);
 const Ops<float> *ops_bf16(int dims, int coll);
-// Kernels compiled for one feature word (lbm_inst_fx_thermal.cu): the
-// word, and the D3Q19 TRT table of a storage format (NULL for others).
+// Kernels compiled for one feature word and wall type
+// (lbm_inst_fx_thermal.cu): the word, the wall type, and the D3Q19 TRT table
+// of a storage format (NULL for others).
 uint32_t feat_fx_thermal();
+int32_t wall_fx_thermal();
 const Ops<float> *ops_fx_thermal(int storage);
 
 // Block shapes of the per-cell step kernel an autotuner can choose from:

@@ -1,7 +1,7 @@
 // lbm_inst_fx_thermal.cu -- kernels compiled for the thermal channel's feature
-// word: D3Q19 TRT with WALE LES, uniform body force, the D3Q7 scalar with
-// Boussinesq buoyancy, an obstacle with mid-link bounce-back, streamwise
-// periodic (no inlet, outlet, sponge or Bouzidi).  The step there is
+// word and wall type: D3Q19 TRT with WALE LES, uniform body force, the D3Q7
+// scalar with Boussinesq buoyancy, an obstacle with mid-link bounce-back,
+// no-slip walls, streamwise periodic (no inlet, outlet, sponge or Bouzidi).  The step there is
 // instruction-bound; with every other feature's branch removed at compile
 // time the step chain is shorter and fits the instruction cache better.
 // Lattices whose feature word is exactly this one take these kernels
@@ -16,11 +16,13 @@
 #define AERO_FIXED_FEAT                                                                                            \
   (FEAT_BODY_FORCE | FEAT_LES | FEAT_LES_WALE | FEAT_THERMAL | FEAT_BUOYANCY | FEAT_SCALAR_REDUCED |               \
    FEAT_OBSTACLE_BB)
+#define AERO_FIXED_WALL WALL_NOSLIP
 #include "lbm_inst.cuh"
 
 namespace aero {
 
 uint32_t feat_fx_thermal() { return AERO_FIXED_FEAT; }
+int32_t wall_fx_thermal() { return AERO_FIXED_WALL; }
 
 const Ops<float> *ops_fx_thermal(int storage) {
   switch (storage) {

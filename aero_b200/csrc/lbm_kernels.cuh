@@ -45,6 +45,11 @@
 #else
 #define FEAT_OF(p) ((p).feat)
 #endif
+#ifdef AERO_FIXED_WALL
+#define WALL_OF(p) ((int32_t)(AERO_FIXED_WALL))
+#else
+#define WALL_OF(p) ((p).wall)
+#endif
 
 namespace aero {
 inline namespace AERO_KNS {
@@ -239,10 +244,10 @@ template <class L, class Real>
 __device__ __forceinline__ void walls(const StepParams<Real> &p, Real (&d)[L::Q], bool bottom) {
   const Real k6 = Real(6.0 * (1.0 / 36.0));
   if constexpr (L::DIMS == 2) {
-    if (p.wall == WALL_SLIP) {
+    if (WALL_OF(p) == WALL_SLIP) {
       if (bottom) { d[2] = d[4]; d[5] = d[8]; d[6] = d[7]; }
       else        { d[4] = d[2]; d[8] = d[5]; d[7] = d[6]; }
-    } else if (p.wall == WALL_NOSLIP) {
+    } else if (WALL_OF(p) == WALL_NOSLIP) {
       if (bottom) { d[2] = d[4]; d[5] = d[7]; d[6] = d[8]; }
       else        { d[4] = d[2]; d[7] = d[5]; d[8] = d[6]; }
     } else {
@@ -257,10 +262,10 @@ __device__ __forceinline__ void walls(const StepParams<Real> &p, Real (&d)[L::Q]
       }
     }
   } else {
-    if (p.wall == WALL_SLIP) {
+    if (WALL_OF(p) == WALL_SLIP) {
       if (bottom) { d[3] = d[4]; d[7] = d[9]; d[8] = d[10]; d[15] = d[16]; d[17] = d[18]; }
       else        { d[4] = d[3]; d[9] = d[7]; d[10] = d[8]; d[16] = d[15]; d[18] = d[17]; }
-    } else if (p.wall == WALL_NOSLIP) {
+    } else if (WALL_OF(p) == WALL_NOSLIP) {
       if (bottom) { d[3] = d[4]; d[7] = d[10]; d[8] = d[9]; d[15] = d[18]; d[17] = d[16]; }
       else        { d[4] = d[3]; d[10] = d[7]; d[9] = d[8]; d[18] = d[15]; d[16] = d[17]; }
     } else {
@@ -682,7 +687,7 @@ __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int
       });
     }
   }
-  if (p.wall != WALL_NONE) {
+  if (WALL_OF(p) != WALL_NONE) {
     if (y == 0) walls<L>(p, d, true);
     if (y == p.ny - 1) walls<L>(p, d, false);
   }

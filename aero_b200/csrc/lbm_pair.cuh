@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(kPairBlock, kPairMinBlocks) k_step_pair(const 
   if (r >= sp.rows || t >= sp.npairs) return;
   const int x = 2 + 2 * t, y = r % p.ny, z = r / p.ny;
   const uint32_t c = cell_index(p, x, y, z);
-  bool plain = !(p.wall != WALL_NONE && (y == 0 || y == p.ny - 1));
+  bool plain = !(WALL_OF(p) != WALL_NONE && (y == 0 || y == p.ny - 1));
   if (plain) plain = *reinterpret_cast<const uint16_t *>(p.flags + c) == 0;  // both flag bytes, c even
   if (plain) {
     pair_step_plain<L, S, COLL>(p, x, y, z, c, step_now);
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(kPairBlock, kPairMinBlocks)
   const uint32_t zz = (uint32_t)r / (uint32_t)sp.ny;  // rows < 2^31
   const int x = 2 + 2 * k, y = (int)((uint32_t)r - zz * (uint32_t)sp.ny), z = (int)zz;
   const uint32_t c = cell_index(sp, x, y, z);
-  bool plain = !(sp.wall != WALL_NONE && (y == 0 || y == sp.ny - 1));
+  bool plain = !(WALL_OF(sp) != WALL_NONE && (y == 0 || y == sp.ny - 1));
   if (plain) plain = *reinterpret_cast<const uint16_t *>(sp.flags + c) == 0;  // both flag bytes, c even
   if (plain) {
     pair_step_plain<L, S, COLL>(sp, x, y, z, c, step_now);

@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(kQuadBlock, kQuadMinBlocks) k_step_quad(const 
   });
   if (!active) return;
   const uint32_t c = cell_index(p, x, y, z);
-  bool plain = !(p.wall != WALL_NONE && (y == 0 || y == p.ny - 1));
+  bool plain = !(WALL_OF(p) != WALL_NONE && (y == 0 || y == p.ny - 1));
   if (plain) plain = *reinterpret_cast<const uint32_t *>(p.flags + c) == 0u;  // the four flag bytes, c % 4 == 0
   if (plain) {
     quad_step_plain<L, S, COLL>(p, x, y, z, c, step_now, sq);

@@ -211,8 +211,8 @@ AERO_API int aero_get_persistent(const AeroLattice *lat, int32_t *active);
  * reference): 0 = the generic kernels, which read the feature word at run
  * time; 1 = kernels compiled for the feature word of the thermal channel
  * (D3Q19 TRT + WALE, body force, D3Q7 scalar with buoyancy, obstacle,
- * streamwise periodic; FP32 / FP16 / BF16 storage), whose other features'
- * branches are removed.  Results agree with the generic kernels' up to FP
+ * no-slip walls, streamwise periodic; FP32 / FP16 / BF16 storage), whose
+ * other features' branches are removed.  Results agree with the generic kernels' up to FP
  * rounding of the compiled variant.  AERO_B200_GENERIC_KERNELS=1 in the
  * environment at aero_bind_workspace keeps the generic set. */
 AERO_API int aero_kernel_variant(const AeroLattice *lat, int32_t *variant);

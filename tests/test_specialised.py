@@ -1,6 +1,7 @@
 """Kernels compiled for one feature word: a lattice whose features are exactly
 the thermal channel's (D3Q19 TRT + WALE, uniform body force, D3Q7 scalar with
-buoyancy, an obstacle with mid-link bounce-back, streamwise periodic) steps
+buoyancy, an obstacle with mid-link bounce-back, no-slip walls, streamwise
+periodic) steps
 with kernels in which every other feature's branch is removed at compile
 time; every other lattice keeps the generic kernels.  Both compute the same
 operations, so the states agree up to the FP rounding of the compiled
@@ -57,7 +58,7 @@ def test_thermal_channel_kernels_equal_generic(precision, monkeypatch):
 def test_other_feature_words_take_the_generic_kernels(monkeypatch):
     monkeypatch.delenv("AERO_B200_GENERIC_KERNELS", raising=False)
     for extra in (dict(precision="fp64"), dict(collision="bgk"), dict(buoyancy=False),
-                  dict(scalar_lattice="full"), dict(les_model="smagorinsky")):
+                  dict(scalar_lattice="full"), dict(les_model="smagorinsky"), dict(wall_bc="slip")):
         kw = dict(precision="fp32")
         kw.update(extra)
         s = _channel(**kw)
