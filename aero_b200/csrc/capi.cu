@@ -214,17 +214,22 @@ template <>
 const Ops<double> *get_ops<double>(const AeroLattice *L) {
   return ops_f64(L->prm.dims, L->prm.collision);
 }
-// Kernels compiled for this lattice's exact feature word, where there are
-// (0: the generic kernels; 1: the thermal channel's).
-int kernel_variant(const AeroLattice *L) {
-  if (!L->generic_kernels && L->prm.dims == 3 && L->prm.collision == AERO_TRT && L->feat == feat_fx_thermal() &&
-      L->prm.wall_bc == wall_fx_thermal() && ops_fx_thermal(L->prm.storage))
-    return 1;
+// The kernel set compiled for this lattice's exact feature word and wall
+// type, where there is one (variant k + 1 of kFxSets[k]); else 0, the
+// generic kernels.
+int kernel_variant(const AeroLattice *L, const Ops<float> **ops = nullptr) {
+  if (L->generic_kernels || is_f64(L)) return 0;
+  for (int k = 0; k < kFxCount; k++)
+    if (const Ops<float> *o = kFxSets[k](L->prm.dims, L->prm.collision, L->prm.storage, L->feat, L->prm.wall_bc)) {
+      if (ops) *ops = o;
+      return k + 1;
+    }
   return 0;
 }
 template <>
 const Ops<float> *get_ops<float>(const AeroLattice *L) {
-  if (kernel_variant(L) == 1) return ops_fx_thermal(L->prm.storage);
+  const Ops<float> *fx = nullptr;
+  if (kernel_variant(L, &fx)) return fx;
   switch (L->prm.storage) {
     case AERO_STORE_F32: return ops_f32(L->prm.dims, L->prm.collision);
     case AERO_STORE_F16: return ops_f16(L->prm.dims, L->prm.collision);
@@ -1466,15 +1471,17 @@ __global__ void k_set_profile_steps(int64_t *const *ctrs, int n, int64_t delta) 
 
 struct ClassKey {
   int dims, storage, coll;
-  bool pair;  // the members take the two-cells-per-thread layout (k_step_batch_pair)
+  bool pair;    // the members take the two-cells-per-thread layout (k_step_batch_pair)
+  int variant;  // the compiled kernel set (kernel_variant)
   bool operator==(const ClassKey &o) const {
-    return dims == o.dims && storage == o.storage && coll == o.coll && pair == o.pair;
+    return dims == o.dims && storage == o.storage && coll == o.coll && pair == o.pair && variant == o.variant;
   }
 };
 
 struct ClassPlan {
   ClassKey key;
   bool f64;
+  const Ops<float> *ops = nullptr;  // the class's kernel table (4- and 2-byte storage)
   int n = 0, n_les = 0;
   int64_t blocks = 0, blocks_les = 0;
   uint64_t params[2] = {0, 0}, first = 0, params_les[2] = {0, 0}, first_les = 0;
@@ -1500,7 +1507,7 @@ bool batch_solo(const AeroLattice *L) { return L->ncells >= kBatchSoloCells; }
 // where the per-cell kernel's traffic, not its instructions, sets the pace.
 ClassKey class_of(const AeroLattice *L) {
   const bool half = L->prm.storage == AERO_STORE_F16 || L->prm.storage == AERO_STORE_BF16;
-  return {L->prm.dims, L->prm.storage, L->prm.collision, half && pair_capable(L, 6)};
+  return {L->prm.dims, L->prm.storage, L->prm.collision, half && pair_capable(L, 6), kernel_variant(L)};
 }
 
 }  // namespace
@@ -1583,6 +1590,7 @@ int batch_build(AeroBatch *B, cudaStream_t st) {
       ClassPlan c;
       c.key = k;
       c.f64 = is_f64(L);
+      if (!c.f64) c.ops = get_ops<float>(L);  // the same for every member: the key holds the variant
       B->classes.push_back(c);
       it = B->classes.end() - 1;
     }
@@ -1728,9 +1736,7 @@ int batch_launch_step(AeroBatch *B, int j, cudaStream_t st, bool branches = fals
                                                c.blocks_les, cs));
       CUDA_TRY(ops->step_batch(P, reinterpret_cast<const int64_t *>(ws + c.first), c.n, c.blocks, cs));
     } else {
-      const Ops<float> *ops = c.key.storage == AERO_STORE_F32   ? ops_f32(c.key.dims, c.key.coll)
-                              : c.key.storage == AERO_STORE_F16 ? ops_f16(c.key.dims, c.key.coll)
-                                                                : ops_bf16(c.key.dims, c.key.coll);
+      const Ops<float> *ops = c.ops;
       auto *P = reinterpret_cast<const StepParams<float> *>(ws + c.params[j]);
       auto *PL = reinterpret_cast<const StepParams<float> *>(ws + c.params_les[j]);
       if (c.n_les) CUDA_TRY(ops->moments_batch(PL, reinterpret_cast<const int64_t *>(ws + c.first_les), c.n_les,

@@ -82,12 +82,19 @@ const Ops<float> *ops_f32(int dims, int coll);
 const Ops<double> *ops_f64(int dims, int coll);
 const Ops<float> *ops_f16(int dims, int coll);
 const Ops<float> *ops_bf16(int dims, int coll);
-// Kernels compiled for one feature word and wall type
-// (lbm_inst_fx_thermal.cu): the word, the wall type, and the D3Q19 TRT table
-// of a storage format (NULL for others).
-uint32_t feat_fx_thermal();
-int32_t wall_fx_thermal();
-const Ops<float> *ops_fx_thermal(int storage);
+// Kernel sets compiled for one feature word and wall type each
+// (lbm_inst_fx_*.cu): the table for a lattice of these dimensions,
+// collision, storage, feature word and wall type, or NULL where the set does
+// not cover it.  kFxSets lists them; its index + 1 is the variant that
+// aero_kernel_variant reports.
+using FxLookup = const Ops<float> *(*)(int dims, int coll, int storage, uint32_t feat, int32_t wall);
+const Ops<float> *ops_fx_thermal(int dims, int coll, int storage, uint32_t feat, int32_t wall);
+const Ops<float> *ops_fx_open2(int dims, int coll, int storage, uint32_t feat, int32_t wall);
+const Ops<float> *ops_fx_open3(int dims, int coll, int storage, uint32_t feat, int32_t wall);
+const Ops<float> *ops_fx_les2(int dims, int coll, int storage, uint32_t feat, int32_t wall);
+const Ops<float> *ops_fx_les3(int dims, int coll, int storage, uint32_t feat, int32_t wall);
+constexpr FxLookup kFxSets[] = {&ops_fx_thermal, &ops_fx_open2, &ops_fx_open3, &ops_fx_les2, &ops_fx_les3};
+constexpr int kFxCount = (int)(sizeof(kFxSets) / sizeof(kFxSets[0]));
 
 // Block shapes of the per-cell step kernel an autotuner can choose from:
 // {threads along x, rows}.  Shape 0 is the default.

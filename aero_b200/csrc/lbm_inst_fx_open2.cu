@@ -1,0 +1,30 @@
+// lbm_inst_fx_open2.cu -- kernels compiled for the 2D wind-tunnel channel of the serving trace and the batched sweep: D2Q9, velocity inlet and outlet columns, an obstacle with mid-link bounce-back, slip walls, no LES, sponge, Bouzidi or scalar.  The
+// feature word and wall type are fixed, so the other features' branches are
+// removed; lattices with exactly this word, wall type, dimension and
+// collision (FP32 storage) take these kernels, single lattices and batch
+// classes alike (capi.cu).
+#include "aero_b200.h"
+#include "lbm_params.h"
+
+// branches made unreachable by the fixed feature word are expected here
+#pragma nv_diag_suppress 128
+
+#define AERO_KNS fx_open2
+#define AERO_FIXED_FEAT (FEAT_OPEN | FEAT_OBSTACLE_BB)
+#define AERO_FIXED_WALL WALL_SLIP
+#include "lbm_inst.cuh"
+
+namespace aero {
+
+const Ops<float> *ops_fx_open2(int dims, int coll, int storage, uint32_t feat, int32_t wall) {
+  if (dims != 2 || storage != AERO_STORE_F32 || feat != (uint32_t)(AERO_FIXED_FEAT) || wall != AERO_FIXED_WALL)
+    return nullptr;
+  switch (coll) {
+    case COLL_BGK: return &fx_open2::inst::Launch<D2Q9, float, COLL_BGK>::table;
+    case COLL_TRT: return &fx_open2::inst::Launch<D2Q9, float, COLL_TRT>::table;
+    case COLL_MRT: return &fx_open2::inst::Launch<D2Q9, float, COLL_MRT>::table;
+  }
+  return nullptr;
+}
+
+}  // namespace aero

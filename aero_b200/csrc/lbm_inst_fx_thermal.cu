@@ -5,7 +5,7 @@
 // instruction-bound; with every other feature's branch removed at compile
 // time the step chain is shorter and fits the instruction cache better.
 // Lattices whose feature word is exactly this one take these kernels
-// (aero_b200's get_ops); every other lattice takes the generic ones.
+// (capi.cu's get_ops); every other lattice takes the generic ones.
 #include "aero_b200.h"
 #include "lbm_params.h"
 
@@ -21,10 +21,9 @@
 
 namespace aero {
 
-uint32_t feat_fx_thermal() { return AERO_FIXED_FEAT; }
-int32_t wall_fx_thermal() { return AERO_FIXED_WALL; }
-
-const Ops<float> *ops_fx_thermal(int storage) {
+const Ops<float> *ops_fx_thermal(int dims, int coll, int storage, uint32_t feat, int32_t wall) {
+  if (dims != 3 || coll != COLL_TRT || feat != (uint32_t)(AERO_FIXED_FEAT) || wall != AERO_FIXED_WALL)
+    return nullptr;
   switch (storage) {
     case AERO_STORE_F32: return &fx_thermal::inst::Launch<D3Q19, float, COLL_TRT>::table;
     case AERO_STORE_F16: return &fx_thermal::inst::Launch<D3Q19, __half, COLL_TRT>::table;

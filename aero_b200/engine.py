@@ -276,8 +276,8 @@ class Engine:
         check("aero_set_persistent", self.lib.aero_set_persistent(self.h, 1 if enable else 0))
 
     def kernel_variant(self) -> int:
-        """0: the generic kernels; 1: the kernels compiled for the thermal
-        channel's feature word (aero_kernel_variant)."""
+        """0: the generic kernels; else the kernel set compiled for the
+        lattice's feature word and wall type (aero_kernel_variant)."""
         k = ctypes.c_int32()
         check("aero_kernel_variant", self.lib.aero_kernel_variant(self.h, ctypes.byref(k)))
         return int(k.value)

@@ -209,12 +209,16 @@ AERO_API int aero_get_persistent(const AeroLattice *lat, int32_t *active);
 
 /* Which compiled kernel set the lattice steps with (no counterpart in the
  * reference): 0 = the generic kernels, which read the feature word at run
- * time; 1 = kernels compiled for the feature word of the thermal channel
- * (D3Q19 TRT + WALE, body force, D3Q7 scalar with buoyancy, obstacle,
- * no-slip walls, streamwise periodic; FP32 / FP16 / BF16 storage), whose
- * other features' branches are removed.  Results agree with the generic kernels' up to FP
- * rounding of the compiled variant.  AERO_B200_GENERIC_KERNELS=1 in the
- * environment at aero_bind_workspace keeps the generic set. */
+ * time; otherwise a set compiled for one feature word and wall type, whose
+ * other features' branches are removed: 1 = the thermal channel (D3Q19 TRT
+ * + WALE, body force, D3Q7 scalar with buoyancy, obstacle, no-slip walls,
+ * streamwise periodic; FP32 / FP16 / BF16 storage); 2, 3 = the open wind
+ * tunnel in 2D, 3D (velocity inlet, outlet, obstacle with mid-link
+ * bounce-back, slip walls; BGK / TRT / MRT; FP32); 4, 5 = the same with
+ * Smagorinsky LES (BGK / TRT).  Batch classes keep their members' set.
+ * Results agree with the generic kernels' up to FP rounding of the compiled
+ * variant.  AERO_B200_GENERIC_KERNELS=1 in the environment at
+ * aero_bind_workspace keeps the generic set. */
 AERO_API int aero_kernel_variant(const AeroLattice *lat, int32_t *variant);
 
 /* Inlet fields of steps first_step .. first_step+n_steps-1 for a lattice
