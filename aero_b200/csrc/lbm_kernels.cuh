@@ -1523,6 +1523,52 @@ __device__ __forceinline__ void moments_cell(const StepParams<typename StoreOps<
   } else if constexpr (AA) {
     full_state<L, S, Real>(p, x, y, z, *p.step, d, nullptr, nullptr, AAGather<L, S, Real>{p, y, z});
   } else {
+    // A fluid cell that no boundary rule touches (no link, not a wall row,
+    // not an inlet / outlet column, not in the sponge) ends its chain as the
+    // pulled populations plus the body-force and buoyancy terms, whose
+    // moments are known in closed form: the Guo term adds bf_coeff rho F to
+    // j and nothing to rho (the lattice's odd moments of third order vanish);
+    // buoyancy adds rho g beta (T - T_ref) to j_y.  Such a cell needs one sum
+    // of its pulled populations instead of the whole chain.
+    const uint32_t fl = p.flags[c];
+    const bool open = FEAT_OF(p) & FEAT_OPEN;
+    const bool plain = !(fl & (FLAG_SOLID | FLAG_LINK)) && !(WALL_OF(p) != WALL_NONE && (y == 0 || y == p.ny - 1)) &&
+                       !(open && (x == 0 || x == p.nx - 1)) && !((FEAT_OF(p) & FEAT_RECYCLE) && x == 0) &&
+                       !((FEAT_OF(p) & FEAT_SPONGE) && x >= p.sponge_start);
+    if (plain) {
+      GlobalGather<L, S, Real>{p, y, z}(x, d);
+      Real drho = 0, jx = 0, jy = 0, jz = 0;
+      static_for<L::Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        drho += d[i];
+        if (Dir<L, i>::x) jx += Dir<L, i>::x * d[i];
+        if (Dir<L, i>::y) jy += Dir<L, i>::y * d[i];
+        if (Dir<L, i>::z) jz += Dir<L, i>::z * d[i];
+      });
+      const Real rho = Real(1) + drho;
+      if constexpr (L::DIMS == 3) {
+        if ((FEAT_OF(p) & FEAT_BODY_FORCE) && rho > Real(0)) {
+          jx += p.bf_coeff * rho * p.bf_x;
+          jy += p.bf_coeff * rho * p.bf_y;
+          jz += p.bf_coeff * rho * p.bf_z;
+        }
+      }
+      if ((FEAT_OF(p) & FEAT_THERMAL) && (FEAT_OF(p) & FEAT_BUOYANCY)) {
+        Real T = 0;
+        if (FEAT_OF(p) & FEAT_SCALAR_REDUCED) {
+          using G = typename ScalarReduced<L>::Lat;
+          static_for<G::Q>([&](auto ic) { T += p.g[elem(p, decltype(ic)::value, c)]; });
+        } else {
+          static_for<L::Q>([&](auto ic) { T += p.g[elem(p, decltype(ic)::value, c)]; });
+        }
+        jy += rho * (p.gbeta * (T - p.T_ref));
+      }
+      const Real inv = rho > Real(0) ? Real(1) / rho : Real(0);
+      p.Uw[c] = jx * inv;
+      p.Uw[p.cs + c] = jy * inv;
+      p.Uw[2 * p.cs + c] = jz * inv;
+      return;
+    }
     full_state<L, S, Real>(p, x, y, z, *p.step, d, nullptr, nullptr);
   }
   Real drho = 0, jx = 0, jy = 0, jz = 0;
