@@ -599,6 +599,11 @@ template <class Real>
 struct ScalarCtx {
   Real T;       // sum of the current scalar populations at the cell
   Real u[3];    // flow velocity before buoyancy (drives the scalar collision)
+  // moments (rho - 1, j) of the final state, buoyancy included: buoyancy
+  // adds rho g beta (T - T_ref) to j_y and nothing to rho, so the collision
+  // need not sum the populations again
+  Real m[4];
+  bool m_set = false;
 };
 
 // Full post-BC state.  When prev_out is non-null the convective outlet writes
@@ -717,12 +722,21 @@ __device__ __forceinline__ void full_state(const StepParams<Real> &p, int x, int
       sc->u[1] = jy * inv;
       sc->u[2] = jz * inv;
     }
+    Real jy_final = jy;
     if (FEAT_OF(p) & FEAT_BUOYANCY) {
       const Real buoy = p.gbeta * (T - p.T_ref);
       static_for<L::Q>([&](auto ic) {
         constexpr int i = decltype(ic)::value;
         if constexpr (Dir<L, i>::y != 0) d[i] += Real(Dir<L, i>::w) * Real(3) * rho * buoy * Real(Dir<L, i>::y);
       });
+      jy_final += rho * buoy;
+    }
+    if (sc) {
+      sc->m[0] = drho;
+      sc->m[1] = jx;
+      sc->m[2] = jy_final;
+      sc->m[3] = jz;
+      sc->m_set = true;
     }
   }
 }
@@ -935,20 +949,30 @@ AERO_HD Real mrt3_adapted(const StepParams<Real> &p, Real (&d)[19], bool solid, 
 }
 
 template <class L, class Real, int COLL>
-AERO_HD Real collide(const StepParams<Real> &p, Real (&d)[L::Q], bool solid, Real om, bool per_cell_omega) {
+AERO_HD Real collide(const StepParams<Real> &p, Real (&d)[L::Q], bool solid, Real om, bool per_cell_omega,
+                     const Real *mom = nullptr) {
   if constexpr (COLL == COLL_MRT && L::DIMS == 3) {
     (void)om;
     (void)per_cell_omega;
+    (void)mom;
     return mrt3_adapted<Real>(p, d, solid, Real(0));
   }
+  // moments of d: given (the state evaluation's, buoyancy included) or summed
   Real drho = 0, jx = 0, jy = 0, jz = 0;
-  static_for<L::Q>([&](auto ic) {
-    constexpr int i = decltype(ic)::value;
-    drho += d[i];
-    if (Dir<L, i>::x) jx += Dir<L, i>::x * d[i];
-    if (Dir<L, i>::y) jy += Dir<L, i>::y * d[i];
-    if (Dir<L, i>::z) jz += Dir<L, i>::z * d[i];
-  });
+  if (mom) {
+    drho = mom[0];
+    jx = mom[1];
+    jy = mom[2];
+    jz = mom[3];
+  } else {
+    static_for<L::Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      drho += d[i];
+      if (Dir<L, i>::x) jx += Dir<L, i>::x * d[i];
+      if (Dir<L, i>::y) jy += Dir<L, i>::y * d[i];
+      if (Dir<L, i>::z) jz += Dir<L, i>::z * d[i];
+    });
+  }
   const Real rho = Real(1) + drho;
   const Real inv = rho > Real(0) ? Real(1) / rho : Real(0);
   Real ux = jx * inv, uy = jy * inv, uz = jz * inv;
@@ -1189,7 +1213,8 @@ __device__ __forceinline__ void finish_cell(const StepParams<typename StoreOps<S
   }
   // the last step of an AA call stores the state itself (uncollided)
   const Real rho = Gather::kAA && p.aa_store_state ? Real(1) + sum_dev<L>(d)
-                                                   : collide<L, Real, COLL>(p, d, solid, om, les);
+                                                   : collide<L, Real, COLL>(p, d, solid, om, les,
+                                                                            sc.m_set ? sc.m : nullptr);
   guard_rho(p, rho, step_now);
   static_for<L::Q>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
