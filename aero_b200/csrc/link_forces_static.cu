@@ -118,46 +118,69 @@ __global__ void k_link_contrib(const double *__restrict__ f_pre, const double *_
   out[12] = g.dims == 3 ? z : y;
 }
 
-// One block: fixed-order sums of the contributions (deterministic), then the
-// per-row (2D) / per-plane (3D) profile.
+// One block: fixed-order sums of the contributions (deterministic); a row
+// with bin -1 (invalid direction or coordinate) makes every output NaN.
 constexpr int kReduceBlock = 256;
-__global__ void __launch_bounds__(kReduceBlock) k_link_reduce(const double *scratch, long long n_links, int nprof,
-                                                              double *out12, double *profile) {
+__global__ void __launch_bounds__(kReduceBlock) k_link_reduce(const double *scratch, long long n_links,
+                                                              double *out12) {
   __shared__ double sm[12][kReduceBlock / 32];
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   double a[12];
   for (int j = 0; j < 12; j++) a[j] = 0.0;
-  for (long long k = t; k < n_links; k += kReduceBlock)
+  int bad = 0;
+  for (long long k = t; k < n_links; k += kReduceBlock) {
     for (int j = 0; j < 12; j++) a[j] += scratch[k * kSlot + j];
+    bad |= scratch[k * kSlot + 12] < 0.0 ? 1 : 0;
+  }
   for (int j = 0; j < 12; j++) {
     double v = a[j];
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
     if (lane == 0) sm[j][wid] = v;
   }
-  // invalid rows (bin -1): counted, and the outputs become NaN
-  int bad = 0;
-  for (long long k = t; k < n_links; k += kReduceBlock) bad += scratch[k * kSlot + 12] < 0.0 ? 1 : 0;
   bad = __syncthreads_or(bad);
   if (t < 12) {
     double v = 0.0;
     for (int w = 0; w < kReduceBlock / 32; w++) v += sm[t][w];
     out12[t] = bad ? __longlong_as_double(0x7ff8000000000000LL) : v;
   }
-  if (profile && bad) {
-    for (int b = t; b < 3 * nprof; b += kReduceBlock) profile[b] = __longlong_as_double(0x7ff8000000000000LL);
-  } else if (profile) {
-    for (int b = t; b < nprof; b += kReduceBlock) {
-      double p0 = 0.0, p1 = 0.0, p2 = 0.0;
-      for (long long k = 0; k < n_links; k++) {
-        if (scratch[k * kSlot + 12] != (double)b) continue;
-        p0 += scratch[k * kSlot + 0];
-        p1 += scratch[k * kSlot + 1];
-        p2 += scratch[k * kSlot + 2];
-      }
-      profile[3 * b + 0] = p0;
-      profile[3 * b + 1] = p1;
-      profile[3 * b + 2] = p2;
-    }
+}
+
+// Block b: the force profile of row (2D) / plane (3D) b, i.e. the sum of
+// (dfx, dfy, dfz) over the links whose bin is b.  Each thread takes a fixed
+// stride of the link list and the block reduces in a fixed order, so the
+// result is deterministic; the blocks run in parallel, one pass over the
+// link list each, instead of one thread scanning every link per bin.  Any
+// invalid row makes the whole profile NaN, as it makes the totals.
+__global__ void __launch_bounds__(kReduceBlock) k_link_profile(const double *scratch, long long n_links,
+                                                               double *profile) {
+  __shared__ double sm[3][kReduceBlock / 32];
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  const double b = (double)blockIdx.x;
+  double p0 = 0.0, p1 = 0.0, p2 = 0.0;
+  int bad = 0;
+  for (long long k = t; k < n_links; k += kReduceBlock) {
+    const double bin = scratch[k * kSlot + 12];
+    bad |= bin < 0.0 ? 1 : 0;
+    if (bin != b) continue;
+    p0 += scratch[k * kSlot + 0];
+    p1 += scratch[k * kSlot + 1];
+    p2 += scratch[k * kSlot + 2];
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    p0 += __shfl_down_sync(0xffffffffu, p0, off);
+    p1 += __shfl_down_sync(0xffffffffu, p1, off);
+    p2 += __shfl_down_sync(0xffffffffu, p2, off);
+  }
+  if (lane == 0) {
+    sm[0][wid] = p0;
+    sm[1][wid] = p1;
+    sm[2][wid] = p2;
+  }
+  bad = __syncthreads_or(bad);
+  if (t < 3) {
+    double v = 0.0;
+    for (int w = 0; w < kReduceBlock / 32; w++) v += sm[t][w];
+    profile[3 * blockIdx.x + t] = bad ? __longlong_as_double(0x7ff8000000000000LL) : v;
   }
 }
 
@@ -225,9 +248,14 @@ int aero_link_forces_static(int32_t dims, int32_t nx, int32_t ny, int32_t nz, co
     e = cudaGetLastError();
     if (e != cudaSuccess) return aero::set_error(AERO_ERR_CUDA, cudaGetErrorString(e));
   }
-  k_link_reduce<<<1, kReduceBlock, 0, st>>>(scratch, n_links, dims == 3 ? nz : ny, out, profile);
+  k_link_reduce<<<1, kReduceBlock, 0, st>>>(scratch, n_links, out);
   e = cudaGetLastError();
   if (e != cudaSuccess) return aero::set_error(AERO_ERR_CUDA, cudaGetErrorString(e));
+  if (profile) {
+    k_link_profile<<<(unsigned)(dims == 3 ? nz : ny), kReduceBlock, 0, st>>>(scratch, n_links, profile);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return aero::set_error(AERO_ERR_CUDA, cudaGetErrorString(e));
+  }
   return AERO_OK;
 }
 

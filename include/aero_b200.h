@@ -291,8 +291,9 @@ AERO_API int aero_kernel_times(AeroLattice *lat, double *step_ms, double *forces
  * any stream capture (otherwise AERO_ERR_STATE).  A row whose direction is
  * outside 1..Q-1 or whose cell is outside the grid (the reference raises
  * IndexError there) makes every output value NaN.  The profile is summed
- * per row/plane in link order by one block (deterministic; its cost grows
- * as rows x links, about 0.3 ms at the cap). */
+ * by one block per row/plane, each thread over a fixed stride of the link
+ * list and the block in a fixed order (deterministic); the blocks run in
+ * parallel, each one pass over the list. */
 AERO_API int aero_link_forces_static(int32_t dims, int32_t nx, int32_t ny, int32_t nz, const double *f_pre,
                                      const double *f_post, const int32_t *links, int64_t n_links,
                                      const double *center, double *out, double *profile, void *stream);
