@@ -67,13 +67,24 @@ class Batch:
         return len(self.members)
 
     def step(self, n: int) -> None:
-        """Advances every member n steps (asynchronous on the current stream)."""
+        """Advances every member n steps (asynchronous on the current stream,
+        except that members with synthetic inflow or an SEM inlet have their
+        fields uploaded before each chunk of at most their ring's steps, which
+        waits for the stream as Solver.run's upload does)."""
         for s in self.members:
             s._flush_host_state()  # raises if a member's state was edited on the host
-        with self.torch.cuda.device(self.device):
-            check("aero_batch_step", self.lib.aero_batch_step(self.h, int(n), self._stream()))
-        for s in self.members:
-            s.step_count += int(n)
+        inflow = [s for s in self.members if getattr(s, "_inflow", None) is not None]
+        chunk = min([s._params.inflow_ring for s in inflow], default=int(n)) or int(n)
+        left = int(n)
+        while left > 0:
+            k = min(left, chunk)
+            with self.torch.cuda.device(self.device):
+                for s in inflow:
+                    s._engine.set_inflow(s._inflow.fields(k), s.step_count)
+                check("aero_batch_step", self.lib.aero_batch_step(self.h, k, self._stream()))
+            for s in self.members:
+                s.step_count += k
+            left -= k
 
     def converge(self, window: int, tol: float) -> np.ndarray:
         """(members, 7) array, join order: ratio, mean|Cd|, std, converged,

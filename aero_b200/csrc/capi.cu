@@ -1852,8 +1852,8 @@ int aero_batch_add(AeroBatch *B, AeroLattice *L, double cd_norm) {
   if (L->device != B->device) return fail(AERO_ERR_INVALID, "the lattice is on another device than the batch");
   if ((int)B->members.size() >= B->max_members) return fail(AERO_ERR_CAPACITY, "batch holds %d members", B->max_members);
   if (!(cd_norm > 0.0) || !std::isfinite(cd_norm)) return fail(AERO_ERR_INVALID, "cd_norm must be > 0");
-  if (L->feat & (FEAT_INFLOW_FIELD | FEAT_RECYCLE))
-    return fail(AERO_ERR_UNSUPPORTED, "lattices with synthetic inflow or a recycling inlet step only on their own");
+  if (L->feat & FEAT_RECYCLE)
+    return fail(AERO_ERR_UNSUPPORTED, "lattices with a recycling inlet step only on their own");
   if (L->aa && !batch_solo(L))
     return fail(AERO_ERR_UNSUPPORTED,
                 "a lattice in the AA layout joins a batch only with at least %lld cells (then it steps on its "
@@ -1886,6 +1886,15 @@ int aero_batch_step(AeroBatch *B, int64_t n, void *stream) {
   if (!B->bound) return fail(AERO_ERR_STATE, "batch workspace not bound");
   if (n < 0) return fail(AERO_ERR_INVALID, "negative step count");
   if (n == 0 || B->members.empty()) return AERO_OK;
+  // members with an inflow field inlet read their fields from their own
+  // device ring (aero_set_inflow), as when they step alone
+  for (size_t k = 0; k < B->members.size(); k++) {
+    const AeroLattice *L = B->members[k];
+    if ((L->feat & FEAT_INFLOW_FIELD) && L->step_count + n > L->inflow_upto)
+      return fail(AERO_ERR_STATE,
+                  "member %d: inflow fields are on the device up to step %lld; upload them with aero_set_inflow",
+                  (int)k, (long long)L->inflow_upto);
+  }
   CUDA_TRY(cudaSetDevice(B->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (B->dirty) {

@@ -291,3 +291,73 @@ def test_large_aa_member_steps_in_the_batch_as_alone():
     with pytest.raises(AeroError):
         b.add(small)
     b.close()
+
+
+def _inflow_cases():
+    from aero_b200 import Cylinder, Solver, Solver3D, Sphere
+
+    def c2d():
+        cyl = Cylinder(radius=4, cx_frac=0.3, cy_frac=0.5)
+        return Solver(Ny=30, Nx=80, solid=cyl.mark_solid(30, 80), omega=1 / 0.6, u0=0.05,
+                      D=cyl.reference_length(), collision="bgk", synthetic_inflow=True,
+                      synthetic_inflow_intensity=0.02, synthetic_inflow_seed=11, precision="fp32")
+
+    def c3d(precision, **kw):
+        sph = Sphere(radius=3, cx_frac=0.3, cy_frac=0.5, cz_frac=0.5)
+        nz, ny, nx = 12, 14, 32
+        return Solver3D(Nz=nz, Ny=ny, Nx=nx, solid=sph.mark_solid(nz, ny, nx), omega=1 / 0.7, u0=0.05,
+                        D=sph.reference_length(), collision="mrt", wall_bc="slip", outlet_bc="convective",
+                        precision=precision, **kw)
+
+    return [c2d,
+            lambda: c3d("fp32", sem_inlet=True, sem_Tu=0.05, sem_L_int=3.0, sem_N=40),
+            lambda: c3d("fp16s", synthetic_inflow=True, synthetic_inflow_intensity=0.03, synthetic_inflow_seed=5)]
+
+
+@pytest.mark.gpu
+def test_inflow_field_members_step_in_the_batch():
+    """Lattices with synthetic inflow (2D, 3D) or an SEM inlet join a batch:
+    Batch.step uploads each one's fields ahead of every chunk of at most its
+    ring's 64 steps, and the members match the same lattices run alone
+    (Solver.run) to the batch tolerances over 150 steps, and are bit-identical
+    alone in a batch and beside a plain member."""
+    from aero_b200 import Batch
+    makes = _inflow_cases()
+    plain = _cases()[0]
+    steps = 150
+    ref = [_alone(m, steps) for m in makes]
+    b = Batch(max_members=4)
+    mix = [m() for m in makes] + [plain()]
+    for s in mix:
+        b.add(s)
+    b.step(steps)
+    for s, (f_ref, cd_ref) in zip(mix, ref):
+        cd = s._coefficients(s._engine.read_forces())["Cd"]
+        assert s.status() == 0
+        _close(s, s.f, f_ref, cd, cd_ref)
+    for m, s in zip(makes, mix):
+        b1 = Batch(max_members=1)
+        t = m()
+        b1.add(t)
+        b1.step(steps)
+        np.testing.assert_array_equal(t._engine.get_state()[0], s._engine.get_state()[0])
+        b1.remove(t)
+        b1.close()
+    b.close()
+
+
+@pytest.mark.gpu
+def test_batch_step_needs_the_inflow_fields():
+    """aero_batch_step refuses (AERO_ERR_STATE) while a member's inflow
+    fields for the call's steps are not on the device, and steps once they
+    are."""
+    from aero_b200 import Batch
+    s = _inflow_cases()[0]()
+    b = Batch(max_members=2)
+    b.add(s)
+    rc = b.lib.aero_batch_step(b.h, 5, b._stream())
+    assert rc == -3, rc
+    assert b"aero_set_inflow" in b.lib.aero_last_error()
+    s._engine.set_inflow(s._inflow.fields(5), s.step_count)
+    assert b.lib.aero_batch_step(b.h, 5, b._stream()) == 0
+    b.close()
