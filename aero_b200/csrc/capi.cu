@@ -1485,6 +1485,9 @@ struct ClassPlan {
   int n = 0, n_les = 0;
   int64_t blocks = 0, blocks_les = 0;
   uint64_t params[2] = {0, 0}, first = 0, params_les[2] = {0, 0}, first_les = 0;
+  // members with a recycling inlet and their parity at the build: each step
+  // launches their plane-mean pass (k_recycle_mean) before the class kernels
+  std::vector<std::pair<AeroLattice *, int>> recycle;
 };
 
 struct FinPlan {
@@ -1596,6 +1599,7 @@ int batch_build(AeroBatch *B, cudaStream_t st) {
     }
     it->n++;
     if (les_active(L)) it->n_les++;
+    if (L->feat & FEAT_RECYCLE) it->recycle.emplace_back(L, L->cur);
     B->fin[is_f64(L) ? 1 : 0].n++;
   }
   std::vector<char> &h = B->host_plan;
@@ -1728,6 +1732,12 @@ int batch_launch_step(AeroBatch *B, int j, cudaStream_t st, bool branches = fals
       cs = B->branch[ci];
       CUDA_TRY(cudaStreamWaitEvent(cs, B->fork, 0));
     }
+    // the recycling members' plane means, as aero_step launches them
+    for (const auto &rm : c.recycle) {
+      const int par = (rm.second + j) & 1;
+      if (c.f64) CUDA_TRY(ops_f64(c.key.dims, c.key.coll)->recycle_mean(make_params<double>(rm.first, par), cs));
+      else CUDA_TRY(c.ops->recycle_mean(make_params<float>(rm.first, par), cs));
+    }
     if (c.f64) {
       const Ops<double> *ops = ops_f64(c.key.dims, c.key.coll);
       auto *P = reinterpret_cast<const StepParams<double> *>(ws + c.params[j]);
@@ -1852,8 +1862,6 @@ int aero_batch_add(AeroBatch *B, AeroLattice *L, double cd_norm) {
   if (L->device != B->device) return fail(AERO_ERR_INVALID, "the lattice is on another device than the batch");
   if ((int)B->members.size() >= B->max_members) return fail(AERO_ERR_CAPACITY, "batch holds %d members", B->max_members);
   if (!(cd_norm > 0.0) || !std::isfinite(cd_norm)) return fail(AERO_ERR_INVALID, "cd_norm must be > 0");
-  if (L->feat & FEAT_RECYCLE)
-    return fail(AERO_ERR_UNSUPPORTED, "lattices with a recycling inlet step only on their own");
   if (L->aa && !batch_solo(L))
     return fail(AERO_ERR_UNSUPPORTED,
                 "a lattice in the AA layout joins a batch only with at least %lld cells (then it steps on its "

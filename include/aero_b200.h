@@ -325,10 +325,11 @@ AERO_API int aero_batch_bind_workspace(AeroBatch *batch, void *device_ptr, uint6
  * its own kernels as a branch of the batch step; only such a lattice may be
  * in the AA layout (AERO_ERR_UNSUPPORTED otherwise): each aero_batch_step
  * then collides the state it stored and ends on a state-storing step, as
- * aero_step does.  A lattice with a recycling inlet cannot join
- * (AERO_ERR_UNSUPPORTED); one with synthetic inflow or an SEM inlet joins,
- * and aero_batch_step needs its inflow fields for all the call's steps on
- * the device first (aero_set_inflow; AERO_ERR_STATE otherwise). */
+ * aero_step does.  A lattice with a recycling inlet joins (its plane-mean
+ * pass runs before each step, as in aero_step); one with synthetic inflow
+ * or an SEM inlet joins, and aero_batch_step needs its inflow fields for
+ * all the call's steps on the device first (aero_set_inflow;
+ * AERO_ERR_STATE otherwise). */
 AERO_API int aero_batch_add(AeroBatch *batch, AeroLattice *lat, double cd_norm);
 /* Removes a member; it can then be stepped, read or destroyed on its own. */
 AERO_API int aero_batch_remove(AeroBatch *batch, AeroLattice *lat);

@@ -361,3 +361,43 @@ def test_batch_step_needs_the_inflow_fields():
     s._engine.set_inflow(s._inflow.fields(5), s.step_count)
     assert b.lib.aero_batch_step(b.h, 5, b._stream()) == 0
     b.close()
+
+
+@pytest.mark.gpu
+def test_recycling_members_step_in_the_batch():
+    """Lattices with the 3D recycling inlet join a batch: each batch step
+    launches their plane-mean pass before the class kernels (the per-cell
+    class in FP32, the pair class in BF16), and they match the same
+    lattices run alone to the batch tolerances, bit-identical alone in a
+    batch and beside a plain member."""
+    from aero_b200 import Batch, Solver3D, Sphere
+
+    def rec(precision):
+        sph = Sphere(radius=3, cx_frac=0.4, cy_frac=0.5, cz_frac=0.5)
+        nz, ny, nx = 12, 14, 40
+        return lambda: Solver3D(Nz=nz, Ny=ny, Nx=nx, solid=sph.mark_solid(nz, ny, nx), omega=1 / 0.7, u0=0.05,
+                                D=sph.reference_length(), collision="mrt", wall_bc="noslip",
+                                streamwise_bc="recycling", precision=precision)
+
+    makes = [rec("fp32"), rec("bf16s")]
+    steps = 41
+    ref = [_alone(m, steps) for m in makes]
+    b = Batch(max_members=4)
+    mix = [m() for m in makes] + [_cases()[0]()]
+    for s in mix:
+        b.add(s)
+    b.step(20)
+    b.step(steps - 20)
+    for s, (f_ref, cd_ref) in zip(mix, ref):
+        cd = s._coefficients(s._engine.read_forces())["Cd"]
+        assert s.status() == 0
+        _close(s, s.f, f_ref, cd, cd_ref)
+    for m, s in zip(makes, mix):
+        b1 = Batch(max_members=1)
+        t = m()
+        b1.add(t)
+        b1.step(steps)
+        np.testing.assert_array_equal(t._engine.get_state()[0], s._engine.get_state()[0])
+        b1.remove(t)
+        b1.close()
+    b.close()
