@@ -367,7 +367,7 @@ def test_batch_step_needs_the_inflow_fields():
 def test_recycling_members_step_in_the_batch():
     """Lattices with the 3D recycling inlet join a batch: each batch step
     launches their plane-mean pass before the class kernels (the per-cell
-    class in FP32, the pair class in BF16), and they match the same
+    classes in FP64 and FP32, the pair class in BF16), and they match the same
     lattices run alone to the batch tolerances, bit-identical alone in a
     batch and beside a plain member."""
     from aero_b200 import Batch, Solver3D, Sphere
@@ -379,7 +379,7 @@ def test_recycling_members_step_in_the_batch():
                                 D=sph.reference_length(), collision="mrt", wall_bc="noslip",
                                 streamwise_bc="recycling", precision=precision)
 
-    makes = [rec("fp32"), rec("bf16s")]
+    makes = [rec("fp64"), rec("fp32"), rec("bf16s")]
     steps = 41
     ref = [_alone(m, steps) for m in makes]
     b = Batch(max_members=4)
