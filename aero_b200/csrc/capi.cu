@@ -295,9 +295,10 @@ StepParams<Real> make_params(const AeroLattice *L, int cur) {
   p.lc_contrib = reinterpret_cast<double *>(ws + L->lay.lc_contrib);
   p.fin_partial = reinterpret_cast<double *>(ws + L->lay.fin_partial);
   {
-    // about 1024 link cells per finalisation block (4 per thread)
+    // about 256 link cells per finalisation block (one per thread): the
+    // pass is latency-bound, so it spreads over as many SMs as it can use
     const int64_t nlc = (int64_t)L->lc_cell.size();
-    const int64_t nb = std::min<int64_t>(std::max<int64_t>((nlc + 1023) / 1024, 1), kFinalizeMaxBlocks);
+    const int64_t nb = std::min<int64_t>(std::max<int64_t>((nlc + 255) / 256, 1), kFinalizeMaxBlocks);
     p.fin_blocks = (int32_t)nb;
     p.fin_chunk = (nlc + nb - 1) / nb;
   }
