@@ -212,3 +212,55 @@ def test_layout_option():
     with pytest.raises(ValueError, match="Unknown layout"):
         Solver(Ny=8, Nx=16, solid=solid, omega=1.0, u0=0.05, D=4.0, layout="soa")
     assert "layout" in dict(_lib.AeroParams._fields_)
+
+
+def test_batch_step_uploads_inflow_fields_in_ring_chunks():
+    """Batch.step (host logic, no GPU): with a member whose inflow ring holds
+    64 steps, 150 steps go to aero_batch_step as 64 + 64 + 22, each chunk's
+    fields uploaded first for that member (starting at its step count) and
+    none for the plain member; without inflow members one call takes all
+    steps."""
+    import contextlib
+    import types
+
+    from aero_b200.batch import Batch
+
+    calls = []
+
+    class Lib:
+        def aero_batch_step(self, h, n, stream):
+            calls.append(("step", n))
+            return 0
+
+    class Eng:
+        def __init__(self, name):
+            self.name = name
+
+        def set_inflow(self, fields, first):
+            calls.append(("inflow", self.name, len(fields), first))
+
+    class Gen:
+        def fields(self, k):
+            return np.zeros((k, 2, 4))
+
+    def member(name, inflow):
+        m = types.SimpleNamespace(step_count=10, _engine=Eng(name), _flush_host_state=lambda: None,
+                                  _params=types.SimpleNamespace(inflow_ring=64))
+        m._inflow = Gen() if inflow else None
+        return m
+
+    fake_torch = types.SimpleNamespace(cuda=types.SimpleNamespace(device=lambda d: contextlib.nullcontext()))
+    b = Batch.__new__(Batch)
+    b.torch, b.lib, b.h, b.device = fake_torch, Lib(), None, None
+    b._stream = lambda: 0
+    a, p = member("a", True), member("p", False)
+    b.members = [a, p]
+    b.step(150)
+    assert calls == [("inflow", "a", 64, 10), ("step", 64), ("inflow", "a", 64, 74), ("step", 64),
+                     ("inflow", "a", 22, 138), ("step", 22)]
+    assert a.step_count == p.step_count == 160
+    calls.clear()
+    b.members = [p]
+    b.step(150)
+    assert calls == [("step", 150)] and p.step_count == 310
+    b.members = []  # nothing for __del__ to release
